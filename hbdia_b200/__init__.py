@@ -1,0 +1,313 @@
+"""hbdia_b200 -- B200-native HBDIA sparse matrix-vector product.
+
+Python mirror of the reference's API (nrottstegge/HBDIA):
+
+* :class:`HBDIA`        -- ``HBDIA<T>`` (include/Format/HBDIA.hpp:24-291)
+* :class:`HBDIAVector`  -- ``HBDIAVector<T>`` (include/Format/HBDIAVector.hpp:23-109)
+* :func:`hbdiaSpMV`     -- ``hbdiaSpMV`` (include/Operations/HBDIASpMV.hpp:8-10)
+
+Everything runs through the C ABI of ``libhbdia_b200.so`` (include/hbdia_b200.h);
+the SpMV itself is one fused sm_100a kernel launch.  There is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes
+from enum import IntEnum
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+from ._lib import (HBDIACudaError, STORE_BF16_SCALED, STORE_F32, STORE_NATIVE, MatrixInfo,
+                   check as _check, load as _load)
+
+__all__ = ["ExecutionMode", "HBDIA", "HBDIAVector", "hbdiaSpMV", "spmv_device", "spmm_device",
+           "spmv_host", "generate_stencil27", "generate_stencil7", "generate_banded", "fill_uniform",
+           "HBDIACudaError", "set_device", "STORE_NATIVE", "STORE_F32", "STORE_BF16_SCALED", "library_path"]
+
+DEFAULT_BLOCK_WIDTH = 32      # include/types.hpp:14
+DEFAULT_THRESHOLD = 1         # include/types.hpp:15
+MAX_COO_ENTRIES = 1000000000  # include/types.hpp:16
+
+
+class ExecutionMode(IntEnum):
+    """include/types.hpp:7-10."""
+    CPU_COO = 0
+    GPU_COO = 1
+
+
+def library_path() -> str:
+    return _lib.LIB_PATH
+
+
+def set_device(device: int) -> None:
+    """Select the GPU for this host thread's library calls (default 0)."""
+    _check(_load().hbdia_set_device(int(device)))
+
+
+def _vp(a: np.ndarray):
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+def _dtype_code(dtype) -> int:
+    dt = np.dtype(dtype)
+    if dt == np.float64:
+        return _lib.HBDIA_F64
+    if dt == np.float32:
+        return _lib.HBDIA_F32
+    raise ValueError(f"unsupported value type {dt}; use float64 or float32")
+
+
+class HBDIA:
+    """``HBDIA<T>``: COO input, conversion to blocked-DIA + COO remainder, and
+    the device layout.  ``dtype`` plays the role of the template argument."""
+
+    def __init__(self, rowIndices: Optional[Sequence[int]] = None, colIndices: Optional[Sequence[int]] = None,
+                 values: Optional[Sequence[float]] = None, numRows: Optional[int] = None,
+                 numCols: Optional[int] = None, dtype=np.float64):
+        lib = _load()
+        self.dtype = np.dtype(dtype)
+        self._h = ctypes.c_void_p()
+        code = _dtype_code(self.dtype)
+        if rowIndices is None and colIndices is None and values is None:
+            _check(lib.hbdia_matrix_create_empty(code, ctypes.byref(self._h)))  # HBDIA()
+            return
+        r = np.ascontiguousarray(rowIndices, np.int32)
+        c = np.ascontiguousarray(colIndices, np.int32)
+        v = np.ascontiguousarray(values, self.dtype)
+        if not (len(r) == len(c) == len(v)):
+            # src/Format/HBDIA.cpp:27-29
+            raise ValueError("Row indices, column indices, and values vectors must have the same size")
+        nr = -1 if numRows is None else int(numRows)
+        nc = -1 if numCols is None else int(numCols)
+        if (numRows is None) != (numCols is None):
+            raise ValueError("give both numRows and numCols, or neither")
+        if numRows is not None and (nr <= 0 or nc <= 0):
+            raise ValueError("Matrix dimensions must be positive")
+        _check(lib.hbdia_matrix_create(code, _vp(r), _vp(c), _vp(v), len(v), nr, nc, ctypes.byref(self._h)))
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _load().hbdia_matrix_destroy(h)
+            self._h = None
+
+    @property
+    def handle(self) -> ctypes.c_void_p:
+        return self._h
+
+    # ---- matrix sources
+    def create3DStencil27Point(self, nx: int, ny: int, nz: int, noise: float = 0.0, iteration: int = 0) -> None:
+        _check(_load().hbdia_matrix_stencil27(self._h, nx, ny, nz, float(noise), iteration))
+
+    def loadMTX(self, filename: str, numRows: Optional[int] = None, numCols: Optional[int] = None) -> bool:
+        ok = ctypes.c_int32(0)
+        _check(_load().hbdia_matrix_load_mtx(self._h, filename.encode(), numRows or 0, numCols or 0,
+                                            ctypes.byref(ok)))
+        return bool(ok.value)
+
+    # ---- conversion
+    def convertToHBDIAFormat(self, blockWidth: int = DEFAULT_BLOCK_WIDTH, threshold: int = DEFAULT_THRESHOLD,
+                             max_coo_entries: int = MAX_COO_ENTRIES, COOisUnique: bool = False,
+                             execMode: ExecutionMode = ExecutionMode.GPU_COO, upload: bool = True) -> None:
+        """src/Format/HBDIA.cpp:507-718.  ``upload=False`` skips the device
+        layout (the reference's partial-matrix behaviour), so it runs without a GPU."""
+        _check(_load().hbdia_matrix_convert(self._h, blockWidth, threshold, int(max_coo_entries),
+                                            int(bool(COOisUnique)), int(execMode), int(bool(upload))))
+
+    def prepareForGPU(self, storage: int = STORE_NATIVE) -> None:
+        _check(_load().hbdia_matrix_prepare_gpu(self._h, storage))
+
+    def initializeCuSparse(self) -> None:
+        """Kept for source compatibility (src/Format/HBDIA.cpp:919-994): the COO
+        remainder runs inside the fused kernel, so there is nothing to set up."""
+
+    # ---- getters (include/Format/HBDIA.hpp:72-115)
+    def info(self) -> MatrixInfo:
+        i = MatrixInfo()
+        _check(_load().hbdia_matrix_get_info(self._h, ctypes.byref(i)))
+        return i
+
+    def getNumRows(self) -> int: return self.info().numRows
+    def getNumCols(self) -> int: return self.info().numCols
+    def getNumNonZeros(self) -> int: return self.info().numNonZeros
+    def getBlockWidth(self) -> int: return self.info().blockWidth
+    def getThreshold(self) -> int: return self.info().threshold
+    def getMaxCooEntries(self) -> int: return self.info().maxCooEntries
+    def getNumBlocks(self) -> int: return self.info().numBlocks
+    def getNumberDiagonals(self) -> int: return self.info().numberDiagonals
+    def getHasCOO(self) -> bool: return bool(self.info().hasCOO)
+    def getHasHBDIA(self) -> bool: return bool(self.info().hasHBDIA)
+    isCOOFormat = getHasCOO
+    isHBDIAFormat = getHasHBDIA
+
+    def layout(self) -> dict:
+        """The host layout as numpy arrays: offsets/block_start (flattened
+        offsetsPerBlock), data, coo_row/coo_col/coo_val, coo_row_ptr, hist_blocks,
+        hist_nnz, number_diagonals, num_blocks."""
+        i = self.info()
+        if not i.hasHBDIA:
+            raise RuntimeError("matrix is not in HBDIA format")
+        out = dict(
+            offsets=np.zeros(i.totalOffsets, np.int32), block_start=np.zeros(i.numBlocks + 1, np.int32),
+            data=np.zeros(i.numSlots, self.dtype), coo_row=np.zeros(i.numCoo, np.int32),
+            coo_col=np.zeros(i.numCoo, np.int32), coo_val=np.zeros(i.numCoo, self.dtype),
+            coo_row_ptr=np.zeros(i.numRows + 1, np.int32), hist_blocks=np.zeros(i.histogramLength, np.int32),
+            hist_nnz=np.zeros(i.histogramLength, np.int32))
+        _check(_load().hbdia_matrix_export_layout(self._h, *[_vp(out[k]) for k in (
+            "offsets", "block_start", "data", "coo_row", "coo_col", "coo_val", "coo_row_ptr",
+            "hist_blocks", "hist_nnz")]))
+        out["number_diagonals"] = i.numberDiagonals
+        out["num_blocks"] = i.numBlocks
+        return out
+
+    def getHBDIAData(self) -> np.ndarray: return self.layout()["data"]
+    def getCpuRowIndices(self) -> np.ndarray: return self.layout()["coo_row"]
+    def getCpuColIndices(self) -> np.ndarray: return self.layout()["coo_col"]
+    def getCpuValues(self) -> np.ndarray: return self.layout()["coo_val"]
+    def getCpuRowPtr(self) -> np.ndarray: return self.layout()["coo_row_ptr"]
+    def getHistogramBlocks(self) -> np.ndarray: return self.layout()["hist_blocks"]
+    def getHistogramNnz(self) -> np.ndarray: return self.layout()["hist_nnz"]
+
+    def getOffsetsPerBlock(self) -> List[List[int]]:
+        L = self.layout()
+        bs = L["block_start"]
+        return [L["offsets"][bs[b]:bs[b + 1]].tolist() for b in range(L["num_blocks"])]
+
+    def _coo(self):
+        i = self.info()
+        r = np.zeros(i.numNonZeros, np.int32)
+        c = np.zeros(i.numNonZeros, np.int32)
+        v = np.zeros(i.numNonZeros, self.dtype)
+        _check(_load().hbdia_matrix_export_coo(self._h, _vp(r), _vp(c), _vp(v)))
+        return r, c, v
+
+    def getRowIndices(self) -> np.ndarray: return self._coo()[0]
+    def getColIndices(self) -> np.ndarray: return self._coo()[1]
+    def getValues(self) -> np.ndarray: return self._coo()[2]
+
+    def getNnzPerRow(self) -> np.ndarray:
+        out = np.zeros(self.info().numRows, np.int32)
+        _check(_load().hbdia_matrix_export_nnz_per_row(self._h, _vp(out)))
+        return out
+
+    def getBDIAStream(self) -> int:
+        s = ctypes.c_void_p()
+        _check(_load().hbdia_matrix_stream(self._h, ctypes.byref(s)))
+        return s.value or 0
+
+    def bytesPerSpmv(self) -> int:
+        """Algorithmic HBM bytes of one SpMV over the device layout."""
+        return self.info().bytesPerSpmv
+
+    def synchronize(self) -> None:
+        _check(_load().hbdia_matrix_synchronize(self._h))
+
+
+class HBDIAVector:
+    """``HBDIAVector<T>`` on one GPU: a device buffer (no halos)."""
+
+    def __init__(self, localData, dtype=None):
+        lib = _load()
+        data = np.ascontiguousarray(localData, dtype if dtype is not None else None)
+        if data.dtype not in (np.float64, np.float32):
+            data = data.astype(np.float64)
+        self.dtype = data.dtype
+        self._h = ctypes.c_void_p()
+        _check(lib.hbdia_vector_create(_dtype_code(self.dtype), _vp(data), len(data), ctypes.byref(self._h)))
+        self._n = len(data)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _load().hbdia_vector_destroy(h)
+            self._h = None
+
+    @property
+    def handle(self) -> ctypes.c_void_p:
+        return self._h
+
+    def getDeviceDataPtr(self) -> int:
+        p = ctypes.c_void_p()
+        _check(_load().hbdia_vector_device_ptr(self._h, ctypes.byref(p)))
+        return p.value or 0
+
+    getDeviceLocalPtr = getDeviceDataPtr
+
+    def getLocalSize(self) -> int:
+        return self._n
+
+    getTotalSize = getLocalSize
+
+    def toHost(self) -> np.ndarray:
+        out = np.empty(self._n, self.dtype)
+        _check(_load().hbdia_vector_download(self._h, _vp(out)))
+        return out
+
+    def upload(self, data) -> None:
+        d = np.ascontiguousarray(data, self.dtype)
+        if len(d) != self._n:
+            raise ValueError("size mismatch")
+        _check(_load().hbdia_vector_upload(self._h, _vp(d)))
+
+
+def hbdiaSpMV(matrix: HBDIA, inputVector: HBDIAVector, outputVector: HBDIAVector,
+              execCOOCPU: bool, execCOOGPU: bool) -> bool:
+    """src/Operations/HBDIASpMV.cpp:186-251: y = A x, asynchronous on the
+    matrix's stream.  Raises RuntimeError("... Invalid COO execution flags")
+    when the matrix has a COO remainder and both flags are False."""
+    _check(_load().hbdia_spmv(matrix.handle, inputVector.handle, outputVector.handle,
+                              int(bool(execCOOCPU)), int(bool(execCOOGPU))))
+    return True
+
+
+def spmv_device(matrix: HBDIA, x_ptr: int, y_ptr: int, stream: int = 0) -> None:
+    """y = A x on raw device pointers (e.g. torch tensors' data_ptr()) on
+    ``stream`` (0: the matrix's stream)."""
+    _check(_load().hbdia_spmv_device(matrix.handle, ctypes.c_void_p(x_ptr), ctypes.c_void_p(y_ptr),
+                                     ctypes.c_void_p(stream or None)))
+
+
+def spmm_device(matrix: HBDIA, X_ptr: int, ldx: int, Y_ptr: int, ldy: int, k: int, stream: int = 0) -> None:
+    """Y = A X for k row-major right-hand sides on raw device pointers."""
+    _check(_load().hbdia_spmm_device(matrix.handle, ctypes.c_void_p(X_ptr), ldx, ctypes.c_void_p(Y_ptr), ldy,
+                                     k, ctypes.c_void_p(stream or None)))
+
+
+def spmv_host(matrix: HBDIA, x: np.ndarray, y: np.ndarray) -> None:
+    """End-to-end y = A x on host arrays (copies in, SpMV, copies out, sync)."""
+    _check(_load().hbdia_spmv_host(matrix.handle, ctypes.c_void_p(x.ctypes.data), ctypes.c_void_p(y.ctypes.data)))
+
+
+# ---------------------------------------------------------------- workloads
+def _two_call(fn, *args):
+    nnz = ctypes.c_int64(0)
+    _check(fn(*args, ctypes.byref(nnz), None, None, None))
+    r = np.empty(nnz.value, np.int32)
+    c = np.empty(nnz.value, np.int32)
+    v = np.empty(nnz.value, np.float64)
+    _check(fn(*args, ctypes.byref(nnz), _vp(r), _vp(c), _vp(v)))
+    return r, c, v
+
+
+def generate_stencil27(nx: int, ny: int, nz: int, center: float = 26.0, neighbor: float = -1.0,
+                       extra_fraction: float = 0.0, extra_lo: float = 0.1, extra_hi: float = 1.0, seed: int = 0):
+    """Seeded 27-point stencil (+ extra off-pattern entries), row-sorted COO."""
+    return _two_call(_load().hbdia_generate_stencil27, nx, ny, nz, center, neighbor, extra_fraction,
+                     extra_lo, extra_hi, seed)
+
+
+def generate_stencil7(nx: int, ny: int, nz: int, center: float = 6.0, neighbor: float = -1.0):
+    return _two_call(_load().hbdia_generate_stencil7, nx, ny, nz, center, neighbor)
+
+
+def generate_banded(n: int, offsets: Sequence[int], lo: float = 0.5, hi: float = 1.5, drop: float = 0.3,
+                    scatter: float = 0.002, seed: int = 2):
+    o = np.ascontiguousarray(offsets, np.int32)
+    return _two_call(_load().hbdia_generate_banded, n, _vp(o), len(o), lo, hi, drop, scatter, seed)
+
+
+def fill_uniform(n: int, lo: float, hi: float, seed: int) -> np.ndarray:
+    out = np.empty(n, np.float64)
+    _check(_load().hbdia_fill_uniform(_vp(out), n, lo, hi, seed))
+    return out

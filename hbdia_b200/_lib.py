@@ -1,0 +1,123 @@
+"""ctypes binding of libhbdia_b200.so (the C ABI in include/hbdia_b200.h).
+
+There is no fallback: if the shared library is missing the import fails with
+instructions to build it.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "libhbdia_b200.so")
+
+c_i32, c_i64, c_u64, c_dbl, c_vp = ctypes.c_int32, ctypes.c_int64, ctypes.c_uint64, ctypes.c_double, ctypes.c_void_p
+c_i32p = ctypes.POINTER(ctypes.c_int32)
+c_i64p = ctypes.POINTER(ctypes.c_int64)
+c_vpp = ctypes.POINTER(ctypes.c_void_p)
+
+HBDIA_OK = 0
+HBDIA_ERR_INVALID_ARGUMENT = -1
+HBDIA_ERR_OUT_OF_RANGE = -2
+HBDIA_ERR_RUNTIME = -3
+HBDIA_ERR_CUDA = -4
+HBDIA_ERR_NO_MEMORY = -5
+HBDIA_ERR_NOT_CONVERTED = -6
+HBDIA_ERR_UNSUPPORTED = -7
+
+HBDIA_F64, HBDIA_F32 = 0, 1
+STORE_NATIVE, STORE_F32, STORE_BF16_SCALED = 0, 1, 2
+
+
+class MatrixInfo(ctypes.Structure):
+    _fields_ = [
+        ("dtype", c_i32), ("numRows", c_i32), ("numCols", c_i32), ("hasCOO", c_i32),
+        ("numNonZeros", c_i64), ("hasHBDIA", c_i32), ("onDevice", c_i32),
+        ("blockWidth", c_i32), ("threshold", c_i32), ("maxCooEntries", c_i64),
+        ("numBlocks", c_i32), ("numberDiagonals", c_i32), ("totalOffsets", c_i64),
+        ("numSlots", c_i64), ("numCoo", c_i64), ("histogramLength", c_i32), ("storage", c_i32),
+        ("deviceBytes", c_i64), ("bytesPerSpmv", c_i64),
+    ]
+
+
+class HBDIACudaError(RuntimeError):
+    """A CUDA runtime call inside the library failed."""
+
+
+_EXC = {
+    HBDIA_ERR_INVALID_ARGUMENT: ValueError,
+    HBDIA_ERR_OUT_OF_RANGE: IndexError,
+    HBDIA_ERR_RUNTIME: RuntimeError,
+    HBDIA_ERR_CUDA: HBDIACudaError,
+    HBDIA_ERR_NO_MEMORY: MemoryError,
+    HBDIA_ERR_NOT_CONVERTED: RuntimeError,
+    HBDIA_ERR_UNSUPPORTED: NotImplementedError,
+}
+
+# (name, restype, argtypes)
+_SIGS = [
+    ("hbdia_last_error", ctypes.c_char_p, []),
+    ("hbdia_version", ctypes.c_char_p, []),
+    ("hbdia_status_string", ctypes.c_char_p, [ctypes.c_int]),
+    ("hbdia_set_device", ctypes.c_int, [c_i32]),
+    ("hbdia_get_device", ctypes.c_int, [c_i32p]),
+    ("hbdia_matrix_create_empty", ctypes.c_int, [ctypes.c_int, c_vpp]),
+    ("hbdia_matrix_create", ctypes.c_int, [ctypes.c_int, c_vp, c_vp, c_vp, c_i64, c_i32, c_i32, c_vpp]),
+    ("hbdia_matrix_destroy", None, [c_vp]),
+    ("hbdia_matrix_stencil27", ctypes.c_int, [c_vp, c_i32, c_i32, c_i32, c_dbl, c_i32]),
+    ("hbdia_matrix_load_mtx", ctypes.c_int, [c_vp, ctypes.c_char_p, c_i32, c_i32, c_i32p]),
+    ("hbdia_matrix_convert", ctypes.c_int, [c_vp, c_i32, c_i32, c_i64, c_i32, c_i32, c_i32]),
+    ("hbdia_matrix_prepare_gpu", ctypes.c_int, [c_vp, c_i32]),
+    ("hbdia_matrix_convert_on_device", ctypes.c_int, [c_vp, c_i32, c_i32, c_i64, c_i32]),
+    ("hbdia_matrix_get_info", ctypes.c_int, [c_vp, ctypes.POINTER(MatrixInfo)]),
+    ("hbdia_matrix_export_layout", ctypes.c_int, [c_vp] * 10),
+    ("hbdia_matrix_export_coo", ctypes.c_int, [c_vp, c_vp, c_vp, c_vp]),
+    ("hbdia_matrix_export_nnz_per_row", ctypes.c_int, [c_vp, c_vp]),
+    ("hbdia_matrix_stream", ctypes.c_int, [c_vp, c_vpp]),
+    ("hbdia_matrix_synchronize", ctypes.c_int, [c_vp]),
+    ("hbdia_vector_create", ctypes.c_int, [ctypes.c_int, c_vp, c_i64, c_vpp]),
+    ("hbdia_vector_destroy", None, [c_vp]),
+    ("hbdia_vector_device_ptr", ctypes.c_int, [c_vp, c_vpp]),
+    ("hbdia_vector_size", ctypes.c_int, [c_vp, c_i64p]),
+    ("hbdia_vector_upload", ctypes.c_int, [c_vp, c_vp]),
+    ("hbdia_vector_download", ctypes.c_int, [c_vp, c_vp]),
+    ("hbdia_spmv", ctypes.c_int, [c_vp, c_vp, c_vp, c_i32, c_i32]),
+    ("hbdia_spmv_device", ctypes.c_int, [c_vp, c_vp, c_vp, c_vp]),
+    ("hbdia_spmm_device", ctypes.c_int, [c_vp, c_vp, c_i64, c_vp, c_i64, c_i32, c_vp]),
+    ("hbdia_spmv_host", ctypes.c_int, [c_vp, c_vp, c_vp]),
+    ("hbdia_generate_stencil27", ctypes.c_int,
+     [c_i32, c_i32, c_i32, c_dbl, c_dbl, c_dbl, c_dbl, c_dbl, c_u64, c_i64p, c_vp, c_vp, c_vp]),
+    ("hbdia_generate_stencil7", ctypes.c_int, [c_i32, c_i32, c_i32, c_dbl, c_dbl, c_i64p, c_vp, c_vp, c_vp]),
+    ("hbdia_generate_banded", ctypes.c_int,
+     [c_i32, c_vp, c_i32, c_dbl, c_dbl, c_dbl, c_dbl, c_u64, c_i64p, c_vp, c_vp, c_vp]),
+    ("hbdia_fill_uniform", ctypes.c_int, [c_vp, c_i64, c_dbl, c_dbl, c_u64]),
+]
+
+# every C-ABI entry point (the exported-symbol check in the tests uses this list)
+EXPORTED = [s[0] for s in _SIGS]
+
+_lib = None
+
+
+def load() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"{LIB_PATH} is missing: build the CUDA library first "
+                "(python -m hbdia_b200.build, or __graft_entry__.build())")
+        lib = ctypes.CDLL(LIB_PATH)
+        for name, res, args in _SIGS:
+            f = getattr(lib, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = lib
+    return _lib
+
+
+def check(status: int) -> None:
+    if status != HBDIA_OK:
+        lib = load()
+        msg = lib.hbdia_last_error().decode(errors="replace")
+        name = lib.hbdia_status_string(status).decode()
+        raise _EXC.get(status, RuntimeError)(f"{name}: {msg}")

@@ -1,0 +1,515 @@
+// The C ABI (include/hbdia_b200.h): matrix and vector handles, conversion,
+// SpMV entry points and workload generators.  Exceptions never cross the ABI;
+// they become hbdia_status codes with a per-thread message.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <new>
+#include <string>
+
+#include "hbdia_internal.hpp"
+
+using hbdia::Error;
+
+struct hbdia_vector {
+    int32_t dtype = HBDIA_F64;
+    int64_t n = 0;
+    void *d = nullptr;
+};
+
+struct hbdia_matrix {
+    int32_t dtype = HBDIA_F64;
+    bool hasCOO = false;
+    bool hasHBDIA = false;
+    bool hostLayout = false;  // host layout materialised
+    hbdia::Coo<double> c64;
+    hbdia::Coo<float> c32;
+    hbdia::HostLayout<double> L64;
+    hbdia::HostLayout<float> L32;
+    hbdia::DevicePlan plan;
+    int32_t blockWidth = 0, threshold = 0;
+    int64_t maxCoo = 0;
+    std::mutex hostMu;  // serialises hbdia_spmv_host's scratch buffers
+};
+
+namespace {
+
+thread_local std::string g_err;
+
+void set_err(const char *m) { g_err = m ? m : ""; }
+
+template <typename F>
+int guarded(F &&f) {
+    try {
+        f();
+        g_err.clear();
+        return HBDIA_OK;
+    } catch (const Error &e) {
+        set_err(e.what());
+        return e.status;
+    } catch (const std::bad_alloc &) {
+        set_err("out of host memory");
+        return HBDIA_ERR_NO_MEMORY;
+    } catch (const std::exception &e) {
+        set_err(e.what());
+        return HBDIA_ERR_RUNTIME;
+    }
+}
+
+size_t esize(int32_t dtype) { return dtype == HBDIA_F32 ? sizeof(float) : sizeof(double); }
+
+void need(bool ok, int status, const char *msg) {
+    if (!ok) throw Error(status, msg);
+}
+
+int64_t coo_nnz(const hbdia_matrix *m) {
+    return m->dtype == HBDIA_F32 ? static_cast<int64_t>(m->c32.vals.size())
+                                 : static_cast<int64_t>(m->c64.vals.size());
+}
+int32_t num_rows(const hbdia_matrix *m) { return m->dtype == HBDIA_F32 ? m->c32.numRows : m->c64.numRows; }
+int32_t num_cols(const hbdia_matrix *m) { return m->dtype == HBDIA_F32 ? m->c32.numCols : m->c64.numCols; }
+
+template <typename T>
+void fill_coo(hbdia::Coo<T> &c, const int32_t *r, const int32_t *col, const void *v, int64_t nnz,
+              int32_t nR, int32_t nC) {
+    // HBDIA(rows, cols, vals[, numRows, numCols]) (src/Format/HBDIA.cpp:23-80)
+    need(nnz >= 0, HBDIA_ERR_INVALID_ARGUMENT, "nnz must be non-negative");
+    need(nnz == 0 || (r && col && v), HBDIA_ERR_INVALID_ARGUMENT, "null COO array");
+    if (nnz > 2147483647LL) throw Error(HBDIA_ERR_UNSUPPORTED, "more than 2^31-1 entries");
+    const bool infer = nR <= 0 && nC <= 0;
+    if (!infer && (nR <= 0 || nC <= 0))
+        throw Error(HBDIA_ERR_INVALID_ARGUMENT, "Matrix dimensions must be positive");
+    c.rows.assign(r, r + nnz);
+    c.cols.assign(col, col + nnz);
+    c.vals.assign(static_cast<const T *>(v), static_cast<const T *>(v) + nnz);
+    c.nnzPerRow.clear();
+    if (infer) {
+        int32_t mr = 0, mc = 0;
+        for (int64_t i = 0; i < nnz; ++i) {
+            // the reference does not check signs here; a negative index has no
+            // place in the layout, so it is rejected like an out-of-range one
+            if (r[i] < 0 || col[i] < 0)
+                throw Error(HBDIA_ERR_OUT_OF_RANGE, "negative index at entry " + std::to_string(i));
+            mr = std::max(mr, r[i] + 1);
+            mc = std::max(mc, col[i] + 1);
+        }
+        c.numRows = mr;
+        c.numCols = mc;
+        return;
+    }
+    for (int64_t i = 0; i < nnz; ++i) {
+        if (r[i] < 0 || r[i] >= nR)
+            throw Error(HBDIA_ERR_OUT_OF_RANGE, "Row index " + std::to_string(r[i]) +
+                                                     " is out of range [0, " + std::to_string(nR - 1) + "]");
+        if (col[i] < 0 || col[i] >= nC)
+            throw Error(HBDIA_ERR_OUT_OF_RANGE, "Column index " + std::to_string(col[i]) +
+                                                     " is out of range [0, " + std::to_string(nC - 1) + "]");
+    }
+    c.numRows = nR;
+    c.numCols = nC;
+}
+
+void reset_hbdia(hbdia_matrix *m) {
+    hbdia::free_plan(m->plan);
+    m->L64 = hbdia::HostLayout<double>();
+    m->L32 = hbdia::HostLayout<float>();
+    m->hasHBDIA = false;
+    m->hostLayout = false;
+}
+
+void prepare(hbdia_matrix *m, int32_t storage) {
+    need(m->hasHBDIA, HBDIA_ERR_NOT_CONVERTED, "matrix is not in HBDIA format");
+    need(m->hostLayout, HBDIA_ERR_NOT_CONVERTED, "no host layout to upload");
+    if (m->dtype == HBDIA_F32) hbdia::build_plan(m->L32, storage, m->plan);
+    else hbdia::build_plan(m->L64, storage, m->plan);
+}
+
+void ensure_device(hbdia_matrix *m) {
+    if (!m->plan.base) prepare(m, HBDIA_STORE_NATIVE);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *hbdia_last_error(void) { return g_err.c_str(); }
+const char *hbdia_version(void) { return "hbdia_b200 0.1 (sm_100a)"; }
+
+int hbdia_set_device(int32_t device) {
+    return guarded([&] { hbdia::check_cuda(cudaSetDevice(device), "cudaSetDevice"); });
+}
+
+int hbdia_get_device(int32_t *device) {
+    return guarded([&] {
+        need(device != nullptr, HBDIA_ERR_INVALID_ARGUMENT, "null argument");
+        int d = 0;
+        hbdia::check_cuda(cudaGetDevice(&d), "cudaGetDevice");
+        *device = d;
+    });
+}
+
+const char *hbdia_status_string(int s) {
+    switch (s) {
+        case HBDIA_OK: return "HBDIA_OK";
+        case HBDIA_ERR_INVALID_ARGUMENT: return "HBDIA_ERR_INVALID_ARGUMENT";
+        case HBDIA_ERR_OUT_OF_RANGE: return "HBDIA_ERR_OUT_OF_RANGE";
+        case HBDIA_ERR_RUNTIME: return "HBDIA_ERR_RUNTIME";
+        case HBDIA_ERR_CUDA: return "HBDIA_ERR_CUDA";
+        case HBDIA_ERR_NO_MEMORY: return "HBDIA_ERR_NO_MEMORY";
+        case HBDIA_ERR_NOT_CONVERTED: return "HBDIA_ERR_NOT_CONVERTED";
+        case HBDIA_ERR_UNSUPPORTED: return "HBDIA_ERR_UNSUPPORTED";
+        default: return "HBDIA_ERR_UNKNOWN";
+    }
+}
+
+int hbdia_matrix_create_empty(hbdia_dtype dtype, hbdia_matrix **out) {
+    return guarded([&] {
+        need(out != nullptr, HBDIA_ERR_INVALID_ARGUMENT, "null output handle");
+        need(dtype == HBDIA_F64 || dtype == HBDIA_F32, HBDIA_ERR_INVALID_ARGUMENT, "unknown dtype");
+        auto *m = new hbdia_matrix();
+        m->dtype = dtype;
+        *out = m;
+    });
+}
+
+int hbdia_matrix_create(hbdia_dtype dtype, const int32_t *rows, const int32_t *cols, const void *values,
+                        int64_t nnz, int32_t numRows, int32_t numCols, hbdia_matrix **out) {
+    return guarded([&] {
+        need(out != nullptr, HBDIA_ERR_INVALID_ARGUMENT, "null output handle");
+        need(dtype == HBDIA_F64 || dtype == HBDIA_F32, HBDIA_ERR_INVALID_ARGUMENT, "unknown dtype");
+        std::unique_ptr<hbdia_matrix> m(new hbdia_matrix());
+        m->dtype = dtype;
+        if (dtype == HBDIA_F32) fill_coo(m->c32, rows, cols, values, nnz, numRows, numCols);
+        else fill_coo(m->c64, rows, cols, values, nnz, numRows, numCols);
+        m->hasCOO = true;
+        *out = m.release();
+    });
+}
+
+void hbdia_matrix_destroy(hbdia_matrix *m) {
+    if (!m) return;
+    hbdia::free_plan(m->plan);
+    delete m;
+}
+
+int hbdia_matrix_stencil27(hbdia_matrix *m, int32_t nx, int32_t ny, int32_t nz, double noise,
+                           int32_t iteration) {
+    return guarded([&] {
+        need(m && nx > 0 && ny > 0 && nz > 0, HBDIA_ERR_INVALID_ARGUMENT, "bad stencil arguments");
+        need(static_cast<int64_t>(nx) * ny * nz * 27 < 2147483647LL, HBDIA_ERR_UNSUPPORTED,
+             "grid too large for the reference's int arithmetic");
+        reset_hbdia(m);
+        if (m->dtype == HBDIA_F32) hbdia::reference_stencil27(nx, ny, nz, noise, iteration, m->c32);
+        else hbdia::reference_stencil27(nx, ny, nz, noise, iteration, m->c64);
+        m->hasCOO = true;
+    });
+}
+
+int hbdia_matrix_load_mtx(hbdia_matrix *m, const char *path, int32_t numRows, int32_t numCols,
+                          int32_t *ok) {
+    return guarded([&] {
+        need(m && path && ok, HBDIA_ERR_INVALID_ARGUMENT, "null argument");
+        bool r;
+        if (m->dtype == HBDIA_F32) {
+            hbdia::Coo<float> c;
+            r = hbdia::load_mtx(path, numRows, numCols, c);
+            if (r || !c.vals.empty()) { reset_hbdia(m); m->c32 = std::move(c); m->hasCOO = true; }
+        } else {
+            hbdia::Coo<double> c;
+            r = hbdia::load_mtx(path, numRows, numCols, c);
+            if (r || !c.vals.empty()) { reset_hbdia(m); m->c64 = std::move(c); m->hasCOO = true; }
+        }
+        *ok = r ? 1 : 0;
+    });
+}
+
+int hbdia_matrix_convert(hbdia_matrix *m, int32_t blockWidth, int32_t threshold, int64_t maxCoo,
+                         int32_t cooIsUnique, int32_t execMode, int32_t upload) {
+    (void)cooIsUnique;  // the reference ignores it too (src/Format/HBDIA.cpp:531-534)
+    (void)execMode;     // the COO remainder always runs fused on the GPU
+    return guarded([&] {
+        need(m != nullptr, HBDIA_ERR_INVALID_ARGUMENT, "null matrix");
+        // early returns of src/Format/HBDIA.cpp:511-524
+        if (m->hasHBDIA || !m->hasCOO || coo_nnz(m) == 0) return;
+        need(blockWidth > 0, HBDIA_ERR_INVALID_ARGUMENT, "blockWidth must be positive");
+        if (m->dtype == HBDIA_F32) hbdia::convert_to_hbdia(m->c32, blockWidth, threshold, maxCoo, m->L32);
+        else hbdia::convert_to_hbdia(m->c64, blockWidth, threshold, maxCoo, m->L64);
+        m->hasHBDIA = true;
+        m->hostLayout = true;
+        m->blockWidth = blockWidth;
+        m->threshold = threshold;
+        m->maxCoo = maxCoo;
+        if (upload) prepare(m, HBDIA_STORE_NATIVE);
+    });
+}
+
+int hbdia_matrix_prepare_gpu(hbdia_matrix *m, int32_t storage) {
+    return guarded([&] {
+        need(m != nullptr, HBDIA_ERR_INVALID_ARGUMENT, "null matrix");
+        prepare(m, storage);
+    });
+}
+
+int hbdia_matrix_convert_on_device(hbdia_matrix *, int32_t, int32_t, int64_t, int32_t) {
+    return guarded([&] { throw Error(HBDIA_ERR_UNSUPPORTED, "device converter not built yet"); });
+}
+
+int hbdia_matrix_get_info(const hbdia_matrix *m, hbdia_matrix_info *info) {
+    return guarded([&] {
+        need(m && info, HBDIA_ERR_INVALID_ARGUMENT, "null argument");
+        hbdia_matrix_info I;
+        std::memset(&I, 0, sizeof(I));
+        I.dtype = m->dtype;
+        I.numRows = num_rows(m);
+        I.numCols = num_cols(m);
+        I.hasCOO = m->hasCOO;
+        I.numNonZeros = coo_nnz(m);
+        I.hasHBDIA = m->hasHBDIA;
+        I.onDevice = m->plan.base != nullptr;
+        I.blockWidth = m->blockWidth;
+        I.threshold = m->threshold;
+        I.maxCooEntries = m->maxCoo;
+        I.storage = m->plan.storage;
+        I.deviceBytes = static_cast<int64_t>(m->plan.bytes);
+        I.bytesPerSpmv = m->plan.bytesPerSpmv;
+        if (m->hostLayout) {
+            auto fill = [&](const auto &L) {
+                I.numBlocks = L.numBlocks;
+                I.numberDiagonals = L.numberDiagonals;
+                I.totalOffsets = static_cast<int64_t>(L.offsets.size());
+                I.numSlots = static_cast<int64_t>(L.data.size());
+                I.numCoo = static_cast<int64_t>(L.cooRow.size());
+                I.histogramLength = static_cast<int32_t>(L.histBlocks.size());
+            };
+            if (m->dtype == HBDIA_F32) fill(m->L32);
+            else fill(m->L64);
+        } else if (m->plan.base) {
+            I.numBlocks = m->plan.numBlocks;
+            I.totalOffsets = m->plan.totalOffsets;
+            I.numSlots = m->plan.slots;
+            I.numCoo = m->plan.nCoo;
+        }
+        *info = I;
+    });
+}
+
+int hbdia_matrix_export_layout(const hbdia_matrix *m, int32_t *offsets, int32_t *blockStart, void *data,
+                               int32_t *cooRow, int32_t *cooCol, void *cooVal, int32_t *cooRowPtr,
+                               int32_t *histBlocks, int32_t *histNnz) {
+    return guarded([&] {
+        need(m != nullptr, HBDIA_ERR_INVALID_ARGUMENT, "null matrix");
+        need(m->hasHBDIA && m->hostLayout, HBDIA_ERR_NOT_CONVERTED, "no host HBDIA layout");
+        auto cp = [](void *dst, const auto &v) {
+            if (dst && !v.empty()) std::memcpy(dst, v.data(), v.size() * sizeof(v[0]));
+        };
+        auto go = [&](const auto &L) {
+            cp(offsets, L.offsets);
+            cp(blockStart, L.blockStart);
+            cp(data, L.data);
+            cp(cooRow, L.cooRow);
+            cp(cooCol, L.cooCol);
+            cp(cooVal, L.cooVal);
+            cp(cooRowPtr, L.cooRowPtr);
+            cp(histBlocks, L.histBlocks);
+            cp(histNnz, L.histNnz);
+        };
+        if (m->dtype == HBDIA_F32) go(m->L32);
+        else go(m->L64);
+    });
+}
+
+int hbdia_matrix_export_coo(const hbdia_matrix *m, int32_t *rows, int32_t *cols, void *values) {
+    return guarded([&] {
+        need(m != nullptr, HBDIA_ERR_INVALID_ARGUMENT, "null matrix");
+        auto go = [&](const auto &c) {
+            if (rows && !c.rows.empty()) std::memcpy(rows, c.rows.data(), c.rows.size() * 4);
+            if (cols && !c.cols.empty()) std::memcpy(cols, c.cols.data(), c.cols.size() * 4);
+            if (values && !c.vals.empty()) std::memcpy(values, c.vals.data(), c.vals.size() * sizeof(c.vals[0]));
+        };
+        if (m->dtype == HBDIA_F32) go(m->c32);
+        else go(m->c64);
+    });
+}
+
+int hbdia_matrix_export_nnz_per_row(const hbdia_matrix *m, int32_t *nnzPerRow) {
+    return guarded([&] {
+        need(m && nnzPerRow, HBDIA_ERR_INVALID_ARGUMENT, "null argument");
+        const auto &v = m->dtype == HBDIA_F32 ? m->c32.nnzPerRow : m->c64.nnzPerRow;
+        if (!v.empty()) std::memcpy(nnzPerRow, v.data(), v.size() * 4);
+    });
+}
+
+int hbdia_matrix_stream(const hbdia_matrix *m, void **stream) {
+    return guarded([&] {
+        need(m && stream, HBDIA_ERR_INVALID_ARGUMENT, "null argument");
+        need(m->plan.base != nullptr, HBDIA_ERR_NOT_CONVERTED, "matrix has no device layout");
+        *stream = m->plan.stream;
+    });
+}
+
+int hbdia_matrix_synchronize(const hbdia_matrix *m) {
+    return guarded([&] {
+        need(m != nullptr, HBDIA_ERR_INVALID_ARGUMENT, "null matrix");
+        if (m->plan.stream)
+            hbdia::check_cuda(cudaStreamSynchronize(static_cast<cudaStream_t>(m->plan.stream)),
+                              "cudaStreamSynchronize");
+    });
+}
+
+// ---------------------------------------------------------------- vectors
+int hbdia_vector_create(hbdia_dtype dtype, const void *host, int64_t n, hbdia_vector **out) {
+    return guarded([&] {
+        need(out != nullptr && n >= 0, HBDIA_ERR_INVALID_ARGUMENT, "bad vector arguments");
+        need(dtype == HBDIA_F64 || dtype == HBDIA_F32, HBDIA_ERR_INVALID_ARGUMENT, "unknown dtype");
+        std::unique_ptr<hbdia_vector> v(new hbdia_vector());
+        v->dtype = dtype;
+        v->n = n;
+        const size_t bytes = static_cast<size_t>(n) * esize(dtype);
+        hbdia::check_cuda(cudaMalloc(&v->d, bytes ? bytes : 256), "cudaMalloc(vector)");
+        int err = host && bytes ? cudaMemcpy(v->d, host, bytes, cudaMemcpyHostToDevice)
+                                : cudaMemset(v->d, 0, bytes ? bytes : 256);
+        if (err != cudaSuccess) {
+            cudaFree(v->d);
+            hbdia::check_cuda(err, "vector initialisation");
+        }
+        *out = v.release();
+    });
+}
+
+void hbdia_vector_destroy(hbdia_vector *v) {
+    if (!v) return;
+    if (v->d) cudaFree(v->d);
+    delete v;
+}
+
+int hbdia_vector_device_ptr(const hbdia_vector *v, void **p) {
+    return guarded([&] {
+        need(v && p, HBDIA_ERR_INVALID_ARGUMENT, "null argument");
+        *p = v->d;
+    });
+}
+
+int hbdia_vector_size(const hbdia_vector *v, int64_t *n) {
+    return guarded([&] {
+        need(v && n, HBDIA_ERR_INVALID_ARGUMENT, "null argument");
+        *n = v->n;
+    });
+}
+
+int hbdia_vector_upload(hbdia_vector *v, const void *host) {
+    return guarded([&] {
+        need(v && host, HBDIA_ERR_INVALID_ARGUMENT, "null argument");
+        hbdia::check_cuda(cudaMemcpy(v->d, host, v->n * esize(v->dtype), cudaMemcpyHostToDevice),
+                          "cudaMemcpy(vector upload)");
+    });
+}
+
+int hbdia_vector_download(const hbdia_vector *v, void *host) {
+    return guarded([&] {
+        need(v && host, HBDIA_ERR_INVALID_ARGUMENT, "null argument");
+        hbdia::check_cuda(cudaDeviceSynchronize(), "cudaDeviceSynchronize");
+        hbdia::check_cuda(cudaMemcpy(host, v->d, v->n * esize(v->dtype), cudaMemcpyDeviceToHost),
+                          "cudaMemcpy(vector download)");
+    });
+}
+
+// ---------------------------------------------------------------- SpMV
+int hbdia_spmv(hbdia_matrix *m, const hbdia_vector *x, hbdia_vector *y, int32_t execCOOCPU,
+               int32_t execCOOGPU) {
+    return guarded([&] {
+        need(m && x && y, HBDIA_ERR_INVALID_ARGUMENT, "null argument");
+        need(x->dtype == m->dtype && y->dtype == m->dtype, HBDIA_ERR_INVALID_ARGUMENT,
+             "vector and matrix value types differ");
+        const int32_t nR = num_rows(m), nC = num_cols(m);
+        need(x->n >= std::max(nR, nC), HBDIA_ERR_INVALID_ARGUMENT, "input vector shorter than the matrix");
+        need(y->n >= nR, HBDIA_ERR_INVALID_ARGUMENT, "output vector shorter than the matrix");
+        if (!m->hasHBDIA) {
+            need(coo_nnz(m) == 0, HBDIA_ERR_NOT_CONVERTED, "matrix is not in HBDIA format");
+            // an empty matrix: y = 0
+            hbdia::check_cuda(cudaMemset(y->d, 0, static_cast<size_t>(nR) * esize(m->dtype)), "cudaMemset");
+            return;
+        }
+        const int64_t nCoo = m->hostLayout ? (m->dtype == HBDIA_F32 ? (int64_t)m->L32.cooRow.size()
+                                                                    : (int64_t)m->L64.cooRow.size())
+                                           : m->plan.nCoo;
+        if (nCoo > 0 && !execCOOCPU && !execCOOGPU)
+            throw Error(HBDIA_ERR_RUNTIME, "Invalid COO execution flags");
+        ensure_device(m);
+        hbdia::launch_spmv(m->plan, x->d, y->d, nullptr);
+    });
+}
+
+int hbdia_spmv_device(const hbdia_matrix *m, const void *x, void *y, void *stream) {
+    return guarded([&] {
+        need(m != nullptr, HBDIA_ERR_INVALID_ARGUMENT, "null matrix");
+        need(m->plan.base != nullptr, HBDIA_ERR_NOT_CONVERTED, "matrix has no device layout");
+        hbdia::launch_spmv(m->plan, x, y, stream);
+    });
+}
+
+int hbdia_spmm_device(const hbdia_matrix *m, const void *X, int64_t ldx, void *Y, int64_t ldy, int32_t k,
+                      void *stream) {
+    return guarded([&] {
+        need(m != nullptr, HBDIA_ERR_INVALID_ARGUMENT, "null matrix");
+        need(m->plan.base != nullptr, HBDIA_ERR_NOT_CONVERTED, "matrix has no device layout");
+        hbdia::launch_spmm(m->plan, X, ldx, Y, ldy, k, stream);
+    });
+}
+
+int hbdia_spmv_host(hbdia_matrix *m, const void *xh, void *yh) {
+    return guarded([&] {
+        need(m && xh && yh, HBDIA_ERR_INVALID_ARGUMENT, "null argument");
+        need(m->hasHBDIA, HBDIA_ERR_NOT_CONVERTED, "matrix is not in HBDIA format");
+        ensure_device(m);
+        std::lock_guard<std::mutex> lk(m->hostMu);
+        hbdia::DevicePlan &P = m->plan;
+        const size_t es = esize(m->dtype);
+        const size_t xb = static_cast<size_t>(std::max(P.n, P.numCols)) * es;
+        const size_t yb = static_cast<size_t>(P.n) * es;
+        if (!P.xScratch) hbdia::check_cuda(cudaMalloc(&P.xScratch, xb), "cudaMalloc(x scratch)");
+        if (!P.yScratch) hbdia::check_cuda(cudaMalloc(&P.yScratch, yb), "cudaMalloc(y scratch)");
+        cudaStream_t s = static_cast<cudaStream_t>(P.stream);
+        hbdia::check_cuda(cudaMemcpyAsync(P.xScratch, xh, xb, cudaMemcpyHostToDevice, s), "cudaMemcpyAsync(x)");
+        hbdia::launch_spmv(P, P.xScratch, P.yScratch, s);
+        hbdia::check_cuda(cudaMemcpyAsync(yh, P.yScratch, yb, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync(y)");
+        hbdia::check_cuda(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+    });
+}
+
+// ---------------------------------------------------------------- workloads
+int hbdia_generate_stencil27(int32_t nx, int32_t ny, int32_t nz, double center, double neighbor,
+                             double frac, double lo, double hi, uint64_t seed, int64_t *nnz,
+                             int32_t *rows, int32_t *cols, double *values) {
+    return guarded([&] {
+        hbdia::generate_stencil(27, nx, ny, nz, center, neighbor, frac, lo, hi, seed, nnz, rows, cols, values);
+    });
+}
+
+int hbdia_generate_stencil7(int32_t nx, int32_t ny, int32_t nz, double center, double neighbor,
+                            int64_t *nnz, int32_t *rows, int32_t *cols, double *values) {
+    return guarded([&] {
+        hbdia::generate_stencil(7, nx, ny, nz, center, neighbor, 0.0, 0.0, 0.0, 0, nnz, rows, cols, values);
+    });
+}
+
+int hbdia_generate_banded(int32_t n, const int32_t *offsets, int32_t numOffsets, double lo, double hi,
+                          double dropProb, double scatterFraction, uint64_t seed, int64_t *nnz,
+                          int32_t *rows, int32_t *cols, double *values) {
+    return guarded([&] {
+        hbdia::generate_banded(n, offsets, numOffsets, lo, hi, dropProb, scatterFraction, seed, nnz, rows,
+                               cols, values);
+    });
+}
+
+int hbdia_fill_uniform(double *out, int64_t n, double lo, double hi, uint64_t seed) {
+    return guarded([&] {
+        need(out != nullptr || n == 0, HBDIA_ERR_INVALID_ARGUMENT, "null output");
+        hbdia::fill_uniform(out, n, lo, hi, seed);
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,106 @@
+// Internal data structures of libhbdia_b200.so (not part of the ABI).
+#pragma once
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "hbdia_b200.h"
+
+namespace hbdia {
+
+// Error carrying an hbdia_status, thrown inside the library and turned into
+// a status code at the C ABI.
+struct Error : std::runtime_error {
+    int status;
+    Error(int s, const std::string &msg) : std::runtime_error(msg), status(s) {}
+};
+
+// COO input of one matrix (the reference's values/rowIndices/colIndices).
+template <typename T>
+struct Coo {
+    std::vector<int32_t> rows, cols;
+    std::vector<T> vals;
+    int32_t numRows = 0, numCols = 0;
+    std::vector<int32_t> nnzPerRow;  // filled by the stencil generator only
+};
+
+// Host HBDIA layout: exactly the reference's host-side members after
+// convertToHBDIAFormat (include/Format/HBDIA.hpp:232-253), with
+// offsetsPerBlock stored flattened.
+template <typename T>
+struct HostLayout {
+    int32_t numRows = 0, numCols = 0, blockWidth = 0, threshold = 0;
+    int64_t maxCoo = 0;
+    int32_t numBlocks = 0;                 // maxNumBlocks
+    std::vector<int32_t> offsets;          // kept offsets, ascending per block
+    std::vector<int32_t> blockStart;       // numBlocks + 1, offset units
+    std::vector<T> data;                   // [block][offsetIdx][lane]
+    std::vector<int32_t> cooRow, cooCol;   // COO remainder, input order
+    std::vector<T> cooVal;
+    std::vector<int32_t> cooRowPtr;        // numRows + 1 (reference's cpuRowPtr)
+    int32_t numberDiagonals = 0;
+    std::vector<int32_t> histBlocks, histNnz;
+    bool cooRowSorted = true;              // COO rows non-decreasing
+};
+
+// Converter: convertToHBDIAFormat restated for speed (OpenMP), bit-exact.
+template <typename T>
+void convert_to_hbdia(const Coo<T> &coo, int32_t blockWidth, int32_t threshold, int64_t maxCoo,
+                      HostLayout<T> &out);
+
+// Generators (generate.cpp)
+template <typename T>
+void reference_stencil27(int nx, int ny, int nz, double noise, int iteration, Coo<T> &out);
+template <typename T>
+bool load_mtx(const std::string &path, int numRows, int numCols, Coo<T> &out);
+
+// Simple sequential stable sort of COO (rows) used when the COO remainder is
+// not row-sorted; returns the permutation.
+std::vector<int64_t> stable_row_order(const std::vector<int32_t> &rows, int32_t numRows);
+
+}  // namespace hbdia
+
+namespace hbdia {
+
+// Device layout of one converted matrix (prepareForGPU's arrays,
+// src/Format/HBDIA.cpp:720-816, in this library's form).  All arrays live in
+// one device allocation, each 256-byte aligned.
+struct DevicePlan {
+    int32_t dtype = HBDIA_F64;          // T of x, y and the COO values
+    int32_t storage = HBDIA_STORE_NATIVE;
+    int32_t n = 0, numCols = 0, bw = 0, numBlocks = 0, numTiles = 0;
+    int64_t totalOffsets = 0, slots = 0, nCoo = 0;
+    void *base = nullptr;
+    size_t bytes = 0;
+    void *vals = nullptr;                // storage type
+    float *scale = nullptr;              // per-block scale (bf16 storage)
+    int32_t *offs = nullptr, *blkOff = nullptr;
+    int32_t *cooRow = nullptr, *cooCol = nullptr;
+    void *cooVal = nullptr;              // T
+    int32_t *cooRowPtr = nullptr, *cooTile = nullptr;
+    void *stream = nullptr;              // cudaStream_t owned by the plan
+    void *xScratch = nullptr, *yScratch = nullptr;  // hbdia_spmv_host buffers
+    int64_t bytesPerSpmv = 0;            // algorithmic HBM bytes of one SpMV
+};
+
+template <typename T>
+void build_plan(const HostLayout<T> &L, int storage, DevicePlan &P);
+void free_plan(DevicePlan &P);
+// y = A x on `stream` (a cudaStream_t; nullptr -> the plan's stream)
+void launch_spmv(const DevicePlan &P, const void *x, void *y, void *stream);
+void launch_spmm(const DevicePlan &P, const void *X, int64_t ldx, void *Y, int64_t ldy, int32_t k,
+                 void *stream);
+// throws Error(HBDIA_ERR_CUDA) with the CUDA error string
+void check_cuda(int err, const char *what);
+
+int generate_stencil(int stencilPoints, int32_t nx, int32_t ny, int32_t nz, double center,
+                     double neighbor, double frac, double lo, double hi, uint64_t seed,
+                     int64_t *nnzOut, int32_t *rows, int32_t *cols, double *vals);
+int generate_banded(int32_t n, const int32_t *offs, int32_t noffs, double lo, double hi, double drop,
+                    double scatter, uint64_t seed, int64_t *nnzOut, int32_t *rows, int32_t *cols,
+                    double *vals);
+void fill_uniform(double *out, int64_t n, double lo, double hi, uint64_t seed);
+
+}  // namespace hbdia

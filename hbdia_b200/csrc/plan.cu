@@ -1,0 +1,254 @@
+// Device layout (prepareForGPU, src/Format/HBDIA.cpp:720-816, in this
+// library's form) and the SpMV launchers.
+//
+// HBM layout of one plan, a single allocation with 256-byte aligned parts:
+//   vals      storage-type values, [block][offsetIdx][lane]   (slots)
+//   scale     float per block (bf16 storage only)
+//   offs      int32 kept offsets, ascending per block           (totalOffsets)
+//   blkOff    int32 block -> first offset index                 (numBlocks + 1)
+//   cooRow/cooCol int32, cooVal T: the COO remainder, row-sorted (nCoo)
+//   cooRowPtr int32 CSR row pointer of the remainder            (numRows + 1)
+//   cooTile   int32 first remainder entry of each 32-row tile   (numTiles + 1)
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <type_traits>
+
+#include "hbdia_internal.hpp"
+#include "spmv_kernels.cuh"
+
+namespace hbdia {
+
+void check_cuda(int err, const char *what) {
+    if (err != cudaSuccess) {
+        throw Error(err == cudaErrorMemoryAllocation ? HBDIA_ERR_NO_MEMORY : HBDIA_ERR_CUDA,
+                    std::string(what) + ": " + cudaGetErrorString(static_cast<cudaError_t>(err)));
+    }
+}
+
+namespace {
+
+constexpr int kUnroll = 9;  // offsets in flight per lane in the bw == 32 kernel
+
+size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
+
+size_t storage_bytes(int storage, int dtype) {
+    if (storage == HBDIA_STORE_F32) return 4;
+    if (storage == HBDIA_STORE_BF16_SCALED) return 2;
+    return dtype == HBDIA_F32 ? 4 : 8;
+}
+
+}  // namespace
+
+void free_plan(DevicePlan &P) {
+    if (P.stream) {
+        cudaStreamSynchronize(static_cast<cudaStream_t>(P.stream));
+        cudaStreamDestroy(static_cast<cudaStream_t>(P.stream));
+    }
+    if (P.base) cudaFree(P.base);
+    if (P.xScratch) cudaFree(P.xScratch);
+    if (P.yScratch) cudaFree(P.yScratch);
+    P = DevicePlan();
+}
+
+template <typename T>
+void build_plan(const HostLayout<T> &L, int storage, DevicePlan &P) {
+    free_plan(P);
+    DevicePlan Q;
+    Q.dtype = std::is_same<T, float>::value ? HBDIA_F32 : HBDIA_F64;
+    if (storage != HBDIA_STORE_NATIVE && Q.dtype != HBDIA_F64)
+        throw Error(HBDIA_ERR_UNSUPPORTED, "reduced value storage needs a double matrix");
+    if (storage < HBDIA_STORE_NATIVE || storage > HBDIA_STORE_BF16_SCALED)
+        throw Error(HBDIA_ERR_INVALID_ARGUMENT, "unknown value storage");
+    Q.storage = storage;
+    Q.n = L.numRows;
+    Q.numCols = L.numCols;
+    Q.bw = L.blockWidth;
+    Q.numBlocks = L.numBlocks;
+    Q.numTiles = static_cast<int32_t>((static_cast<int64_t>(L.numRows) + 31) / 32);
+    Q.totalOffsets = static_cast<int64_t>(L.offsets.size());
+    Q.slots = static_cast<int64_t>(L.data.size());
+    Q.nCoo = static_cast<int64_t>(L.cooRow.size());
+
+    // The fused kernels walk the COO remainder row by row: use a stable
+    // row-sorted copy when the input order was not row-sorted (the reference
+    // assumes row-sorted input here, src/Format/HBDIA.cpp:671-703).
+    const int32_t *cr = L.cooRow.data(), *cc = L.cooCol.data();
+    const T *cv = L.cooVal.data();
+    const int32_t *crp = L.cooRowPtr.data();
+    std::vector<int32_t> sr, sc, srp;
+    std::vector<T> sv;
+    for (int64_t e = 0; e < Q.nCoo; ++e) {
+        if (cr[e] < 0 || cr[e] >= Q.n || cc[e] < 0 || cc[e] >= Q.numCols)
+            throw Error(HBDIA_ERR_OUT_OF_RANGE, "COO entry (" + std::to_string(cr[e]) + ", " +
+                                                     std::to_string(cc[e]) + ") outside the matrix");
+    }
+    if (!L.cooRowSorted) {
+        std::vector<int64_t> order = stable_row_order(L.cooRow, Q.n);
+        sr.resize(Q.nCoo);
+        sc.resize(Q.nCoo);
+        sv.resize(Q.nCoo);
+        for (int64_t e = 0; e < Q.nCoo; ++e) {
+            sr[e] = cr[order[e]];
+            sc[e] = cc[order[e]];
+            sv[e] = cv[order[e]];
+        }
+        srp.assign(static_cast<size_t>(Q.n) + 1, 0);
+        for (int64_t e = 0; e < Q.nCoo; ++e) srp[sr[e] + 1]++;
+        for (int32_t r = 0; r < Q.n; ++r) srp[r + 1] += srp[r];
+        cr = sr.data();
+        cc = sc.data();
+        cv = sv.data();
+        crp = srp.data();
+    }
+    std::vector<int32_t> tile(static_cast<size_t>(Q.numTiles) + 1);
+    for (int64_t t = 0; t <= Q.numTiles; ++t) tile[t] = crp[std::min<int64_t>(t * 32, Q.n)];
+
+    // host-side value conversion for reduced storage
+    const size_t vsz = storage_bytes(storage, Q.dtype);
+    std::vector<float> vf, sf;
+    std::vector<__nv_bfloat16> vb;
+    const void *valSrc = L.data.data();
+    if (storage == HBDIA_STORE_F32) {
+        vf.resize(Q.slots);
+        for (int64_t i = 0; i < Q.slots; ++i) vf[i] = static_cast<float>(L.data[i]);
+        valSrc = vf.data();
+    } else if (storage == HBDIA_STORE_BF16_SCALED) {
+        vb.resize(Q.slots);
+        sf.assign(static_cast<size_t>(Q.numBlocks), 1.0f);
+        for (int32_t b = 0; b < Q.numBlocks; ++b) {
+            const int64_t s0 = static_cast<int64_t>(L.blockStart[b]) * Q.bw;
+            const int64_t s1 = static_cast<int64_t>(L.blockStart[b + 1]) * Q.bw;
+            double m = 0.0;
+            for (int64_t i = s0; i < s1; ++i) m = std::max(m, std::fabs(static_cast<double>(L.data[i])));
+            const float s = m > 0.0 ? static_cast<float>(m) : 1.0f;
+            sf[b] = s;
+            for (int64_t i = s0; i < s1; ++i)
+                vb[i] = __float2bfloat16_rn(static_cast<float>(static_cast<double>(L.data[i]) / s));
+        }
+        valSrc = vb.data();
+    }
+
+    // one allocation
+    size_t off = 0;
+    auto carve = [&](size_t bytes) {
+        const size_t o = off;
+        off += align256(bytes);
+        return o;
+    };
+    const size_t oVals = carve(Q.slots * vsz);
+    const size_t oScale = carve(storage == HBDIA_STORE_BF16_SCALED ? Q.numBlocks * sizeof(float) : 0);
+    const size_t oOffs = carve(Q.totalOffsets * sizeof(int32_t));
+    const size_t oBlk = carve((static_cast<size_t>(Q.numBlocks) + 1) * sizeof(int32_t));
+    const size_t oCR = carve(Q.nCoo * sizeof(int32_t));
+    const size_t oCC = carve(Q.nCoo * sizeof(int32_t));
+    const size_t oCV = carve(Q.nCoo * sizeof(T));
+    const size_t oRP = carve((static_cast<size_t>(Q.n) + 1) * sizeof(int32_t));
+    const size_t oTile = carve((static_cast<size_t>(Q.numTiles) + 1) * sizeof(int32_t));
+    Q.bytes = off;
+    check_cuda(cudaMalloc(&Q.base, Q.bytes), "cudaMalloc(matrix layout)");
+    char *base = static_cast<char *>(Q.base);
+    try {
+        Q.vals = base + oVals;
+        Q.scale = storage == HBDIA_STORE_BF16_SCALED ? reinterpret_cast<float *>(base + oScale) : nullptr;
+        Q.offs = reinterpret_cast<int32_t *>(base + oOffs);
+        Q.blkOff = reinterpret_cast<int32_t *>(base + oBlk);
+        Q.cooRow = reinterpret_cast<int32_t *>(base + oCR);
+        Q.cooCol = reinterpret_cast<int32_t *>(base + oCC);
+        Q.cooVal = base + oCV;
+        Q.cooRowPtr = reinterpret_cast<int32_t *>(base + oRP);
+        Q.cooTile = reinterpret_cast<int32_t *>(base + oTile);
+        auto up = [](void *dst, const void *src, size_t bytes) {
+            if (bytes) check_cuda(cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice), "cudaMemcpy(layout)");
+        };
+        up(Q.vals, valSrc, Q.slots * vsz);
+        if (Q.scale) up(Q.scale, sf.data(), Q.numBlocks * sizeof(float));
+        up(Q.offs, L.offsets.data(), Q.totalOffsets * sizeof(int32_t));
+        up(Q.blkOff, L.blockStart.data(), (static_cast<size_t>(Q.numBlocks) + 1) * sizeof(int32_t));
+        up(Q.cooRow, cr, Q.nCoo * sizeof(int32_t));
+        up(Q.cooCol, cc, Q.nCoo * sizeof(int32_t));
+        up(Q.cooVal, cv, Q.nCoo * sizeof(T));
+        up(Q.cooRowPtr, crp, (static_cast<size_t>(Q.n) + 1) * sizeof(int32_t));
+        up(Q.cooTile, tile.data(), (static_cast<size_t>(Q.numTiles) + 1) * sizeof(int32_t));
+        cudaStream_t s;
+        check_cuda(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "cudaStreamCreate");
+        Q.stream = s;
+    } catch (...) {
+        free_plan(Q);
+        throw;
+    }
+
+    // Algorithmic HBM bytes of one SpMV: every stored value, offset and index
+    // read once, x read once, y written once, one x gather per COO entry.
+    const int64_t xs = static_cast<int64_t>(sizeof(T));
+    int64_t bytes = Q.slots * static_cast<int64_t>(vsz) + 4 * Q.totalOffsets +
+                    4 * (static_cast<int64_t>(Q.numBlocks) + 1) + 2 * xs * Q.n +
+                    (8 + xs) * Q.nCoo + xs * Q.nCoo;
+    if (Q.scale) bytes += 4 * static_cast<int64_t>(Q.numBlocks);
+    if (Q.nCoo > 0) bytes += Q.bw == 32 ? 4 * (static_cast<int64_t>(Q.numTiles) + 1)
+                                        : 4 * (static_cast<int64_t>(Q.n) + 1);
+    Q.bytesPerSpmv = bytes;
+    P = Q;
+}
+
+template void build_plan<double>(const HostLayout<double> &, int, DevicePlan &);
+template void build_plan<float>(const HostLayout<float> &, int, DevicePlan &);
+
+namespace {
+
+template <typename VT, typename XT>
+void launch_typed(const DevicePlan &P, const void *x, void *y, cudaStream_t s) {
+    dev::SpmvArgs<VT, XT> a;
+    a.vals = static_cast<const VT *>(P.vals);
+    a.scale = P.scale;
+    a.offs = P.offs;
+    a.blkOff = P.blkOff;
+    a.cooRow = P.cooRow;
+    a.cooCol = P.cooCol;
+    a.cooVal = static_cast<const XT *>(P.cooVal);
+    a.cooRowPtr = P.cooRowPtr;
+    a.cooTile = P.cooTile;
+    a.n = P.n;
+    a.bw = P.bw;
+    a.numBlocks = P.numBlocks;
+    a.numTiles = P.numTiles;
+    a.hasCoo = P.nCoo > 0;
+    const XT *xp = static_cast<const XT *>(x);
+    XT *yp = static_cast<XT *>(y);
+    if (P.bw == 32) {
+        const int64_t warpsPerCta = 8;
+        const unsigned grid = static_cast<unsigned>((P.numTiles + warpsPerCta - 1) / warpsPerCta);
+        dev::spmv_bw32<VT, XT, kUnroll><<<grid, 256, 0, s>>>(a, xp, yp);
+    } else {
+        const unsigned grid = static_cast<unsigned>((static_cast<int64_t>(P.n) + 255) / 256);
+        dev::spmv_rowwise<VT, XT><<<grid, 256, 0, s>>>(a, xp, yp);
+    }
+    check_cuda(cudaGetLastError(), "SpMV launch");
+}
+
+}  // namespace
+
+void launch_spmv(const DevicePlan &P, const void *x, void *y, void *stream) {
+    if (!P.base) throw Error(HBDIA_ERR_NOT_CONVERTED, "matrix has no device layout");
+    if (!x || !y) throw Error(HBDIA_ERR_INVALID_ARGUMENT, "null vector pointer");
+    cudaStream_t s = static_cast<cudaStream_t>(stream ? stream : P.stream);
+    if (P.dtype == HBDIA_F32) {
+        launch_typed<float, float>(P, x, y, s);
+    } else if (P.storage == HBDIA_STORE_F32) {
+        launch_typed<float, double>(P, x, y, s);
+    } else if (P.storage == HBDIA_STORE_BF16_SCALED) {
+        launch_typed<__nv_bfloat16, double>(P, x, y, s);
+    } else {
+        launch_typed<double, double>(P, x, y, s);
+    }
+}
+
+void launch_spmm(const DevicePlan &, const void *, int64_t, void *, int64_t, int32_t, void *) {
+    throw Error(HBDIA_ERR_UNSUPPORTED, "SpMM is not built yet");
+}
+
+}  // namespace hbdia

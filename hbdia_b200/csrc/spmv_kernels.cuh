@@ -1,0 +1,188 @@
+// Device-side kernels of the fused HBDIA SpMV (sm_100a).
+//
+// y = A x for A in HBDIA form: a blocked-DIA part (per row block of width bw,
+// an ascending list of diagonal offsets, bw values per offset) plus a
+// row-sorted COO remainder.  One launch computes both parts and writes every
+// row of y once; the reference needs a DIA kernel, a separate COO SpMV and a
+// vector_add kernel (src/Operations/HBDIASpMV.cu:7-88,
+// src/Operations/HBDIASpMV.cpp:186-251).
+//
+// Arithmetic matches the reference's hbdiaSpMV bit for bit:
+//  * DIA part: per row, offsets in ascending order, stored zeros and columns
+//    outside [0, numRows) skipped, sum = fma(v, x[col], sum) -- what nvcc
+//    makes of `sum += matrixValue * vectorValue` (src/Operations/HBDIASpMV.cu:42-71);
+//  * COO part: per row, entries in list order, c = c + v * x[col] with a
+//    separately rounded multiply and add -- the reference's host COO SpMV
+//    (src/Operations/HBDIASpMV.cpp:76-92) built without FMA contraction;
+//  * merge: y = dia + coo when the matrix has a COO remainder, else y = dia
+//    (src/Operations/HBDIASpMV.cu:77-88, src/Operations/HBDIASpMV.cpp:235-250).
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace hbdia {
+namespace dev {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+// Kernel arguments (device pointers into one plan allocation).
+template <typename VT, typename XT>
+struct SpmvArgs {
+    const VT *vals;          // DIA values [slots], [block][offsetIdx][lane]
+    const float *scale;      // per-block scale (bf16 storage) or nullptr
+    const int32_t *offs;     // kept offsets, ascending per block
+    const int32_t *blkOff;   // numBlocks + 1, offset units
+    const int32_t *cooRow;   // row-sorted COO remainder
+    const int32_t *cooCol;
+    const XT *cooVal;
+    const int32_t *cooRowPtr;  // numRows + 1 (row-per-thread kernel)
+    const int32_t *cooTile;    // numTiles + 1 (warp kernels): COO range of each 32-row tile
+    int32_t n;               // numRows
+    int32_t bw;              // blockWidth
+    int32_t numBlocks;       // DIA blocks
+    int32_t numTiles;        // ceil(n / 32)
+    int32_t hasCoo;          // COO remainder non-empty
+};
+
+__device__ __forceinline__ double fma_rn(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ float fma_rn(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+
+// Streaming loads of the value arrays (read once: evict-first, no L1 fill).
+__device__ __forceinline__ double ld_stream(const double *p) { return __ldcs(p); }
+__device__ __forceinline__ float ld_stream(const float *p) { return __ldcs(p); }
+__device__ __forceinline__ __nv_bfloat16 ld_stream(const __nv_bfloat16 *p) {
+    unsigned short r = __ldcs(reinterpret_cast<const unsigned short *>(p));
+    return __ushort_as_bfloat16(r);
+}
+
+// Stored value -> accumulation type.
+template <typename XT>
+__device__ __forceinline__ XT widen(double v, float) { return static_cast<XT>(v); }
+template <typename XT>
+__device__ __forceinline__ XT widen(float v, float) { return static_cast<XT>(v); }
+template <typename XT>
+__device__ __forceinline__ XT widen(__nv_bfloat16 v, float s) {
+    return static_cast<XT>(__bfloat162float(v)) * static_cast<XT>(s);
+}
+
+// ---------------------------------------------------------------------------
+// Row-per-thread kernel for any block width (the reference's thread mapping),
+// with the row's COO entries summed through the CSR row pointer.
+template <typename VT, typename XT>
+__global__ void __launch_bounds__(256)
+spmv_rowwise(const SpmvArgs<VT, XT> a, const XT *__restrict__ x, XT *__restrict__ y) {
+    const int64_t row = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (row >= a.n) return;
+    XT sum = XT(0);
+    const int32_t b = static_cast<int32_t>(row / a.bw);
+    const int32_t lane = static_cast<int32_t>(row - static_cast<int64_t>(b) * a.bw);
+    if (b < a.numBlocks) {
+        const int32_t k0 = __ldg(a.blkOff + b), k1 = __ldg(a.blkOff + b + 1);
+        const float s = a.scale ? __ldg(a.scale + b) : 1.0f;
+        for (int32_t k = k0; k < k1; ++k) {
+            const XT v = widen<XT>(ld_stream(a.vals + static_cast<int64_t>(k) * a.bw + lane), s);
+            if (v == XT(0)) continue;
+            const int64_t col = row + __ldg(a.offs + k);
+            if (col < 0 || col >= a.n) continue;
+            sum = fma_rn(v, __ldg(x + col), sum);
+        }
+    }
+    if (a.hasCoo) {
+        XT c = XT(0);
+        const int32_t e1 = __ldg(a.cooRowPtr + row + 1);
+        for (int32_t e = __ldg(a.cooRowPtr + row); e < e1; ++e)
+            c = add_rn(c, mul_rn(__ldg(a.cooVal + e), __ldg(x + __ldg(a.cooCol + e))));
+        sum = add_rn(sum, c);
+    }
+    y[row] = sum;
+}
+
+// ---------------------------------------------------------------------------
+// COO remainder of one 32-row tile, summed by the warp: entries are loaded
+// coalesced (32 per step), each lane forms one product, and the products are
+// handed to their row's lane by warp shuffles in list order, so every row's
+// sum keeps the sequential order of the reference.
+template <typename XT>
+__device__ __forceinline__ XT tile_coo(const int32_t *__restrict__ cooRow,
+                                       const int32_t *__restrict__ cooCol,
+                                       const XT *__restrict__ cooVal, int32_t e0, int32_t e1,
+                                       int64_t tileRow0, int lane, const XT *__restrict__ x) {
+    XT c = XT(0);
+    for (int32_t base = e0; base < e1; base += 32) {
+        const int32_t e = base + lane;
+        int lr = -1;
+        XT p = XT(0);
+        if (e < e1) {
+            lr = static_cast<int>(__ldg(cooRow + e) - tileRow0);
+            p = mul_rn(__ldg(cooVal + e), __ldg(x + __ldg(cooCol + e)));
+        }
+        const int m = min(32, e1 - base);
+        for (int t = 0; t < m; ++t) {
+            const int rt = __shfl_sync(kFull, lr, t);
+            const XT pt = __shfl_sync(kFull, p, t);
+            if (rt == lane) c = add_rn(c, pt);
+        }
+    }
+    return c;
+}
+
+// ---------------------------------------------------------------------------
+// blockWidth == 32: one warp per row block, lane = row within the block.
+// The block's offsets are fetched once (one coalesced load of up to 32) and
+// broadcast by shuffles; each offset's 32 values are one coalesced 256-byte
+// (fp64) load; U offsets are in flight per lane at a time; x is read through
+// L1, where the block's neighbouring diagonals (col, col+1, ...) and the
+// neighbouring blocks of the same CTA hit the same lines.
+template <typename VT, typename XT, int U>
+__global__ void __launch_bounds__(256)
+spmv_bw32(const SpmvArgs<VT, XT> a, const XT *__restrict__ x, XT *__restrict__ y) {
+    const int lane = threadIdx.x & 31;
+    const int32_t tile = static_cast<int32_t>((static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5);
+    if (tile >= a.numTiles) return;  // warp-uniform
+    const int64_t row0 = static_cast<int64_t>(tile) * 32;
+    const int64_t row = row0 + lane;
+    XT sum = XT(0);
+    if (tile < a.numBlocks) {
+        const int32_t k0 = __ldg(a.blkOff + tile), k1 = __ldg(a.blkOff + tile + 1);
+        const float s = a.scale ? __ldg(a.scale + tile) : 1.0f;
+        for (int32_t kb = k0; kb < k1; kb += 32) {
+            const int cnt = min(32, k1 - kb);
+            const int32_t myoff = lane < cnt ? __ldg(a.offs + kb + lane) : 0;
+            const VT *vp = a.vals + static_cast<int64_t>(kb) * 32 + lane;
+            for (int j = 0; j < cnt; j += U) {
+                VT v[U];
+                XT xv[U];
+                bool ok[U];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int jj = j + u;
+                    const int32_t off = __shfl_sync(kFull, myoff, jj & 31);
+                    const int64_t col = row + off;
+                    const bool act = jj < cnt;
+                    ok[u] = act && col >= 0 && col < a.n;
+                    v[u] = act ? ld_stream(vp + static_cast<int64_t>(jj) * 32) : VT(0);
+                    xv[u] = ok[u] ? __ldg(x + col) : XT(0);
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const XT vv = widen<XT>(v[u], s);
+                    if (ok[u] && vv != XT(0)) sum = fma_rn(vv, xv[u], sum);
+                }
+            }
+        }
+    }
+    if (a.hasCoo) {
+        const int32_t e0 = __ldg(a.cooTile + tile), e1 = __ldg(a.cooTile + tile + 1);
+        sum = add_rn(sum, tile_coo<XT>(a.cooRow, a.cooCol, a.cooVal, e0, e1, row0, lane, x));
+    }
+    if (row < a.n) __stcs(y + row, sum);
+}
+
+}  // namespace dev
+}  // namespace hbdia

@@ -1,0 +1,250 @@
+/*
+ * hbdia_b200 -- C ABI of the B200-native HBDIA SpMV library (libhbdia_b200.so).
+ *
+ * This is the drop-in boundary under the C++ API of include/hbdia/HBDIA.hpp,
+ * HBDIAVector.hpp and HBDIASpMV.hpp (HBDIA<T>, HBDIAVector<T>, hbdiaSpMV), which mirror the reference's
+ * classes.  Every entry point names the reference interface it replaces
+ * (paths relative to the reference project root).  The signatures use plain
+ * pointers and sizes only; CUDA streams are passed as `void*`
+ * (a cudaStream_t), NULL meaning the matrix's own stream.
+ *
+ * Conventions
+ *  - Every function returns an hbdia_status (0 = success).  No function exits
+ *    the process: the reference's CHECK_CUDA calls exit(1)
+ *    (include/types.hpp:37-44); here CUDA errors become HBDIA_ERR_CUDA and the
+ *    C++ layer throws.  hbdia_last_error() returns the calling thread's
+ *    message for the last failing call.
+ *  - Value type T is chosen per object with hbdia_dtype (double or float, the
+ *    two instantiations of hbdiaSpMV, src/Operations/HBDIASpMV.cpp:254-255).
+ *  - All SpMV entry points are asynchronous on their stream, as the
+ *    reference's hbdiaSpMV is (it returns without synchronizing,
+ *    src/Operations/HBDIASpMV.cpp:251); hbdia_spmv_host is the exception.
+ *  - A converted matrix is immutable until destroyed, so concurrent SpMVs on
+ *    different streams over the same matrix are allowed.
+ */
+#ifndef HBDIA_B200_H
+#define HBDIA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum hbdia_status {
+    HBDIA_OK = 0,
+    HBDIA_ERR_INVALID_ARGUMENT = -1, /* reference: std::invalid_argument      */
+    HBDIA_ERR_OUT_OF_RANGE = -2,     /* reference: std::out_of_range (indices) */
+    HBDIA_ERR_RUNTIME = -3,          /* reference: std::runtime_error          */
+    HBDIA_ERR_CUDA = -4,             /* a CUDA runtime call failed             */
+    HBDIA_ERR_NO_MEMORY = -5,        /* host or device allocation failed       */
+    HBDIA_ERR_NOT_CONVERTED = -6,    /* matrix has no HBDIA layout yet         */
+    HBDIA_ERR_UNSUPPORTED = -7       /* combination not implemented            */
+} hbdia_status;
+
+typedef enum hbdia_dtype { HBDIA_F64 = 0, HBDIA_F32 = 1 } hbdia_dtype;
+
+/* ExecutionMode (include/types.hpp:7-10).  Kept for source compatibility:
+ * the COO remainder always runs on the GPU, fused into the SpMV launch. */
+typedef enum hbdia_exec_mode { HBDIA_CPU_COO = 0, HBDIA_GPU_COO = 1 } hbdia_exec_mode;
+
+/* Device storage of the blocked-DIA values.  NATIVE stores T.  F32 and
+ * BF16_SCALED store float / bfloat16 (with one float scale per block) for a
+ * double matrix; the SpMV then still accumulates in double. */
+typedef enum hbdia_value_storage {
+    HBDIA_STORE_NATIVE = 0,
+    HBDIA_STORE_F32 = 1,
+    HBDIA_STORE_BF16_SCALED = 2
+} hbdia_value_storage;
+
+typedef struct hbdia_matrix hbdia_matrix; /* HBDIA<T>       (include/Format/HBDIA.hpp:24-291)      */
+typedef struct hbdia_vector hbdia_vector; /* HBDIAVector<T> (include/Format/HBDIAVector.hpp:23-109) */
+
+const char *hbdia_last_error(void);
+const char *hbdia_version(void);
+
+/* The library carries its own (static) CUDA runtime, which shares the
+ * device's primary context with any other CUDA user in the process.  Its
+ * current device is per host thread and starts at 0: a process driving
+ * another GPU calls hbdia_set_device first (the reference relies on the
+ * caller's cudaSetDevice, src/DataExchange/MPICommunicator.cpp).  No
+ * counterpart is needed on one GPU. */
+int hbdia_set_device(int32_t device);
+int hbdia_get_device(int32_t *device);
+/* Status name, e.g. "HBDIA_ERR_RUNTIME". */
+const char *hbdia_status_string(int status);
+
+/* ---------------------------------------------------------------- matrices */
+
+/* HBDIA() (src/Format/HBDIA.cpp:20-21): empty matrix, to be filled by
+ * hbdia_matrix_stencil27 or hbdia_matrix_load_mtx. */
+int hbdia_matrix_create_empty(hbdia_dtype dtype, hbdia_matrix **out);
+
+/* HBDIA(rowIndices, colIndices, values, numRows, numCols)
+ * (src/Format/HBDIA.cpp:51-80): copies the COO triplets, validates sizes
+ * (HBDIA_ERR_INVALID_ARGUMENT) and index bounds (HBDIA_ERR_OUT_OF_RANGE).
+ * numRows <= 0 and numCols <= 0 together select the dimension-inferring
+ * constructor HBDIA(rowIndices, colIndices, values) (src/Format/HBDIA.cpp:23-49). */
+int hbdia_matrix_create(hbdia_dtype dtype, const int32_t *rowIndices, const int32_t *colIndices,
+                        const void *values, int64_t nnz, int32_t numRows, int32_t numCols,
+                        hbdia_matrix **out);
+
+void hbdia_matrix_destroy(hbdia_matrix *m); /* ~HBDIA (src/Format/HBDIA.cpp:156-159) */
+
+/* create3DStencil27Point(nx, ny, nz, noise, iteration)
+ * (src/Format/HBDIA.cpp:1416-1607): replaces the matrix's COO data with the
+ * reference's 27-point stencil; identical entries and order. */
+int hbdia_matrix_stencil27(hbdia_matrix *m, int32_t nx, int32_t ny, int32_t nz, double noise,
+                           int32_t iteration);
+
+/* loadMTX(filename) / loadMTX(filename, numRows, numCols)
+ * (src/Format/HBDIA.cpp:161-263 and :265-370).  numRows, numCols <= 0 select
+ * the first overload.  *ok receives the reference's boolean result. */
+int hbdia_matrix_load_mtx(hbdia_matrix *m, const char *path, int32_t numRows, int32_t numCols,
+                          int32_t *ok);
+
+/* convertToHBDIAFormat(blockWidth, threshold, max_coo_entries, COOisUnique,
+ * execMode) (src/Format/HBDIA.cpp:507-718).  The host layout is bit-exact with
+ * the reference's.  With upload != 0 it then builds the device layout
+ * (prepareForGPU, src/Format/HBDIA.cpp:720-816), as the reference does for
+ * every non-partial matrix; upload == 0 converts on the host only (no GPU
+ * needed).  Like the reference, it is a no-op on an already converted or
+ * empty matrix. */
+int hbdia_matrix_convert(hbdia_matrix *m, int32_t blockWidth, int32_t threshold,
+                         int64_t maxCooEntries, int32_t cooIsUnique, int32_t execMode,
+                         int32_t upload);
+
+/* prepareForGPU (src/Format/HBDIA.cpp:720-816): upload the layout, creating
+ * the matrix's stream.  storage selects the device value format. */
+int hbdia_matrix_prepare_gpu(hbdia_matrix *m, int32_t storage);
+
+/* Builds the device layout straight from COO with the GPU converter (same
+ * layout as hbdia_matrix_convert + prepare_gpu, but the host layout is not
+ * materialised).  Requires row-sorted COO; otherwise HBDIA_ERR_UNSUPPORTED. */
+int hbdia_matrix_convert_on_device(hbdia_matrix *m, int32_t blockWidth, int32_t threshold,
+                                   int64_t maxCooEntries, int32_t storage);
+
+typedef struct hbdia_matrix_info {
+    int32_t dtype;            /* hbdia_dtype                                    */
+    int32_t numRows;          /* getNumRows   (include/Format/HBDIA.hpp:74)     */
+    int32_t numCols;          /* getNumCols                                     */
+    int32_t hasCOO;           /* getHasCOO                                      */
+    int64_t numNonZeros;      /* getNumNonZeros                                 */
+    int32_t hasHBDIA;         /* getHasHBDIA                                    */
+    int32_t onDevice;         /* device layout present                          */
+    int32_t blockWidth;       /* getBlockWidth                                  */
+    int32_t threshold;        /* getThreshold                                   */
+    int64_t maxCooEntries;    /* getMaxCooEntries                               */
+    int32_t numBlocks;        /* getNumBlocks                                   */
+    int32_t numberDiagonals;  /* getNumberDiagonals                             */
+    int64_t totalOffsets;     /* sum of |getOffsetsPerBlock()[b]|               */
+    int64_t numSlots;         /* getHBDIAData().size()                          */
+    int64_t numCoo;           /* getCpuValues().size()                          */
+    int32_t histogramLength;  /* getHistogramBlocks().size()                    */
+    int32_t storage;          /* hbdia_value_storage on the device              */
+    int64_t deviceBytes;      /* bytes held on the device by the layout         */
+    int64_t bytesPerSpmv;     /* algorithmic HBM bytes of one SpMV              */
+} hbdia_matrix_info;
+
+int hbdia_matrix_get_info(const hbdia_matrix *m, hbdia_matrix_info *info);
+
+/* Copy out the host layout (getters, include/Format/HBDIA.hpp:88-114).
+ * offsetsPerBlock is returned flattened: offsets[blockStart[b] ..
+ * blockStart[b+1]) are block b's ascending offsets (the form of
+ * prepareForGPU, src/Format/HBDIA.cpp:733-760).  Any NULL pointer is skipped.
+ * Sizes come from hbdia_matrix_get_info (cooRowPtr has numRows+1 entries). */
+int hbdia_matrix_export_layout(const hbdia_matrix *m, int32_t *offsets, int32_t *blockStart,
+                               void *data, int32_t *cooRow, int32_t *cooCol, void *cooVal,
+                               int32_t *cooRowPtr, int32_t *histogramBlocks,
+                               int32_t *histogramNnz);
+
+/* getRowIndices / getColIndices / getValues (include/Format/HBDIA.hpp:82-84)
+ * and getNnzPerRow (numRows entries, filled by stencil27 only). */
+int hbdia_matrix_export_coo(const hbdia_matrix *m, int32_t *rowIndices, int32_t *colIndices,
+                            void *values);
+int hbdia_matrix_export_nnz_per_row(const hbdia_matrix *m, int32_t *nnzPerRow);
+
+/* getBDIAStream (include/Format/HBDIA.hpp:168): the stream the matrix's
+ * SpMVs run on (created by prepare_gpu). */
+int hbdia_matrix_stream(const hbdia_matrix *m, void **stream);
+
+/* ---------------------------------------------------------------- vectors */
+
+/* HBDIAVector(localData) (src/Format/HBDIAVector.cpp:17-23): device buffer
+ * holding n elements copied from host (hostData may be NULL: zeros).  On one
+ * GPU the halo parts are empty, so the data and local pointers coincide. */
+int hbdia_vector_create(hbdia_dtype dtype, const void *hostData, int64_t n, hbdia_vector **out);
+void hbdia_vector_destroy(hbdia_vector *v);
+/* getDeviceDataPtr / getDeviceLocalPtr (include/Format/HBDIAVector.hpp:48-50) */
+int hbdia_vector_device_ptr(const hbdia_vector *v, void **devicePtr);
+int hbdia_vector_size(const hbdia_vector *v, int64_t *n);
+/* blocking host<->device copies of the whole vector */
+int hbdia_vector_upload(hbdia_vector *v, const void *hostData);
+int hbdia_vector_download(const hbdia_vector *v, void *hostData);
+
+/* ---------------------------------------------------------------- SpMV */
+
+/* hbdiaSpMV(matrix, inputVector, outputVector, execCOOCPU, execCOOGPU)
+ * (src/Operations/HBDIASpMV.cpp:186-251; declared include/Operations/HBDIASpMV.hpp:8-10).
+ * y = A x in ONE fused launch (blocked-DIA part and COO remainder) on the
+ * matrix's stream; returns without synchronizing.  If the matrix has COO
+ * entries and both flags are 0 it fails with HBDIA_ERR_RUNTIME, as the
+ * reference throws std::runtime_error("Invalid COO execution flags")
+ * (src/Operations/HBDIASpMV.cpp:229-232).  Either flag selects the same fused
+ * GPU path.  Every row of y is written. */
+int hbdia_spmv(hbdia_matrix *m, const hbdia_vector *x, hbdia_vector *y, int32_t execCOOCPU,
+               int32_t execCOOGPU);
+
+/* Same product on caller-owned device buffers (numRows elements of T each)
+ * and the caller's stream (NULL: the matrix's stream).  No allocation, so it
+ * can be captured in a CUDA graph. */
+int hbdia_spmv_device(const hbdia_matrix *m, const void *x, void *y, void *stream);
+
+/* Multi-RHS product Y = A X for k right-hand sides.  X and Y are device
+ * buffers in row-major layout with leading dimensions ldx, ldy >= k
+ * (element (i, j) at i*ld + j).  Each value load is reused across all k. */
+int hbdia_spmm_device(const hbdia_matrix *m, const void *X, int64_t ldx, void *Y, int64_t ldy,
+                      int32_t k, void *stream);
+
+/* End-to-end form on HOST buffers: copies x to the device, runs the SpMV,
+ * copies y back and synchronizes.  Page-locked host buffers are fastest. */
+int hbdia_spmv_host(hbdia_matrix *m, const void *xHost, void *yHost);
+
+/* Blocks until the matrix's stream is idle. */
+int hbdia_matrix_synchronize(const hbdia_matrix *m);
+
+/* ---------------------------------------------------------------- workloads */
+
+/* Seeded synthetic 27-point stencil on an nx*ny*nz grid (Dirichlet boundary,
+ * index k*nx*ny + j*nx + i), centre value `center`, the 26 neighbours
+ * `neighbor`, plus floor(extraFraction * stencil_nnz) extra entries at
+ * uniformly drawn (row, col) positions outside the row's stencil pattern,
+ * without repeats, values uniform in [extraLo, extraHi).  Output is row-sorted;
+ * within a row the stencil entries come in ascending column order, then the
+ * row's extras in draw order.  Call once with rows == NULL to get *nnz, then
+ * again with arrays of that size. */
+int hbdia_generate_stencil27(int32_t nx, int32_t ny, int32_t nz, double center, double neighbor,
+                             double extraFraction, double extraLo, double extraHi, uint64_t seed,
+                             int64_t *nnz, int32_t *rows, int32_t *cols, double *values);
+
+/* Same for the 7-point stencil (faces only). */
+int hbdia_generate_stencil7(int32_t nx, int32_t ny, int32_t nz, double center, double neighbor,
+                            int64_t *nnz, int32_t *rows, int32_t *cols, double *values);
+
+/* Banded matrix of order n with the given diagonal offsets: off-diagonal
+ * values uniform in [lo, hi), each entry dropped with probability dropProb,
+ * centre = |row sum| + 1 when offset 0 is listed, plus floor(scatterFraction
+ * * band_nnz) scattered entries.  Row-sorted.  Two-call protocol as above. */
+int hbdia_generate_banded(int32_t n, const int32_t *offsets, int32_t numOffsets, double lo,
+                          double hi, double dropProb, double scatterFraction, uint64_t seed,
+                          int64_t *nnz, int32_t *rows, int32_t *cols, double *values);
+
+/* n doubles uniform in [lo, hi) from the library's seeded generator. */
+int hbdia_fill_uniform(double *out, int64_t n, double lo, double hi, uint64_t seed);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HBDIA_B200_H */

@@ -1,0 +1,285 @@
+/* Test infrastructure only -- the ORACLE.  A plain-C, single-threaded
+ * restatement of the reference's HBDIA conversion and SpMV, written for
+ * clarity rather than speed.  tests/, __graft_entry__.smoke() and bench.py's
+ * CPU baseline load it as the checker; the product (hbdia_b200) never does.
+ *
+ * Every function cites the reference code it restates (paths relative to the
+ * reference project root).
+ */
+#include "hbdia_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+struct orc_layout {
+    int32_t numRows, numCols, bw, threshold;
+    int64_t maxCoo;
+    int is_f32;
+    int has_hbdia;
+    int32_t numBlocks;       /* maxNumBlocks */
+    int64_t totalOffsets;
+    int64_t slots;
+    int32_t *offsets;        /* kept offsets, ascending per block, flattened */
+    int32_t *blockStart;     /* numBlocks+1 prefix in offset units */
+    void *data;              /* slots values, [block][offsetIdx][lane] */
+    int64_t nCoo;
+    int32_t *cooRow, *cooCol;
+    void *cooVal;
+    int32_t *cooRowPtr;      /* numRows+1 */
+    int32_t numberDiagonals;
+    int32_t histLen;
+    int32_t *histBlocks, *histNnz;
+};
+
+static int cmp_i32(const void *a, const void *b) {
+    int32_t x = *(const int32_t *)a, y = *(const int32_t *)b;
+    return (x > y) - (x < y);
+}
+
+/* Binary search in an ascending, duplicate-free list; -1 when absent.  The
+ * reference uses std::find over the same list (src/Format/HBDIA.cpp:662),
+ * which returns the same index because the list is unique. */
+static int64_t find_offset(const int32_t *list, int64_t n, int32_t key) {
+    int64_t lo = 0, hi = n;
+    while (lo < hi) {
+        int64_t mid = lo + (hi - lo) / 2;
+        if (list[mid] < key) lo = mid + 1; else hi = mid;
+    }
+    return (lo < n && list[lo] == key) ? lo : -1;
+}
+
+int orc_convert(const int32_t *rows, const int32_t *cols, const void *vals, int is_f32,
+                int64_t nnz, int32_t numRows, int32_t numCols, int32_t bw, int32_t threshold,
+                int64_t maxCoo, orc_layout **out) {
+    if (!out || bw <= 0 || numRows <= 0 || numCols <= 0 || nnz < 0) return -1;
+    orc_layout *h = (orc_layout *)calloc(1, sizeof(orc_layout));
+    if (!h) return -1;
+    const size_t esz = is_f32 ? sizeof(float) : sizeof(double);
+    h->numRows = numRows; h->numCols = numCols; h->bw = bw; h->threshold = threshold;
+    h->maxCoo = maxCoo; h->is_f32 = is_f32;
+    *out = h;
+    /* Empty matrix: the reference returns without converting
+     * (src/Format/HBDIA.cpp:521-524). */
+    if (nnz == 0) return 0;
+
+    /* Step 2: maxNumBlocks = ceil(min(numRows, numCols) / bw)  (HBDIA.cpp:537) */
+    const int32_t nb = (int32_t)(((int64_t)(numRows < numCols ? numRows : numCols) + bw - 1) / bw);
+    h->numBlocks = nb;
+
+    /* Step 3: per-block offset counts (HBDIA.cpp:540-560).  Entries are
+     * bucketed by block (stable), then each bucket's offsets are sorted and
+     * run-length counted; this yields the same ascending (offset, count)
+     * sequence as iterating the reference's std::map<int,int>. */
+    int64_t *bcount = (int64_t *)calloc((size_t)nb + 1, sizeof(int64_t));
+    for (int64_t i = 0; i < nnz; ++i) {
+        int32_t b = rows[i] / bw;
+        if (b < nb) bcount[b + 1]++;
+    }
+    for (int32_t b = 0; b < nb; ++b) bcount[b + 1] += bcount[b];
+    int32_t *boffs = (int32_t *)malloc(sizeof(int32_t) * (size_t)(bcount[nb] > 0 ? bcount[nb] : 1));
+    int64_t *fillp = (int64_t *)malloc(sizeof(int64_t) * (size_t)(nb > 0 ? nb : 1));
+    for (int32_t b = 0; b < nb; ++b) fillp[b] = bcount[b];
+    for (int64_t i = 0; i < nnz; ++i) {
+        int32_t b = rows[i] / bw;
+        if (b < nb) boffs[fillp[b]++] = cols[i] - rows[i];
+    }
+    free(fillp);
+    /* distinct (offset,count) per block, in place: uniq[] holds offsets,
+     * ucnt[] counts; ustart[b]..ustart[b+1] the block's run */
+    int64_t *ustart = (int64_t *)calloc((size_t)nb + 1, sizeof(int64_t));
+    int64_t *ucnt = (int64_t *)malloc(sizeof(int64_t) * (size_t)(bcount[nb] > 0 ? bcount[nb] : 1));
+    int32_t *uniq = (int32_t *)malloc(sizeof(int32_t) * (size_t)(bcount[nb] > 0 ? bcount[nb] : 1));
+    int64_t nu = 0;
+    for (int32_t b = 0; b < nb; ++b) {
+        int64_t s = bcount[b], e = bcount[b + 1];
+        qsort(boffs + s, (size_t)(e - s), sizeof(int32_t), cmp_i32);
+        ustart[b] = nu;
+        for (int64_t i = s; i < e;) {
+            int64_t j = i;
+            while (j < e && boffs[j] == boffs[i]) ++j;
+            uniq[nu] = boffs[i];
+            ucnt[nu] = j - i;
+            ++nu;
+            i = j;
+        }
+    }
+    ustart[nb] = nu;
+
+    /* Step 4: filter, blocks in order, offsets ascending (HBDIA.cpp:567-586):
+     * keep if count >= threshold or the running COO count already reached
+     * max_coo_entries; otherwise the entries go to the COO remainder. */
+    char *keep = (char *)malloc((size_t)(nu > 0 ? nu : 1));
+    int64_t cpu_entries = 0;
+    int64_t kept = 0;
+    for (int32_t b = 0; b < nb; ++b) {
+        for (int64_t u = ustart[b]; u < ustart[b + 1]; ++u) {
+            if (ucnt[u] >= threshold || cpu_entries >= maxCoo) { keep[u] = 1; ++kept; }
+            else { keep[u] = 0; cpu_entries += ucnt[u]; }
+        }
+    }
+    /* numberDiagonals: distinct offsets over all blocks (HBDIA.cpp:563,585) */
+    {
+        int32_t *all = (int32_t *)malloc(sizeof(int32_t) * (size_t)(nu > 0 ? nu : 1));
+        memcpy(all, uniq, sizeof(int32_t) * (size_t)nu);
+        qsort(all, (size_t)nu, sizeof(int32_t), cmp_i32);
+        int32_t nd = 0;
+        for (int64_t i = 0; i < nu; ++i) if (i == 0 || all[i] != all[i - 1]) ++nd;
+        h->numberDiagonals = nd;
+        free(all);
+    }
+
+    /* Step 5: storage (HBDIA.cpp:589-614) */
+    h->totalOffsets = kept;
+    h->slots = kept * bw;
+    if ((double)h->slots > 1e11) {
+        free(bcount); free(boffs); free(ustart); free(ucnt); free(uniq); free(keep);
+        return -2;
+    }
+    h->offsets = (int32_t *)malloc(sizeof(int32_t) * (size_t)(kept > 0 ? kept : 1));
+    h->blockStart = (int32_t *)malloc(sizeof(int32_t) * ((size_t)nb + 1));
+    {
+        int64_t p = 0;
+        for (int32_t b = 0; b < nb; ++b) {
+            h->blockStart[b] = (int32_t)p;
+            for (int64_t u = ustart[b]; u < ustart[b + 1]; ++u)
+                if (keep[u]) h->offsets[p++] = uniq[u];
+        }
+        h->blockStart[nb] = (int32_t)p;
+    }
+    /* Step 6: zero fill (HBDIA.cpp:617) */
+    h->data = calloc((size_t)(h->slots > 0 ? h->slots : 1), esz);
+
+    /* histograms (HBDIA.cpp:619-631) */
+    int32_t maxd = 0;
+    for (int32_t b = 0; b < nb; ++b) {
+        int32_t k = h->blockStart[b + 1] - h->blockStart[b];
+        if (k > maxd) maxd = k;
+    }
+    h->histLen = maxd + 1;
+    h->histBlocks = (int32_t *)calloc((size_t)h->histLen, sizeof(int32_t));
+    h->histNnz = (int32_t *)calloc((size_t)h->histLen, sizeof(int32_t));
+    for (int32_t b = 0; b < nb; ++b) h->histBlocks[h->blockStart[b + 1] - h->blockStart[b]]++;
+
+    /* Step 7: fill pass in input order (HBDIA.cpp:634-703).  A kept
+     * (block, offset) slot is ASSIGNED, so duplicates are last-wins; every
+     * other entry is appended to the COO remainder in input order and the
+     * CSR row pointer is built assuming rows arrive non-decreasing. */
+    h->cooRow = (int32_t *)malloc(sizeof(int32_t) * (size_t)(nnz > 0 ? nnz : 1));
+    h->cooCol = (int32_t *)malloc(sizeof(int32_t) * (size_t)(nnz > 0 ? nnz : 1));
+    h->cooVal = malloc(esz * (size_t)(nnz > 0 ? nnz : 1));
+    h->cooRowPtr = (int32_t *)calloc((size_t)numRows + 1, sizeof(int32_t));
+    int32_t currentRow = -1;
+    int64_t nextOffset = 0;
+    for (int64_t i = 0; i < nnz; ++i) {
+        const int32_t r = rows[i], c = cols[i];
+        const int32_t b = r / bw, off = c - r, lane = r % bw;
+        int64_t idx = -1;
+        if (b < nb && h->blockStart[b + 1] > h->blockStart[b])
+            idx = find_offset(h->offsets + h->blockStart[b],
+                              h->blockStart[b + 1] - h->blockStart[b], off);
+        if (idx >= 0) {
+            int64_t slot = ((int64_t)h->blockStart[b] + idx) * bw + lane;
+            memcpy((char *)h->data + slot * esz, (const char *)vals + i * esz, esz);
+            h->histNnz[h->blockStart[b + 1] - h->blockStart[b]]++;
+        } else {
+            if (r != currentRow) {
+                for (int32_t q = currentRow + 1; q <= r; ++q) h->cooRowPtr[q] = (int32_t)nextOffset;
+                currentRow = r;
+            }
+            h->cooRow[nextOffset] = r;
+            h->cooCol[nextOffset] = c;
+            memcpy((char *)h->cooVal + nextOffset * esz, (const char *)vals + i * esz, esz);
+            ++nextOffset;
+        }
+    }
+    for (int32_t q = currentRow + 1; q <= numRows; ++q) h->cooRowPtr[q] = (int32_t)nextOffset;
+    h->nCoo = nextOffset;
+    h->has_hbdia = 1;
+
+    free(bcount); free(boffs); free(ustart); free(ucnt); free(uniq); free(keep);
+    return 0;
+}
+
+void orc_sizes(const orc_layout *h, int64_t *s) {
+    s[0] = h->numBlocks; s[1] = h->totalOffsets; s[2] = h->slots; s[3] = h->nCoo;
+    s[4] = h->numberDiagonals; s[5] = h->histLen; s[6] = h->has_hbdia;
+    s[7] = h->numRows; s[8] = h->numCols; s[9] = h->has_hbdia ? (int64_t)h->numRows + 1 : 0;
+}
+
+void orc_export(const orc_layout *h, int32_t *offsets, int32_t *blockStart, void *data,
+                int32_t *cooRow, int32_t *cooCol, void *cooVal, int32_t *cooRowPtr,
+                int32_t *histBlocks, int32_t *histNnz) {
+    if (!h->has_hbdia) return;
+    const size_t esz = h->is_f32 ? sizeof(float) : sizeof(double);
+    memcpy(offsets, h->offsets, sizeof(int32_t) * (size_t)h->totalOffsets);
+    memcpy(blockStart, h->blockStart, sizeof(int32_t) * ((size_t)h->numBlocks + 1));
+    memcpy(data, h->data, esz * (size_t)h->slots);
+    memcpy(cooRow, h->cooRow, sizeof(int32_t) * (size_t)h->nCoo);
+    memcpy(cooCol, h->cooCol, sizeof(int32_t) * (size_t)h->nCoo);
+    memcpy(cooVal, h->cooVal, esz * (size_t)h->nCoo);
+    memcpy(cooRowPtr, h->cooRowPtr, sizeof(int32_t) * ((size_t)h->numRows + 1));
+    memcpy(histBlocks, h->histBlocks, sizeof(int32_t) * (size_t)h->histLen);
+    memcpy(histNnz, h->histNnz, sizeof(int32_t) * (size_t)h->histLen);
+}
+
+void orc_destroy(orc_layout *h) {
+    if (!h) return;
+    free(h->offsets); free(h->blockStart); free(h->data);
+    free(h->cooRow); free(h->cooCol); free(h->cooVal); free(h->cooRowPtr);
+    free(h->histBlocks); free(h->histNnz);
+    free(h);
+}
+
+/* Per-row COO sums in list order.  For row-sorted COO this is exactly what
+ * cpu_coo_spmv_kernel computes (src/Operations/HBDIASpMV.cpp:76-92): start at
+ * zero, `row_sum += val * x[col]` with a separate multiply and add. */
+#define ORC_SPMV_BODY(T, FMA)                                                             \
+    const int32_t n = h->numRows, bw = h->bw;                                             \
+    const T *data = (const T *)h->data;                                                   \
+    const T *cv = (const T *)h->cooVal;                                                   \
+    T *coo = (T *)calloc((size_t)n + 1, sizeof(T));                                       \
+    for (int64_t e = 0; e < h->nCoo; ++e) {                                               \
+        T p = cv[e] * x[h->cooCol[e]];                                                    \
+        coo[h->cooRow[e]] = coo[h->cooRow[e]] + p;                                        \
+    }                                                                                     \
+    for (int32_t row = 0; row < n; ++row) {                                               \
+        /* src/Operations/HBDIASpMV.cu:22-71: ascending offsets, skip stored zeros and  \
+         * columns outside [0, numRows), fused multiply-add (nvcc contracts          \
+         * `sum += v * x`). */                                                        \
+        T sum = (T)0;                                                                     \
+        const int32_t b = row / bw, lane = row % bw;                                      \
+        if (h->has_hbdia && b < h->numBlocks) {                                           \
+            for (int32_t k = h->blockStart[b]; k < h->blockStart[b + 1]; ++k) {           \
+                T v = data[(int64_t)k * bw + lane];                                       \
+                if (v == (T)0) continue;                                                  \
+                int64_t col = (int64_t)row + h->offsets[k];                               \
+                if (col < 0 || col >= n) continue;                                        \
+                sum = FMA(v, x[col], sum);                                                \
+            }                                                                             \
+        }                                                                                 \
+        /* merge, src/Operations/HBDIASpMV.cu:77-88 (only when COO work exists,     \
+         * src/Operations/HBDIASpMV.cpp:235-250) */                                    \
+        y[row] = (h->nCoo > 0) ? (T)(sum + coo[row]) : sum;                               \
+    }                                                                                     \
+    free(coo);
+
+void orc_spmv_f64(const orc_layout *h, const double *x, double *y) { ORC_SPMV_BODY(double, fma) }
+void orc_spmv_f32(const orc_layout *h, const float *x, float *y) { ORC_SPMV_BODY(float, fmaf) }
+
+void orc_coo_spmv_f64(const int32_t *rows, const int32_t *cols, const double *vals,
+                      int64_t nnz, const double *x, int32_t numRows, double *y) {
+    /* single-thread instance of src/Operations/HBDIASpMV.cpp:36-99 */
+    double row_sum = 0.0;
+    int32_t current = -1;
+    for (int64_t i = 0; i < nnz; ++i) {
+        const int32_t r = rows[i];
+        if (r != current) {
+            if (current >= 0 && current < numRows) y[current] = row_sum;
+            current = r;
+            row_sum = 0.0;
+        }
+        row_sum += vals[i] * x[cols[i]];
+    }
+    if (current >= 0 && current < numRows) y[current] = row_sum;
+}
