@@ -43,6 +43,8 @@ WORKLOAD = dict(nx=256, ny=256, nz=256, center=26.0, neighbor=-1.0, extra_fracti
                 extra_lo=0.1, extra_hi=1.0, extra_seed=1, x_seed=1, block_width=32, threshold=2)
 METRIC = "SpMV HBM GB/s"
 UNIT = "GB/s"
+KERNEL_NAMES = {1: "spmv_rowwise<double,double>", 2: "spmv_bw32<double,double>",
+                3: "spmv_bw32_tma<double,double> (TMA-staged)"}
 
 
 def log(*a):
@@ -262,6 +264,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--cpu-budget", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--kernel", default=None, choices=["staged", "warp", "rowwise"],
+                    help="force one SpMV kernel (default: the library's choice)")
     ap.add_argument("--size", type=int, default=256,
                     help="grid edge of the stencil workload (256 is the benchmark; smaller sizes for profiling)")
     args = ap.parse_args()
@@ -290,9 +294,14 @@ def main():
     info = m.info()
     bytes_per_spmv = hbm_bytes_model(info)
     assert bytes_per_spmv == info.bytesPerSpmv, (bytes_per_spmv, info.bytesPerSpmv)
+    if args.kernel:
+        m.setKernel({"staged": hb.KERNEL_STAGED, "warp": hb.KERNEL_WARP, "rowwise": hb.KERNEL_ROWWISE}[args.kernel])
     xt = torch.from_numpy(x).cuda()
+    kernel_used = m.selectedKernel(xt.data_ptr())
     yt = torch.zeros(n, dtype=torch.float64, device="cuda")
-    stream = torch.cuda.current_stream()
+    # a dedicated stream: the kernels and every timing event live on it
+    stream = torch.cuda.Stream()
+    torch.cuda.synchronize()
     sp = stream.cuda_stream
 
     for _ in range(args.warmup):
@@ -318,6 +327,7 @@ def main():
         dist.barrier()
     total_ms = t_all0.elapsed_time(t_all1)
     launch_ms = [a.elapsed_time(b) for a, b in evs]
+    m.synchronize()  # raises if a bounded device-side wait ran out
     if dist:
         tt = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
@@ -363,7 +373,7 @@ def main():
             "config": dict(workload_config(), parallelism=f"replicas{world}"),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": profiled_traffic(), "peak_source": peak_kind,
-                         "kernel": "spmv_bw32<double,double>", "bytes_per_launch": bytes_per_spmv,
+                         "kernel": KERNEL_NAMES[kernel_used], "bytes_per_launch": bytes_per_spmv,
                          "avg_launch_ms": avg_launch_ms},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n,
                     "steps": args.e2e_steps, "ms_per_step": e2e_ms / args.e2e_steps, "matches_device": ok},

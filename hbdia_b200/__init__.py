@@ -18,7 +18,8 @@ from typing import List, Optional, Sequence
 import numpy as np
 
 from . import _lib
-from ._lib import (HBDIACudaError, STORE_BF16_SCALED, STORE_F32, STORE_NATIVE, MatrixInfo,
+from ._lib import (KERNEL_AUTO, KERNEL_ROWWISE, KERNEL_STAGED, KERNEL_WARP, HBDIACudaError,
+                   HBDIADeviceTimeout, STORE_BF16_SCALED, STORE_F32, STORE_NATIVE, MatrixInfo,
                    check as _check, load as _load)
 
 __all__ = ["ExecutionMode", "HBDIA", "HBDIAVector", "hbdiaSpMV", "spmv_device", "spmm_device",
@@ -201,7 +202,30 @@ class HBDIA:
         return self.info().bytesPerSpmv
 
     def synchronize(self) -> None:
+        """Wait for the matrix's stream; raises HBDIADeviceTimeout when a
+        bounded device-side wait ran out since the last check."""
         _check(_load().hbdia_matrix_synchronize(self._h))
+
+    def deviceStatus(self) -> int:
+        b = ctypes.c_int32(0)
+        _check(_load().hbdia_matrix_device_status(self._h, ctypes.byref(b)))
+        return b.value
+
+    def setKernel(self, kernel: int) -> None:
+        """KERNEL_AUTO / KERNEL_ROWWISE / KERNEL_WARP / KERNEL_STAGED."""
+        _check(_load().hbdia_matrix_set_kernel(self._h, int(kernel)))
+
+    def selectedKernel(self, x_ptr: int) -> int:
+        k = ctypes.c_int32(0)
+        _check(_load().hbdia_matrix_selected_kernel(self._h, ctypes.c_void_p(x_ptr), ctypes.byref(k)))
+        return k.value
+
+    def setWaitTimeout(self, nanoseconds: int) -> None:
+        _check(_load().hbdia_matrix_set_wait_timeout(self._h, int(nanoseconds)))
+
+    def testSkipChunk(self, chunk: int) -> None:
+        """Test hook: the staged kernel never publishes `chunk` (-1: off)."""
+        _check(_load().hbdia_matrix_test_skip_chunk(self._h, int(chunk)))
 
 
 class HBDIAVector:
@@ -261,17 +285,31 @@ def hbdiaSpMV(matrix: HBDIA, inputVector: HBDIAVector, outputVector: HBDIAVector
     return True
 
 
-def spmv_device(matrix: HBDIA, x_ptr: int, y_ptr: int, stream: int = 0) -> None:
+_CUDA_STREAM_LEGACY = 1  # cudaStreamLegacy: the handle value 0 means the legacy default stream
+
+
+def _stream_arg(stream: Optional[int]) -> ctypes.c_void_p:
+    """None -> the matrix's own stream (NULL at the ABI); an int is a
+    cudaStream_t handle, where 0 (e.g. torch's default stream) is the legacy
+    default stream."""
+    if stream is None:
+        return ctypes.c_void_p(None)
+    return ctypes.c_void_p(int(stream) or _CUDA_STREAM_LEGACY)
+
+
+def spmv_device(matrix: HBDIA, x_ptr: int, y_ptr: int, stream: Optional[int] = None) -> None:
     """y = A x on raw device pointers (e.g. torch tensors' data_ptr()) on
-    ``stream`` (0: the matrix's stream)."""
+    ``stream`` (None: the matrix's stream; torch's ``cuda_stream`` values,
+    0 included, are passed as they are)."""
     _check(_load().hbdia_spmv_device(matrix.handle, ctypes.c_void_p(x_ptr), ctypes.c_void_p(y_ptr),
-                                     ctypes.c_void_p(stream or None)))
+                                     _stream_arg(stream)))
 
 
-def spmm_device(matrix: HBDIA, X_ptr: int, ldx: int, Y_ptr: int, ldy: int, k: int, stream: int = 0) -> None:
+def spmm_device(matrix: HBDIA, X_ptr: int, ldx: int, Y_ptr: int, ldy: int, k: int,
+                stream: Optional[int] = None) -> None:
     """Y = A X for k row-major right-hand sides on raw device pointers."""
     _check(_load().hbdia_spmm_device(matrix.handle, ctypes.c_void_p(X_ptr), ldx, ctypes.c_void_p(Y_ptr), ldy,
-                                     k, ctypes.c_void_p(stream or None)))
+                                     k, _stream_arg(stream)))
 
 
 def spmv_host(matrix: HBDIA, x: np.ndarray, y: np.ndarray) -> None:

@@ -24,6 +24,9 @@ HBDIA_ERR_CUDA = -4
 HBDIA_ERR_NO_MEMORY = -5
 HBDIA_ERR_NOT_CONVERTED = -6
 HBDIA_ERR_UNSUPPORTED = -7
+HBDIA_ERR_DEVICE_TIMEOUT = -8
+
+KERNEL_AUTO, KERNEL_ROWWISE, KERNEL_WARP, KERNEL_STAGED = 0, 1, 2, 3
 
 HBDIA_F64, HBDIA_F32 = 0, 1
 STORE_NATIVE, STORE_F32, STORE_BF16_SCALED = 0, 1, 2
@@ -44,6 +47,10 @@ class HBDIACudaError(RuntimeError):
     """A CUDA runtime call inside the library failed."""
 
 
+class HBDIADeviceTimeout(RuntimeError):
+    """A bounded wait inside an SpMV kernel ran out; that result is invalid."""
+
+
 _EXC = {
     HBDIA_ERR_INVALID_ARGUMENT: ValueError,
     HBDIA_ERR_OUT_OF_RANGE: IndexError,
@@ -52,6 +59,7 @@ _EXC = {
     HBDIA_ERR_NO_MEMORY: MemoryError,
     HBDIA_ERR_NOT_CONVERTED: RuntimeError,
     HBDIA_ERR_UNSUPPORTED: NotImplementedError,
+    HBDIA_ERR_DEVICE_TIMEOUT: HBDIADeviceTimeout,
 }
 
 # (name, restype, argtypes)
@@ -75,6 +83,11 @@ _SIGS = [
     ("hbdia_matrix_export_nnz_per_row", ctypes.c_int, [c_vp, c_vp]),
     ("hbdia_matrix_stream", ctypes.c_int, [c_vp, c_vpp]),
     ("hbdia_matrix_synchronize", ctypes.c_int, [c_vp]),
+    ("hbdia_matrix_device_status", ctypes.c_int, [c_vp, c_i32p]),
+    ("hbdia_matrix_set_kernel", ctypes.c_int, [c_vp, c_i32]),
+    ("hbdia_matrix_selected_kernel", ctypes.c_int, [c_vp, c_vp, c_i32p]),
+    ("hbdia_matrix_set_wait_timeout", ctypes.c_int, [c_vp, c_u64]),
+    ("hbdia_matrix_test_skip_chunk", ctypes.c_int, [c_vp, c_i32]),
     ("hbdia_vector_create", ctypes.c_int, [ctypes.c_int, c_vp, c_i64, c_vpp]),
     ("hbdia_vector_destroy", None, [c_vp]),
     ("hbdia_vector_device_ptr", ctypes.c_int, [c_vp, c_vpp]),

@@ -26,8 +26,8 @@ NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 CU_SOURCES = ["plan.cu"]
-CPP_SOURCES = ["convert.cpp", "generate.cpp", "capi.cpp", "hbdia_cxx.cpp"]
-HEADERS = ["hbdia_internal.hpp", "spmv_kernels.cuh"]
+CPP_SOURCES = ["convert.cpp", "generate.cpp", "chunks.cpp", "capi.cpp", "hbdia_cxx.cpp"]
+HEADERS = ["hbdia_internal.hpp", "spmv_kernels.cuh", "spmv_tma.cuh", "chunks.hpp"]
 
 
 def _cxx() -> str:

@@ -162,6 +162,7 @@ const char *hbdia_status_string(int s) {
         case HBDIA_ERR_NO_MEMORY: return "HBDIA_ERR_NO_MEMORY";
         case HBDIA_ERR_NOT_CONVERTED: return "HBDIA_ERR_NOT_CONVERTED";
         case HBDIA_ERR_UNSUPPORTED: return "HBDIA_ERR_UNSUPPORTED";
+        case HBDIA_ERR_DEVICE_TIMEOUT: return "HBDIA_ERR_DEVICE_TIMEOUT";
         default: return "HBDIA_ERR_UNKNOWN";
     }
 }
@@ -351,12 +352,72 @@ int hbdia_matrix_stream(const hbdia_matrix *m, void **stream) {
     });
 }
 
+}  // extern "C"
+
+namespace {
+int32_t read_status(const hbdia_matrix *m, bool clear) {
+    int32_t bits = 0;
+    if (!m->plan.status) return 0;
+    hbdia::check_cuda(cudaStreamSynchronize(static_cast<cudaStream_t>(m->plan.stream)), "cudaStreamSynchronize");
+    hbdia::check_cuda(cudaMemcpy(&bits, m->plan.status, sizeof(bits), cudaMemcpyDeviceToHost), "cudaMemcpy(status)");
+    if (clear && bits) hbdia::check_cuda(cudaMemset(m->plan.status, 0, sizeof(bits)), "cudaMemset(status)");
+    return bits;
+}
+void throw_if_timeout(int32_t bits) {
+    if (bits)
+        throw Error(HBDIA_ERR_DEVICE_TIMEOUT, "a bounded wait in the SpMV kernel ran out (status bits " +
+                                                  std::to_string(bits) + "); the result is invalid");
+}
+}  // namespace
+
+extern "C" {
+
 int hbdia_matrix_synchronize(const hbdia_matrix *m) {
     return guarded([&] {
         need(m != nullptr, HBDIA_ERR_INVALID_ARGUMENT, "null matrix");
-        if (m->plan.stream)
+        if (m->plan.stream) {
             hbdia::check_cuda(cudaStreamSynchronize(static_cast<cudaStream_t>(m->plan.stream)),
                               "cudaStreamSynchronize");
+            throw_if_timeout(read_status(m, true));
+        }
+    });
+}
+
+int hbdia_matrix_device_status(const hbdia_matrix *m, int32_t *bits) {
+    return guarded([&] {
+        need(m && bits, HBDIA_ERR_INVALID_ARGUMENT, "null argument");
+        *bits = read_status(m, false);
+    });
+}
+
+int hbdia_matrix_set_kernel(hbdia_matrix *m, int32_t kernel) {
+    return guarded([&] {
+        need(m != nullptr, HBDIA_ERR_INVALID_ARGUMENT, "null matrix");
+        need(kernel >= HBDIA_KERNEL_AUTO && kernel <= HBDIA_KERNEL_STAGED, HBDIA_ERR_INVALID_ARGUMENT,
+             "unknown kernel");
+        m->plan.kernel = kernel;
+    });
+}
+
+int hbdia_matrix_selected_kernel(const hbdia_matrix *m, const void *x, int32_t *kernel) {
+    return guarded([&] {
+        need(m && kernel, HBDIA_ERR_INVALID_ARGUMENT, "null argument");
+        need(m->plan.base != nullptr, HBDIA_ERR_NOT_CONVERTED, "matrix has no device layout");
+        *kernel = hbdia::select_kernel(m->plan, x);
+    });
+}
+
+int hbdia_matrix_set_wait_timeout(hbdia_matrix *m, uint64_t ns) {
+    return guarded([&] {
+        need(m != nullptr && ns > 0, HBDIA_ERR_INVALID_ARGUMENT, "bad timeout");
+        m->plan.waitTimeoutNs = ns;
+    });
+}
+
+int hbdia_matrix_test_skip_chunk(hbdia_matrix *m, int32_t chunk) {
+    return guarded([&] {
+        need(m != nullptr && chunk >= -1, HBDIA_ERR_INVALID_ARGUMENT, "bad chunk");
+        m->plan.skipChunk = chunk;
     });
 }
 
@@ -477,6 +538,7 @@ int hbdia_spmv_host(hbdia_matrix *m, const void *xh, void *yh) {
         hbdia::launch_spmv(P, P.xScratch, P.yScratch, s);
         hbdia::check_cuda(cudaMemcpyAsync(yh, P.yScratch, yb, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync(y)");
         hbdia::check_cuda(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+        throw_if_timeout(read_status(m, true));
     });
 }
 

@@ -27,10 +27,14 @@ namespace hbdia {
 // (seed 42 + iteration, noise rows first, then per row column/value draws) and
 // its final std::sort of an index permutation by row (not stable, so the
 // same sort call is needed to get the same order of entries within a row).
-// Like the reference, the loop bounds use nz for the coordinate that is
-// checked against nx; the two only agree for cubic grids.
+// The reference loops the coordinate it multiplies by 1 up to nz and the one
+// it multiplies by nx*ny up to nx, so its indices stay inside the matrix only
+// when nx == nz (otherwise it writes past nnzPerRow); that case is rejected.
 template <typename T>
 void reference_stencil27(int nx, int ny, int nz, double noise, int iteration, Coo<T> &out) {
+    if (nx != nz)
+        throw Error(HBDIA_ERR_UNSUPPORTED,
+                    "create3DStencil27Point indexes outside the matrix unless nx == nz");
     const int total = nx * ny * nz;
     std::vector<int> &rows = out.rows;
     std::vector<int> &cols = out.cols;

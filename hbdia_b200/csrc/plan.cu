@@ -20,6 +20,7 @@
 
 #include "hbdia_internal.hpp"
 #include "spmv_kernels.cuh"
+#include "spmv_tma.cuh"
 
 namespace hbdia {
 
@@ -57,8 +58,11 @@ void free_plan(DevicePlan &P) {
 
 template <typename T>
 void build_plan(const HostLayout<T> &L, int storage, DevicePlan &P) {
-    free_plan(P);
     DevicePlan Q;
+    Q.kernel = P.kernel;  // settings survive a rebuild
+    Q.waitTimeoutNs = P.waitTimeoutNs;
+    Q.skipChunk = P.skipChunk;
+    free_plan(P);
     Q.dtype = std::is_same<T, float>::value ? HBDIA_F32 : HBDIA_F64;
     if (storage != HBDIA_STORE_NATIVE && Q.dtype != HBDIA_F64)
         throw Error(HBDIA_ERR_UNSUPPORTED, "reduced value storage needs a double matrix");
@@ -108,6 +112,16 @@ void build_plan(const HostLayout<T> &L, int storage, DevicePlan &P) {
     std::vector<int32_t> tile(static_cast<size_t>(Q.numTiles) + 1);
     for (int64_t t = 0; t <= Q.numTiles; ++t) tile[t] = crp[std::min<int64_t>(t * 32, Q.n)];
 
+    // chunk schedule of the staged kernel (blockWidth 32)
+    std::vector<int32_t> rec;
+    std::vector<XWindow> win;
+    if (Q.bw == 32) {
+        build_chunk_schedule(Q.n, Q.numBlocks, Q.numTiles, L.blockStart.data(), L.offsets.data(), tile.data(),
+                             dev::kVRows, dev::kXCap, static_cast<int>(sizeof(T)), rec, win);
+        Q.numChunks = static_cast<int32_t>(rec.size() / kRecInts);
+        Q.numWindows = static_cast<int64_t>(win.size());
+    }
+
     // host-side value conversion for reduced storage
     const size_t vsz = storage_bytes(storage, Q.dtype);
     std::vector<float> vf, sf;
@@ -149,6 +163,9 @@ void build_plan(const HostLayout<T> &L, int storage, DevicePlan &P) {
     const size_t oCV = carve(Q.nCoo * sizeof(T));
     const size_t oRP = carve((static_cast<size_t>(Q.n) + 1) * sizeof(int32_t));
     const size_t oTile = carve((static_cast<size_t>(Q.numTiles) + 1) * sizeof(int32_t));
+    const size_t oRec = carve(rec.size() * sizeof(int32_t));
+    const size_t oWin = carve(win.size() * sizeof(XWindow));
+    const size_t oStatus = carve(sizeof(int32_t));
     Q.bytes = off;
     check_cuda(cudaMalloc(&Q.base, Q.bytes), "cudaMalloc(matrix layout)");
     char *base = static_cast<char *>(Q.base);
@@ -162,6 +179,10 @@ void build_plan(const HostLayout<T> &L, int storage, DevicePlan &P) {
         Q.cooVal = base + oCV;
         Q.cooRowPtr = reinterpret_cast<int32_t *>(base + oRP);
         Q.cooTile = reinterpret_cast<int32_t *>(base + oTile);
+        Q.chunkRec = rec.empty() ? nullptr : reinterpret_cast<int32_t *>(base + oRec);
+        Q.windows = win.empty() ? nullptr : base + oWin;
+        Q.status = reinterpret_cast<int32_t *>(base + oStatus);
+        check_cuda(cudaMemset(Q.status, 0, sizeof(int32_t)), "cudaMemset(status)");
         auto up = [](void *dst, const void *src, size_t bytes) {
             if (bytes) check_cuda(cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice), "cudaMemcpy(layout)");
         };
@@ -174,6 +195,8 @@ void build_plan(const HostLayout<T> &L, int storage, DevicePlan &P) {
         up(Q.cooVal, cv, Q.nCoo * sizeof(T));
         up(Q.cooRowPtr, crp, (static_cast<size_t>(Q.n) + 1) * sizeof(int32_t));
         up(Q.cooTile, tile.data(), (static_cast<size_t>(Q.numTiles) + 1) * sizeof(int32_t));
+        if (Q.chunkRec) up(Q.chunkRec, rec.data(), rec.size() * sizeof(int32_t));
+        if (Q.windows) up(Q.windows, win.data(), win.size() * sizeof(XWindow));
         cudaStream_t s;
         check_cuda(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "cudaStreamCreate");
         Q.stream = s;
@@ -219,7 +242,30 @@ void launch_typed(const DevicePlan &P, const void *x, void *y, cudaStream_t s) {
     a.hasCoo = P.nCoo > 0;
     const XT *xp = static_cast<const XT *>(x);
     XT *yp = static_cast<XT *>(y);
-    if (P.bw == 32) {
+    const int32_t kern = select_kernel(P, x);
+    if (kern == HBDIA_KERNEL_STAGED) {
+        dev::TmaArgs<VT, XT> T;
+        T.a = a;
+        T.rec = P.chunkRec;
+        T.win = static_cast<const XWindow *>(P.windows);
+        T.numChunks = P.numChunks;
+        T.status = P.status;
+        T.timeoutNs = P.waitTimeoutNs;
+        T.skipChunk = P.skipChunk;
+        const size_t smem = sizeof(dev::TmaSmem<VT, XT>);
+        static bool configured = false;  // per template instance
+        if (!configured) {
+            check_cuda(cudaFuncSetAttribute(dev::spmv_bw32_tma<VT, XT, kUnroll>,
+                                            cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
+                       "cudaFuncSetAttribute(staged SpMV)");
+            configured = true;
+        }
+        int dev = 0, sms = 0;
+        check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
+        check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "cudaDeviceGetAttribute");
+        const unsigned grid = static_cast<unsigned>(std::min<int64_t>(sms, P.numChunks));
+        dev::spmv_bw32_tma<VT, XT, kUnroll><<<grid, dev::kTmaThreads, smem, s>>>(T, xp, yp);
+    } else if (kern == HBDIA_KERNEL_WARP) {
         const int64_t warpsPerCta = 8;
         const unsigned grid = static_cast<unsigned>((P.numTiles + warpsPerCta - 1) / warpsPerCta);
         dev::spmv_bw32<VT, XT, kUnroll><<<grid, 256, 0, s>>>(a, xp, yp);
@@ -231,6 +277,20 @@ void launch_typed(const DevicePlan &P, const void *x, void *y, cudaStream_t s) {
 }
 
 }  // namespace
+
+int32_t select_kernel(const DevicePlan &P, const void *x) {
+    const bool bw32 = P.bw == 32;
+    const bool aligned = (reinterpret_cast<uintptr_t>(x) & 15) == 0;
+    const bool stagedOk = bw32 && aligned && P.numChunks > 0;
+    switch (P.kernel) {
+        case HBDIA_KERNEL_ROWWISE: return HBDIA_KERNEL_ROWWISE;
+        case HBDIA_KERNEL_WARP: return bw32 ? HBDIA_KERNEL_WARP : HBDIA_KERNEL_ROWWISE;
+        case HBDIA_KERNEL_STAGED:
+        default:
+            if (stagedOk) return HBDIA_KERNEL_STAGED;
+            return bw32 ? HBDIA_KERNEL_WARP : HBDIA_KERNEL_ROWWISE;
+    }
+}
 
 void launch_spmv(const DevicePlan &P, const void *x, void *y, void *stream) {
     if (!P.base) throw Error(HBDIA_ERR_NOT_CONVERTED, "matrix has no device layout");

@@ -1,0 +1,424 @@
+// Staged HBDIA SpMV for blockWidth 32 on sm_100a: a persistent,
+// warp-specialised kernel.
+//
+// One CTA per SM walks the chunks (kTilesPerChunk consecutive 32-row tiles)
+// blockIdx.x, blockIdx.x + gridDim.x, ...  A producer warp fills a ring of
+// kStages shared-memory stages, one chunk per stage:
+//   * the chunk's values (one contiguous cp.async.bulk, L2 evict-first: they
+//     are read once), its offsets, its COO remainder (rows, values) and the x
+//     windows its diagonals read (one cp.async.bulk each, 16-byte aligned), all
+//     completing on the stage's "full" mbarrier through the transaction count;
+//   * the x values the COO entries gather, with per-lane cp.async copies that
+//     the same mbarrier tracks (cp.async.mbarrier.arrive.noinc).
+// The producer's own metadata (chunk records, window tables, COO columns) is
+// prefetched 2-4 chunks ahead with cp.async groups, so no producer step waits
+// on a global-memory round trip.
+// kTilesPerChunk consumer warps compute one tile each from the stage -- the
+// same arithmetic, in the same order, as the reference (see spmv_kernels.cuh)
+// -- and release the stage on its "empty" mbarrier.
+//
+// Chunks whose rows do not fit a stage, x ranges beyond a stage's capacity
+// and COO entries beyond its capacity are read straight from global memory.
+//
+// Every wait is bounded by a time limit; on expiry the kernel records an error
+// bit in *status, drains the copies it has in flight (again bounded) and
+// returns.
+#pragma once
+
+#include "chunks.hpp"
+#include "spmv_kernels.cuh"
+
+namespace hbdia {
+namespace dev {
+
+constexpr int kStages = 4;
+constexpr int kVRows = kTilesPerChunk * 32;  // stored offsets a stage holds
+constexpr int kXCap = 2048;                  // x elements a stage holds
+constexpr int kCCap = 128;                   // COO entries a stage holds
+constexpr int kRecRing = 5;                  // chunk records in flight (distance 4)
+constexpr int kMetaRing = 3;                 // window tables / COO columns in flight (distance 2)
+constexpr int kConsumerWarps = kTilesPerChunk;
+constexpr int kTmaThreads = (kConsumerWarps + 1) * 32;
+
+enum : int { kErrConsumerWait = 1, kErrProducerWait = 2, kErrDrain = 4 };
+
+// ---------------------------------------------------------------- PTX wrappers
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.release.cta.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_test(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.acquire.cta.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// Wait for the phase of parity `parity` to complete, for at most timeoutNs.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint64_t timeoutNs) {
+    if (mbar_test(bar, parity)) return true;
+    const uint64_t t0 = global_ns();
+    for (;;) {
+        if (mbar_test(bar, parity)) return true;
+        if (global_ns() - t0 > timeoutNs) return false;
+        __nanosleep(20);
+    }
+}
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ void bulk_g2s_hint(void *dst, const void *src, uint32_t bytes, uint64_t *bar,
+                                              uint64_t policy) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], "
+        "%4;" ::"r"(smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar)), "l"(policy)
+        : "memory");
+}
+__device__ __forceinline__ uint64_t l2_evict_first_policy() {
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+template <int B>
+__device__ __forceinline__ void cp_async(void *dst, const void *src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(smem_u32(dst)), "l"(src), "n"(B) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+__device__ __forceinline__ void cp_async_arrive_noinc(uint64_t *bar) {
+    asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// ---------------------------------------------------------------- layout
+template <typename VT, typename XT>
+struct __align__(16) Stage {
+    VT vals[kVRows * 32];
+    XT xs[kXCap];
+    XT cval[kCCap + 16 / sizeof(XT)];
+    XT xg[kCCap];
+    int32_t offs[kVRows + 8];
+    int32_t crow[kCCap + 8];
+    XWindow win[kMaxWindows];
+    int32_t hdr[kRecInts];
+};
+
+template <typename VT, typename XT>
+struct __align__(16) TmaSmem {
+    Stage<VT, XT> stage[kStages];
+    int32_t rec[kRecRing][kRecInts];
+    XWindow win[kMetaRing][kMaxWindows];
+    int32_t cols[kMetaRing][kCCap];
+    uint64_t full[kStages];
+    uint64_t empty[kStages];
+};
+
+template <typename VT, typename XT>
+struct TmaArgs {
+    SpmvArgs<VT, XT> a;
+    const int32_t *rec;     // chunk records, kRecInts per chunk
+    const XWindow *win;     // window lists
+    int32_t numChunks;
+    int32_t *status;        // error bits (0 = fine)
+    uint64_t timeoutNs;     // limit of every wait
+    int32_t skipChunk;      // test hook: the producer never publishes this chunk (-1: off)
+};
+
+// One tile straight from global memory (chunks that are not staged).
+template <typename VT, typename XT>
+__device__ __forceinline__ XT tile_direct(const SpmvArgs<VT, XT> &a, int32_t tile, int lane,
+                                          const XT *__restrict__ x) {
+    const int64_t row0 = static_cast<int64_t>(tile) * 32;
+    const int64_t row = row0 + lane;
+    XT sum = XT(0);
+    if (tile < a.numBlocks) {
+        const int32_t k0 = __ldg(a.blkOff + tile), k1 = __ldg(a.blkOff + tile + 1);
+        const float s = a.scale ? __ldg(a.scale + tile) : 1.0f;
+        for (int32_t k = k0; k < k1; ++k) {
+            const XT v = widen<XT>(ld_stream(a.vals + static_cast<int64_t>(k) * 32 + lane), s);
+            const int64_t col = row + __ldg(a.offs + k);
+            if (v != XT(0) && col >= 0 && col < a.n) sum = fma_rn(v, __ldg(x + col), sum);
+        }
+    }
+    if (a.hasCoo) {
+        const int32_t e0 = __ldg(a.cooTile + tile), e1 = __ldg(a.cooTile + tile + 1);
+        sum = add_rn(sum, tile_coo<XT>(a.cooRow, a.cooCol, a.cooVal, e0, e1, row0, lane, x));
+    }
+    return sum;
+}
+
+template <typename VT, typename XT, int U>
+__device__ __forceinline__ XT tile_staged(const SpmvArgs<VT, XT> &a, const Stage<VT, XT> &S, int w, int lane,
+                                          const XT *__restrict__ x) {
+    const int32_t *H = S.hdr;
+    const int32_t tile = H[kRecT0] + w;
+    const int64_t row0 = static_cast<int64_t>(tile) * 32;
+    const int64_t row = row0 + lane;
+    const int32_t k0c = H[kRecK0];
+    const int32_t kAl = k0c & ~3;
+    const int32_t kt0 = H[kRecTileK + w], kt1 = H[kRecTileK + w + 1];
+    const int32_t nWin = H[kRecNWin];
+    const float s = (a.scale && tile < a.numBlocks) ? __ldg(a.scale + tile) : 1.0f;
+    XT sum = XT(0);
+    for (int32_t kb = kt0; kb < kt1; kb += 32) {
+        const int cnt = min(32, kt1 - kb);
+        const int32_t offL = lane < cnt ? S.offs[kb + lane - kAl] : 0;
+        // x window of this lane's offset (windows are disjoint and sorted)
+        const int64_t target = max(row0 + offL, int64_t(0));
+        int lo = 0, hi = nWin;
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (S.win[mid].end <= target) lo = mid + 1;
+            else hi = mid;
+        }
+        int32_t dL = 0, aL = 0, eL = 0;  // staged range [aL, eL) at xs[dL + col]
+        if (lo < nWin && S.win[lo].pos >= 0) {
+            aL = S.win[lo].alignedStart;
+            eL = S.win[lo].stagedEnd;
+            dL = S.win[lo].pos - aL;
+        }
+        const VT *vrow = S.vals + static_cast<int64_t>(kb - k0c) * 32 + lane;
+        for (int j = 0; j < cnt; j += U) {
+            VT v[U];
+            XT xv[U];
+            bool ok[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int kk = j + u;
+                const int src = kk & 31;
+                const int32_t off = __shfl_sync(kFull, offL, src);
+                const int32_t d = __shfl_sync(kFull, dL, src);
+                const int32_t wa = __shfl_sync(kFull, aL, src);
+                const int32_t we = __shfl_sync(kFull, eL, src);
+                const bool act = kk < cnt;
+                const int64_t col = row + off;
+                ok[u] = act && col >= 0 && col < a.n;
+                v[u] = act ? vrow[kk * 32] : VT(0);
+                const bool st = col >= wa && col < we;
+                xv[u] = ok[u] ? (st ? S.xs[d + col] : __ldg(x + col)) : XT(0);
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const XT vv = widen<XT>(v[u], s);
+                if (ok[u] && vv != XT(0)) sum = fma_rn(vv, xv[u], sum);
+            }
+        }
+    }
+    if (a.hasCoo) {
+        const int32_t c0 = H[kRecC0], c1 = H[kRecC1];
+        const int32_t crAl = c0 & ~3;
+        const int32_t cvAl = c0 & ~(16 / static_cast<int>(sizeof(XT)) - 1);
+        const int32_t ncs = min(c1 - c0, kCCap);
+        const int32_t ct0 = H[kRecTileC + w], ct1 = H[kRecTileC + w + 1];
+        XT c = XT(0);
+        for (int32_t base = ct0; base < ct1; base += 32) {
+            const int32_t e = base + lane;
+            int lr = -1;
+            XT p = XT(0);
+            if (e < ct1) {
+                int32_t r;
+                XT v, xg;
+                if (e - c0 < ncs) {
+                    r = S.crow[e - crAl];
+                    v = S.cval[e - cvAl];
+                    xg = S.xg[e - c0];
+                } else {
+                    r = __ldg(a.cooRow + e);
+                    v = __ldg(a.cooVal + e);
+                    xg = __ldg(x + __ldg(a.cooCol + e));
+                }
+                lr = static_cast<int>(r - row0);
+                p = mul_rn(v, xg);
+            }
+            const int m = min(32, ct1 - base);
+            for (int t = 0; t < m; ++t) {
+                const int rt = __shfl_sync(kFull, lr, t);
+                const XT pt = __shfl_sync(kFull, p, t);
+                if (rt == lane) c = add_rn(c, pt);
+            }
+        }
+        sum = add_rn(sum, c);
+    }
+    return sum;
+}
+
+template <typename VT, typename XT, int U>
+__global__ void __launch_bounds__(kTmaThreads, 1)
+spmv_bw32_tma(const TmaArgs<VT, XT> T, const XT *__restrict__ x, XT *__restrict__ y) {
+    extern __shared__ __align__(128) unsigned char smemRaw[];
+    TmaSmem<VT, XT> &sm = *reinterpret_cast<TmaSmem<VT, XT> *>(smemRaw);
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const SpmvArgs<VT, XT> &a = T.a;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kStages; ++s) {
+            mbar_init(&sm.full[s], 1 + 32);            // producer arrive.expect_tx + 32 cp.async arrivals
+            mbar_init(&sm.empty[s], kConsumerWarps);   // one arrival per consumer warp
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    const int32_t G = gridDim.x;
+    const int32_t first = blockIdx.x;
+    // local step i handles chunk first + i * G
+    const int32_t nSteps = first < T.numChunks ? (T.numChunks - first + G - 1) / G : 0;
+
+    if (warp == kConsumerWarps) {
+        // ------------------------------------------------------------ producer
+        const uint64_t policy = l2_evict_first_policy();
+        auto chunkOf = [&](int32_t i) { return first + i * G; };
+        auto prefetchRec = [&](int32_t i) {
+            if (i < nSteps && lane < kRecInts / 4)
+                cp_async<16>(&sm.rec[i % kRecRing][lane * 4],
+                             T.rec + static_cast<int64_t>(chunkOf(i)) * kRecInts + lane * 4);
+        };
+        auto prefetchMeta = [&](int32_t i) {  // needs rec(i) complete
+            if (i >= nSteps) return;
+            const int32_t *R = sm.rec[i % kRecRing];
+            if (!(R[kRecFlags] & 1)) return;
+            const int32_t nWin = R[kRecNWin];
+            if (lane < nWin) cp_async<16>(&sm.win[i % kMetaRing][lane], T.win + R[kRecWin0] + lane);
+            const int32_t c0 = R[kRecC0];
+            const int32_t ncs = min(R[kRecC1] - c0, kCCap);
+            for (int32_t e = lane; e < ncs; e += 32) cp_async<4>(&sm.cols[i % kMetaRing][e], a.cooCol + c0 + e);
+        };
+        for (int32_t i = 0; i < 4; ++i) prefetchRec(i);
+        cp_async_commit();
+        cp_async_wait<0>();
+        __syncwarp();
+        prefetchMeta(0);
+        prefetchMeta(1);
+        cp_async_commit();
+        cp_async_wait<0>();
+        __syncwarp();
+        int32_t issued = 0;
+        bool failed = false;
+        for (int32_t i = 0; i < nSteps; ++i) {
+            cp_async_wait<1>();
+            __syncwarp();
+            const int slot = i % kStages;
+            const uint32_t use = static_cast<uint32_t>(i / kStages);
+            if (!mbar_wait(&sm.empty[slot], (use & 1u) ^ 1u, T.timeoutNs)) {
+                if (lane == 0) atomicOr(T.status, kErrProducerWait);
+                failed = true;
+                break;
+            }
+            Stage<VT, XT> &S = sm.stage[slot];
+            const int32_t *R = sm.rec[i % kRecRing];
+            const XWindow *W = sm.win[i % kMetaRing];
+            const int32_t *cols = sm.cols[i % kMetaRing];
+            const bool staged = R[kRecFlags] & 1;
+            const int32_t nWin = staged ? R[kRecNWin] : 0;
+            if (lane < kRecInts) S.hdr[lane] = R[lane];
+            if (lane < nWin) S.win[lane] = W[lane];
+            __syncwarp();
+            uint32_t bytes = 0;
+            int32_t k0 = 0, k1 = 0, kAl = 0, kEnd = 0, c0 = 0, ncs = 0, crAl = 0, crEnd = 0, cvAl = 0, cvEnd = 0;
+            if (staged) {
+                k0 = R[kRecK0];
+                k1 = R[kRecK1];
+                kAl = k0 & ~3;
+                kEnd = (k1 + 3) & ~3;
+                c0 = R[kRecC0];
+                ncs = min(R[kRecC1] - c0, kCCap);
+                constexpr int vAl = 16 / static_cast<int>(sizeof(XT));
+                crAl = c0 & ~3;
+                crEnd = (c0 + ncs + 3) & ~3;
+                cvAl = c0 & ~(vAl - 1);
+                cvEnd = (c0 + ncs + vAl - 1) & ~(vAl - 1);
+                if (ncs == 0) crEnd = crAl, cvEnd = cvAl;
+                if (k1 == k0) kEnd = kAl;
+                bytes = static_cast<uint32_t>(k1 - k0) * 32u * sizeof(VT) + static_cast<uint32_t>(kEnd - kAl) * 4u +
+                        static_cast<uint32_t>(crEnd - crAl) * 4u +
+                        static_cast<uint32_t>(cvEnd - cvAl) * sizeof(XT) + static_cast<uint32_t>(R[kRecXBytes]);
+            }
+            const bool skip = chunkOf(i) == T.skipChunk;
+            if (lane == 0 && !skip) mbar_arrive_expect_tx(&sm.full[slot], bytes);
+            __syncwarp();
+            if (staged && !skip) {
+                if (lane == 0 && k1 > k0)
+                    bulk_g2s_hint(S.vals, a.vals + static_cast<int64_t>(k0) * 32,
+                                  static_cast<uint32_t>(k1 - k0) * 32u * sizeof(VT), &sm.full[slot], policy);
+                if (lane == 1 && kEnd > kAl)
+                    bulk_g2s(S.offs, a.offs + kAl, static_cast<uint32_t>(kEnd - kAl) * 4u, &sm.full[slot]);
+                if (lane == 2 && crEnd > crAl)
+                    bulk_g2s(S.crow, a.cooRow + crAl, static_cast<uint32_t>(crEnd - crAl) * 4u, &sm.full[slot]);
+                if (lane == 3 && cvEnd > cvAl)
+                    bulk_g2s(S.cval, a.cooVal + cvAl, static_cast<uint32_t>(cvEnd - cvAl) * sizeof(XT),
+                             &sm.full[slot]);
+                if (lane < nWin) {
+                    const XWindow w = W[lane];
+                    if (w.pos >= 0 && w.stagedEnd > w.alignedStart)
+                        bulk_g2s(S.xs + w.pos, x + w.alignedStart,
+                                 static_cast<uint32_t>(w.stagedEnd - w.alignedStart) * sizeof(XT), &sm.full[slot]);
+                }
+                for (int32_t e = lane; e < ncs; e += 32) cp_async<sizeof(XT)>(&S.xg[e], x + cols[e]);
+            }
+            if (!skip) cp_async_arrive_noinc(&sm.full[slot]);
+            issued = i + 1;
+            prefetchMeta(i + 2);
+            prefetchRec(i + 4);
+            cp_async_commit();
+        }
+        // drain: every copy this warp started has landed before the CTA exits
+        cp_async_wait<0>();
+        __syncwarp();
+        for (int32_t j = max(0, issued - kStages); j < issued; ++j) {
+            if (chunkOf(j) == T.skipChunk) continue;
+            if (!mbar_wait(&sm.full[j % kStages], static_cast<uint32_t>(j / kStages) & 1u, T.timeoutNs)) {
+                if (lane == 0) atomicOr(T.status, kErrDrain);
+                break;
+            }
+        }
+        (void)failed;
+    } else {
+        // ------------------------------------------------------------ consumers
+        for (int32_t i = 0; i < nSteps; ++i) {
+            const int slot = i % kStages;
+            const uint32_t use = static_cast<uint32_t>(i / kStages);
+            if (!mbar_wait(&sm.full[slot], use & 1u, T.timeoutNs)) {
+                if (lane == 0) atomicOr(T.status, kErrConsumerWait);
+                break;
+            }
+            const Stage<VT, XT> &S = sm.stage[slot];
+            const int32_t tile = S.hdr[kRecT0] + warp;
+            if (tile < a.numTiles) {
+                const XT sum = (S.hdr[kRecFlags] & 1) ? tile_staged<VT, XT, U>(a, S, warp, lane, x)
+                                                      : tile_direct<VT, XT>(a, tile, lane, x);
+                const int64_t row = static_cast<int64_t>(tile) * 32 + lane;
+                if (row < a.n) __stcs(y + row, sum);
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&sm.empty[slot]);
+        }
+    }
+}
+
+}  // namespace dev
+}  // namespace hbdia

@@ -40,7 +40,8 @@ typedef enum hbdia_status {
     HBDIA_ERR_CUDA = -4,             /* a CUDA runtime call failed             */
     HBDIA_ERR_NO_MEMORY = -5,        /* host or device allocation failed       */
     HBDIA_ERR_NOT_CONVERTED = -6,    /* matrix has no HBDIA layout yet         */
-    HBDIA_ERR_UNSUPPORTED = -7       /* combination not implemented            */
+    HBDIA_ERR_UNSUPPORTED = -7,      /* combination not implemented            */
+    HBDIA_ERR_DEVICE_TIMEOUT = -8    /* a bounded device-side wait ran out     */
 } hbdia_status;
 
 typedef enum hbdia_dtype { HBDIA_F64 = 0, HBDIA_F32 = 1 } hbdia_dtype;
@@ -57,6 +58,15 @@ typedef enum hbdia_value_storage {
     HBDIA_STORE_F32 = 1,
     HBDIA_STORE_BF16_SCALED = 2
 } hbdia_value_storage;
+
+/* SpMV kernel choice (all give bit-identical y).  AUTO picks STAGED for
+ * blockWidth 32 with 16-byte aligned x, else ROWWISE. */
+typedef enum hbdia_kernel {
+    HBDIA_KERNEL_AUTO = 0,
+    HBDIA_KERNEL_ROWWISE = 1, /* one thread per row, any blockWidth             */
+    HBDIA_KERNEL_WARP = 2,    /* one warp per 32-row block, blockWidth 32       */
+    HBDIA_KERNEL_STAGED = 3   /* persistent TMA-staged pipeline, blockWidth 32  */
+} hbdia_kernel;
 
 typedef struct hbdia_matrix hbdia_matrix; /* HBDIA<T>       (include/Format/HBDIA.hpp:24-291)      */
 typedef struct hbdia_vector hbdia_vector; /* HBDIAVector<T> (include/Format/HBDIAVector.hpp:23-109) */
@@ -211,8 +221,26 @@ int hbdia_spmm_device(const hbdia_matrix *m, const void *X, int64_t ldx, void *Y
  * copies y back and synchronizes.  Page-locked host buffers are fastest. */
 int hbdia_spmv_host(hbdia_matrix *m, const void *xHost, void *yHost);
 
-/* Blocks until the matrix's stream is idle. */
+/* Blocks until the matrix's stream is idle, then reports (and clears) the
+ * device status: HBDIA_ERR_DEVICE_TIMEOUT when a bounded wait inside a
+ * kernel ran out since the last check (the affected y is invalid). */
 int hbdia_matrix_synchronize(const hbdia_matrix *m);
+
+/* Device status bits of the matrix's kernels (0: fine) without clearing. */
+int hbdia_matrix_device_status(const hbdia_matrix *m, int32_t *bits);
+
+/* Kernel choice for this matrix's SpMVs (hbdia_kernel). */
+int hbdia_matrix_set_kernel(hbdia_matrix *m, int32_t kernel);
+/* The kernel hbdia_spmv_device would launch for this x pointer. */
+int hbdia_matrix_selected_kernel(const hbdia_matrix *m, const void *x, int32_t *kernel);
+
+/* Time limit of every device-side wait of the staged kernel (default 2 s). */
+int hbdia_matrix_set_wait_timeout(hbdia_matrix *m, uint64_t nanoseconds);
+
+/* Test hook of the staged kernel: its producer never publishes chunk
+ * `chunk`, so the waiting consumers run into their time limit and the kernel
+ * reports HBDIA_ERR_DEVICE_TIMEOUT at the next synchronize.  -1 turns it off. */
+int hbdia_matrix_test_skip_chunk(hbdia_matrix *m, int32_t chunk);
 
 /* ---------------------------------------------------------------- workloads */
 

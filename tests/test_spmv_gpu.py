@@ -22,31 +22,41 @@ def _scaled_err(y, yref, rows, cols, vals, x):
     return np.abs(y - yref) / np.maximum(scale, np.finfo(float).tiny)
 
 
-def _run(lib, orc, rows, cols, vals, nr, nc, bw, thr, x, max_coo=1_000_000_000, dtype=np.float64):
+KERNELS = {"staged": 3, "warp": 2, "rowwise": 1}
+
+
+@pytest.fixture(params=list(KERNELS), ids=list(KERNELS))
+def kernel(request):
+    return KERNELS[request.param]
+
+
+def _run(lib, orc, rows, cols, vals, nr, nc, bw, thr, x, max_coo=1_000_000_000, dtype=np.float64, kernel=0):
     v = np.asarray(vals, dtype)
     m = lib.HBDIA(rows, cols, v, nr, nc, dtype=dtype)
     m.convertToHBDIAFormat(bw, thr, max_coo)
+    m.setKernel(kernel)
     xv = lib.HBDIAVector(np.asarray(x, dtype))
     yv = lib.HBDIAVector(np.zeros(max(nr, 1), dtype))
     lib.hbdiaSpMV(m, xv, yv, True, False)
+    m.synchronize()
     y = yv.toHost()[:nr]
     yref = orc.convert(rows, cols, v, nr, nc, bw, thr, max_coo).spmv(np.asarray(x, dtype)[:nr])
     return y, yref, m
 
 
 @pytest.mark.parametrize("bw", [32, 1, 4, 8, 16, 64, 5])
-def test_random_bitexact(lib, orc, bw):
+def test_random_bitexact(lib, orc, bw, kernel):
     rng = np.random.default_rng(100 + bw)
     for trial in range(12):
         n = int(rng.integers(1, 700))
         rows, cols, vals = random_coo(rng, n, n, int(rng.integers(1, 6 * n + 2)))
         x = rng.standard_normal(n)
         thr = int(rng.integers(1, 4))
-        y, yref, _ = _run(lib, orc, rows, cols, vals, n, n, bw, thr, x)
+        y, yref, _ = _run(lib, orc, rows, cols, vals, n, n, bw, thr, x, kernel=kernel)
         assert bits_equal(y, yref), (bw, trial, np.flatnonzero(y != yref)[:10])
 
 
-def test_banded_rows_not_multiple_of_32(lib, orc):
+def test_banded_rows_not_multiple_of_32(lib, orc, kernel):
     rng = np.random.default_rng(7)
     for n in (33, 65, 1000, 4097):
         offs = [-70, -3, -1, 0, 1, 2, 40]
@@ -63,11 +73,11 @@ def test_banded_rows_not_multiple_of_32(lib, orc):
         rows, cols = rows[keep], cols[keep]
         vals = rng.uniform(-1, 1, len(rows))
         x = rng.uniform(-1, 1, n)
-        y, yref, _ = _run(lib, orc, rows, cols, vals, n, n, 32, 2, x)
+        y, yref, _ = _run(lib, orc, rows, cols, vals, n, n, 32, 2, x, kernel=kernel)
         assert bits_equal(y, yref), n
 
 
-def test_unsorted_duplicates_and_maxcoo(lib, orc):
+def test_unsorted_duplicates_and_maxcoo(lib, orc, kernel):
     rng = np.random.default_rng(11)
     n = 300
     rows, cols, vals = random_coo(rng, n, n, 2500, sort=False)
@@ -80,11 +90,11 @@ def test_unsorted_duplicates_and_maxcoo(lib, orc):
     rows, cols, vals = rows[o], cols[o], vals[o]
     x = rng.standard_normal(n)
     for max_coo in (0, 5, 1_000_000_000):
-        y, yref, _ = _run(lib, orc, rows, cols, vals, n, n, 32, 3, x, max_coo=max_coo)
+        y, yref, _ = _run(lib, orc, rows, cols, vals, n, n, 32, 3, x, max_coo=max_coo, kernel=kernel)
         assert bits_equal(y, yref), max_coo
 
 
-def test_nonsquare(lib, orc):
+def test_nonsquare(lib, orc, kernel):
     rng = np.random.default_rng(12)
     for nr, nc in ((200, 90), (90, 200), (64, 31)):
         rows, cols, vals = random_coo(rng, nr, nc, 1500)
@@ -92,6 +102,7 @@ def test_nonsquare(lib, orc):
         v = vals
         m = lib.HBDIA(rows, cols, v, nr, nc)
         m.convertToHBDIAFormat(32, 2)
+        m.setKernel(kernel)
         xv = lib.HBDIAVector(x)
         yv = lib.HBDIAVector(np.zeros(nr))
         lib.hbdiaSpMV(m, xv, yv, False, True)
@@ -107,18 +118,18 @@ def test_nonsquare(lib, orc):
         assert bits_equal(y, yref), (nr, nc)
 
 
-def test_float32(lib, orc):
+def test_float32(lib, orc, kernel):
     rng = np.random.default_rng(13)
     for bw in (32, 8):
         n = 5000
         rows, cols, vals = random_coo(rng, n, n, 40000)
         x = rng.standard_normal(n).astype(np.float32)
-        y, yref, _ = _run(lib, orc, rows, cols, vals, n, n, bw, 2, x, dtype=np.float32)
+        y, yref, _ = _run(lib, orc, rows, cols, vals, n, n, bw, 2, x, dtype=np.float32, kernel=kernel)
         assert y.dtype == np.float32
         assert bits_equal(y, yref), bw
 
 
-def test_no_coo_and_all_coo(lib, orc):
+def test_no_coo_and_all_coo(lib, orc, kernel):
     rng = np.random.default_rng(14)
     n = 1000
     # pure band: nothing goes to COO
@@ -129,10 +140,10 @@ def test_no_coo_and_all_coo(lib, orc):
     rows, cols = rows[o], cols[o]
     vals = rng.uniform(-1, 1, len(rows))
     x = rng.uniform(-1, 1, n)
-    y, yref, m = _run(lib, orc, rows, cols, vals, n, n, 32, 1, x)
+    y, yref, m = _run(lib, orc, rows, cols, vals, n, n, 32, 1, x, kernel=kernel)
     assert m.info().numCoo == 0 and bits_equal(y, yref)
     # threshold above any count: everything in COO, blocks empty
-    y, yref, m = _run(lib, orc, rows, cols, vals, n, n, 32, 10**6, x)
+    y, yref, m = _run(lib, orc, rows, cols, vals, n, n, 32, 10**6, x, kernel=kernel)
     assert m.info().totalOffsets == 0 and bits_equal(y, yref)
 
 
@@ -160,13 +171,13 @@ def test_empty_matrix_writes_zero(lib):
     assert np.all(y.toHost() == 0.0)
 
 
-def test_config1_64cube_bitexact(lib, orc):
+def test_config1_64cube_bitexact(lib, orc, kernel):
     """64^3 27-point stencil, centre 26, neighbours -1, 0.5% extras (seed 0),
     bw=32, thr=2, x[i] = i+1, y = 0, execCOOCPU=true."""
     n = 64 ** 3
     rows, cols, vals = lib.generate_stencil27(64, 64, 64, 26.0, -1.0, 0.005, 0.1, 1.0, 0)
     x = np.arange(1, n + 1, dtype=np.float64)
-    y, yref, m = _run(lib, orc, rows, cols, vals, n, n, 32, 2, x)
+    y, yref, m = _run(lib, orc, rows, cols, vals, n, n, 32, 2, x, kernel=kernel)
     assert bits_equal(y, yref)
     assert np.max(_scaled_err(y, yref, rows, cols, vals, x)) <= TOL
 
@@ -205,11 +216,65 @@ def test_spmv_device_and_host_paths(lib, orc):
     m.convertToHBDIAFormat(32, 2)
     yref = orc.convert(rows, cols, vals, n, n, 32, 2).spmv(x)
     xt = torch.from_numpy(x).cuda()
-    yt = torch.zeros(n, dtype=torch.float64, device="cuda")
-    s = torch.cuda.current_stream()
-    lib.spmv_device(m, xt.data_ptr(), yt.data_ptr(), s.cuda_stream)
-    s.synchronize()
-    assert bits_equal(yt.cpu().numpy(), yref)
+    # torch's default stream (handle 0) and a side stream
+    for s in (torch.cuda.current_stream(), torch.cuda.Stream()):
+        yt = torch.zeros(n, dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        lib.spmv_device(m, xt.data_ptr(), yt.data_ptr(), s.cuda_stream)
+        s.synchronize()
+        assert bits_equal(yt.cpu().numpy(), yref)
     yh = np.zeros(n)
     lib.spmv_host(m, x, yh)
     assert bits_equal(yh, yref)
+
+
+def test_dense_band_chunks_fall_back(lib, orc, kernel):
+    """Blocks with more stored offsets than a stage holds (here 70 per
+    32-row block, 280 per 4-block chunk) take the global-memory path of the
+    staged kernel; x ranges wider than the stage's window capacity too."""
+    rng = np.random.default_rng(21)
+    n = 3000
+    offs = np.concatenate([np.arange(-35, 35), [1200, -1500, 2999, -2999]])
+    r, c = [], []
+    for o in offs:
+        i = np.arange(max(0, -o), min(n, n - o))
+        r.append(i)
+        c.append(i + o)
+    rows = np.concatenate(r).astype(np.int32)
+    cols = np.concatenate(c).astype(np.int32)
+    o = np.argsort(rows, kind="stable")
+    rows, cols = rows[o], cols[o]
+    vals = rng.uniform(-1, 1, len(rows))
+    x = rng.uniform(-1, 1, n)
+    y, yref, _ = _run(lib, orc, rows, cols, vals, n, n, 32, 1, x, kernel=kernel)
+    assert bits_equal(y, yref)
+    # many scattered offsets per chunk: more windows than the table holds
+    rows2, cols2, vals2 = random_coo(rng, n, n, 60000)
+    y, yref, _ = _run(lib, orc, rows2, cols2, vals2, n, n, 32, 1, x, kernel=kernel)
+    assert bits_equal(y, yref)
+
+
+def test_kernel_selection(lib):
+    import torch
+    n = 4096
+    rows, cols, vals = lib.generate_stencil27(16, 16, 16)
+    m = lib.HBDIA(rows, cols, vals, n, n)
+    m.convertToHBDIAFormat(32, 2)
+    xt = torch.zeros(n + 2, dtype=torch.float64, device="cuda")
+    assert m.selectedKernel(xt.data_ptr()) == lib.KERNEL_STAGED
+    assert m.selectedKernel(xt.data_ptr() + 8) == lib.KERNEL_WARP      # x not 16-byte aligned
+    m8 = lib.HBDIA(rows, cols, vals, n, n)
+    m8.convertToHBDIAFormat(8, 2)
+    assert m8.selectedKernel(xt.data_ptr()) == lib.KERNEL_ROWWISE
+    # misaligned x still gives the exact result (warp kernel)
+    x = np.random.default_rng(1).uniform(-1, 1, n)
+    xt[1:n + 1] = torch.from_numpy(x).cuda()
+    yt = torch.zeros(n, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    lib.spmv_device(m, xt.data_ptr() + 8, yt.data_ptr())
+    m.synchronize()
+    m2 = lib.HBDIA(rows, cols, vals, n, n)
+    m2.convertToHBDIAFormat(32, 2)
+    yv = lib.HBDIAVector(np.zeros(n))
+    lib.hbdiaSpMV(m2, lib.HBDIAVector(x), yv, True, False)
+    assert bits_equal(yt.cpu().numpy(), yv.toHost())
