@@ -83,7 +83,21 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> str:
         _run([_cxx(), "-shared", "-o", LIB, *objs, "-L", os.path.join(CUDA_HOME, "lib64"),
               "-l:libcudart_static.a", "-ldl", "-lrt", "-lpthread",
               "-l:libstdc++.so.6", "-l:libgomp.so.1", "-Wl,--no-undefined"], verbose)
+    build_cpp_tests(verbose)
     return LIB
+
+
+CPP_TEST_SRC = os.path.join(ROOT, "tests", "cpp", "test_dropin.cpp")
+CPP_TEST_BIN = os.path.join(BUILD, "test_dropin")
+
+
+def build_cpp_tests(verbose: bool = False) -> str:
+    """The C++ drop-in test program (tests/cpp/test_dropin.cpp), linked
+    against the in-tree library."""
+    if os.path.exists(CPP_TEST_SRC) and _stale(CPP_TEST_BIN, [CPP_TEST_SRC, LIB]):
+        _run([_cxx(), "-std=c++17", "-O2", "-ffp-contract=off", "-I", os.path.join(ROOT, "include"),
+              CPP_TEST_SRC, "-o", CPP_TEST_BIN, LIB, "-Wl,-rpath,$ORIGIN/..", "-l:libstdc++.so.6"], verbose)
+    return CPP_TEST_BIN
 
 
 if __name__ == "__main__":

@@ -33,7 +33,10 @@ void check_cuda(int err, const char *what) {
 
 namespace {
 
-constexpr int kUnroll = 9;  // offsets in flight per lane in the bw == 32 kernel
+constexpr int kUnroll = 9;  // offsets in flight per lane in the bw == 32 kernels
+// the staged kernel's shared memory must fit one CTA per SM (227 KB on sm_100)
+static_assert(sizeof(dev::TmaSmem<double, double>) <= 232448, "staged SpMV stage ring too large");
+static_assert(sizeof(dev::TmaSmem<float, float>) <= 232448, "staged SpMV stage ring too large");
 
 size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
 
@@ -116,8 +119,9 @@ void build_plan(const HostLayout<T> &L, int storage, DevicePlan &P) {
     std::vector<int32_t> rec;
     std::vector<XWindow> win;
     if (Q.bw == 32) {
+        // x windows are prefetched into L2, not staged: no capacity limit
         build_chunk_schedule(Q.n, Q.numBlocks, Q.numTiles, L.blockStart.data(), L.offsets.data(), tile.data(),
-                             dev::kVRows, dev::kXCap, static_cast<int>(sizeof(T)), rec, win);
+                             dev::kVRows, 1 << 30, static_cast<int>(sizeof(T)), rec, win);
         Q.numChunks = static_cast<int32_t>(rec.size() / kRecInts);
         Q.numWindows = static_cast<int64_t>(win.size());
     }

@@ -4,21 +4,26 @@
 // One CTA per SM walks the chunks (kTilesPerChunk consecutive 32-row tiles)
 // blockIdx.x, blockIdx.x + gridDim.x, ...  A producer warp fills a ring of
 // kStages shared-memory stages, one chunk per stage:
-//   * the chunk's values (one contiguous cp.async.bulk, L2 evict-first: they
-//     are read once), its offsets, its COO remainder (rows, values) and the x
-//     windows its diagonals read (one cp.async.bulk each, 16-byte aligned), all
-//     completing on the stage's "full" mbarrier through the transaction count;
-//   * the x values the COO entries gather, with per-lane cp.async copies that
-//     the same mbarrier tracks (cp.async.mbarrier.arrive.noinc).
+//   * the chunk's values (one contiguous cp.async.bulk with an L2 evict-first
+//     hint: they are read once), its offsets and its COO remainder (rows,
+//     values), each one cp.async.bulk completing on the stage's "full"
+//     mbarrier through the transaction count;
+//   * the x values its COO entries gather, with per-lane cp.async copies that
+//     the same mbarrier tracks (cp.async.mbarrier.arrive.noinc);
+//   * an L2 prefetch (cp.async.bulk.prefetch.L2) of the x windows the chunk's
+//     diagonals read, so the consumers' x loads find their lines on chip.
 // The producer's own metadata (chunk records, window tables, COO columns) is
 // prefetched 2-4 chunks ahead with cp.async groups, so no producer step waits
 // on a global-memory round trip.
-// kTilesPerChunk consumer warps compute one tile each from the stage -- the
-// same arithmetic, in the same order, as the reference (see spmv_kernels.cuh)
-// -- and release the stage on its "empty" mbarrier.
 //
-// Chunks whose rows do not fit a stage, x ranges beyond a stage's capacity
-// and COO entries beyond its capacity are read straight from global memory.
+// kGroups groups of kTilesPerChunk consumer warps take the stages in turn
+// (group g handles local steps g, g + kGroups, ...); within a group, warp w
+// computes tile w of the chunk -- the reference's arithmetic in the
+// reference's order (spmv_kernels.cuh) -- and the group releases the stage on
+// its "empty" mbarrier.
+//
+// Chunks whose rows do not fit a stage and COO entries beyond a stage's
+// capacity are read straight from global memory.
 //
 // Every wait is bounded by a time limit; on expiry the kernel records an error
 // bit in *status, drains the copies it has in flight (again bounded) and
@@ -31,14 +36,19 @@
 namespace hbdia {
 namespace dev {
 
-constexpr int kStages = 4;
+constexpr int kStages = 6;
+constexpr int kGroups = 3;                   // consumer groups (stages computed at once)
 constexpr int kVRows = kTilesPerChunk * 32;  // stored offsets a stage holds
-constexpr int kXCap = 2048;                  // x elements a stage holds
 constexpr int kCCap = 128;                   // COO entries a stage holds
 constexpr int kRecRing = 5;                  // chunk records in flight (distance 4)
 constexpr int kMetaRing = 3;                 // window tables / COO columns in flight (distance 2)
-constexpr int kConsumerWarps = kTilesPerChunk;
+constexpr int kConsumerWarps = kGroups * kTilesPerChunk;
 constexpr int kTmaThreads = (kConsumerWarps + 1) * 32;
+static_assert(kStages > kGroups, "stages must outnumber consumer groups");
+// Each slot is then always consumed by the same group, which has finished the
+// slot's previous phase before it waits on the next one, so a parity wait can
+// never match a phase two uses old.
+static_assert(kStages % kGroups == 0, "a slot must always belong to the same consumer group");
 
 enum : int { kErrConsumerWait = 1, kErrProducerWait = 2, kErrDrain = 4 };
 
@@ -98,6 +108,9 @@ __device__ __forceinline__ void bulk_g2s_hint(void *dst, const void *src, uint32
         "l"(src), "r"(bytes), "r"(smem_u32(bar)), "l"(policy)
         : "memory");
 }
+__device__ __forceinline__ void bulk_prefetch_l2(const void *src, uint32_t bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
+}
 __device__ __forceinline__ uint64_t l2_evict_first_policy() {
     uint64_t p;
     asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
@@ -120,12 +133,10 @@ __device__ __forceinline__ void cp_async_arrive_noinc(uint64_t *bar) {
 template <typename VT, typename XT>
 struct __align__(16) Stage {
     VT vals[kVRows * 32];
-    XT xs[kXCap];
     XT cval[kCCap + 16 / sizeof(XT)];
     XT xg[kCCap];
     int32_t offs[kVRows + 8];
     int32_t crow[kCCap + 8];
-    XWindow win[kMaxWindows];
     int32_t hdr[kRecInts];
 };
 
@@ -143,7 +154,7 @@ template <typename VT, typename XT>
 struct TmaArgs {
     SpmvArgs<VT, XT> a;
     const int32_t *rec;     // chunk records, kRecInts per chunk
-    const XWindow *win;     // window lists
+    const XWindow *win;     // window lists (x ranges to prefetch into L2)
     int32_t numChunks;
     int32_t *status;        // error bits (0 = fine)
     uint64_t timeoutNs;     // limit of every wait
@@ -173,6 +184,8 @@ __device__ __forceinline__ XT tile_direct(const SpmvArgs<VT, XT> &a, int32_t til
     return sum;
 }
 
+// One tile from a staged chunk: values, offsets and the COO remainder from
+// shared memory, x through L1 (its lines were prefetched into L2).
 template <typename VT, typename XT, int U>
 __device__ __forceinline__ XT tile_staged(const SpmvArgs<VT, XT> &a, const Stage<VT, XT> &S, int w, int lane,
                                           const XT *__restrict__ x) {
@@ -181,53 +194,30 @@ __device__ __forceinline__ XT tile_staged(const SpmvArgs<VT, XT> &a, const Stage
     const int64_t row0 = static_cast<int64_t>(tile) * 32;
     const int64_t row = row0 + lane;
     const int32_t k0c = H[kRecK0];
-    const int32_t kAl = k0c & ~3;
     const int32_t kt0 = H[kRecTileK + w], kt1 = H[kRecTileK + w + 1];
-    const int32_t nWin = H[kRecNWin];
     const float s = (a.scale && tile < a.numBlocks) ? __ldg(a.scale + tile) : 1.0f;
+    const int32_t *offs = S.offs + (kt0 - (k0c & ~3));
+    const VT *vrow = S.vals + static_cast<int64_t>(kt0 - k0c) * 32 + lane;
+    const int cnt = kt1 - kt0;
+    const uint64_t n = static_cast<uint64_t>(a.n);
     XT sum = XT(0);
-    for (int32_t kb = kt0; kb < kt1; kb += 32) {
-        const int cnt = min(32, kt1 - kb);
-        const int32_t offL = lane < cnt ? S.offs[kb + lane - kAl] : 0;
-        // x window of this lane's offset (windows are disjoint and sorted)
-        const int64_t target = max(row0 + offL, int64_t(0));
-        int lo = 0, hi = nWin;
-        while (lo < hi) {
-            const int mid = (lo + hi) >> 1;
-            if (S.win[mid].end <= target) lo = mid + 1;
-            else hi = mid;
-        }
-        int32_t dL = 0, aL = 0, eL = 0;  // staged range [aL, eL) at xs[dL + col]
-        if (lo < nWin && S.win[lo].pos >= 0) {
-            aL = S.win[lo].alignedStart;
-            eL = S.win[lo].stagedEnd;
-            dL = S.win[lo].pos - aL;
-        }
-        const VT *vrow = S.vals + static_cast<int64_t>(kb - k0c) * 32 + lane;
-        for (int j = 0; j < cnt; j += U) {
-            VT v[U];
-            XT xv[U];
-            bool ok[U];
+    for (int j = 0; j < cnt; j += U) {
+        VT v[U];
+        XT xv[U];
+        bool ok[U];
 #pragma unroll
-            for (int u = 0; u < U; ++u) {
-                const int kk = j + u;
-                const int src = kk & 31;
-                const int32_t off = __shfl_sync(kFull, offL, src);
-                const int32_t d = __shfl_sync(kFull, dL, src);
-                const int32_t wa = __shfl_sync(kFull, aL, src);
-                const int32_t we = __shfl_sync(kFull, eL, src);
-                const bool act = kk < cnt;
-                const int64_t col = row + off;
-                ok[u] = act && col >= 0 && col < a.n;
-                v[u] = act ? vrow[kk * 32] : VT(0);
-                const bool st = col >= wa && col < we;
-                xv[u] = ok[u] ? (st ? S.xs[d + col] : __ldg(x + col)) : XT(0);
-            }
+        for (int u = 0; u < U; ++u) {
+            const int kk = j + u;
+            const bool act = kk < cnt;
+            const int64_t col = row + (act ? offs[kk] : 0);
+            ok[u] = act && static_cast<uint64_t>(col) < n;
+            v[u] = act ? vrow[kk * 32] : VT(0);
+            xv[u] = ok[u] ? __ldg(x + col) : XT(0);
+        }
 #pragma unroll
-            for (int u = 0; u < U; ++u) {
-                const XT vv = widen<XT>(v[u], s);
-                if (ok[u] && vv != XT(0)) sum = fma_rn(vv, xv[u], sum);
-            }
+        for (int u = 0; u < U; ++u) {
+            const XT vv = widen<XT>(v[u], s);
+            if (ok[u] && vv != XT(0)) sum = fma_rn(vv, xv[u], sum);
         }
     }
     if (a.hasCoo) {
@@ -279,7 +269,7 @@ spmv_bw32_tma(const TmaArgs<VT, XT> T, const XT *__restrict__ x, XT *__restrict_
     if (threadIdx.x == 0) {
         for (int s = 0; s < kStages; ++s) {
             mbar_init(&sm.full[s], 1 + 32);            // producer arrive.expect_tx + 32 cp.async arrivals
-            mbar_init(&sm.empty[s], kConsumerWarps);   // one arrival per consumer warp
+            mbar_init(&sm.empty[s], kTilesPerChunk);   // one arrival per warp of the consuming group
         }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -318,7 +308,6 @@ spmv_bw32_tma(const TmaArgs<VT, XT> T, const XT *__restrict__ x, XT *__restrict_
         cp_async_wait<0>();
         __syncwarp();
         int32_t issued = 0;
-        bool failed = false;
         for (int32_t i = 0; i < nSteps; ++i) {
             cp_async_wait<1>();
             __syncwarp();
@@ -326,7 +315,6 @@ spmv_bw32_tma(const TmaArgs<VT, XT> T, const XT *__restrict__ x, XT *__restrict_
             const uint32_t use = static_cast<uint32_t>(i / kStages);
             if (!mbar_wait(&sm.empty[slot], (use & 1u) ^ 1u, T.timeoutNs)) {
                 if (lane == 0) atomicOr(T.status, kErrProducerWait);
-                failed = true;
                 break;
             }
             Stage<VT, XT> &S = sm.stage[slot];
@@ -334,9 +322,7 @@ spmv_bw32_tma(const TmaArgs<VT, XT> T, const XT *__restrict__ x, XT *__restrict_
             const XWindow *W = sm.win[i % kMetaRing];
             const int32_t *cols = sm.cols[i % kMetaRing];
             const bool staged = R[kRecFlags] & 1;
-            const int32_t nWin = staged ? R[kRecNWin] : 0;
             if (lane < kRecInts) S.hdr[lane] = R[lane];
-            if (lane < nWin) S.win[lane] = W[lane];
             __syncwarp();
             uint32_t bytes = 0;
             int32_t k0 = 0, k1 = 0, kAl = 0, kEnd = 0, c0 = 0, ncs = 0, crAl = 0, crEnd = 0, cvAl = 0, cvEnd = 0;
@@ -344,19 +330,16 @@ spmv_bw32_tma(const TmaArgs<VT, XT> T, const XT *__restrict__ x, XT *__restrict_
                 k0 = R[kRecK0];
                 k1 = R[kRecK1];
                 kAl = k0 & ~3;
-                kEnd = (k1 + 3) & ~3;
+                kEnd = k1 > k0 ? (k1 + 3) & ~3 : kAl;
                 c0 = R[kRecC0];
                 ncs = min(R[kRecC1] - c0, kCCap);
                 constexpr int vAl = 16 / static_cast<int>(sizeof(XT));
                 crAl = c0 & ~3;
-                crEnd = (c0 + ncs + 3) & ~3;
+                crEnd = ncs > 0 ? (c0 + ncs + 3) & ~3 : crAl;
                 cvAl = c0 & ~(vAl - 1);
-                cvEnd = (c0 + ncs + vAl - 1) & ~(vAl - 1);
-                if (ncs == 0) crEnd = crAl, cvEnd = cvAl;
-                if (k1 == k0) kEnd = kAl;
+                cvEnd = ncs > 0 ? (c0 + ncs + vAl - 1) & ~(vAl - 1) : cvAl;
                 bytes = static_cast<uint32_t>(k1 - k0) * 32u * sizeof(VT) + static_cast<uint32_t>(kEnd - kAl) * 4u +
-                        static_cast<uint32_t>(crEnd - crAl) * 4u +
-                        static_cast<uint32_t>(cvEnd - cvAl) * sizeof(XT) + static_cast<uint32_t>(R[kRecXBytes]);
+                        static_cast<uint32_t>(crEnd - crAl) * 4u + static_cast<uint32_t>(cvEnd - cvAl) * sizeof(XT);
             }
             const bool skip = chunkOf(i) == T.skipChunk;
             if (lane == 0 && !skip) mbar_arrive_expect_tx(&sm.full[slot], bytes);
@@ -372,11 +355,11 @@ spmv_bw32_tma(const TmaArgs<VT, XT> T, const XT *__restrict__ x, XT *__restrict_
                 if (lane == 3 && cvEnd > cvAl)
                     bulk_g2s(S.cval, a.cooVal + cvAl, static_cast<uint32_t>(cvEnd - cvAl) * sizeof(XT),
                              &sm.full[slot]);
-                if (lane < nWin) {
+                if (lane < R[kRecNWin]) {
                     const XWindow w = W[lane];
-                    if (w.pos >= 0 && w.stagedEnd > w.alignedStart)
-                        bulk_g2s(S.xs + w.pos, x + w.alignedStart,
-                                 static_cast<uint32_t>(w.stagedEnd - w.alignedStart) * sizeof(XT), &sm.full[slot]);
+                    if (w.stagedEnd > w.alignedStart)
+                        bulk_prefetch_l2(x + w.alignedStart,
+                                         static_cast<uint32_t>(w.stagedEnd - w.alignedStart) * sizeof(XT));
                 }
                 for (int32_t e = lane; e < ncs; e += 32) cp_async<sizeof(XT)>(&S.xg[e], x + cols[e]);
             }
@@ -396,10 +379,11 @@ spmv_bw32_tma(const TmaArgs<VT, XT> T, const XT *__restrict__ x, XT *__restrict_
                 break;
             }
         }
-        (void)failed;
     } else {
         // ------------------------------------------------------------ consumers
-        for (int32_t i = 0; i < nSteps; ++i) {
+        const int group = warp / kTilesPerChunk;
+        const int w = warp % kTilesPerChunk;
+        for (int32_t i = group; i < nSteps; i += kGroups) {
             const int slot = i % kStages;
             const uint32_t use = static_cast<uint32_t>(i / kStages);
             if (!mbar_wait(&sm.full[slot], use & 1u, T.timeoutNs)) {
@@ -407,9 +391,9 @@ spmv_bw32_tma(const TmaArgs<VT, XT> T, const XT *__restrict__ x, XT *__restrict_
                 break;
             }
             const Stage<VT, XT> &S = sm.stage[slot];
-            const int32_t tile = S.hdr[kRecT0] + warp;
+            const int32_t tile = S.hdr[kRecT0] + w;
             if (tile < a.numTiles) {
-                const XT sum = (S.hdr[kRecFlags] & 1) ? tile_staged<VT, XT, U>(a, S, warp, lane, x)
+                const XT sum = (S.hdr[kRecFlags] & 1) ? tile_staged<VT, XT, U>(a, S, w, lane, x)
                                                       : tile_direct<VT, XT>(a, tile, lane, x);
                 const int64_t row = static_cast<int64_t>(tile) * 32 + lane;
                 if (row < a.n) __stcs(y + row, sum);

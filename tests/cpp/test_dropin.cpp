@@ -1,0 +1,125 @@
+// C++ drop-in check: the reference's single-GPU usage
+// (simple_hbdia_example.cpp:15-33) and the shape of its cuSPARSE comparison
+// test (tests/run_HBDIA_cusparse_comparison.cpp:128-250), written against
+// include/hbdia/*.hpp.  The expected y is computed here from the layout
+// getters with the reference's arithmetic (ascending-offset FMA chain for the
+// blocked-DIA part, sequential multiply-then-add for the COO remainder), so
+// the comparison is exact.  Exit status 0 only if every check passes.
+#include <cmath>
+#include <cstdio>
+#include <stdexcept>
+#include <vector>
+
+#include "hbdia/HBDIA.hpp"
+#include "hbdia/HBDIASpMV.hpp"
+#include "hbdia/HBDIAVector.hpp"
+
+static int failures = 0;
+#define CHECK(cond, what)                                   \
+    do {                                                    \
+        if (!(cond)) {                                      \
+            std::printf("FAIL: %s\n", what);                \
+            ++failures;                                     \
+        } else {                                            \
+            std::printf("ok:   %s\n", what);                \
+        }                                                   \
+    } while (0)
+
+template <typename T>
+static std::vector<T> expected(const HBDIA<T> &m, const std::vector<T> &x) {
+    const int n = m.getNumRows(), bw = m.getBlockWidth();
+    const auto &opb = m.getOffsetsPerBlock();
+    const auto &data = m.getHBDIAData();
+    std::vector<T> y(n, T(0)), coo(n, T(0));
+    const auto &cr = m.getCpuRowIndices();
+    const auto &cc = m.getCpuColIndices();
+    const auto &cv = m.getCpuValues();
+    for (size_t e = 0; e < cr.size(); ++e) {
+        volatile T p = cv[e] * x[cc[e]];  // separate rounding of the product
+        coo[cr[e]] = coo[cr[e]] + p;
+    }
+    size_t base = 0;
+    for (int b = 0; b < static_cast<int>(opb.size()); ++b) {
+        for (int lane = 0; lane < bw; ++lane) {
+            const int row = b * bw + lane;
+            if (row >= n) break;
+            T sum = T(0);
+            for (size_t k = 0; k < opb[b].size(); ++k) {
+                const T v = data[(base + k) * bw + lane];
+                const long col = static_cast<long>(row) + opb[b][k];
+                if (v == T(0) || col < 0 || col >= n) continue;
+                sum = std::fma(v, x[col], sum);
+            }
+            y[row] = sum;
+        }
+        base += opb[b].size();
+    }
+    if (!cr.empty())
+        for (int r = 0; r < n; ++r) y[r] = y[r] + coo[r];
+    return y;
+}
+
+template <typename T>
+static void run_case(const char *name, HBDIA<T> &m, int bw, int thr, const std::vector<T> &xv) {
+    m.convertToHBDIAFormat(bw, thr);
+    HBDIAVector<T> x(xv);
+    HBDIAVector<T> y(std::vector<T>(m.getNumRows(), T(0)));
+    hbdiaSpMV(m, x, y, true, false);
+    m.synchronize();
+    std::vector<T> got;
+    y.copyToHost(got);
+    const std::vector<T> want = expected(m, xv);
+    bool same = got.size() == want.size();
+    for (size_t i = 0; same && i < got.size(); ++i) same = got[i] == want[i];
+    CHECK(same, name);
+}
+
+int main() {
+    {  // simple_hbdia_example.cpp single-GPU part
+        HBDIA<double> m;
+        m.create3DStencil27Point(8, 8, 8, 0.0);
+        std::vector<double> x(m.getNumRows());
+        for (int i = 0; i < m.getNumRows(); i++) x[i] = static_cast<double>(i + 1);
+        run_case("8^3 stencil, bw 32 thr 2, x = i+1", m, 32, 2, x);
+        CHECK(m.getNumBlocks() == 16, "8^3 stencil has 16 row blocks");
+        CHECK(m.getCpuValues().empty(), "no COO remainder without noise");
+    }
+    {  // the comparison test's shape: stencil with noise, bw 32, GPU COO flag
+        HBDIA<double> m;
+        m.create3DStencil27Point(24, 24, 24, 0.01, 1);
+        std::vector<double> x(m.getNumRows());
+        for (int i = 0; i < m.getNumRows(); i++) x[i] = static_cast<double>(i);
+        run_case("24^3 stencil with noise, bw 32 thr 2", m, 32, 2, x);
+        CHECK(!m.getCpuValues().empty(), "noise lands in the COO remainder");
+    }
+    {  // float instantiation, block width 8
+        HBDIA<float> m;
+        m.create3DStencil27Point(12, 12, 12, 0.02, 3);
+        std::vector<float> x(m.getNumRows());
+        for (int i = 0; i < m.getNumRows(); i++) x[i] = 0.001f * static_cast<float>(i % 997);
+        run_case("float 12^3 stencil, bw 8 thr 2", m, 8, 2, x);
+    }
+    {  // invalid flags throw like the reference
+        std::vector<int> r = {0, 0, 1, 3}, c = {0, 3, 1, 0};
+        std::vector<double> v = {1, 2, 3, 4};
+        HBDIA<double> m(r, c, v, 4, 4);
+        m.convertToHBDIAFormat(2, 2);
+        HBDIAVector<double> x(std::vector<double>(4, 1.0)), y(std::vector<double>(4, 0.0));
+        bool threw = false;
+        try {
+            hbdiaSpMV(m, x, y, false, false);
+        } catch (const std::runtime_error &) {
+            threw = true;
+        }
+        CHECK(threw, "both COO flags false with a COO remainder throws std::runtime_error");
+        bool oor = false;
+        try {
+            HBDIA<double> bad(std::vector<int>{5}, std::vector<int>{0}, std::vector<double>{1.0}, 4, 4);
+        } catch (const std::out_of_range &) {
+            oor = true;
+        }
+        CHECK(oor, "out-of-range index throws std::out_of_range");
+    }
+    std::printf(failures ? "FAILED (%d)\n" : "ALL PASSED\n", failures);
+    return failures ? 1 : 0;
+}
