@@ -131,6 +131,22 @@ class ClockSampler:
                 "samples": len(self.samples)}
 
 
+def reduce_max(value: float, dist, device) -> float:
+    """Max over ranks of a per-rank time (identity on one rank)."""
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_gbs(bytes_per_step: int, steps: int, world: int, max_ms: float) -> float:
+    """Whole-job GB/s: every rank ran `steps` SpMVs of `bytes_per_step`; the
+    job took the slowest rank's time."""
+    return bytes_per_step * steps * world / (max_ms / 1e3) / 1e9
+
+
 def build_workload(hb, torch, device):
     w = WORKLOAD
     n = w["nx"] * w["ny"] * w["nz"]
@@ -264,6 +280,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--cpu-budget", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--unroll", type=int, default=0, choices=[0, 9, 27],
+                    help="offsets in flight per lane in the staged kernel (0: default)")
     ap.add_argument("--kernel", default=None, choices=["staged", "warp", "rowwise"],
                     help="force one SpMV kernel (default: the library's choice)")
     ap.add_argument("--size", type=int, default=256,
@@ -296,6 +314,8 @@ def main():
     assert bytes_per_spmv == info.bytesPerSpmv, (bytes_per_spmv, info.bytesPerSpmv)
     if args.kernel:
         m.setKernel({"staged": hb.KERNEL_STAGED, "warp": hb.KERNEL_WARP, "rowwise": hb.KERNEL_ROWWISE}[args.kernel])
+    if args.unroll:
+        m.setTuning(hb.TUNE_UNROLL, args.unroll)
     xt = torch.from_numpy(x).cuda()
     kernel_used = m.selectedKernel(xt.data_ptr())
     yt = torch.zeros(n, dtype=torch.float64, device="cuda")
@@ -328,11 +348,8 @@ def main():
     total_ms = t_all0.elapsed_time(t_all1)
     launch_ms = [a.elapsed_time(b) for a, b in evs]
     m.synchronize()  # raises if a bounded device-side wait ran out
-    if dist:
-        tt = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        total_ms = float(tt.item())
-    value = bytes_per_spmv * args.steps * world / (total_ms / 1e3) / 1e9
+    total_ms = reduce_max(total_ms, dist, "cuda")
+    value = aggregate_gbs(bytes_per_spmv, args.steps, world, total_ms)
     avg_launch_ms = sum(launch_ms) / len(launch_ms)
     achieved = bytes_per_spmv / (avg_launch_ms / 1e3) / 1e9
     peak, peak_kind = measured_peak()
@@ -351,12 +368,8 @@ def main():
         hb.spmv_host(m, xh_np, yh_np)
     e1.record(ms)
     e1.synchronize()
-    e2e_ms = e0.elapsed_time(e1)
-    if dist:
-        tt = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_ms = float(tt.item())
-    e2e_value = bytes_per_spmv * args.e2e_steps * world / (e2e_ms / 1e3) / 1e9
+    e2e_ms = reduce_max(e0.elapsed_time(e1), dist, "cuda")
+    e2e_value = aggregate_gbs(bytes_per_spmv, args.e2e_steps, world, e2e_ms)
     # the e2e result must be the device result
     ok = bool(np.array_equal(yh_np.view(np.uint64), yt.cpu().numpy().view(np.uint64)))
 

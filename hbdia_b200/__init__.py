@@ -18,7 +18,7 @@ from typing import List, Optional, Sequence
 import numpy as np
 
 from . import _lib
-from ._lib import (KERNEL_AUTO, KERNEL_ROWWISE, KERNEL_STAGED, KERNEL_WARP, HBDIACudaError,
+from ._lib import (KERNEL_AUTO, KERNEL_ROWWISE, KERNEL_STAGED, KERNEL_WARP, TUNE_UNROLL, HBDIACudaError,
                    HBDIADeviceTimeout, STORE_BF16_SCALED, STORE_F32, STORE_NATIVE, MatrixInfo,
                    check as _check, load as _load)
 
@@ -219,6 +219,10 @@ class HBDIA:
         k = ctypes.c_int32(0)
         _check(_load().hbdia_matrix_selected_kernel(self._h, ctypes.c_void_p(x_ptr), ctypes.byref(k)))
         return k.value
+
+    def setTuning(self, key: int, value: int) -> None:
+        """Kernel tuning knob (TUNE_UNROLL: 0, 9 or 27); results stay bit-identical."""
+        _check(_load().hbdia_matrix_set_tuning(self._h, int(key), int(value)))
 
     def setWaitTimeout(self, nanoseconds: int) -> None:
         _check(_load().hbdia_matrix_set_wait_timeout(self._h, int(nanoseconds)))

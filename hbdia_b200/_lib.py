@@ -27,6 +27,7 @@ HBDIA_ERR_UNSUPPORTED = -7
 HBDIA_ERR_DEVICE_TIMEOUT = -8
 
 KERNEL_AUTO, KERNEL_ROWWISE, KERNEL_WARP, KERNEL_STAGED = 0, 1, 2, 3
+TUNE_UNROLL = 1
 
 HBDIA_F64, HBDIA_F32 = 0, 1
 STORE_NATIVE, STORE_F32, STORE_BF16_SCALED = 0, 1, 2
@@ -87,6 +88,7 @@ _SIGS = [
     ("hbdia_matrix_set_kernel", ctypes.c_int, [c_vp, c_i32]),
     ("hbdia_matrix_selected_kernel", ctypes.c_int, [c_vp, c_vp, c_i32p]),
     ("hbdia_matrix_set_wait_timeout", ctypes.c_int, [c_vp, c_u64]),
+    ("hbdia_matrix_set_tuning", ctypes.c_int, [c_vp, c_i32, c_i32]),
     ("hbdia_matrix_test_skip_chunk", ctypes.c_int, [c_vp, c_i32]),
     ("hbdia_vector_create", ctypes.c_int, [ctypes.c_int, c_vp, c_i64, c_vpp]),
     ("hbdia_vector_destroy", None, [c_vp]),

@@ -407,6 +407,18 @@ int hbdia_matrix_selected_kernel(const hbdia_matrix *m, const void *x, int32_t *
     });
 }
 
+int hbdia_matrix_set_tuning(hbdia_matrix *m, int32_t key, int32_t value) {
+    return guarded([&] {
+        need(m != nullptr, HBDIA_ERR_INVALID_ARGUMENT, "null matrix");
+        if (key == HBDIA_TUNE_UNROLL) {
+            need(value == 0 || value == 9 || value == 27, HBDIA_ERR_INVALID_ARGUMENT, "unroll must be 0, 9 or 27");
+            m->plan.unroll = value;
+            return;
+        }
+        throw Error(HBDIA_ERR_INVALID_ARGUMENT, "unknown tuning key");
+    });
+}
+
 int hbdia_matrix_set_wait_timeout(hbdia_matrix *m, uint64_t ns) {
     return guarded([&] {
         need(m != nullptr && ns > 0, HBDIA_ERR_INVALID_ARGUMENT, "bad timeout");

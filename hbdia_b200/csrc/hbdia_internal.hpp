@@ -93,6 +93,7 @@ struct DevicePlan {
     int32_t kernel = HBDIA_KERNEL_AUTO;  // hbdia_kernel choice
     uint64_t waitTimeoutNs = 2000000000ull;
     int32_t skipChunk = -1;              // test hook of the staged kernel
+    int32_t unroll = 0;                  // offsets in flight per lane (0: default)
 };
 
 void build_chunk_schedule(int32_t n, int32_t numBlocks, int32_t numTiles, const int32_t *blkOff,

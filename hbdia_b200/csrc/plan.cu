@@ -227,6 +227,25 @@ template void build_plan<float>(const HostLayout<float> &, int, DevicePlan &);
 
 namespace {
 
+// One CTA per SM (the stage ring fills the SM's shared memory).  The
+// dynamic shared-memory opt-in is a per-device function attribute.
+template <typename VT, typename XT, int U>
+void launch_staged(const dev::TmaArgs<VT, XT> &T, int32_t numChunks, const XT *x, XT *y, cudaStream_t s) {
+    const size_t smem = sizeof(dev::TmaSmem<VT, XT>);
+    static uint64_t configured = 0;  // bit d: attribute set on device d
+    int dev = 0, sms = 0;
+    check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
+    if (dev >= 64 || !(configured & (uint64_t(1) << dev))) {
+        check_cuda(cudaFuncSetAttribute(dev::spmv_bw32_tma<VT, XT, U>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        static_cast<int>(smem)),
+                   "cudaFuncSetAttribute(staged SpMV)");
+        if (dev < 64) configured |= uint64_t(1) << dev;
+    }
+    check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "cudaDeviceGetAttribute");
+    const unsigned grid = static_cast<unsigned>(std::min<int64_t>(sms, numChunks));
+    dev::spmv_bw32_tma<VT, XT, U><<<grid, dev::kTmaThreads, smem, s>>>(T, x, y);
+}
+
 template <typename VT, typename XT>
 void launch_typed(const DevicePlan &P, const void *x, void *y, cudaStream_t s) {
     dev::SpmvArgs<VT, XT> a;
@@ -256,19 +275,8 @@ void launch_typed(const DevicePlan &P, const void *x, void *y, cudaStream_t s) {
         T.status = P.status;
         T.timeoutNs = P.waitTimeoutNs;
         T.skipChunk = P.skipChunk;
-        const size_t smem = sizeof(dev::TmaSmem<VT, XT>);
-        static bool configured = false;  // per template instance
-        if (!configured) {
-            check_cuda(cudaFuncSetAttribute(dev::spmv_bw32_tma<VT, XT, kUnroll>,
-                                            cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
-                       "cudaFuncSetAttribute(staged SpMV)");
-            configured = true;
-        }
-        int dev = 0, sms = 0;
-        check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
-        check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "cudaDeviceGetAttribute");
-        const unsigned grid = static_cast<unsigned>(std::min<int64_t>(sms, P.numChunks));
-        dev::spmv_bw32_tma<VT, XT, kUnroll><<<grid, dev::kTmaThreads, smem, s>>>(T, xp, yp);
+        if (P.unroll == 27) launch_staged<VT, XT, 27>(T, P.numChunks, xp, yp, s);
+        else launch_staged<VT, XT, kUnroll>(T, P.numChunks, xp, yp, s);
     } else if (kern == HBDIA_KERNEL_WARP) {
         const int64_t warpsPerCta = 8;
         const unsigned grid = static_cast<unsigned>((P.numTiles + warpsPerCta - 1) / warpsPerCta);
@@ -285,7 +293,8 @@ void launch_typed(const DevicePlan &P, const void *x, void *y, cudaStream_t s) {
 int32_t select_kernel(const DevicePlan &P, const void *x) {
     const bool bw32 = P.bw == 32;
     const bool aligned = (reinterpret_cast<uintptr_t>(x) & 15) == 0;
-    const bool stagedOk = bw32 && aligned && P.numChunks > 0;
+    // the staged kernel does row/column arithmetic in 32 bits (n <= 2^30)
+    const bool stagedOk = bw32 && aligned && P.numChunks > 0 && P.n <= (1 << 30);
     switch (P.kernel) {
         case HBDIA_KERNEL_ROWWISE: return HBDIA_KERNEL_ROWWISE;
         case HBDIA_KERNEL_WARP: return bw32 ? HBDIA_KERNEL_WARP : HBDIA_KERNEL_ROWWISE;

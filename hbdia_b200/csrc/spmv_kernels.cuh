@@ -155,25 +155,33 @@ spmv_bw32(const SpmvArgs<VT, XT> a, const XT *__restrict__ x, XT *__restrict__ y
             const int cnt = min(32, k1 - kb);
             const int32_t myoff = lane < cnt ? __ldg(a.offs + kb + lane) : 0;
             const VT *vp = a.vals + static_cast<int64_t>(kb) * 32 + lane;
-            for (int j = 0; j < cnt; j += U) {
+            int j = 0;
+            for (; j + U <= cnt; j += U) {  // full groups: U values and x loads in flight
                 VT v[U];
                 XT xv[U];
                 bool ok[U];
+                int64_t col[U];
 #pragma unroll
                 for (int u = 0; u < U; ++u) {
-                    const int jj = j + u;
-                    const int32_t off = __shfl_sync(kFull, myoff, jj & 31);
-                    const int64_t col = row + off;
-                    const bool act = jj < cnt;
-                    ok[u] = act && col >= 0 && col < a.n;
-                    v[u] = act ? ld_stream(vp + static_cast<int64_t>(jj) * 32) : VT(0);
-                    xv[u] = ok[u] ? __ldg(x + col) : XT(0);
+                    col[u] = row + __shfl_sync(kFull, myoff, j + u);
+                    ok[u] = static_cast<uint64_t>(col[u]) < static_cast<uint64_t>(a.n);
+                    v[u] = ld_stream(vp + static_cast<int64_t>(j + u) * 32);
+                    xv[u] = XT(0);
                 }
+#pragma unroll
+                for (int u = 0; u < U; ++u)
+                    if (ok[u]) xv[u] = __ldg(x + col[u]);
 #pragma unroll
                 for (int u = 0; u < U; ++u) {
                     const XT vv = widen<XT>(v[u], s);
                     if (ok[u] && vv != XT(0)) sum = fma_rn(vv, xv[u], sum);
                 }
+            }
+            for (; j < cnt; ++j) {  // warp-uniform tail
+                const int64_t col = row + __shfl_sync(kFull, myoff, j);
+                const XT vv = widen<XT>(ld_stream(vp + static_cast<int64_t>(j) * 32), s);
+                if (static_cast<uint64_t>(col) < static_cast<uint64_t>(a.n) && vv != XT(0))
+                    sum = fma_rn(vv, __ldg(x + col), sum);
             }
         }
     }

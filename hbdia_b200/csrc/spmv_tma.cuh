@@ -191,34 +191,46 @@ __device__ __forceinline__ XT tile_staged(const SpmvArgs<VT, XT> &a, const Stage
                                           const XT *__restrict__ x) {
     const int32_t *H = S.hdr;
     const int32_t tile = H[kRecT0] + w;
-    const int64_t row0 = static_cast<int64_t>(tile) * 32;
-    const int64_t row = row0 + lane;
+    // 32-bit row/column arithmetic: the staged kernel runs only for n <= 2^30,
+    // so row + offset (offsets lie in (-n, n)) cannot overflow
+    const int32_t row0 = tile * 32;
+    const int32_t row = row0 + lane;
     const int32_t k0c = H[kRecK0];
     const int32_t kt0 = H[kRecTileK + w], kt1 = H[kRecTileK + w + 1];
     const float s = (a.scale && tile < a.numBlocks) ? __ldg(a.scale + tile) : 1.0f;
     const int32_t *offs = S.offs + (kt0 - (k0c & ~3));
-    const VT *vrow = S.vals + static_cast<int64_t>(kt0 - k0c) * 32 + lane;
+    const VT *vrow = S.vals + (kt0 - k0c) * 32 + lane;
     const int cnt = kt1 - kt0;
-    const uint64_t n = static_cast<uint64_t>(a.n);
+    const uint32_t n = static_cast<uint32_t>(a.n);
     XT sum = XT(0);
-    for (int j = 0; j < cnt; j += U) {
+    int j = 0;
+    // full groups of U offsets: U independent x loads in flight, then the
+    // FMA chain in ascending offset order
+    for (; j + U <= cnt; j += U) {
+        int32_t col[U];
+        bool ok[U];
         VT v[U];
         XT xv[U];
-        bool ok[U];
 #pragma unroll
         for (int u = 0; u < U; ++u) {
-            const int kk = j + u;
-            const bool act = kk < cnt;
-            const int64_t col = row + (act ? offs[kk] : 0);
-            ok[u] = act && static_cast<uint64_t>(col) < n;
-            v[u] = act ? vrow[kk * 32] : VT(0);
-            xv[u] = ok[u] ? __ldg(x + col) : XT(0);
+            col[u] = row + offs[j + u];
+            ok[u] = static_cast<uint32_t>(col[u]) < n;
+            v[u] = vrow[(j + u) * 32];
+            xv[u] = XT(0);
         }
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+            if (ok[u]) xv[u] = __ldg(x + col[u]);
 #pragma unroll
         for (int u = 0; u < U; ++u) {
             const XT vv = widen<XT>(v[u], s);
             if (ok[u] && vv != XT(0)) sum = fma_rn(vv, xv[u], sum);
         }
+    }
+    for (; j < cnt; ++j) {
+        const int32_t col = row + offs[j];
+        const XT vv = widen<XT>(vrow[j * 32], s);
+        if (static_cast<uint32_t>(col) < n && vv != XT(0)) sum = fma_rn(vv, __ldg(x + col), sum);
     }
     if (a.hasCoo) {
         const int32_t c0 = H[kRecC0], c1 = H[kRecC1];

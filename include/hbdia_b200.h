@@ -234,6 +234,12 @@ int hbdia_matrix_set_kernel(hbdia_matrix *m, int32_t kernel);
 /* The kernel hbdia_spmv_device would launch for this x pointer. */
 int hbdia_matrix_selected_kernel(const hbdia_matrix *m, const void *x, int32_t *kernel);
 
+/* Kernel tuning knobs (used by the autotuner; results stay bit-identical).
+ * HBDIA_TUNE_UNROLL: offsets in flight per lane in the staged kernel
+ * (0 = default 9, or 27). */
+typedef enum hbdia_tuning_key { HBDIA_TUNE_UNROLL = 1 } hbdia_tuning_key;
+int hbdia_matrix_set_tuning(hbdia_matrix *m, int32_t key, int32_t value);
+
 /* Time limit of every device-side wait of the staged kernel (default 2 s). */
 int hbdia_matrix_set_wait_timeout(hbdia_matrix *m, uint64_t nanoseconds);
 

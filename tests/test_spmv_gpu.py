@@ -147,6 +147,22 @@ def test_no_coo_and_all_coo(lib, orc, kernel):
     assert m.info().totalOffsets == 0 and bits_equal(y, yref)
 
 
+@pytest.mark.parametrize("unroll", [9, 27])
+def test_tuning_keeps_bits(lib, orc, unroll):
+    """Tuning knobs change speed, never results."""
+    n = 48 ** 3
+    rows, cols, vals = lib.generate_stencil27(48, 48, 48, 26.0, -1.0, 0.01, 0.1, 1.0, 6)
+    x = np.random.default_rng(8).uniform(-1, 1, n)
+    m = lib.HBDIA(rows, cols, vals, n, n)
+    m.convertToHBDIAFormat(32, 2)
+    m.setKernel(lib.KERNEL_STAGED)
+    m.setTuning(lib.TUNE_UNROLL, unroll)
+    yv = lib.HBDIAVector(np.zeros(n))
+    lib.hbdiaSpMV(m, lib.HBDIAVector(x), yv, True, False)
+    m.synchronize()
+    assert bits_equal(yv.toHost(), orc.convert(rows, cols, vals, n, n, 32, 2).spmv(x))
+
+
 def test_flags_and_errors(lib):
     rows = np.array([0, 1, 1, 5], np.int32)
     cols = np.array([0, 1, 9, 5], np.int32)
