@@ -13,8 +13,8 @@
 //   * an L2 prefetch (cp.async.bulk.prefetch.L2) of the x windows the chunk's
 //     diagonals read, so the consumers' x loads find their lines on chip.
 // The producer's own metadata (chunk records, window tables, COO columns) is
-// prefetched 2-4 chunks ahead with cp.async groups, so no producer step waits
-// on a global-memory round trip.
+// bulk-copied 2-4 chunks ahead onto per-slot mbarriers, so no producer step
+// waits on a global-memory round trip (nor on the COO gathers in flight).
 //
 // kGroups groups of kTilesPerChunk consumer warps take the stages in turn
 // (group g handles local steps g, g + kGroups, ...); within a group, warp w
@@ -145,9 +145,11 @@ struct __align__(16) TmaSmem {
     Stage<VT, XT> stage[kStages];
     int32_t rec[kRecRing][kRecInts];
     XWindow win[kMetaRing][kMaxWindows];
-    int32_t cols[kMetaRing][kCCap];
+    int32_t cols[kMetaRing][kCCap + 8];
     uint64_t full[kStages];
     uint64_t empty[kStages];
+    uint64_t recBar[kRecRing];    // chunk record landed (bulk copy)
+    uint64_t metaBar[kMetaRing];  // window table + COO columns landed (bulk copies)
 };
 
 template <typename VT, typename XT>
@@ -283,6 +285,8 @@ spmv_bw32_tma(const TmaArgs<VT, XT> T, const XT *__restrict__ x, XT *__restrict_
             mbar_init(&sm.full[s], 1 + 32);            // producer arrive.expect_tx + 32 cp.async arrivals
             mbar_init(&sm.empty[s], kTilesPerChunk);   // one arrival per warp of the consuming group
         }
+        for (int r = 0; r < kRecRing; ++r) mbar_init(&sm.recBar[r], 1);
+        for (int r = 0; r < kMetaRing; ++r) mbar_init(&sm.metaBar[r], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
@@ -295,44 +299,66 @@ spmv_bw32_tma(const TmaArgs<VT, XT> T, const XT *__restrict__ x, XT *__restrict_
         // ------------------------------------------------------------ producer
         const uint64_t policy = l2_evict_first_policy();
         auto chunkOf = [&](int32_t i) { return first + i * G; };
-        auto prefetchRec = [&](int32_t i) {
-            if (i < nSteps && lane < kRecInts / 4)
-                cp_async<16>(&sm.rec[i % kRecRing][lane * 4],
-                             T.rec + static_cast<int64_t>(chunkOf(i)) * kRecInts + lane * 4);
+        // The producer's own metadata arrives by bulk copies on per-slot
+        // mbarriers, never through cp.async groups: waiting on a group would
+        // also wait for the (older) COO x gathers, which are random DRAM reads.
+        int32_t recIssued = 0, metaIssued = 0;
+        auto prefetchRec = [&](int32_t i) {  // chunk record of step i
+            if (i >= nSteps) return;
+            if (lane == 0) {
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                mbar_arrive_expect_tx(&sm.recBar[i % kRecRing], kRecInts * 4);
+                bulk_g2s(sm.rec[i % kRecRing], T.rec + static_cast<int64_t>(chunkOf(i)) * kRecInts, kRecInts * 4,
+                         &sm.recBar[i % kRecRing]);
+            }
+            recIssued = i + 1;
         };
-        auto prefetchMeta = [&](int32_t i) {  // needs rec(i) complete
+        auto waitRec = [&](int32_t i) {
+            return mbar_wait(&sm.recBar[i % kRecRing], static_cast<uint32_t>(i / kRecRing) & 1u, T.timeoutNs);
+        };
+        auto waitMeta = [&](int32_t i) {
+            return mbar_wait(&sm.metaBar[i % kMetaRing], static_cast<uint32_t>(i / kMetaRing) & 1u, T.timeoutNs);
+        };
+        auto prefetchMeta = [&](int32_t i) {  // window table + COO columns of step i; rec(i) has landed
             if (i >= nSteps) return;
             const int32_t *R = sm.rec[i % kRecRing];
-            if (!(R[kRecFlags] & 1)) return;
-            const int32_t nWin = R[kRecNWin];
-            if (lane < nWin) cp_async<16>(&sm.win[i % kMetaRing][lane], T.win + R[kRecWin0] + lane);
+            const bool staged = R[kRecFlags] & 1;
+            const int32_t nWin = staged ? R[kRecNWin] : 0;
             const int32_t c0 = R[kRecC0];
-            const int32_t ncs = min(R[kRecC1] - c0, kCCap);
-            for (int32_t e = lane; e < ncs; e += 32) cp_async<4>(&sm.cols[i % kMetaRing][e], a.cooCol + c0 + e);
+            const int32_t ncs = staged ? min(R[kRecC1] - c0, kCCap) : 0;
+            const int32_t colAl = c0 & ~3;
+            const int32_t colEnd = ncs > 0 ? (c0 + ncs + 3) & ~3 : colAl;
+            if (lane == 0) {
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                mbar_arrive_expect_tx(&sm.metaBar[i % kMetaRing],
+                                      static_cast<uint32_t>(nWin) * 16u + static_cast<uint32_t>(colEnd - colAl) * 4u);
+                if (nWin > 0)
+                    bulk_g2s(sm.win[i % kMetaRing], T.win + R[kRecWin0], static_cast<uint32_t>(nWin) * 16u,
+                             &sm.metaBar[i % kMetaRing]);
+                if (colEnd > colAl)
+                    bulk_g2s(sm.cols[i % kMetaRing], a.cooCol + colAl, static_cast<uint32_t>(colEnd - colAl) * 4u,
+                             &sm.metaBar[i % kMetaRing]);
+            }
+            metaIssued = i + 1;
         };
+        bool ok = true;
         for (int32_t i = 0; i < 4; ++i) prefetchRec(i);
-        cp_async_commit();
-        cp_async_wait<0>();
-        __syncwarp();
-        prefetchMeta(0);
-        prefetchMeta(1);
-        cp_async_commit();
-        cp_async_wait<0>();
+        for (int32_t i = 0; i < 2 && i < nSteps && ok; ++i) {
+            ok = waitRec(i);
+            if (ok) prefetchMeta(i);
+        }
         __syncwarp();
         int32_t issued = 0;
-        for (int32_t i = 0; i < nSteps; ++i) {
-            cp_async_wait<1>();
-            __syncwarp();
+        for (int32_t i = 0; i < nSteps && ok; ++i) {
             const int slot = i % kStages;
             const uint32_t use = static_cast<uint32_t>(i / kStages);
-            if (!mbar_wait(&sm.empty[slot], (use & 1u) ^ 1u, T.timeoutNs)) {
-                if (lane == 0) atomicOr(T.status, kErrProducerWait);
+            if (!waitRec(i) || !waitMeta(i) || !mbar_wait(&sm.empty[slot], (use & 1u) ^ 1u, T.timeoutNs)) {
+                ok = false;
                 break;
             }
             Stage<VT, XT> &S = sm.stage[slot];
             const int32_t *R = sm.rec[i % kRecRing];
             const XWindow *W = sm.win[i % kMetaRing];
-            const int32_t *cols = sm.cols[i % kMetaRing];
             const bool staged = R[kRecFlags] & 1;
             if (lane < kRecInts) S.hdr[lane] = R[lane];
             __syncwarp();
@@ -373,24 +399,35 @@ spmv_bw32_tma(const TmaArgs<VT, XT> T, const XT *__restrict__ x, XT *__restrict_
                         bulk_prefetch_l2(x + w.alignedStart,
                                          static_cast<uint32_t>(w.stagedEnd - w.alignedStart) * sizeof(XT));
                 }
+                const int32_t *cols = sm.cols[i % kMetaRing] + (c0 - (c0 & ~3));
                 for (int32_t e = lane; e < ncs; e += 32) cp_async<sizeof(XT)>(&S.xg[e], x + cols[e]);
             }
             if (!skip) cp_async_arrive_noinc(&sm.full[slot]);
+            __syncwarp();
             issued = i + 1;
-            prefetchMeta(i + 2);
+            if (i + 2 < nSteps) {
+                if (!waitRec(i + 2)) {
+                    ok = false;
+                    break;
+                }
+                prefetchMeta(i + 2);
+            }
             prefetchRec(i + 4);
-            cp_async_commit();
+            __syncwarp();
         }
+        if (!ok && lane == 0) atomicOr(T.status, kErrProducerWait);
         // drain: every copy this warp started has landed before the CTA exits
+        cp_async_commit();
         cp_async_wait<0>();
         __syncwarp();
-        for (int32_t j = max(0, issued - kStages); j < issued; ++j) {
+        bool drained = true;
+        for (int32_t j = max(0, issued - kStages); j < issued && drained; ++j) {
             if (chunkOf(j) == T.skipChunk) continue;
-            if (!mbar_wait(&sm.full[j % kStages], static_cast<uint32_t>(j / kStages) & 1u, T.timeoutNs)) {
-                if (lane == 0) atomicOr(T.status, kErrDrain);
-                break;
-            }
+            drained = mbar_wait(&sm.full[j % kStages], static_cast<uint32_t>(j / kStages) & 1u, T.timeoutNs);
         }
+        for (int32_t j = max(0, recIssued - kRecRing); j < recIssued && drained; ++j) drained = waitRec(j);
+        for (int32_t j = max(0, metaIssued - kMetaRing); j < metaIssued && drained; ++j) drained = waitMeta(j);
+        if (!drained && lane == 0) atomicOr(T.status, kErrDrain);
     } else {
         // ------------------------------------------------------------ consumers
         const int group = warp / kTilesPerChunk;

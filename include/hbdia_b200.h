@@ -59,8 +59,9 @@ typedef enum hbdia_value_storage {
     HBDIA_STORE_BF16_SCALED = 2
 } hbdia_value_storage;
 
-/* SpMV kernel choice (all give bit-identical y).  AUTO picks STAGED for
- * blockWidth 32 with 16-byte aligned x, else ROWWISE. */
+/* SpMV kernel choice (all give bit-identical y).  AUTO picks the kernel
+ * measured fastest on B200: WARP for blockWidth 32, else ROWWISE.  STAGED
+ * needs a 16-byte aligned x (else WARP runs). */
 typedef enum hbdia_kernel {
     HBDIA_KERNEL_AUTO = 0,
     HBDIA_KERNEL_ROWWISE = 1, /* one thread per row, any blockWidth             */
