@@ -44,7 +44,8 @@ WORKLOAD = dict(nx=256, ny=256, nz=256, center=26.0, neighbor=-1.0, extra_fracti
 METRIC = "SpMV HBM GB/s"
 UNIT = "GB/s"
 KERNEL_NAMES = {1: "spmv_rowwise<double,double>", 2: "spmv_bw32<double,double>",
-                3: "spmv_bw32_tma<double,double> (TMA-staged)"}
+                3: "spmv_bw32_tma<double,double> (TMA-staged)",
+                4: "spmv_bw32_pipe<double,double> (persistent, pipelined)"}
 
 
 def log(*a):
@@ -282,7 +283,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--unroll", type=int, default=0, choices=[0, 9, 27],
                     help="offsets in flight per lane in the staged kernel (0: default)")
-    ap.add_argument("--kernel", default=None, choices=["staged", "warp", "rowwise"],
+    ap.add_argument("--kernel", default=None, choices=["pipe", "staged", "warp", "rowwise"],
                     help="force one SpMV kernel (default: the library's choice)")
     ap.add_argument("--size", type=int, default=256,
                     help="grid edge of the stencil workload (256 is the benchmark; smaller sizes for profiling)")
@@ -313,7 +314,8 @@ def main():
     bytes_per_spmv = hbm_bytes_model(info)
     assert bytes_per_spmv == info.bytesPerSpmv, (bytes_per_spmv, info.bytesPerSpmv)
     if args.kernel:
-        m.setKernel({"staged": hb.KERNEL_STAGED, "warp": hb.KERNEL_WARP, "rowwise": hb.KERNEL_ROWWISE}[args.kernel])
+        m.setKernel({"pipe": hb.KERNEL_PIPE, "staged": hb.KERNEL_STAGED, "warp": hb.KERNEL_WARP,
+                     "rowwise": hb.KERNEL_ROWWISE}[args.kernel])
     if args.unroll:
         m.setTuning(hb.TUNE_UNROLL, args.unroll)
     xt = torch.from_numpy(x).cuda()

@@ -26,7 +26,7 @@ HBDIA_ERR_NOT_CONVERTED = -6
 HBDIA_ERR_UNSUPPORTED = -7
 HBDIA_ERR_DEVICE_TIMEOUT = -8
 
-KERNEL_AUTO, KERNEL_ROWWISE, KERNEL_WARP, KERNEL_STAGED = 0, 1, 2, 3
+KERNEL_AUTO, KERNEL_ROWWISE, KERNEL_WARP, KERNEL_STAGED, KERNEL_PIPE = 0, 1, 2, 3, 4
 TUNE_UNROLL = 1
 
 HBDIA_F64, HBDIA_F32 = 0, 1

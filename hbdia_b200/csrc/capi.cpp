@@ -393,7 +393,7 @@ int hbdia_matrix_device_status(const hbdia_matrix *m, int32_t *bits) {
 int hbdia_matrix_set_kernel(hbdia_matrix *m, int32_t kernel) {
     return guarded([&] {
         need(m != nullptr, HBDIA_ERR_INVALID_ARGUMENT, "null matrix");
-        need(kernel >= HBDIA_KERNEL_AUTO && kernel <= HBDIA_KERNEL_STAGED, HBDIA_ERR_INVALID_ARGUMENT,
+        need(kernel >= HBDIA_KERNEL_AUTO && kernel <= HBDIA_KERNEL_PIPE, HBDIA_ERR_INVALID_ARGUMENT,
              "unknown kernel");
         m->plan.kernel = kernel;
     });

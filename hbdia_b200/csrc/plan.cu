@@ -246,6 +246,21 @@ void launch_staged(const dev::TmaArgs<VT, XT> &T, int32_t numChunks, const XT *x
     dev::spmv_bw32_tma<VT, XT, U><<<grid, dev::kTmaThreads, smem, s>>>(T, x, y);
 }
 
+// Persistent grid: as many 256-thread CTAs as fit on all SMs at once (the
+// warps then walk the tiles grid-stride).
+template <typename VT, typename XT, int U>
+void launch_pipe(const dev::SpmvArgs<VT, XT> &a, int32_t numTiles, const XT *x, XT *y, cudaStream_t s) {
+    int dev = 0, sms = 0, perSm = 0;
+    check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
+    check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "cudaDeviceGetAttribute");
+    check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, dev::spmv_bw32_pipe<VT, XT, U>, 256, 0),
+               "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+    const int64_t ctasNeeded = (static_cast<int64_t>(numTiles) + 7) / 8;
+    const unsigned grid = static_cast<unsigned>(std::max<int64_t>(1, std::min<int64_t>(ctasNeeded,
+                                                                                       int64_t(sms) * std::max(1, perSm))));
+    dev::spmv_bw32_pipe<VT, XT, U><<<grid, 256, 0, s>>>(a, x, y);
+}
+
 template <typename VT, typename XT>
 void launch_typed(const DevicePlan &P, const void *x, void *y, cudaStream_t s) {
     dev::SpmvArgs<VT, XT> a;
@@ -277,6 +292,9 @@ void launch_typed(const DevicePlan &P, const void *x, void *y, cudaStream_t s) {
         T.skipChunk = P.skipChunk;
         if (P.unroll == 27) launch_staged<VT, XT, 27>(T, P.numChunks, xp, yp, s);
         else launch_staged<VT, XT, kUnroll>(T, P.numChunks, xp, yp, s);
+    } else if (kern == HBDIA_KERNEL_PIPE) {
+        if (P.unroll == 27) launch_pipe<VT, XT, 27>(a, P.numTiles, xp, yp, s);
+        else launch_pipe<VT, XT, kUnroll>(a, P.numTiles, xp, yp, s);
     } else if (kern == HBDIA_KERNEL_WARP) {
         const int64_t warpsPerCta = 8;
         const unsigned grid = static_cast<unsigned>((P.numTiles + warpsPerCta - 1) / warpsPerCta);
@@ -295,10 +313,14 @@ int32_t select_kernel(const DevicePlan &P, const void *x) {
     const bool aligned = (reinterpret_cast<uintptr_t>(x) & 15) == 0;
     // the staged kernel does row/column arithmetic in 32 bits (n <= 2^30)
     const bool stagedOk = bw32 && aligned && P.numChunks > 0 && P.n <= (1 << 30);
+    const bool pipeOk = bw32 && P.n <= (1 << 30);  // 32-bit row/column arithmetic
     switch (P.kernel) {
         case HBDIA_KERNEL_ROWWISE: return HBDIA_KERNEL_ROWWISE;
         case HBDIA_KERNEL_STAGED:
             if (stagedOk) return HBDIA_KERNEL_STAGED;
+            return bw32 ? HBDIA_KERNEL_WARP : HBDIA_KERNEL_ROWWISE;
+        case HBDIA_KERNEL_PIPE:
+            if (pipeOk) return HBDIA_KERNEL_PIPE;
             return bw32 ? HBDIA_KERNEL_WARP : HBDIA_KERNEL_ROWWISE;
         case HBDIA_KERNEL_WARP:
         default:  // AUTO: the fastest measured on B200 for blockWidth 32

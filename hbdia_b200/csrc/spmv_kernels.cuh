@@ -112,8 +112,9 @@ template <typename XT>
 __device__ __forceinline__ XT tile_coo(const int32_t *__restrict__ cooRow,
                                        const int32_t *__restrict__ cooCol,
                                        const XT *__restrict__ cooVal, int32_t e0, int32_t e1,
-                                       int64_t tileRow0, int lane, const XT *__restrict__ x) {
-    XT c = XT(0);
+                                       int64_t tileRow0, int lane, const XT *__restrict__ x,
+                                       XT c = XT(0)) {
+    // c: this lane's row sum of the entries before e0 (continued in order)
     for (int32_t base = e0; base < e1; base += 32) {
         const int32_t e = base + lane;
         int lr = -1;
@@ -190,6 +191,122 @@ spmv_bw32(const SpmvArgs<VT, XT> a, const XT *__restrict__ x, XT *__restrict__ y
         sum = add_rn(sum, tile_coo<XT>(a.cooRow, a.cooCol, a.cooVal, e0, e1, row0, lane, x));
     }
     if (row < a.n) __stcs(y + row, sum);
+}
+
+// ---------------------------------------------------------------------------
+// blockWidth == 32, persistent and software-pipelined across tiles.  Warp g of
+// W walks tiles g, g + W, ... (neighbouring warps stay on neighbouring tiles,
+// so x lines are shared through L1/L2).  While it computes tile t it already
+// has tile t+W's block / COO pointers and first 32 offsets in registers (loaded
+// during t-W) and the first 32 COO entries of tile t plus their x values in
+// flight, so nearly every stall is a stall on value loads.  Same arithmetic
+// and order as spmv_bw32.
+struct TileMeta {
+    int32_t k0, k1, c0, c1;
+};
+
+template <typename VT, typename XT>
+__device__ __forceinline__ TileMeta load_meta(const SpmvArgs<VT, XT> &a, int32_t t) {
+    TileMeta m{0, 0, 0, 0};
+    if (t < a.numBlocks) {
+        m.k0 = __ldg(a.blkOff + t);
+        m.k1 = __ldg(a.blkOff + t + 1);
+    }
+    if (a.hasCoo && t < a.numTiles) {
+        m.c0 = __ldg(a.cooTile + t);
+        m.c1 = __ldg(a.cooTile + t + 1);
+    }
+    return m;
+}
+
+template <typename VT, typename XT, int U>
+__global__ void __launch_bounds__(256)
+spmv_bw32_pipe(const SpmvArgs<VT, XT> a, const XT *__restrict__ x, XT *__restrict__ y) {
+    const int lane = threadIdx.x & 31;
+    const int32_t W = static_cast<int32_t>((static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5);
+    int32_t t = static_cast<int32_t>((static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5);
+    if (t >= a.numTiles) return;  // warp-uniform
+    const uint32_t n = static_cast<uint32_t>(a.n);
+    TileMeta m = load_meta(a, t);
+    int32_t offNext = (lane < m.k1 - m.k0) ? __ldg(a.offs + m.k0 + lane) : 0;
+    while (t < a.numTiles) {
+        const int32_t tn = t + W;
+        const TileMeta mn = tn < a.numTiles ? load_meta(a, tn) : TileMeta{0, 0, 0, 0};
+        const int32_t row0 = t * 32;
+        const int32_t row = row0 + lane;
+        // first 32 COO entries of this tile and their x values, consumed at the end
+        int lr = -1;
+        XT cv = XT(0), cx = XT(0);
+        int32_t ccol = 0;
+        const int32_t ce = m.c0 + lane;
+        const bool hasC = ce < min(m.c1, m.c0 + 32);
+        if (hasC) {
+            lr = __ldg(a.cooRow + ce) - row0;
+            ccol = __ldg(a.cooCol + ce);
+            cv = __ldg(a.cooVal + ce);
+        }
+        XT sum = XT(0);
+        const float s = a.scale && t < a.numBlocks ? __ldg(a.scale + t) : 1.0f;
+        int32_t myoff = offNext;
+        bool gathered = false;
+        for (int32_t kb = m.k0; kb < m.k1; kb += 32) {
+            const int cnt = min(32, m.k1 - kb);
+            if (kb != m.k0) myoff = lane < cnt ? __ldg(a.offs + kb + lane) : 0;
+            const VT *vp = a.vals + static_cast<int64_t>(kb) * 32 + lane;
+            int j = 0;
+            for (; j + U <= cnt; j += U) {
+                VT v[U];
+                XT xv[U];
+                bool ok[U];
+                int32_t col[U];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    col[u] = row + __shfl_sync(kFull, myoff, j + u);
+                    ok[u] = static_cast<uint32_t>(col[u]) < n;
+                    v[u] = ld_stream(vp + (j + u) * 32);
+                    xv[u] = XT(0);
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u)
+                    if (ok[u]) xv[u] = __ldg(x + col[u]);
+                if (!gathered) {  // COO columns have arrived by now
+                    if (hasC) cx = __ldg(x + ccol);
+                    gathered = true;
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const XT vv = widen<XT>(v[u], s);
+                    if (ok[u] && vv != XT(0)) sum = fma_rn(vv, xv[u], sum);
+                }
+            }
+            for (; j < cnt; ++j) {
+                const int32_t col = row + __shfl_sync(kFull, myoff, j);
+                const XT vv = widen<XT>(ld_stream(vp + j * 32), s);
+                if (static_cast<uint32_t>(col) < n && vv != XT(0)) sum = fma_rn(vv, __ldg(x + col), sum);
+            }
+        }
+        // next tile's first offsets (its pointers arrived during this tile)
+        offNext = (lane < mn.k1 - mn.k0) ? __ldg(a.offs + mn.k0 + lane) : 0;
+        if (a.hasCoo) {
+            if (!gathered && hasC) cx = __ldg(x + ccol);
+            XT c = XT(0);
+            {
+                const XT p = mul_rn(cv, cx);
+                const int mcnt = min(32, m.c1 - m.c0);
+                for (int q = 0; q < mcnt; ++q) {
+                    const int rt = __shfl_sync(kFull, lr, q);
+                    const XT pt = __shfl_sync(kFull, p, q);
+                    if (rt == lane) c = add_rn(c, pt);
+                }
+            }
+            if (m.c1 - m.c0 > 32)  // rare: more than 32 entries in the tile, continue in order
+                c = tile_coo<XT>(a.cooRow, a.cooCol, a.cooVal, m.c0 + 32, m.c1, row0, lane, x, c);
+            sum = add_rn(sum, c);
+        }
+        if (row < a.n) __stcs(y + row, sum);
+        t = tn;
+        m = mn;
+    }
 }
 
 }  // namespace dev

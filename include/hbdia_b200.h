@@ -66,7 +66,8 @@ typedef enum hbdia_kernel {
     HBDIA_KERNEL_AUTO = 0,
     HBDIA_KERNEL_ROWWISE = 1, /* one thread per row, any blockWidth             */
     HBDIA_KERNEL_WARP = 2,    /* one warp per 32-row block, blockWidth 32       */
-    HBDIA_KERNEL_STAGED = 3   /* persistent TMA-staged pipeline, blockWidth 32  */
+    HBDIA_KERNEL_STAGED = 3,  /* persistent TMA-staged pipeline, blockWidth 32  */
+    HBDIA_KERNEL_PIPE = 4     /* persistent warp per block, pipelined across blocks, blockWidth 32 */
 } hbdia_kernel;
 
 typedef struct hbdia_matrix hbdia_matrix; /* HBDIA<T>       (include/Format/HBDIA.hpp:24-291)      */

@@ -108,6 +108,7 @@ class Restated:
         lib.orc_destroy.argtypes = [_vp]
         lib.orc_spmv_f64.argtypes = [_vp, _vp, _vp]
         lib.orc_spmv_f32.argtypes = [_vp, _vp, _vp]
+        lib.orc_spmv_f64_values.argtypes = [_vp, _vp, _vp, _vp]
         lib.orc_coo_spmv_f64.argtypes = [_vp, _vp, _vp, ctypes.c_int64, _vp, ctypes.c_int32, _vp]
         self.lib = lib
 
@@ -155,6 +156,34 @@ class _OracleMatrix:
         f = self._o.lib.orc_spmv_f32 if self.dtype == np.float32 else self._o.lib.orc_spmv_f64
         f(self._h, _ptr(x), _ptr(y))
         return y
+
+    def spmv_with_values(self, values: np.ndarray, x: np.ndarray) -> np.ndarray:
+        """Double SpMV with the blocked-DIA values replaced (reduced-precision storage)."""
+        values = np.ascontiguousarray(values, np.float64)
+        x = np.ascontiguousarray(x, np.float64)
+        y = np.zeros_like(x)
+        self._o.lib.orc_spmv_f64_values(self._h, _ptr(values), _ptr(y), _ptr(x))
+        return y
+
+
+def bf16_block_scaled(data: np.ndarray, block_start: np.ndarray, bw: int) -> np.ndarray:
+    """Values as stored with bfloat16 + one float scale per block, widened
+    back to double: scale = float(max |v| of the block) (1 if all zero),
+    q = bf16_round_nearest_even(float(v / scale)), value = double(q) * scale."""
+    out = np.empty_like(data)
+    for b in range(len(block_start) - 1):
+        s0, s1 = int(block_start[b]) * bw, int(block_start[b + 1]) * bw
+        if s1 == s0:
+            continue
+        v = data[s0:s1]
+        m = float(np.max(np.abs(v)))
+        s = np.float32(m) if m > 0 else np.float32(1.0)
+        q = (v / np.float64(s)).astype(np.float32)
+        bits = q.view(np.uint32).astype(np.uint64)
+        bits = ((bits + 0x7FFF + ((bits >> 16) & 1)) >> 16) << 16
+        f = bits.astype(np.uint32).view(np.float32)
+        out[s0:s1] = f.astype(np.float64) * np.float64(s)
+    return out
 
 
 # --------------------------------------------------------------------------- reference

@@ -267,6 +267,15 @@ void orc_destroy(orc_layout *h) {
 void orc_spmv_f64(const orc_layout *h, const double *x, double *y) { ORC_SPMV_BODY(double, fma) }
 void orc_spmv_f32(const orc_layout *h, const float *x, float *y) { ORC_SPMV_BODY(float, fmaf) }
 
+/* The same double-precision SpMV with the blocked-DIA values replaced by
+ * `values` (same layout): the expected result of reduced-precision value
+ * storage, where each stored value is first rounded and then widened. */
+void orc_spmv_f64_values(const orc_layout *h, const double *values, double *y, const double *x) {
+    orc_layout g = *h;
+    g.data = (void *)values;
+    orc_spmv_f64(&g, x, y);
+}
+
 void orc_coo_spmv_f64(const int32_t *rows, const int32_t *cols, const double *vals,
                       int64_t nnz, const double *x, int32_t numRows, double *y) {
     /* single-thread instance of src/Operations/HBDIASpMV.cpp:36-99 */

@@ -38,6 +38,8 @@ void orc_destroy(orc_layout *h);
  * (src/Operations/HBDIASpMV.cu:77-88).  x and y hold numRows elements. */
 void orc_spmv_f64(const orc_layout *h, const double *x, double *y);
 void orc_spmv_f32(const orc_layout *h, const float *x, float *y);
+/* orc_spmv_f64 with the blocked-DIA values taken from `values` instead. */
+void orc_spmv_f64_values(const orc_layout *h, const double *values, double *y, const double *x);
 
 /* Whole-matrix COO SpMV over row-sorted COO, one thread, in the order of
  * cpu_coo_spmv_kernel (src/Operations/HBDIASpMV.cpp:36-99).  Rows without

@@ -22,7 +22,7 @@ def _scaled_err(y, yref, rows, cols, vals, x):
     return np.abs(y - yref) / np.maximum(scale, np.finfo(float).tiny)
 
 
-KERNELS = {"staged": 3, "warp": 2, "rowwise": 1}
+KERNELS = {"pipe": 4, "staged": 3, "warp": 2, "rowwise": 1}
 
 
 @pytest.fixture(params=list(KERNELS), ids=list(KERNELS))
