@@ -65,6 +65,7 @@ void build_plan(const HostLayout<T> &L, int storage, DevicePlan &P) {
     Q.kernel = P.kernel;  // settings survive a rebuild
     Q.waitTimeoutNs = P.waitTimeoutNs;
     Q.skipChunk = P.skipChunk;
+    Q.unroll = P.unroll;
     free_plan(P);
     Q.dtype = std::is_same<T, float>::value ? HBDIA_F32 : HBDIA_F64;
     if (storage != HBDIA_STORE_NATIVE && Q.dtype != HBDIA_F64)
@@ -248,17 +249,26 @@ void launch_staged(const dev::TmaArgs<VT, XT> &T, int32_t numChunks, const XT *x
 
 // Persistent grid: as many 256-thread CTAs as fit on all SMs at once (the
 // warps then walk the tiles grid-stride).
-template <typename VT, typename XT, int U>
-void launch_pipe(const dev::SpmvArgs<VT, XT> &a, int32_t numTiles, const XT *x, XT *y, cudaStream_t s) {
+template <typename VT, typename XT, typename Kernel>
+void launch_pipe(Kernel kernel, const dev::SpmvArgs<VT, XT> &a, int32_t numTiles, const XT *x, XT *y,
+                 cudaStream_t s) {
     int dev = 0, sms = 0, perSm = 0;
     check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
     check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "cudaDeviceGetAttribute");
-    check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, dev::spmv_bw32_pipe<VT, XT, U>, 256, 0),
+    check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kernel, 256, 0),
                "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
     const int64_t ctasNeeded = (static_cast<int64_t>(numTiles) + 7) / 8;
     const unsigned grid = static_cast<unsigned>(std::max<int64_t>(1, std::min<int64_t>(ctasNeeded,
                                                                                        int64_t(sms) * std::max(1, perSm))));
-    dev::spmv_bw32_pipe<VT, XT, U><<<grid, 256, 0, s>>>(a, x, y);
+    kernel<<<grid, 256, 0, s>>>(a, x, y);
+}
+
+template <typename VT, typename XT>
+void launch_pipe_tuned(const DevicePlan &P, const dev::SpmvArgs<VT, XT> &a, const XT *x, XT *y, cudaStream_t s) {
+    // Forcing 4-6 CTAs per SM through __launch_bounds__ made ptxas spill and
+    // ran 3-45% slower on B200; the compiler's own register choice is kept.
+    if (P.unroll == 27) return launch_pipe(dev::spmv_bw32_pipe<VT, XT, 27>, a, P.numTiles, x, y, s);
+    return launch_pipe(dev::spmv_bw32_pipe<VT, XT, kUnroll>, a, P.numTiles, x, y, s);
 }
 
 template <typename VT, typename XT>
@@ -293,8 +303,7 @@ void launch_typed(const DevicePlan &P, const void *x, void *y, cudaStream_t s) {
         if (P.unroll == 27) launch_staged<VT, XT, 27>(T, P.numChunks, xp, yp, s);
         else launch_staged<VT, XT, kUnroll>(T, P.numChunks, xp, yp, s);
     } else if (kern == HBDIA_KERNEL_PIPE) {
-        if (P.unroll == 27) launch_pipe<VT, XT, 27>(a, P.numTiles, xp, yp, s);
-        else launch_pipe<VT, XT, kUnroll>(a, P.numTiles, xp, yp, s);
+        launch_pipe_tuned<VT, XT>(P, a, xp, yp, s);
     } else if (kern == HBDIA_KERNEL_WARP) {
         const int64_t warpsPerCta = 8;
         const unsigned grid = static_cast<unsigned>((P.numTiles + warpsPerCta - 1) / warpsPerCta);
@@ -322,8 +331,9 @@ int32_t select_kernel(const DevicePlan &P, const void *x) {
         case HBDIA_KERNEL_PIPE:
             if (pipeOk) return HBDIA_KERNEL_PIPE;
             return bw32 ? HBDIA_KERNEL_WARP : HBDIA_KERNEL_ROWWISE;
-        case HBDIA_KERNEL_WARP:
+        case HBDIA_KERNEL_WARP: return bw32 ? HBDIA_KERNEL_WARP : HBDIA_KERNEL_ROWWISE;
         default:  // AUTO: the fastest measured on B200 for blockWidth 32
+            if (pipeOk) return HBDIA_KERNEL_PIPE;
             return bw32 ? HBDIA_KERNEL_WARP : HBDIA_KERNEL_ROWWISE;
     }
 }

@@ -60,8 +60,9 @@ typedef enum hbdia_value_storage {
 } hbdia_value_storage;
 
 /* SpMV kernel choice (all give bit-identical y).  AUTO picks the kernel
- * measured fastest on B200: WARP for blockWidth 32, else ROWWISE.  STAGED
- * needs a 16-byte aligned x (else WARP runs). */
+ * measured fastest on B200: PIPE for blockWidth 32, else ROWWISE.  STAGED
+ * needs a 16-byte aligned x (else WARP runs); PIPE and STAGED need
+ * numRows <= 2^30. */
 typedef enum hbdia_kernel {
     HBDIA_KERNEL_AUTO = 0,
     HBDIA_KERNEL_ROWWISE = 1, /* one thread per row, any blockWidth             */
@@ -237,8 +238,8 @@ int hbdia_matrix_set_kernel(hbdia_matrix *m, int32_t kernel);
 int hbdia_matrix_selected_kernel(const hbdia_matrix *m, const void *x, int32_t *kernel);
 
 /* Kernel tuning knobs (used by the autotuner; results stay bit-identical).
- * HBDIA_TUNE_UNROLL: offsets in flight per lane in the staged kernel
- * (0 = default 9, or 27). */
+ * HBDIA_TUNE_UNROLL: offsets in flight per lane in the staged and pipelined
+ * kernels (0 = default 9, or 27). */
 typedef enum hbdia_tuning_key { HBDIA_TUNE_UNROLL = 1 } hbdia_tuning_key;
 int hbdia_matrix_set_tuning(hbdia_matrix *m, int32_t key, int32_t value);
 

@@ -277,7 +277,7 @@ def test_kernel_selection(lib):
     m = lib.HBDIA(rows, cols, vals, n, n)
     m.convertToHBDIAFormat(32, 2)
     xt = torch.zeros(n + 2, dtype=torch.float64, device="cuda")
-    assert m.selectedKernel(xt.data_ptr()) == lib.KERNEL_WARP          # AUTO: fastest measured
+    assert m.selectedKernel(xt.data_ptr()) == lib.KERNEL_PIPE          # AUTO: fastest measured
     m.setKernel(lib.KERNEL_STAGED)
     assert m.selectedKernel(xt.data_ptr()) == lib.KERNEL_STAGED
     assert m.selectedKernel(xt.data_ptr() + 8) == lib.KERNEL_WARP      # x not 16-byte aligned
