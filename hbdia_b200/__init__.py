@@ -18,8 +18,8 @@ from typing import List, Optional, Sequence
 import numpy as np
 
 from . import _lib
-from ._lib import (KERNEL_AUTO, KERNEL_PIPE, KERNEL_ROWWISE, KERNEL_STAGED, KERNEL_WARP, TUNE_UNROLL,
-                   HBDIACudaError,
+from ._lib import (KERNEL_AUTO, KERNEL_PIPE, KERNEL_ROWWISE, KERNEL_STAGED, KERNEL_WARP, TUNE_SPMM_TILE,
+                   TUNE_UNROLL, HBDIACudaError,
                    HBDIADeviceTimeout, STORE_BF16_SCALED, STORE_F32, STORE_NATIVE, MatrixInfo,
                    check as _check, load as _load)
 
@@ -225,6 +225,16 @@ class HBDIA:
         """Kernel tuning knob (TUNE_UNROLL: 0, 9 or 27); results stay bit-identical."""
         _check(_load().hbdia_matrix_set_tuning(self._h, int(key), int(value)))
 
+    def autotune(self, X_ptr: int, Y_ptr: int, k: int = 1, ldx: int = 0, ldy: int = 0,
+                 stream: Optional[int] = None, force: bool = False) -> "_lib.TuneResult":
+        """Time this matrix's SpMV (k = 1) or SpMM (k > 1) configurations on the
+        given device buffers, keep the fastest (see hbdia_matrix_autotune)."""
+        r = _lib.TuneResult()
+        _check(_load().hbdia_matrix_autotune(self._h, ctypes.c_void_p(X_ptr), ldx or k, ctypes.c_void_p(Y_ptr),
+                                             ldy or k, int(k), _stream_arg(stream), int(bool(force)),
+                                             ctypes.byref(r)))
+        return r
+
     def setWaitTimeout(self, nanoseconds: int) -> None:
         _check(_load().hbdia_matrix_set_wait_timeout(self._h, int(nanoseconds)))
 
@@ -308,6 +318,11 @@ def spmv_device(matrix: HBDIA, x_ptr: int, y_ptr: int, stream: Optional[int] = N
     0 included, are passed as they are)."""
     _check(_load().hbdia_spmv_device(matrix.handle, ctypes.c_void_p(x_ptr), ctypes.c_void_p(y_ptr),
                                      _stream_arg(stream)))
+
+
+def autotune_clear() -> None:
+    """Forget the process-wide autotuning table."""
+    _check(_load().hbdia_autotune_clear())
 
 
 def spmm_device(matrix: HBDIA, X_ptr: int, ldx: int, Y_ptr: int, ldy: int, k: int,

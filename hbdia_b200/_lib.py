@@ -27,7 +27,7 @@ HBDIA_ERR_UNSUPPORTED = -7
 HBDIA_ERR_DEVICE_TIMEOUT = -8
 
 KERNEL_AUTO, KERNEL_ROWWISE, KERNEL_WARP, KERNEL_STAGED, KERNEL_PIPE = 0, 1, 2, 3, 4
-TUNE_UNROLL = 1
+TUNE_UNROLL, TUNE_SPMM_TILE = 1, 2
 
 HBDIA_F64, HBDIA_F32 = 0, 1
 STORE_NATIVE, STORE_F32, STORE_BF16_SCALED = 0, 1, 2
@@ -42,6 +42,11 @@ class MatrixInfo(ctypes.Structure):
         ("numSlots", c_i64), ("numCoo", c_i64), ("histogramLength", c_i32), ("storage", c_i32),
         ("deviceBytes", c_i64), ("bytesPerSpmv", c_i64),
     ]
+
+
+class TuneResult(ctypes.Structure):
+    _fields_ = [("kernel", c_i32), ("unroll", c_i32), ("spmmTile", c_i32), ("fromCache", c_i32),
+                ("msPerCall", ctypes.c_float)]
 
 
 class HBDIACudaError(RuntimeError):
@@ -89,6 +94,9 @@ _SIGS = [
     ("hbdia_matrix_selected_kernel", ctypes.c_int, [c_vp, c_vp, c_i32p]),
     ("hbdia_matrix_set_wait_timeout", ctypes.c_int, [c_vp, c_u64]),
     ("hbdia_matrix_set_tuning", ctypes.c_int, [c_vp, c_i32, c_i32]),
+    ("hbdia_matrix_autotune", ctypes.c_int, [c_vp, c_vp, c_i64, c_vp, c_i64, c_i32, c_vp, c_i32,
+                                             ctypes.POINTER(TuneResult)]),
+    ("hbdia_autotune_clear", ctypes.c_int, []),
     ("hbdia_matrix_test_skip_chunk", ctypes.c_int, [c_vp, c_i32]),
     ("hbdia_vector_create", ctypes.c_int, [ctypes.c_int, c_vp, c_i64, c_vpp]),
     ("hbdia_vector_destroy", None, [c_vp]),

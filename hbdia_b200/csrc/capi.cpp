@@ -415,8 +415,30 @@ int hbdia_matrix_set_tuning(hbdia_matrix *m, int32_t key, int32_t value) {
             m->plan.unroll = value;
             return;
         }
+        if (key == HBDIA_TUNE_SPMM_TILE) {
+            need(value == 0 || value == 4 || value == 8 || value == 16 || value == 32, HBDIA_ERR_INVALID_ARGUMENT,
+                 "SpMM tile must be 0, 4, 8, 16 or 32");
+            m->plan.spmmTileForced = value;
+            return;
+        }
         throw Error(HBDIA_ERR_INVALID_ARGUMENT, "unknown tuning key");
     });
+}
+
+int hbdia_matrix_autotune(hbdia_matrix *m, const void *X, int64_t ldx, void *Y, int64_t ldy, int32_t k,
+                          void *stream, int32_t force, hbdia_tune_result *out) {
+    return guarded([&] {
+        need(m && X && Y, HBDIA_ERR_INVALID_ARGUMENT, "null argument");
+        hbdia_tune_result r;
+        std::memset(&r, 0, sizeof(r));
+        hbdia::autotune(m->plan, X, ldx, Y, ldy, k, stream, force != 0, &r.kernel, &r.unroll, &r.spmmTile,
+                        &r.fromCache, &r.msPerCall);
+        if (out) *out = r;
+    });
+}
+
+int hbdia_autotune_clear(void) {
+    return guarded([&] { hbdia::autotune_clear_cache(); });
 }
 
 int hbdia_matrix_set_wait_timeout(hbdia_matrix *m, uint64_t ns) {

@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cstdint>
+#include <map>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -94,6 +95,8 @@ struct DevicePlan {
     uint64_t waitTimeoutNs = 2000000000ull;
     int32_t skipChunk = -1;              // test hook of the staged kernel
     int32_t unroll = 0;                  // offsets in flight per lane (0: default)
+    std::map<int32_t, int32_t> spmmTile; // autotuned RHS tile per k
+    int32_t spmmTileForced = 0;          // HBDIA_TUNE_SPMM_TILE (0: autotuned / default)
 };
 
 void build_chunk_schedule(int32_t n, int32_t numBlocks, int32_t numTiles, const int32_t *blkOff,
@@ -109,6 +112,12 @@ void free_plan(DevicePlan &P);
 void launch_spmv(const DevicePlan &P, const void *x, void *y, void *stream);
 void launch_spmm(const DevicePlan &P, const void *X, int64_t ldx, void *Y, int64_t ldy, int32_t k,
                  void *stream);
+void launch_spmm_tile(const DevicePlan &P, const void *X, int64_t ldx, void *Y, int64_t ldy, int32_t k,
+                      int32_t tile, void *stream);
+int32_t default_spmm_tile(int32_t k);
+void autotune(DevicePlan &P, const void *X, int64_t ldx, void *Y, int64_t ldy, int32_t k, void *stream, bool force,
+              int32_t *kernel, int32_t *unroll, int32_t *tile, int32_t *fromCache, float *ms);
+void autotune_clear_cache();
 // throws Error(HBDIA_ERR_CUDA) with the CUDA error string
 void check_cuda(int err, const char *what);
 

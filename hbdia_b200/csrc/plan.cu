@@ -21,6 +21,7 @@
 #include "hbdia_internal.hpp"
 #include "spmv_kernels.cuh"
 #include "spmv_tma.cuh"
+#include "spmm_kernels.cuh"
 
 namespace hbdia {
 
@@ -228,6 +229,26 @@ template void build_plan<float>(const HostLayout<float> &, int, DevicePlan &);
 
 namespace {
 
+template <typename VT, typename XT>
+dev::SpmvArgs<VT, XT> make_args(const DevicePlan &P) {
+    dev::SpmvArgs<VT, XT> a;
+    a.vals = static_cast<const VT *>(P.vals);
+    a.scale = P.scale;
+    a.offs = P.offs;
+    a.blkOff = P.blkOff;
+    a.cooRow = P.cooRow;
+    a.cooCol = P.cooCol;
+    a.cooVal = static_cast<const XT *>(P.cooVal);
+    a.cooRowPtr = P.cooRowPtr;
+    a.cooTile = P.cooTile;
+    a.n = P.n;
+    a.bw = P.bw;
+    a.numBlocks = P.numBlocks;
+    a.numTiles = P.numTiles;
+    a.hasCoo = P.nCoo > 0;
+    return a;
+}
+
 // One CTA per SM (the stage ring fills the SM's shared memory).  The
 // dynamic shared-memory opt-in is a per-device function attribute.
 template <typename VT, typename XT, int U>
@@ -273,21 +294,7 @@ void launch_pipe_tuned(const DevicePlan &P, const dev::SpmvArgs<VT, XT> &a, cons
 
 template <typename VT, typename XT>
 void launch_typed(const DevicePlan &P, const void *x, void *y, cudaStream_t s) {
-    dev::SpmvArgs<VT, XT> a;
-    a.vals = static_cast<const VT *>(P.vals);
-    a.scale = P.scale;
-    a.offs = P.offs;
-    a.blkOff = P.blkOff;
-    a.cooRow = P.cooRow;
-    a.cooCol = P.cooCol;
-    a.cooVal = static_cast<const XT *>(P.cooVal);
-    a.cooRowPtr = P.cooRowPtr;
-    a.cooTile = P.cooTile;
-    a.n = P.n;
-    a.bw = P.bw;
-    a.numBlocks = P.numBlocks;
-    a.numTiles = P.numTiles;
-    a.hasCoo = P.nCoo > 0;
+    const dev::SpmvArgs<VT, XT> a = make_args<VT, XT>(P);
     const XT *xp = static_cast<const XT *>(x);
     XT *yp = static_cast<XT *>(y);
     const int32_t kern = select_kernel(P, x);
@@ -353,8 +360,64 @@ void launch_spmv(const DevicePlan &P, const void *x, void *y, void *stream) {
     }
 }
 
-void launch_spmm(const DevicePlan &, const void *, int64_t, void *, int64_t, int32_t, void *) {
-    throw Error(HBDIA_ERR_UNSUPPORTED, "SpMM is not built yet");
+namespace {
+
+template <typename VT, typename XT, int KT>
+void launch_spmm_kt(const DevicePlan &P, const dev::SpmvArgs<VT, XT> &a, const XT *X, int64_t ldx, XT *Y,
+                    int64_t ldy, int32_t k, cudaStream_t s) {
+    if (P.bw == 32) {
+        const unsigned grid = static_cast<unsigned>((static_cast<int64_t>(P.numTiles) + 7) / 8);
+        dev::spmm_bw32<VT, XT, KT><<<grid, 256, 0, s>>>(a, X, ldx, Y, ldy, k);
+    } else {
+        const unsigned grid = static_cast<unsigned>((static_cast<int64_t>(P.n) + 255) / 256);
+        dev::spmm_rowwise<VT, XT, KT><<<grid, 256, 0, s>>>(a, X, ldx, Y, ldy, k);
+    }
+}
+
+template <typename VT, typename XT>
+void launch_spmm_typed(const DevicePlan &P, const void *X, int64_t ldx, void *Y, int64_t ldy, int32_t k,
+                       int32_t tile, cudaStream_t s) {
+    dev::SpmvArgs<VT, XT> a = make_args<VT, XT>(P);
+    const XT *xp = static_cast<const XT *>(X);
+    XT *yp = static_cast<XT *>(Y);
+    switch (tile) {
+        case 4: launch_spmm_kt<VT, XT, 4>(P, a, xp, ldx, yp, ldy, k, s); break;
+        case 8: launch_spmm_kt<VT, XT, 8>(P, a, xp, ldx, yp, ldy, k, s); break;
+        case 16: launch_spmm_kt<VT, XT, 16>(P, a, xp, ldx, yp, ldy, k, s); break;
+        default: launch_spmm_kt<VT, XT, 32>(P, a, xp, ldx, yp, ldy, k, s); break;
+    }
+    check_cuda(cudaGetLastError(), "SpMM launch");
+}
+
+}  // namespace
+
+int32_t default_spmm_tile(int32_t k) {
+    // smallest supported tile covering k, at most 16 (32 costs occupancy)
+    if (k <= 4) return 4;
+    if (k <= 8) return 8;
+    return 16;
+}
+
+void launch_spmm_tile(const DevicePlan &P, const void *X, int64_t ldx, void *Y, int64_t ldy, int32_t k,
+                      int32_t tile, void *stream) {
+    if (!P.base) throw Error(HBDIA_ERR_NOT_CONVERTED, "matrix has no device layout");
+    if (!X || !Y) throw Error(HBDIA_ERR_INVALID_ARGUMENT, "null matrix pointer");
+    if (k <= 0 || ldx < k || ldy < k) throw Error(HBDIA_ERR_INVALID_ARGUMENT, "need k > 0 and ldx, ldy >= k");
+    cudaStream_t s = static_cast<cudaStream_t>(stream ? stream : P.stream);
+    if (P.dtype == HBDIA_F32) launch_spmm_typed<float, float>(P, X, ldx, Y, ldy, k, tile, s);
+    else if (P.storage == HBDIA_STORE_F32) launch_spmm_typed<float, double>(P, X, ldx, Y, ldy, k, tile, s);
+    else if (P.storage == HBDIA_STORE_BF16_SCALED)
+        launch_spmm_typed<__nv_bfloat16, double>(P, X, ldx, Y, ldy, k, tile, s);
+    else launch_spmm_typed<double, double>(P, X, ldx, Y, ldy, k, tile, s);
+}
+
+void launch_spmm(const DevicePlan &P, const void *X, int64_t ldx, void *Y, int64_t ldy, int32_t k, void *stream) {
+    int32_t tile = P.spmmTileForced;
+    if (!tile) {
+        auto it = P.spmmTile.find(k);
+        tile = it != P.spmmTile.end() ? it->second : default_spmm_tile(k);
+    }
+    launch_spmm_tile(P, X, ldx, Y, ldy, k, tile, stream);
 }
 
 }  // namespace hbdia

@@ -1,0 +1,129 @@
+"""Benchmark suite for the configurations beside the headline SpMV.
+
+    python -m hbdia_b200.suite precision   # banded n = 8M, FP64 / FP32 / BF16-scaled value storage
+    python -m hbdia_b200.suite spmm        # 7-point Laplacian 128^3, k in {4, 16, 32}, FP64 and FP32 storage
+
+Each measurement prints one JSON line.  Times are CUDA-event device times on
+a dedicated stream after warm-up; inputs exceed L2 unless stated.  Accuracy
+is the maximum over rows of |y - y_fp64| / sum_j |a_ij x_j| against the FP64
+SpMV of the same matrix (this library's, which tests/ pin bit for bit to the
+oracle).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import sys
+
+import numpy as np
+
+PEAK_NOTE = "fraction of the measured HBM copy bandwidth (MEASURED_PEAKS.json)"
+
+
+def _peak():
+    import os
+    p = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"])
+    except Exception:
+        return 6650.0
+
+
+def _time(fn, stream, reps=20, warmup=3):
+    import torch
+    for _ in range(warmup):
+        fn()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(reps):
+        fn()
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def _scaled_err(y, yref, rows, cols, vals, x):
+    scale = np.zeros(len(y))
+    np.add.at(scale, rows, np.abs(vals * x[cols]))
+    return float(np.max(np.abs(y - yref) / np.maximum(scale, np.finfo(float).tiny)))
+
+
+def precision(args):
+    import torch
+    import hbdia_b200 as hb
+    n = args.n
+    offs = [0, 1, -1, 2, -2, 64, -64, 4096, -4096]
+    rows, cols, vals = hb.generate_banded(n, offs, 0.5, 1.5, 0.3, 0.002, 2)
+    x = hb.fill_uniform(n, -1.0, 1.0, 2)
+    xt = torch.from_numpy(x).cuda()
+    stream = torch.cuda.Stream()
+    yref = None
+    base_rate = None
+    for name, st in (("fp64", hb.STORE_NATIVE), ("fp32", hb.STORE_F32), ("bf16_scaled", hb.STORE_BF16_SCALED)):
+        m = hb.HBDIA(rows, cols, vals, n, n)
+        m.convertToHBDIAFormat(32, 2, upload=False)
+        m.prepareForGPU(st)
+        yt = torch.zeros(n, dtype=torch.float64, device="cuda")
+        ms = _time(lambda: hb.spmv_device(m, xt.data_ptr(), yt.data_ptr(), stream.cuda_stream), stream)
+        m.synchronize()
+        y = yt.cpu().numpy()
+        if yref is None:
+            yref = y
+            base_rate = 1e3 / ms
+        err = _scaled_err(y, yref, rows, cols, vals, x)
+        b = m.bytesPerSpmv()
+        print(json.dumps({"suite": "precision", "workload": f"banded n={n} offsets {offs}, drop 0.3, 0.2% scattered",
+                          "storage": name, "accumulate": "fp64", "ms_per_spmv": ms, "spmv_per_s": 1e3 / ms,
+                          "speedup_vs_fp64": (1e3 / ms) / base_rate, "bytes_per_spmv": b,
+                          "gbs": b / (ms / 1e3) / 1e9, "frac_of_peak": b / (ms / 1e3) / 1e9 / _peak(),
+                          "max_scaled_err_vs_fp64": err, "nnz": int(len(vals))}), flush=True)
+        del m
+
+
+def spmm(args):
+    import torch
+    import hbdia_b200 as hb
+    g = args.grid
+    n = g ** 3
+    rows, cols, vals = hb.generate_stencil7(g, g, g, 6.0, -1.0)
+    stream = torch.cuda.Stream()
+    for stname, st in (("fp64", hb.STORE_NATIVE), ("fp32", hb.STORE_F32)):
+        m = hb.HBDIA(rows, cols, vals, n, n)
+        m.convertToHBDIAFormat(32, 2, upload=False)
+        m.prepareForGPU(st)
+        info = m.info()
+        vbytes = info.numSlots * (8 if st == hb.STORE_NATIVE else 4) + 4 * info.totalOffsets + 4 * (info.numBlocks + 1)
+        for k in (4, 16, 32):
+            X = torch.from_numpy(np.random.default_rng(3).uniform(-1, 1, (n, k))).cuda().contiguous()
+            Y = torch.zeros((n, k), dtype=torch.float64, device="cuda")
+            tune = m.autotune(X.data_ptr(), Y.data_ptr(), k=k, stream=stream.cuda_stream)
+            ms = _time(lambda: hb.spmm_device(m, X.data_ptr(), k, Y.data_ptr(), k, k, stream.cuda_stream), stream)
+            x1 = X[:, 0].contiguous()
+            y1 = torch.zeros(n, dtype=torch.float64, device="cuda")
+            ms1 = _time(lambda: hb.spmv_device(m, x1.data_ptr(), y1.data_ptr(), stream.cuda_stream), stream)
+            m.synchronize()
+            b = vbytes + k * 16 * n
+            print(json.dumps({"suite": "spmm", "workload": f"7-point Laplacian {g}^3 (centre 6, -1)",
+                              "storage": stname, "k": k, "rhs_tile": tune.spmmTile, "ms": ms,
+                              "ms_k_spmv": k * ms1, "speedup_vs_k_spmv": k * ms1 / ms,
+                              "bytes": b, "gbs": b / (ms / 1e3) / 1e9,
+                              "frac_of_peak": b / (ms / 1e3) / 1e9 / _peak()}), flush=True)
+        del m
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("what", choices=["precision", "spmm"])
+    ap.add_argument("--n", type=int, default=8 * 1024 * 1024)
+    ap.add_argument("--grid", type=int, default=128)
+    args = ap.parse_args(argv)
+    import torch
+    torch.cuda.set_device(0)
+    {"precision": precision, "spmm": spmm}[args.what](args)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

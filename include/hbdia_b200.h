@@ -239,9 +239,29 @@ int hbdia_matrix_selected_kernel(const hbdia_matrix *m, const void *x, int32_t *
 
 /* Kernel tuning knobs (used by the autotuner; results stay bit-identical).
  * HBDIA_TUNE_UNROLL: offsets in flight per lane in the staged and pipelined
- * kernels (0 = default 9, or 27). */
-typedef enum hbdia_tuning_key { HBDIA_TUNE_UNROLL = 1 } hbdia_tuning_key;
+ * kernels (0 = default 9, or 27).
+ * HBDIA_TUNE_SPMM_TILE: right-hand sides per pass of the SpMM kernels for
+ * every k (0 = autotuned / default, or 4, 8, 16, 32). */
+typedef enum hbdia_tuning_key { HBDIA_TUNE_UNROLL = 1, HBDIA_TUNE_SPMM_TILE = 2 } hbdia_tuning_key;
 int hbdia_matrix_set_tuning(hbdia_matrix *m, int32_t key, int32_t value);
+
+/* Autotuner.  Times the candidate configurations of this matrix's SpMV
+ * (k == 1: kernel x unroll; X, Y are x, y and ldx, ldy are ignored) or SpMM
+ * (k > 1: RHS tile 4/8/16/32) on the given device buffers and stream, keeps
+ * the fastest for the matrix, and records it in a process-wide table keyed on
+ * (blockWidth, stored offsets per block, COO fraction, k, value type,
+ * storage) so later matrices of the same class skip the timing (force != 0
+ * times again).  All candidates give bit-identical results.  Overwrites Y. */
+typedef struct hbdia_tune_result {
+    int32_t kernel;     /* hbdia_kernel chosen for k == 1   */
+    int32_t unroll;     /* HBDIA_TUNE_UNROLL value (k == 1) */
+    int32_t spmmTile;   /* RHS tile (k > 1)                 */
+    int32_t fromCache;  /* 1: taken from the table          */
+    float msPerCall;    /* measured time of the choice      */
+} hbdia_tune_result;
+int hbdia_matrix_autotune(hbdia_matrix *m, const void *X, int64_t ldx, void *Y, int64_t ldy, int32_t k,
+                          void *stream, int32_t force, hbdia_tune_result *out);
+int hbdia_autotune_clear(void);
 
 /* Time limit of every device-side wait of the staged kernel (default 2 s). */
 int hbdia_matrix_set_wait_timeout(hbdia_matrix *m, uint64_t nanoseconds);
