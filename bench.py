@@ -64,8 +64,8 @@ def measured_peak():
 
 def profiled_traffic():
     """Per-launch DRAM bytes of the SpMV kernel from the committed ncu summary
-    (profiles/spmv_bw32_f64_256cube.md, line 'traffic_bytes_per_launch: N')."""
-    p = os.path.join(ROOT, "profiles", "spmv_bw32_f64_256cube.md")
+    (line 'traffic_bytes_per_launch: N')."""
+    p = os.path.join(ROOT, "profiles", "spmv_bw32_pipe_fp64_stencil27_256cube.md")
     try:
         with open(p) as f:
             for line in f:
