@@ -365,6 +365,24 @@ def generate_banded(n: int, offsets: Sequence[int], lo: float = 0.5, hi: float =
     return _two_call(_load().hbdia_generate_banded, n, _vp(o), len(o), lo, hi, drop, scatter, seed)
 
 
+def generate_stencil27_spd(nx: int, ny: int, nz: int, shift: float = 1e-3, seed: int = 7):
+    """SPD symmetrised 27-point stencil (symmetric random off-diagonals -(0.5 + u),
+    diagonal (1 + shift) * row |sum|)."""
+    return _two_call(_load().hbdia_generate_stencil27_spd, nx, ny, nz, float(shift), seed)
+
+
+def cg_solve(matrix: HBDIA, b_ptr: int, x_ptr: int, tol: float = 1e-10, inner_storage: int = STORE_F32,
+             inner_tol: float = 1e-6, max_outer: int = 50, max_inner: int = 5000, check_every: int = 10,
+             stream: Optional[int] = None) -> "_lib.CgResult":
+    """Mixed-precision CG (FP64 refinement around reduced-storage inner CG) on
+    device buffers b, x (x: initial guess in, solution out)."""
+    o = _lib.CgOptions(tol, inner_tol, max_outer, max_inner, inner_storage, check_every)
+    r = _lib.CgResult()
+    _check(_load().hbdia_cg_solve(matrix.handle, ctypes.c_void_p(b_ptr), ctypes.c_void_p(x_ptr), ctypes.byref(o),
+                                  _stream_arg(stream), ctypes.byref(r)))
+    return r
+
+
 def fill_uniform(n: int, lo: float, hi: float, seed: int) -> np.ndarray:
     out = np.empty(n, np.float64)
     _check(_load().hbdia_fill_uniform(_vp(out), n, lo, hi, seed))

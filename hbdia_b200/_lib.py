@@ -49,6 +49,16 @@ class TuneResult(ctypes.Structure):
                 ("msPerCall", ctypes.c_float)]
 
 
+class CgOptions(ctypes.Structure):
+    _fields_ = [("tol", c_dbl), ("innerTol", c_dbl), ("maxOuter", c_i32), ("maxInner", c_i32),
+                ("innerStorage", c_i32), ("checkEvery", c_i32)]
+
+
+class CgResult(ctypes.Structure):
+    _fields_ = [("outerIterations", c_i32), ("innerIterations", c_i32), ("converged", c_i32),
+                ("relResidual", c_dbl), ("seconds", c_dbl)]
+
+
 class HBDIACudaError(RuntimeError):
     """A CUDA runtime call inside the library failed."""
 
@@ -114,6 +124,8 @@ _SIGS = [
     ("hbdia_generate_banded", ctypes.c_int,
      [c_i32, c_vp, c_i32, c_dbl, c_dbl, c_dbl, c_dbl, c_u64, c_i64p, c_vp, c_vp, c_vp]),
     ("hbdia_fill_uniform", ctypes.c_int, [c_vp, c_i64, c_dbl, c_dbl, c_u64]),
+    ("hbdia_generate_stencil27_spd", ctypes.c_int, [c_i32, c_i32, c_i32, c_dbl, c_u64, c_i64p, c_vp, c_vp, c_vp]),
+    ("hbdia_cg_solve", ctypes.c_int, [c_vp, c_vp, c_vp, ctypes.POINTER(CgOptions), c_vp, ctypes.POINTER(CgResult)]),
 ]
 
 # every C-ABI entry point (the exported-symbol check in the tests uses this list)

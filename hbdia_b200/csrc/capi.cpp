@@ -31,6 +31,8 @@ struct hbdia_matrix {
     hbdia::HostLayout<double> L64;
     hbdia::HostLayout<float> L32;
     hbdia::DevicePlan plan;
+    hbdia::DevicePlan innerPlan;        // reduced-storage copy for the CG inner iterations
+    hbdia::CgWork *cg = nullptr;        // CG workspace
     int32_t blockWidth = 0, threshold = 0;
     int64_t maxCoo = 0;
     std::mutex hostMu;  // serialises hbdia_spmv_host's scratch buffers
@@ -115,6 +117,9 @@ void fill_coo(hbdia::Coo<T> &c, const int32_t *r, const int32_t *col, const void
 
 void reset_hbdia(hbdia_matrix *m) {
     hbdia::free_plan(m->plan);
+    hbdia::free_plan(m->innerPlan);
+    hbdia::cg_free(m->cg);
+    m->cg = nullptr;
     m->L64 = hbdia::HostLayout<double>();
     m->L32 = hbdia::HostLayout<float>();
     m->hasHBDIA = false;
@@ -193,7 +198,7 @@ int hbdia_matrix_create(hbdia_dtype dtype, const int32_t *rows, const int32_t *c
 
 void hbdia_matrix_destroy(hbdia_matrix *m) {
     if (!m) return;
-    hbdia::free_plan(m->plan);
+    reset_hbdia(m);
     delete m;
 }
 
@@ -576,6 +581,38 @@ int hbdia_spmv_host(hbdia_matrix *m, const void *xh, void *yh) {
     });
 }
 
+// ---------------------------------------------------------------- solver
+int hbdia_cg_solve(hbdia_matrix *m, const double *b, double *x, const hbdia_cg_options *opt, void *stream,
+                   hbdia_cg_result *out) {
+    return guarded([&] {
+        need(m && b && x && opt, HBDIA_ERR_INVALID_ARGUMENT, "null argument");
+        need(m->dtype == HBDIA_F64, HBDIA_ERR_UNSUPPORTED, "the CG solver needs a double matrix");
+        need(m->hasHBDIA, HBDIA_ERR_NOT_CONVERTED, "matrix is not in HBDIA format");
+        need(num_rows(m) == num_cols(m), HBDIA_ERR_INVALID_ARGUMENT, "CG needs a square matrix");
+        need(opt->tol > 0 && opt->innerTol > 0 && opt->maxOuter >= 0 && opt->maxInner > 0 && opt->checkEvery > 0,
+             HBDIA_ERR_INVALID_ARGUMENT, "bad CG options");
+        ensure_device(m);
+        const hbdia::DevicePlan *inner = &m->plan;
+        if (opt->innerStorage != HBDIA_STORE_NATIVE) {
+            if (!m->innerPlan.base || m->innerPlan.storage != opt->innerStorage) {
+                need(m->hostLayout, HBDIA_ERR_NOT_CONVERTED, "no host layout to build the inner operator");
+                hbdia::build_plan(m->L64, opt->innerStorage, m->innerPlan);
+                m->innerPlan.kernel = m->plan.kernel;
+                m->innerPlan.unroll = m->plan.unroll;
+            }
+            inner = &m->innerPlan;
+        }
+        m->cg = hbdia::cg_work(m->cg, num_rows(m));
+        hbdia_cg_result r;
+        std::memset(&r, 0, sizeof(r));
+        hbdia::cg_solve(m->plan, *inner, m->cg, b, x, opt->tol, opt->maxOuter, opt->maxInner, opt->innerTol,
+                        opt->checkEvery, stream, &r.outerIterations, &r.innerIterations, &r.relResidual, &r.seconds);
+        r.converged = r.relResidual <= opt->tol;
+        throw_if_timeout(read_status(m, true));
+        if (out) *out = r;
+    });
+}
+
 // ---------------------------------------------------------------- workloads
 int hbdia_generate_stencil27(int32_t nx, int32_t ny, int32_t nz, double center, double neighbor,
                              double frac, double lo, double hi, uint64_t seed, int64_t *nnz,
@@ -599,6 +636,11 @@ int hbdia_generate_banded(int32_t n, const int32_t *offsets, int32_t numOffsets,
         hbdia::generate_banded(n, offsets, numOffsets, lo, hi, dropProb, scatterFraction, seed, nnz, rows,
                                cols, values);
     });
+}
+
+int hbdia_generate_stencil27_spd(int32_t nx, int32_t ny, int32_t nz, double shift, uint64_t seed, int64_t *nnz,
+                                 int32_t *rows, int32_t *cols, double *values) {
+    return guarded([&] { hbdia::generate_stencil27_spd(nx, ny, nz, shift, seed, nnz, rows, cols, values); });
 }
 
 int hbdia_fill_uniform(double *out, int64_t n, double lo, double hi, uint64_t seed) {

@@ -424,6 +424,66 @@ int generate_banded(int32_t n, const int32_t *offs, int32_t noffs, double lo, do
     return HBDIA_OK;
 }
 
+namespace {
+inline uint64_t splitmix(uint64_t z) {
+    z += 0x9e3779b97f4a7c15ULL;
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+    return z ^ (z >> 31);
+}
+}  // namespace
+
+int generate_stencil27_spd(int32_t nx, int32_t ny, int32_t nz, double shift, uint64_t seed, int64_t *nnzOut,
+                           int32_t *rows, int32_t *cols, double *vals) {
+    if (nx <= 0 || ny <= 0 || nz <= 0 || !nnzOut || shift < 0)
+        throw Error(HBDIA_ERR_INVALID_ARGUMENT, "bad SPD stencil arguments");
+    const int64_t n = static_cast<int64_t>(nx) * ny * nz;
+    if (n > 2147483647LL) throw Error(HBDIA_ERR_INVALID_ARGUMENT, "grid too large for int32 indices");
+    *nnzOut = (3LL * nx - 2) * (3LL * ny - 2) * (3LL * nz - 2);
+    if (!rows) return HBDIA_OK;
+    const int64_t plane = static_cast<int64_t>(nx) * ny;
+    auto span = [](int64_t c, int64_t len) { return 1 + (c > 0) + (c < len - 1); };
+    std::vector<int64_t> rstart(static_cast<size_t>(n) + 1, 0);
+#pragma omp parallel for schedule(static)
+    for (int64_t r = 0; r < n; ++r)
+        rstart[r + 1] = span(r % nx, nx) * span((r / nx) % ny, ny) * span(r / plane, nz);
+    for (int64_t r = 0; r < n; ++r) rstart[r + 1] += rstart[r];
+    // symmetric weights: -(0.5 + u), u from a hash of the unordered pair
+    auto weight = [&](int64_t i, int64_t j) {
+        const int64_t a = std::min(i, j), b = std::max(i, j);
+        const uint64_t h = splitmix(static_cast<uint64_t>(a) * 0x100000001b3ULL ^ static_cast<uint64_t>(b) ^ seed);
+        return -(0.5 + static_cast<double>(h >> 11) * 0x1.0p-53);
+    };
+#pragma omp parallel for schedule(static)
+    for (int64_t r = 0; r < n; ++r) {
+        const int64_t x = r % nx, y = (r / nx) % ny, z = r / plane;
+        int64_t p = rstart[r], diagPos = -1;
+        double absSum = 0.0;
+        for (int dz = -1; dz <= 1; ++dz) {
+            if (z + dz < 0 || z + dz >= nz) continue;
+            for (int dy = -1; dy <= 1; ++dy) {
+                if (y + dy < 0 || y + dy >= ny) continue;
+                for (int dx = -1; dx <= 1; ++dx) {
+                    if (x + dx < 0 || x + dx >= nx) continue;
+                    const int64_t c = r + dz * plane + dy * nx + dx;
+                    rows[p] = static_cast<int32_t>(r);
+                    cols[p] = static_cast<int32_t>(c);
+                    if (c == r) {
+                        diagPos = p;
+                        vals[p] = 0.0;
+                    } else {
+                        vals[p] = weight(r, c);
+                        absSum += -vals[p];
+                    }
+                    ++p;
+                }
+            }
+        }
+        vals[diagPos] = (1.0 + shift) * absSum;
+    }
+    return HBDIA_OK;
+}
+
 void fill_uniform(double *out, int64_t n, double lo, double hi, uint64_t seed) {
     std::mt19937_64 g(seed);
     for (int64_t i = 0; i < n; ++i) out[i] = lo + (hi - lo) * unit(g);

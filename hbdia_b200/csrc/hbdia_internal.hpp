@@ -118,6 +118,14 @@ int32_t default_spmm_tile(int32_t k);
 void autotune(DevicePlan &P, const void *X, int64_t ldx, void *Y, int64_t ldy, int32_t k, void *stream, bool force,
               int32_t *kernel, int32_t *unroll, int32_t *tile, int32_t *fromCache, float *ms);
 void autotune_clear_cache();
+
+// CG with mixed-precision refinement (cg.cu)
+struct CgWork;
+CgWork *cg_work(CgWork *w, int64_t n);
+void cg_free(CgWork *w);
+void cg_solve(const DevicePlan &A64, const DevicePlan &Ainner, CgWork *w, const double *b, double *x, double tol,
+              int maxOuter, int maxInner, double innerTol, int checkEvery, void *stream, int32_t *outerIt,
+              int32_t *innerIt, double *relRes, double *seconds);
 // throws Error(HBDIA_ERR_CUDA) with the CUDA error string
 void check_cuda(int err, const char *what);
 
@@ -128,5 +136,7 @@ int generate_banded(int32_t n, const int32_t *offs, int32_t noffs, double lo, do
                     double scatter, uint64_t seed, int64_t *nnzOut, int32_t *rows, int32_t *cols,
                     double *vals);
 void fill_uniform(double *out, int64_t n, double lo, double hi, uint64_t seed);
+int generate_stencil27_spd(int32_t nx, int32_t ny, int32_t nz, double shift, uint64_t seed, int64_t *nnzOut,
+                           int32_t *rows, int32_t *cols, double *vals);
 
 }  // namespace hbdia

@@ -113,15 +113,44 @@ def spmm(args):
         del m
 
 
+def cg(args):
+    import torch
+    import hbdia_b200 as hb
+    g = args.grid
+    n = g ** 3
+    rows, cols, vals = hb.generate_stencil27_spd(g, g, g, 1e-3, 7)
+    b = hb.fill_uniform(n, -1.0, 1.0, 11)
+    bt = torch.from_numpy(b).cuda()
+    m = hb.HBDIA(rows, cols, vals, n, n)
+    m.convertToHBDIAFormat(32, 2)
+    for name, st, itol in (("mixed fp32-storage inner + fp64 refinement", hb.STORE_F32, 1e-6),
+                           ("plain fp64 CG", hb.STORE_NATIVE, 1e-11)):
+        xt = torch.zeros(n, dtype=torch.float64, device="cuda")
+        hb.cg_solve(m, bt.data_ptr(), xt.data_ptr(), tol=1e-10, inner_storage=st, inner_tol=itol)  # warm
+        xt.zero_()
+        torch.cuda.synchronize()
+        r = hb.cg_solve(m, bt.data_ptr(), xt.data_ptr(), tol=1e-10, inner_storage=st, inner_tol=itol)
+        x = xt.cpu().numpy()
+        ax = np.zeros(n)
+        np.add.at(ax, rows, vals * x[cols])
+        host_res = float(np.linalg.norm(b - ax) / np.linalg.norm(b))
+        print(json.dumps({"suite": "cg", "workload": f"SPD symmetrised 27-point stencil {g}^3, b ~ U(-1,1)",
+                          "method": name, "outer_iterations": r.outerIterations,
+                          "inner_spmvs": r.innerIterations, "seconds": r.seconds,
+                          "ms_per_inner_iteration": 1e3 * r.seconds / max(1, r.innerIterations),
+                          "rel_residual": r.relResidual, "rel_residual_host_check": host_res,
+                          "converged": bool(r.converged)}), flush=True)
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("what", choices=["precision", "spmm"])
+    ap.add_argument("what", choices=["precision", "spmm", "cg"])
     ap.add_argument("--n", type=int, default=8 * 1024 * 1024)
     ap.add_argument("--grid", type=int, default=128)
     args = ap.parse_args(argv)
     import torch
     torch.cuda.set_device(0)
-    {"precision": precision, "spmm": spmm}[args.what](args)
+    {"precision": precision, "spmm": spmm, "cg": cg}[args.what](args)
     return 0
 
 

@@ -271,6 +271,36 @@ int hbdia_matrix_set_wait_timeout(hbdia_matrix *m, uint64_t nanoseconds);
  * reports HBDIA_ERR_DEVICE_TIMEOUT at the next synchronize.  -1 turns it off. */
 int hbdia_matrix_test_skip_chunk(hbdia_matrix *m, int32_t chunk);
 
+/* ---------------------------------------------------------------- solver */
+
+/* Conjugate gradients for a symmetric positive definite double matrix, with
+ * mixed-precision iterative refinement: the residual r = b - A x, the dot
+ * products, norms and the solution update are FP64; each refinement step
+ * solves A d = r with CG whose SpMVs use the `innerStorage` copy of the values
+ * (HBDIA_STORE_F32: mixed precision; HBDIA_STORE_NATIVE: plain FP64 CG).  No
+ * counterpart in the reference (its SpMV has no solver); it runs on the same
+ * SpMV kernels.  x holds the initial guess on entry and the solution on
+ * return (device buffers of numRows doubles).  Synchronous. */
+typedef struct hbdia_cg_options {
+    double tol;           /* target ||b - A x|| / ||b|| (FP64), e.g. 1e-10       */
+    double innerTol;      /* inner CG stops at ||r_in|| <= innerTol ||r||        */
+    int32_t maxOuter;     /* refinement steps                                    */
+    int32_t maxInner;     /* inner iterations per step                           */
+    int32_t innerStorage; /* hbdia_value_storage of the inner operator           */
+    int32_t checkEvery;   /* inner iterations per CUDA-graph replay / host check */
+} hbdia_cg_options;
+
+typedef struct hbdia_cg_result {
+    int32_t outerIterations;
+    int32_t innerIterations;   /* inner SpMVs */
+    int32_t converged;
+    double relResidual;        /* final ||b - A x|| / ||b|| in FP64 */
+    double seconds;
+} hbdia_cg_result;
+
+int hbdia_cg_solve(hbdia_matrix *m, const double *b, double *x, const hbdia_cg_options *options, void *stream,
+                   hbdia_cg_result *result);
+
 /* ---------------------------------------------------------------- workloads */
 
 /* Seeded synthetic 27-point stencil on an nx*ny*nz grid (Dirichlet boundary,
@@ -296,6 +326,13 @@ int hbdia_generate_stencil7(int32_t nx, int32_t ny, int32_t nz, double center, d
 int hbdia_generate_banded(int32_t n, const int32_t *offsets, int32_t numOffsets, double lo,
                           double hi, double dropProb, double scatterFraction, uint64_t seed,
                           int64_t *nnz, int32_t *rows, int32_t *cols, double *values);
+
+/* Symmetric positive definite 27-point stencil: off-diagonal a_ij = a_ji =
+ * -(0.5 + u), u in [0, 1) drawn from a hash of the unordered pair (i, j) and
+ * the seed, diagonal (1 + shift) * sum_j |a_ij| (shift >= 0).  Row-sorted,
+ * ascending columns.  Two-call protocol as above. */
+int hbdia_generate_stencil27_spd(int32_t nx, int32_t ny, int32_t nz, double shift, uint64_t seed, int64_t *nnz,
+                                 int32_t *rows, int32_t *cols, double *values);
 
 /* n doubles uniform in [lo, hi) from the library's seeded generator. */
 int hbdia_fill_uniform(double *out, int64_t n, double lo, double hi, uint64_t seed);
