@@ -337,6 +337,13 @@ def spmv_host(matrix: HBDIA, x: np.ndarray, y: np.ndarray) -> None:
     _check(_load().hbdia_spmv_host(matrix.handle, ctypes.c_void_p(x.ctypes.data), ctypes.c_void_p(y.ctypes.data)))
 
 
+def spmv_host_noalloc(matrix: HBDIA, x: np.ndarray, y: np.ndarray) -> None:
+    """spmv_host through the library's fixed per-device array (no device
+    allocation; max(numRows, numCols) <= 2^21; calls must not overlap)."""
+    _check(_load().hbdia_spmv_host_noalloc(matrix.handle, ctypes.c_void_p(x.ctypes.data),
+                                           ctypes.c_void_p(y.ctypes.data)))
+
+
 # ---------------------------------------------------------------- workloads
 def _two_call(fn, *args):
     nnz = ctypes.c_int64(0)

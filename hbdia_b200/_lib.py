@@ -118,6 +118,7 @@ _SIGS = [
     ("hbdia_spmv_device", ctypes.c_int, [c_vp, c_vp, c_vp, c_vp]),
     ("hbdia_spmm_device", ctypes.c_int, [c_vp, c_vp, c_i64, c_vp, c_i64, c_i32, c_vp]),
     ("hbdia_spmv_host", ctypes.c_int, [c_vp, c_vp, c_vp]),
+    ("hbdia_spmv_host_noalloc", ctypes.c_int, [c_vp, c_vp, c_vp]),
     ("hbdia_generate_stencil27", ctypes.c_int,
      [c_i32, c_i32, c_i32, c_dbl, c_dbl, c_dbl, c_dbl, c_dbl, c_u64, c_i64p, c_vp, c_vp, c_vp]),
     ("hbdia_generate_stencil7", ctypes.c_int, [c_i32, c_i32, c_i32, c_dbl, c_dbl, c_i64p, c_vp, c_vp, c_vp]),

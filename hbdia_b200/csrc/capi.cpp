@@ -139,6 +139,11 @@ void ensure_device(hbdia_matrix *m) {
 
 }  // namespace
 
+int hbdia::record_error(int status, const std::string &msg) {
+    g_err = msg;
+    return status;
+}
+
 extern "C" {
 
 const char *hbdia_last_error(void) { return g_err.c_str(); }

@@ -128,6 +128,8 @@ void cg_solve(const DevicePlan &A64, const DevicePlan &Ainner, CgWork *w, const 
               int32_t *innerIt, double *relRes, double *seconds);
 // throws Error(HBDIA_ERR_CUDA) with the CUDA error string
 void check_cuda(int err, const char *what);
+// Sets the message hbdia_last_error() reports on this thread; returns status.
+int record_error(int status, const std::string &msg);
 
 int generate_stencil(int stencilPoints, int32_t nx, int32_t ny, int32_t nz, double center,
                      double neighbor, double frac, double lo, double hi, uint64_t seed,

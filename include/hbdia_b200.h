@@ -224,6 +224,21 @@ int hbdia_spmm_device(const hbdia_matrix *m, const void *X, int64_t ldx, void *Y
  * copies y back and synchronizes.  Page-locked host buffers are fastest. */
 int hbdia_spmv_host(hbdia_matrix *m, const void *xHost, void *yHost);
 
+/* hbdia_spmv_host without any device allocation.  No counterpart in the
+ * reference.  For callers whose device memory belongs to another allocator
+ * or budget, where the cudaMalloc that hbdia_spmv_host makes on its first
+ * call could fail or stall a request.  x and y pass through one fixed
+ * per-device array of the library (32 MiB), so:
+ *  - max(numRows, numCols) must be <= 2^21 (HBDIA_ERR_INVALID_ARGUMENT
+ *    otherwise), and the matrix must already be on the device
+ *    (hbdia_matrix_prepare_gpu; HBDIA_ERR_NOT_CONVERTED otherwise);
+ *  - every call shares that array: calls that overlap in time race and give
+ *    undefined y, so callers serialise them;
+ *  - the first call on a device does the set-up (a symbol-address lookup);
+ *    make it before any stream capture on that device.
+ * Same kernels and results as hbdia_spmv_host; synchronous. */
+int hbdia_spmv_host_noalloc(hbdia_matrix *m, const void *xHost, void *yHost);
+
 /* Blocks until the matrix's stream is idle, then reports (and clears) the
  * device status: HBDIA_ERR_DEVICE_TIMEOUT when a bounded wait inside a
  * kernel ran out since the last check (the affected y is invalid). */
