@@ -390,6 +390,73 @@ def cg_solve(matrix: HBDIA, b_ptr: int, x_ptr: int, tol: float = 1e-10, inner_st
     return r
 
 
+class Batch:
+    """Many device-resident matrices (block width 32, one value type and
+    storage) computed by one persistent launch (hbdia_batch_*).  Every y is bit
+    for bit what spmv_device / spmm_device give for that matrix alone.  The
+    matrices must stay alive and on the device while the batch exists."""
+
+    def __init__(self, matrices: Sequence[HBDIA]):
+        self._mats = list(matrices)  # keeps the matrices alive
+        arr = (ctypes.c_void_p * len(self._mats))(*[m.handle.value for m in self._mats])
+        h = ctypes.c_void_p()
+        _check(_load().hbdia_batch_create(arr, len(self._mats), ctypes.byref(h)))
+        self.handle = h
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h is not None and h.value:
+            _load().hbdia_batch_destroy(h)
+            self.handle = None
+
+    def __len__(self) -> int:
+        return len(self._mats)
+
+    def bind(self, x_ptrs: Sequence[int], y_ptrs: Sequence[int], k: Optional[Sequence[int]] = None,
+             ldx: Optional[Sequence[int]] = None, ldy: Optional[Sequence[int]] = None) -> None:
+        """Device pointers per matrix; k[i] right-hand sides (row-major n x k
+        blocks with leading dimensions ldx[i], ldy[i]); k[i] == 0 leaves
+        matrix i out.  Runs already enqueued keep their old binding."""
+        n = len(self._mats)
+        X = (ctypes.c_void_p * n)(*[int(p) or None for p in x_ptrs])
+        Y = (ctypes.c_void_p * n)(*[int(p) or None for p in y_ptrs])
+        K = (ctypes.c_int32 * n)(*k) if k is not None else None
+        LX = (ctypes.c_int64 * n)(*ldx) if ldx is not None else None
+        LY = (ctypes.c_int64 * n)(*ldy) if ldy is not None else None
+        _check(_load().hbdia_batch_bind(self.handle, X, LX, Y, LY, K))
+
+    def run(self, stream: Optional[int] = None) -> None:
+        _check(_load().hbdia_batch_run(self.handle, _stream_arg(stream)))
+
+    def set_config(self, threads: int = 256, grab: int = 2, rhs_tile: int = 8, graph: bool = True) -> None:
+        c = _lib.BatchConfig(threads, grab, rhs_tile, 1 if graph else 0)
+        _check(_load().hbdia_batch_set_config(self.handle, ctypes.byref(c)))
+
+    def config(self) -> "_lib.BatchConfig":
+        c = _lib.BatchConfig()
+        _check(_load().hbdia_batch_get_config(self.handle, ctypes.byref(c)))
+        return c
+
+    def autotune(self, stream: Optional[int] = None):
+        """Times every configuration on the bound vectors and keeps the
+        fastest; returns (ms per run of the best, candidates timed)."""
+        ms = ctypes.c_float(0)
+        n = ctypes.c_int32(0)
+        _check(_load().hbdia_batch_autotune(self.handle, _stream_arg(stream), ctypes.byref(ms), ctypes.byref(n)))
+        return ms.value, n.value
+
+    def info(self):
+        """(count, total 32-row tiles, algorithmic HBM bytes per run)."""
+        c, t, b = ctypes.c_int32(0), ctypes.c_int32(0), ctypes.c_int64(0)
+        _check(_load().hbdia_batch_info(self.handle, ctypes.byref(c), ctypes.byref(t), ctypes.byref(b)))
+        return c.value, t.value, b.value
+
+    def stream(self) -> int:
+        s = ctypes.c_void_p()
+        _check(_load().hbdia_batch_stream(self.handle, ctypes.byref(s)))
+        return s.value or 0
+
+
 def fill_uniform(n: int, lo: float, hi: float, seed: int) -> np.ndarray:
     out = np.empty(n, np.float64)
     _check(_load().hbdia_fill_uniform(_vp(out), n, lo, hi, seed))

@@ -59,6 +59,10 @@ class CgResult(ctypes.Structure):
                 ("relResidual", c_dbl), ("seconds", c_dbl)]
 
 
+class BatchConfig(ctypes.Structure):
+    _fields_ = [("threadsPerBlock", c_i32), ("tilesPerGrab", c_i32), ("rhsTile", c_i32), ("useGraph", c_i32)]
+
+
 class HBDIACudaError(RuntimeError):
     """A CUDA runtime call inside the library failed."""
 
@@ -127,6 +131,15 @@ _SIGS = [
     ("hbdia_fill_uniform", ctypes.c_int, [c_vp, c_i64, c_dbl, c_dbl, c_u64]),
     ("hbdia_generate_stencil27_spd", ctypes.c_int, [c_i32, c_i32, c_i32, c_dbl, c_u64, c_i64p, c_vp, c_vp, c_vp]),
     ("hbdia_cg_solve", ctypes.c_int, [c_vp, c_vp, c_vp, ctypes.POINTER(CgOptions), c_vp, ctypes.POINTER(CgResult)]),
+    ("hbdia_batch_create", ctypes.c_int, [c_vpp, c_i32, c_vpp]),
+    ("hbdia_batch_destroy", None, [c_vp]),
+    ("hbdia_batch_bind", ctypes.c_int, [c_vp, c_vpp, c_i64p, c_vpp, c_i64p, c_i32p]),
+    ("hbdia_batch_run", ctypes.c_int, [c_vp, c_vp]),
+    ("hbdia_batch_set_config", ctypes.c_int, [c_vp, ctypes.POINTER(BatchConfig)]),
+    ("hbdia_batch_get_config", ctypes.c_int, [c_vp, ctypes.POINTER(BatchConfig)]),
+    ("hbdia_batch_autotune", ctypes.c_int, [c_vp, c_vp, ctypes.POINTER(ctypes.c_float), c_i32p]),
+    ("hbdia_batch_info", ctypes.c_int, [c_vp, c_i32p, c_i32p, c_i64p]),
+    ("hbdia_batch_stream", ctypes.c_int, [c_vp, c_vpp]),
 ]
 
 # every C-ABI entry point (the exported-symbol check in the tests uses this list)

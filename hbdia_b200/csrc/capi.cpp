@@ -38,6 +38,10 @@ struct hbdia_matrix {
     std::mutex hostMu;  // serialises hbdia_spmv_host's scratch buffers
 };
 
+struct hbdia_batch {
+    hbdia::Batch *B = nullptr;
+};
+
 namespace {
 
 thread_local std::string g_err;
@@ -615,6 +619,79 @@ int hbdia_cg_solve(hbdia_matrix *m, const double *b, double *x, const hbdia_cg_o
         r.converged = r.relResidual <= opt->tol;
         throw_if_timeout(read_status(m, true));
         if (out) *out = r;
+    });
+}
+
+// ---------------------------------------------------------------- batches
+int hbdia_batch_create(hbdia_matrix *const *mats, int32_t count, hbdia_batch **out) {
+    return guarded([&] {
+        need(mats && out && count > 0, HBDIA_ERR_INVALID_ARGUMENT, "null argument or empty batch");
+        *out = nullptr;
+        std::vector<const hbdia::DevicePlan *> plans(static_cast<size_t>(count));
+        for (int32_t i = 0; i < count; ++i) {
+            need(mats[i] != nullptr, HBDIA_ERR_INVALID_ARGUMENT, "null matrix in batch");
+            need(mats[i]->hasHBDIA, HBDIA_ERR_NOT_CONVERTED, "matrix is not in HBDIA format");
+            plans[i] = &mats[i]->plan;
+        }
+        auto b = std::make_unique<hbdia_batch>();
+        b->B = hbdia::batch_create(plans);
+        *out = b.release();
+    });
+}
+
+void hbdia_batch_destroy(hbdia_batch *b) {
+    if (!b) return;
+    hbdia::batch_free(b->B);
+    delete b;
+}
+
+int hbdia_batch_bind(hbdia_batch *b, const void *const *X, const int64_t *ldx, void *const *Y, const int64_t *ldy,
+                     const int32_t *k) {
+    return guarded([&] {
+        need(b != nullptr, HBDIA_ERR_INVALID_ARGUMENT, "null batch");
+        hbdia::batch_bind(b->B, X, ldx, Y, ldy, k);
+    });
+}
+
+int hbdia_batch_run(hbdia_batch *b, void *stream) {
+    return guarded([&] {
+        need(b != nullptr, HBDIA_ERR_INVALID_ARGUMENT, "null batch");
+        hbdia::batch_run(b->B, stream);
+    });
+}
+
+int hbdia_batch_set_config(hbdia_batch *b, const hbdia_batch_config *c) {
+    return guarded([&] {
+        need(b && c, HBDIA_ERR_INVALID_ARGUMENT, "null argument");
+        hbdia::batch_set_config(b->B, c->threadsPerBlock, c->tilesPerGrab, c->rhsTile, c->useGraph);
+    });
+}
+
+int hbdia_batch_get_config(const hbdia_batch *b, hbdia_batch_config *c) {
+    return guarded([&] {
+        need(b && c, HBDIA_ERR_INVALID_ARGUMENT, "null argument");
+        hbdia::batch_get_config(b->B, &c->threadsPerBlock, &c->tilesPerGrab, &c->rhsTile, &c->useGraph);
+    });
+}
+
+int hbdia_batch_autotune(hbdia_batch *b, void *stream, float *ms, int32_t *candidates) {
+    return guarded([&] {
+        need(b != nullptr, HBDIA_ERR_INVALID_ARGUMENT, "null batch");
+        hbdia::batch_autotune(b->B, stream, ms, candidates);
+    });
+}
+
+int hbdia_batch_info(const hbdia_batch *b, int32_t *count, int32_t *totalTiles, int64_t *bytesPerRun) {
+    return guarded([&] {
+        need(b && count && totalTiles && bytesPerRun, HBDIA_ERR_INVALID_ARGUMENT, "null argument");
+        hbdia::batch_info(b->B, count, totalTiles, bytesPerRun);
+    });
+}
+
+int hbdia_batch_stream(const hbdia_batch *b, void **stream) {
+    return guarded([&] {
+        need(b && stream, HBDIA_ERR_INVALID_ARGUMENT, "null argument");
+        *stream = hbdia::batch_stream(b->B);
     });
 }
 

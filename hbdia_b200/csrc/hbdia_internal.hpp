@@ -126,6 +126,19 @@ void cg_free(CgWork *w);
 void cg_solve(const DevicePlan &A64, const DevicePlan &Ainner, CgWork *w, const double *b, double *x, double tol,
               int maxOuter, int maxInner, double innerTol, int checkEvery, void *stream, int32_t *outerIt,
               int32_t *innerIt, double *relRes, double *seconds);
+// Many matrices in one persistent launch (batch.cu)
+struct Batch;
+Batch *batch_create(const std::vector<const DevicePlan *> &plans);
+void batch_free(Batch *b);
+void batch_bind(Batch *b, const void *const *X, const int64_t *ldx, void *const *Y, const int64_t *ldy,
+                const int32_t *k);
+void batch_run(Batch *b, void *stream);
+void batch_set_config(Batch *b, int32_t threads, int32_t grab, int32_t rhsTile, int32_t useGraph);
+void batch_get_config(const Batch *b, int32_t *threads, int32_t *grab, int32_t *rhsTile, int32_t *useGraph);
+void batch_autotune(Batch *b, void *stream, float *ms, int32_t *candidates);
+void batch_info(const Batch *b, int32_t *count, int32_t *totalTiles, int64_t *bytesPerRun);
+void *batch_stream(const Batch *b);
+
 // throws Error(HBDIA_ERR_CUDA) with the CUDA error string
 void check_cuda(int err, const char *what);
 // Sets the message hbdia_last_error() reports on this thread; returns status.

@@ -18,6 +18,7 @@
 #include <cstring>
 #include <type_traits>
 
+#include "args.cuh"
 #include "hbdia_internal.hpp"
 #include "spmv_kernels.cuh"
 #include "spmv_tma.cuh"
@@ -228,26 +229,6 @@ template void build_plan<double>(const HostLayout<double> &, int, DevicePlan &);
 template void build_plan<float>(const HostLayout<float> &, int, DevicePlan &);
 
 namespace {
-
-template <typename VT, typename XT>
-dev::SpmvArgs<VT, XT> make_args(const DevicePlan &P) {
-    dev::SpmvArgs<VT, XT> a;
-    a.vals = static_cast<const VT *>(P.vals);
-    a.scale = P.scale;
-    a.offs = P.offs;
-    a.blkOff = P.blkOff;
-    a.cooRow = P.cooRow;
-    a.cooCol = P.cooCol;
-    a.cooVal = static_cast<const XT *>(P.cooVal);
-    a.cooRowPtr = P.cooRowPtr;
-    a.cooTile = P.cooTile;
-    a.n = P.n;
-    a.bw = P.bw;
-    a.numBlocks = P.numBlocks;
-    a.numTiles = P.numTiles;
-    a.hasCoo = P.nCoo > 0;
-    return a;
-}
 
 // One CTA per SM (the stage ring fills the SM's shared memory).  The
 // dynamic shared-memory opt-in is a per-device function attribute.

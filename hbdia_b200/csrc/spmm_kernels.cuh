@@ -37,12 +37,9 @@ __device__ __forceinline__ void load_x_row(const XT *__restrict__ p, int kc, boo
 
 // blockWidth 32: one warp per 32-row block, lane = row.
 template <typename VT, typename XT, int KT>
-__global__ void __launch_bounds__(256)
-spmm_bw32(const SpmvArgs<VT, XT> a, const XT *__restrict__ X, int64_t ldx, XT *__restrict__ Y, int64_t ldy,
-          int32_t k) {
-    const int lane = threadIdx.x & 31;
-    const int32_t tile = static_cast<int32_t>((static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5);
-    if (tile >= a.numTiles) return;  // warp-uniform
+__device__ __forceinline__ void bw32_spmm_tile(const SpmvArgs<VT, XT> &a, const XT *__restrict__ X, int64_t ldx,
+                                               XT *__restrict__ Y, int64_t ldy, int32_t k, int32_t tile,
+                                               int lane) {
     const int64_t row0 = static_cast<int64_t>(tile) * 32;
     const int64_t row = row0 + lane;
     int32_t k0 = 0, k1 = 0;
@@ -107,6 +104,16 @@ spmm_bw32(const SpmvArgs<VT, XT> a, const XT *__restrict__ X, int64_t ldx, XT *_
                 if (q < kc) yp[q] = acc[q];
         }
     }
+}
+
+template <typename VT, typename XT, int KT>
+__global__ void __launch_bounds__(256)
+spmm_bw32(const SpmvArgs<VT, XT> a, const XT *__restrict__ X, int64_t ldx, XT *__restrict__ Y, int64_t ldy,
+          int32_t k) {
+    const int lane = threadIdx.x & 31;
+    const int32_t tile = static_cast<int32_t>((static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5);
+    if (tile >= a.numTiles) return;  // warp-uniform
+    bw32_spmm_tile<VT, XT, KT>(a, X, ldx, Y, ldy, k, tile, lane);
 }
 
 // Any block width: one thread per row (the reference's mapping).

@@ -141,11 +141,8 @@ __device__ __forceinline__ XT tile_coo(const int32_t *__restrict__ cooRow,
 // L1, where the block's neighbouring diagonals (col, col+1, ...) and the
 // neighbouring blocks of the same CTA hit the same lines.
 template <typename VT, typename XT, int U>
-__global__ void __launch_bounds__(256)
-spmv_bw32(const SpmvArgs<VT, XT> a, const XT *__restrict__ x, XT *__restrict__ y) {
-    const int lane = threadIdx.x & 31;
-    const int32_t tile = static_cast<int32_t>((static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5);
-    if (tile >= a.numTiles) return;  // warp-uniform
+__device__ __forceinline__ void bw32_tile(const SpmvArgs<VT, XT> &a, const XT *__restrict__ x, XT *__restrict__ y,
+                                          int32_t tile, int lane) {
     const int64_t row0 = static_cast<int64_t>(tile) * 32;
     const int64_t row = row0 + lane;
     XT sum = XT(0);
@@ -191,6 +188,15 @@ spmv_bw32(const SpmvArgs<VT, XT> a, const XT *__restrict__ x, XT *__restrict__ y
         sum = add_rn(sum, tile_coo<XT>(a.cooRow, a.cooCol, a.cooVal, e0, e1, row0, lane, x));
     }
     if (row < a.n) __stcs(y + row, sum);
+}
+
+template <typename VT, typename XT, int U>
+__global__ void __launch_bounds__(256)
+spmv_bw32(const SpmvArgs<VT, XT> a, const XT *__restrict__ x, XT *__restrict__ y) {
+    const int lane = threadIdx.x & 31;
+    const int32_t tile = static_cast<int32_t>((static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5);
+    if (tile >= a.numTiles) return;  // warp-uniform
+    bw32_tile<VT, XT, U>(a, x, y, tile, lane);
 }
 
 // ---------------------------------------------------------------------------

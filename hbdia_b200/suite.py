@@ -2,6 +2,8 @@
 
     python -m hbdia_b200.suite precision   # banded n = 8M, FP64 / FP32 / BF16-scaled value storage
     python -m hbdia_b200.suite spmm        # 7-point Laplacian 128^3, k in {4, 16, 32}, FP64 and FP32 storage
+    python -m hbdia_b200.suite cg          # SPD 27-point 128^3: mixed-precision vs plain FP64 CG
+    python -m hbdia_b200.suite batched     # 64 stencils of edge U[16,96]: separate launches vs one batched launch
 
 Each measurement prints one JSON line.  Times are CUDA-event device times on
 a dedicated stream after warm-up; inputs exceed L2 unless stated.  Accuracy
@@ -142,15 +144,82 @@ def cg(args):
                           "converged": bool(r.converged)}), flush=True)
 
 
+def batched(args):
+    """64 27-point stencils of edge U[16, 96] (numpy default_rng(4)), matrix i
+    with 0.5 % off-pattern extras (seed 100 + i) and x ~ U(-1, 1) (seed
+    200 + i).  Timed on one stream: 64 single-matrix launches, the same
+    launches replayed from one CUDA graph, and one persistent batched launch
+    (graph-replayed; default configuration, then autotuned)."""
+    import torch
+    import hbdia_b200 as hb
+    edges = np.random.default_rng(4).integers(16, 97, args.count)
+    mats, xs, ys = [], [], []
+    for i, e in enumerate(edges.tolist()):
+        r, c, v = hb.generate_stencil27(e, e, e, extra_fraction=0.005, seed=100 + i)
+        n = e ** 3
+        m = hb.HBDIA(r, c, v, n, n)
+        m.convertToHBDIAFormat(32, 2, upload=False)
+        m.prepareForGPU(args.storage)
+        mats.append(m)
+        xs.append(torch.from_numpy(hb.fill_uniform(n, -1.0, 1.0, 200 + i)).cuda())
+        ys.append(torch.zeros(n, dtype=torch.float64, device="cuda"))
+    stream = torch.cuda.Stream()
+    sp = stream.cuda_stream
+    total_bytes = sum(m.bytesPerSpmv() for m in mats)
+    rows = int(sum(int(e) ** 3 for e in edges))
+    peak = _peak()
+
+    def report(name, ms, extra=None):
+        d = {"suite": "batched", "workload": f"{len(mats)} 27-point stencils, edge U[16,96] seed 4, "
+             f"0.5% extras, {rows} rows", "storage": ["fp64", "fp32", "bf16_scaled"][args.storage],
+             "method": name, "ms_per_batch": ms, "spmv_per_s": len(mats) * 1e3 / ms,
+             "bytes_per_batch": total_bytes, "gbs": total_bytes / (ms / 1e3) / 1e9,
+             "frac_of_peak": total_bytes / (ms / 1e3) / 1e9 / peak}
+        if extra:
+            d.update(extra)
+        print(json.dumps(d), flush=True)
+
+    def separate():
+        for m, x, y in zip(mats, xs, ys):
+            hb.spmv_device(m, x.data_ptr(), y.data_ptr(), sp)
+
+    report("64 single-matrix launches", _time(separate, stream))
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.stream(stream):
+        separate()  # warm (per-device kernel attributes set outside capture)
+        torch.cuda.synchronize()
+        with torch.cuda.graph(g, stream=stream):
+            for m, x, y in zip(mats, xs, ys):
+                hb.spmv_device(m, x.data_ptr(), y.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    with torch.cuda.stream(stream):  # replay() launches on the current stream
+        report("64 single-matrix launches in one CUDA graph", _time(g.replay, stream))
+    ref = [y.clone() for y in ys]
+    for y in ys:
+        y.zero_()
+    b = hb.Batch(mats)
+    b.bind([x.data_ptr() for x in xs], [y.data_ptr() for y in ys])
+    report("one persistent batched launch (graph), default config", _time(lambda: b.run(sp), stream))
+    ms_tune, ncand = b.autotune(sp)
+    c = b.config()
+    ms = _time(lambda: b.run(sp), stream)
+    torch.cuda.synchronize()
+    same = all(torch.equal(a.view(torch.int64), y.view(torch.int64)) for a, y in zip(ref, ys))
+    report("one persistent batched launch (graph), autotuned", ms,
+           {"config": {"threads": c.threadsPerBlock, "tiles_per_grab": c.tilesPerGrab, "graph": c.useGraph},
+            "candidates": ncand, "bit_identical_to_single": same})
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("what", choices=["precision", "spmm", "cg"])
+    ap.add_argument("what", choices=["precision", "spmm", "cg", "batched"])
+    ap.add_argument("--count", type=int, default=64)
+    ap.add_argument("--storage", type=int, default=0)
     ap.add_argument("--n", type=int, default=8 * 1024 * 1024)
     ap.add_argument("--grid", type=int, default=128)
     args = ap.parse_args(argv)
     import torch
     torch.cuda.set_device(0)
-    {"precision": precision, "spmm": spmm, "cg": cg}[args.what](args)
+    {"precision": precision, "spmm": spmm, "cg": cg, "batched": batched}[args.what](args)
     return 0
 
 

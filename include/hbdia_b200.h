@@ -316,6 +316,63 @@ typedef struct hbdia_cg_result {
 int hbdia_cg_solve(hbdia_matrix *m, const double *b, double *x, const hbdia_cg_options *options, void *stream,
                    hbdia_cg_result *result);
 
+/* ---------------------------------------------------------------- batches */
+
+/* Many matrices in one persistent launch.  No counterpart in the reference
+ * (its hbdiaSpMV, src/Operations/HBDIASpMV.cpp:186-251, takes one matrix per
+ * call); every y equals what hbdia_spmv_device / hbdia_spmm_device give for
+ * that matrix alone, bit for bit.  The matrices must be on the device, have
+ * blockWidth 32 and share value type and storage; they must outlive the
+ * batch and keep their device layout (no further hbdia_matrix_prepare_gpu)
+ * while it exists.  The matrices are cut into launch segments of up to 160;
+ * each segment is one kernel whose entry table is its parameter block.  Runs
+ * of one batch must not overlap (they share work counters): issue them on
+ * one stream.  Streams: NULL = the batch's own stream. */
+typedef struct hbdia_batch hbdia_batch;
+
+int hbdia_batch_create(hbdia_matrix *const *matrices, int32_t count, hbdia_batch **out);
+/* Waits only for the batch's own stream: synchronize the others first. */
+void hbdia_batch_destroy(hbdia_batch *b);
+
+/* Vectors of every matrix (device pointers): k[i] right-hand sides, X[i] an
+ * x of max(numRows, numCols) elements (k[i] == 1) or a row-major
+ * max(numRows, numCols) x k[i] block with leading dimension ldx[i]; Y[i] the
+ * same for y.  k == NULL means 1 for all; k[i] == 0 leaves matrix i out of
+ * the runs.  ldx / ldy == NULL mean k[i]; a k[i] == 1 vector is contiguous
+ * (ldx[i] = ldy[i] = 1 when given).  Binding only writes host-side
+ * parameter blocks: runs already enqueued keep the binding they were issued
+ * with, later runs use the new one.  On an error the previous binding
+ * stays. */
+int hbdia_batch_bind(hbdia_batch *b, const void *const *X, const int64_t *ldx, void *const *Y, const int64_t *ldy,
+                     const int32_t *k);
+
+/* One run over all bound matrices, asynchronous on `stream`.  With useGraph
+ * (the default) a CUDA graph (counter reset, then one kernel node per
+ * segment) is built on the first run of a configuration and replayed
+ * afterwards, its parameter blocks updated in place after a rebind. */
+int hbdia_batch_run(hbdia_batch *b, void *stream);
+
+typedef struct hbdia_batch_config {
+    int32_t threadsPerBlock; /* 128, 256 or 512 (default 256)                */
+    int32_t tilesPerGrab;    /* 32-row tiles a warp takes per atomic, 1-64    */
+    int32_t rhsTile;         /* right-hand sides per pass when k > 1: 4/8/16  */
+    int32_t useGraph;        /* replay a captured CUDA graph                  */
+} hbdia_batch_config;
+
+int hbdia_batch_set_config(hbdia_batch *b, const hbdia_batch_config *config);
+int hbdia_batch_get_config(const hbdia_batch *b, hbdia_batch_config *config);
+
+/* Times every configuration (threads x tiles per grab x RHS tile when some
+ * k > 1) on the bound vectors, on `stream`, and keeps the fastest.  The
+ * bound Y are overwritten. */
+int hbdia_batch_autotune(hbdia_batch *b, void *stream, float *msPerRun, int32_t *candidates);
+
+/* count, total 32-row tiles, and the algorithmic HBM bytes of one run with
+ * the current binding (per matrix: the SpMV's bytes, plus x, y and COO
+ * gathers for every further right-hand side). */
+int hbdia_batch_info(const hbdia_batch *b, int32_t *count, int32_t *totalTiles, int64_t *bytesPerRun);
+int hbdia_batch_stream(const hbdia_batch *b, void **stream);
+
 /* ---------------------------------------------------------------- workloads */
 
 /* Seeded synthetic 27-point stencil on an nx*ny*nz grid (Dirichlet boundary,
