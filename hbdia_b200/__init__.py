@@ -18,7 +18,7 @@ from typing import List, Optional, Sequence
 import numpy as np
 
 from . import _lib
-from ._lib import (KERNEL_AUTO, KERNEL_PIPE, KERNEL_ROWWISE, KERNEL_STAGED, KERNEL_WARP, TUNE_SPMM_TILE,
+from ._lib import (BATCH_CONCURRENT, BATCH_QUEUE, KERNEL_AUTO, KERNEL_PIPE, KERNEL_ROWWISE, KERNEL_STAGED, KERNEL_WARP, TUNE_SPMM_TILE,
                    TUNE_UNROLL, HBDIACudaError,
                    HBDIADeviceTimeout, STORE_BF16_SCALED, STORE_F32, STORE_NATIVE, MatrixInfo,
                    check as _check, load as _load)
@@ -428,8 +428,15 @@ class Batch:
     def run(self, stream: Optional[int] = None) -> None:
         _check(_load().hbdia_batch_run(self.handle, _stream_arg(stream)))
 
-    def set_config(self, threads: int = 256, grab: int = 2, rhs_tile: int = 8, graph: bool = True) -> None:
-        c = _lib.BatchConfig(threads, grab, rhs_tile, 1 if graph else 0)
+    def set_config(self, schedule: int = _lib.BATCH_CONCURRENT, streams: Optional[int] = None, threads: int = 256,
+                   grab: int = 4, rhs_tile: int = 8, graph: bool = True) -> None:
+        """schedule: BATCH_CONCURRENT (each matrix's own kernel on a ring of
+        ``streams`` streams) or BATCH_QUEUE (one persistent launch per 160
+        matrices, ``threads`` per CTA, ``grab`` tiles per atomic, ``rhs_tile``
+        right-hand sides per pass)."""
+        if streams is None:
+            streams = min(16, len(self._mats))
+        c = _lib.BatchConfig(schedule, streams, threads, grab, rhs_tile, 1 if graph else 0)
         _check(_load().hbdia_batch_set_config(self.handle, ctypes.byref(c)))
 
     def config(self) -> "_lib.BatchConfig":

@@ -30,6 +30,7 @@ KERNEL_AUTO, KERNEL_ROWWISE, KERNEL_WARP, KERNEL_STAGED, KERNEL_PIPE = 0, 1, 2, 
 TUNE_UNROLL, TUNE_SPMM_TILE = 1, 2
 
 HBDIA_F64, HBDIA_F32 = 0, 1
+BATCH_CONCURRENT, BATCH_QUEUE = 0, 1
 STORE_NATIVE, STORE_F32, STORE_BF16_SCALED = 0, 1, 2
 
 
@@ -60,7 +61,8 @@ class CgResult(ctypes.Structure):
 
 
 class BatchConfig(ctypes.Structure):
-    _fields_ = [("threadsPerBlock", c_i32), ("tilesPerGrab", c_i32), ("rhsTile", c_i32), ("useGraph", c_i32)]
+    _fields_ = [("schedule", c_i32), ("streams", c_i32), ("threadsPerBlock", c_i32), ("tilesPerGrab", c_i32),
+                ("rhsTile", c_i32), ("useGraph", c_i32)]
 
 
 class HBDIACudaError(RuntimeError):

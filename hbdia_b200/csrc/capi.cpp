@@ -663,14 +663,14 @@ int hbdia_batch_run(hbdia_batch *b, void *stream) {
 int hbdia_batch_set_config(hbdia_batch *b, const hbdia_batch_config *c) {
     return guarded([&] {
         need(b && c, HBDIA_ERR_INVALID_ARGUMENT, "null argument");
-        hbdia::batch_set_config(b->B, c->threadsPerBlock, c->tilesPerGrab, c->rhsTile, c->useGraph);
+        hbdia::batch_set_config(b->B, *c);
     });
 }
 
 int hbdia_batch_get_config(const hbdia_batch *b, hbdia_batch_config *c) {
     return guarded([&] {
         need(b && c, HBDIA_ERR_INVALID_ARGUMENT, "null argument");
-        hbdia::batch_get_config(b->B, &c->threadsPerBlock, &c->tilesPerGrab, &c->rhsTile, &c->useGraph);
+        hbdia::batch_get_config(b->B, *c);
     });
 }
 

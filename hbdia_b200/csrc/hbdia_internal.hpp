@@ -133,8 +133,8 @@ void batch_free(Batch *b);
 void batch_bind(Batch *b, const void *const *X, const int64_t *ldx, void *const *Y, const int64_t *ldy,
                 const int32_t *k);
 void batch_run(Batch *b, void *stream);
-void batch_set_config(Batch *b, int32_t threads, int32_t grab, int32_t rhsTile, int32_t useGraph);
-void batch_get_config(const Batch *b, int32_t *threads, int32_t *grab, int32_t *rhsTile, int32_t *useGraph);
+void batch_set_config(Batch *b, const hbdia_batch_config &c);
+void batch_get_config(const Batch *b, hbdia_batch_config &c);
 void batch_autotune(Batch *b, void *stream, float *ms, int32_t *candidates);
 void batch_info(const Batch *b, int32_t *count, int32_t *totalTiles, int64_t *bytesPerRun);
 void *batch_stream(const Batch *b);

@@ -148,8 +148,8 @@ def batched(args):
     """64 27-point stencils of edge U[16, 96] (numpy default_rng(4)), matrix i
     with 0.5 % off-pattern extras (seed 100 + i) and x ~ U(-1, 1) (seed
     200 + i).  Timed on one stream: 64 single-matrix launches, the same
-    launches replayed from one CUDA graph, and one persistent batched launch
-    (graph-replayed; default configuration, then autotuned)."""
+    launches replayed from one CUDA graph, and the batch (hbdia_batch_*)
+    with its concurrent and queue schedules, then autotuned."""
     import torch
     import hbdia_b200 as hb
     edges = np.random.default_rng(4).integers(16, 97, args.count)
@@ -198,14 +198,17 @@ def batched(args):
         y.zero_()
     b = hb.Batch(mats)
     b.bind([x.data_ptr() for x in xs], [y.data_ptr() for y in ys])
-    report("one persistent batched launch (graph), default config", _time(lambda: b.run(sp), stream))
+    report("batch, concurrent schedule (graph, 16 streams)", _time(lambda: b.run(sp), stream))
+    b.set_config(hb.BATCH_QUEUE)
+    report("batch, queue schedule (one persistent launch, graph)", _time(lambda: b.run(sp), stream))
     ms_tune, ncand = b.autotune(sp)
     c = b.config()
     ms = _time(lambda: b.run(sp), stream)
     torch.cuda.synchronize()
     same = all(torch.equal(a.view(torch.int64), y.view(torch.int64)) for a, y in zip(ref, ys))
-    report("one persistent batched launch (graph), autotuned", ms,
-           {"config": {"threads": c.threadsPerBlock, "tiles_per_grab": c.tilesPerGrab, "graph": c.useGraph},
+    report("batch, autotuned", ms,
+           {"config": {"schedule": ["concurrent", "queue"][c.schedule], "streams": c.streams,
+                       "threads": c.threadsPerBlock, "tiles_per_grab": c.tilesPerGrab, "graph": c.useGraph},
             "candidates": ncand, "bit_identical_to_single": same})
 
 

@@ -318,17 +318,22 @@ int hbdia_cg_solve(hbdia_matrix *m, const double *b, double *x, const hbdia_cg_o
 
 /* ---------------------------------------------------------------- batches */
 
-/* Many matrices in one persistent launch.  No counterpart in the reference
- * (its hbdiaSpMV, src/Operations/HBDIASpMV.cpp:186-251, takes one matrix per
- * call); every y equals what hbdia_spmv_device / hbdia_spmm_device give for
- * that matrix alone, bit for bit.  The matrices must be on the device, have
- * blockWidth 32 and share value type and storage; they must outlive the
- * batch and keep their device layout (no further hbdia_matrix_prepare_gpu)
- * while it exists.  The matrices are cut into launch segments of up to 160;
- * each segment is one kernel whose entry table is its parameter block.  Runs
- * of one batch must not overlap (they share work counters): issue them on
- * one stream.  Streams: NULL = the batch's own stream. */
+/* Many matrices computed as one unit of work.  No counterpart in the
+ * reference (its hbdiaSpMV, src/Operations/HBDIASpMV.cpp:186-251, takes one
+ * matrix per call); every y equals what hbdia_spmv_device / hbdia_spmm_device
+ * give for that matrix alone, bit for bit.  The matrices must be on the
+ * device, have blockWidth 32 and share value type and storage; they must
+ * outlive the batch and keep their device layout (no further
+ * hbdia_matrix_prepare_gpu) while it exists.  Two schedules:
+ *  - CONCURRENT (default): each matrix's own single-matrix kernel, on a ring
+ *    of auxiliary streams forked from and joined into the run's stream, so
+ *    the kernels overlap on the GPU;
+ *  - QUEUE: one persistent launch per segment of up to 160 matrices, warps
+ *    taking 32-row tiles from an atomic counter (for many tiny matrices).
+ * Runs of one batch must not overlap (they share streams and counters):
+ * issue them on one stream.  Streams: NULL = the batch's own stream. */
 typedef struct hbdia_batch hbdia_batch;
+typedef enum hbdia_batch_schedule { HBDIA_BATCH_CONCURRENT = 0, HBDIA_BATCH_QUEUE = 1 } hbdia_batch_schedule;
 
 int hbdia_batch_create(hbdia_matrix *const *matrices, int32_t count, hbdia_batch **out);
 /* Waits only for the batch's own stream: synchronize the others first. */
@@ -347,24 +352,26 @@ int hbdia_batch_bind(hbdia_batch *b, const void *const *X, const int64_t *ldx, v
                      const int32_t *k);
 
 /* One run over all bound matrices, asynchronous on `stream`.  With useGraph
- * (the default) a CUDA graph (counter reset, then one kernel node per
- * segment) is built on the first run of a configuration and replayed
- * afterwards, its parameter blocks updated in place after a rebind. */
+ * (the default) the run is a CUDA graph, made on the first run of a
+ * configuration and replayed afterwards; a rebind updates it in place. */
 int hbdia_batch_run(hbdia_batch *b, void *stream);
 
 typedef struct hbdia_batch_config {
-    int32_t threadsPerBlock; /* 128, 256 or 512 (default 256)                */
-    int32_t tilesPerGrab;    /* 32-row tiles a warp takes per atomic, 1-64    */
-    int32_t rhsTile;         /* right-hand sides per pass when k > 1: 4/8/16  */
-    int32_t useGraph;        /* replay a captured CUDA graph                  */
+    int32_t schedule;        /* hbdia_batch_schedule (default CONCURRENT)             */
+    int32_t streams;         /* CONCURRENT: auxiliary streams, 1-64 (min(16, count))  */
+    int32_t threadsPerBlock; /* QUEUE: 128, 256 or 512 (default 256)                  */
+    int32_t tilesPerGrab;    /* QUEUE: 32-row tiles a warp takes per atomic, 1-64 (4) */
+    int32_t rhsTile;         /* QUEUE: right-hand sides per pass when k > 1: 4/8/16   */
+    int32_t useGraph;        /* replay a CUDA graph (default 1)                       */
 } hbdia_batch_config;
 
 int hbdia_batch_set_config(hbdia_batch *b, const hbdia_batch_config *config);
 int hbdia_batch_get_config(const hbdia_batch *b, hbdia_batch_config *config);
 
-/* Times every configuration (threads x tiles per grab x RHS tile when some
- * k > 1) on the bound vectors, on `stream`, and keeps the fastest.  The
- * bound Y are overwritten. */
+/* Times the configurations (CONCURRENT with 4, 16, 64 streams; QUEUE with
+ * threads x tiles per grab x, when some k > 1, RHS tile) on the bound
+ * vectors, on `stream`, and keeps the fastest.  The bound Y are
+ * overwritten. */
 int hbdia_batch_autotune(hbdia_batch *b, void *stream, float *msPerRun, int32_t *candidates);
 
 /* count, total 32-row tiles, and the algorithmic HBM bytes of one run with

@@ -103,24 +103,37 @@ def test_batch_matches_single_matrix(lib, orc):
 @pytest.mark.parametrize("threads", [128, 256, 512])
 @pytest.mark.parametrize("grab", [1, 3, 8])
 @pytest.mark.parametrize("graph", [False, True])
-def test_batch_configs_identical(lib, threads, grab, graph):
+def test_batch_queue_configs_identical(lib, threads, grab, graph):
     mats = _matrices(lib)
     xs, ys = _vectors(mats, np.float64)
     b = lib.Batch(mats)
-    b.set_config(threads, grab, 8, graph)
+    b.set_config(lib.BATCH_QUEUE, None, threads, grab, 8, graph)
     _bind(b, xs, ys)
     b.run(0)
     b.run(0)  # replay
     _check_all(lib, mats, xs, ys)
 
 
-@pytest.mark.parametrize("tile", [4, 8, 16])
-def test_batch_mixed_rhs(lib, tile):
+@pytest.mark.parametrize("streams", [1, 3, 16, 64])
+@pytest.mark.parametrize("graph", [False, True])
+def test_batch_concurrent_configs_identical(lib, streams, graph):
+    mats = _matrices(lib)
+    xs, ys = _vectors(mats, np.float64)
+    b = lib.Batch(mats)
+    b.set_config(lib.BATCH_CONCURRENT, streams, graph=graph)
+    _bind(b, xs, ys)
+    b.run(0)
+    b.run(0)  # replay
+    _check_all(lib, mats, xs, ys)
+
+
+@pytest.mark.parametrize("schedule,tile", [(0, 8), (1, 4), (1, 8), (1, 16)])
+def test_batch_mixed_rhs(lib, schedule, tile):
     mats = _matrices(lib)
     k = [1, 3, 8, 0, 2, 17, 1, 5, 1]
     xs, ys = _vectors(mats, np.float64, k)
     b = lib.Batch(mats)
-    b.set_config(256, 2, tile, True)
+    b.set_config(schedule, None, 256, 2, tile, True)
     _bind(b, xs, ys, k)
     b.run(0)
     _check_all(lib, mats, xs, ys, k)
@@ -149,11 +162,13 @@ def test_batch_strided_rhs(lib):
         assert (y[:, :2] == 0).all() and (y[:, 2 + ki:] == 0).all()
 
 
-def test_batch_rebind_under_graph(lib):
+@pytest.mark.parametrize("schedule", [0, 1])
+def test_batch_rebind_under_graph(lib, schedule):
     """New pointers and a switch between single-vector and multi-RHS bindings
     replay the right graph."""
     mats = _matrices(lib)
     b = lib.Batch(mats)
+    b.set_config(schedule)
     for seed, k in ((1, None), (2, [1, 2, 1, 1, 3, 1, 1, 1, 1]), (3, None), (4, [2] * 9)):
         xs, ys = _vectors(mats, np.float64, k, seed=seed)
         _bind(b, xs, ys, k)
@@ -162,11 +177,14 @@ def test_batch_rebind_under_graph(lib):
 
 
 @pytest.mark.parametrize("dtype,storage", [(np.float64, 1), (np.float64, 2), (np.float32, 0)])
-def test_batch_storage_and_dtype(lib, dtype, storage):
+@pytest.mark.parametrize("multi", [False, True])
+@pytest.mark.parametrize("schedule", [0, 1])
+def test_batch_storage_and_dtype(lib, dtype, storage, multi, schedule):
     mats = _matrices(lib, dtype, storage)
-    k = [1, 2, 1, 1, 6, 1, 1, 3, 1]
+    k = [1, 2, 1, 1, 6, 1, 1, 3, 1] if multi else [1, 1, 0, 1, 1, 1, 1, 1, 1]
     xs, ys = _vectors(mats, dtype, k)
     b = lib.Batch(mats)
+    b.set_config(schedule)
     _bind(b, xs, ys, k)
     b.run(0)
     _check_all(lib, mats, xs, ys, k)
@@ -179,13 +197,27 @@ def test_batch_autotune_keeps_results(lib):
     b = lib.Batch(mats)
     _bind(b, xs, ys, k)
     ms, n = b.autotune(0)
-    assert ms > 0 and n == 3 * 5 * 3
+    assert ms > 0 and n == 3 + 3 * 5 * 3  # 3 stream counts + threads x grab x RHS tile
     c = b.config()
+    assert c.schedule in (0, 1) and c.streams in (4, 9, 16, 64)
     assert c.threadsPerBlock in (128, 256, 512) and c.tilesPerGrab in (1, 2, 4, 8, 16) and c.rhsTile in (4, 8, 16)
     for y in ys:
         y.fill_(float("nan"))
     b.run(0)
     _check_all(lib, mats, xs, ys, k)
+
+
+def test_batch_autotune_single_vector(lib):
+    mats = _matrices(lib)
+    xs, ys = _vectors(mats, np.float64)
+    b = lib.Batch(mats)
+    _bind(b, xs, ys)
+    ms, n = b.autotune(0)
+    assert ms > 0 and n == 3 + 3 * 5  # 3 stream counts + threads x grab
+    for y in ys:
+        y.fill_(float("nan"))
+    b.run(0)
+    _check_all(lib, mats, xs, ys)
 
 
 def test_batch_rejections(lib):
@@ -195,7 +227,11 @@ def test_batch_rejections(lib):
     with pytest.raises(ValueError):
         b.run(0)  # nothing bound
     with pytest.raises(ValueError):
-        b.set_config(192, 2, 8, True)
+        b.set_config(lib.BATCH_QUEUE, None, 192, 2, 8, True)
+    with pytest.raises(ValueError):
+        b.set_config(lib.BATCH_CONCURRENT, 65)
+    with pytest.raises(ValueError):
+        b.set_config(7)
     with pytest.raises(ValueError):
         b.bind([0, 0], [0, 0])
     r, c, v = lib.generate_stencil7(6, 6, 6, 6.0, -1.0)
@@ -219,9 +255,10 @@ def test_batch_rejections(lib):
         b.bind([x.data_ptr()] * 2, [x.data_ptr()] * 2, k=[1, 1], ldx=[7, 1], ldy=[1, 1])
 
 
-def test_batch_many_segments(lib):
-    """More matrices than one launch segment holds (160): three segments,
-    each its own kernel node, rebound and replayed."""
+@pytest.mark.parametrize("schedule", [0, 1])
+def test_batch_many_segments(lib, schedule):
+    """330 matrices: three queue segments (each its own kernel node), or 330
+    concurrent launches; rebound and replayed."""
     rng = np.random.default_rng(29)
     mats = []
     for i in range(330):
@@ -232,6 +269,7 @@ def test_batch_many_segments(lib):
         m.prepareForGPU(0)
         mats.append(m)
     b = lib.Batch(mats)
+    b.set_config(schedule)
     for seed, k in ((5, None), (6, [int(rng.integers(0, 4)) for _ in range(330)])):
         xs, ys = _vectors(mats, np.float64, k, seed=seed)
         _bind(b, xs, ys, k)
