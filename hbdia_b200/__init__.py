@@ -18,7 +18,7 @@ from typing import List, Optional, Sequence
 import numpy as np
 
 from . import _lib
-from ._lib import (BATCH_CONCURRENT, BATCH_QUEUE, KERNEL_AUTO, KERNEL_PIPE, KERNEL_ROWWISE, KERNEL_STAGED, KERNEL_WARP, TUNE_SPMM_TILE,
+from ._lib import (BATCH_CONCURRENT, BATCH_QUEUE, REQ_CG, REQ_SPMV, KERNEL_AUTO, KERNEL_PIPE, KERNEL_ROWWISE, KERNEL_STAGED, KERNEL_WARP, TUNE_SPMM_TILE,
                    TUNE_UNROLL, HBDIACudaError,
                    HBDIADeviceTimeout, STORE_BF16_SCALED, STORE_F32, STORE_NATIVE, MatrixInfo,
                    check as _check, load as _load)
@@ -332,6 +332,13 @@ def spmm_device(matrix: HBDIA, X_ptr: int, ldx: int, Y_ptr: int, ldy: int, k: in
                                      k, _stream_arg(stream)))
 
 
+def spmm_device_colmajor(matrix: HBDIA, X_ptr: int, ldx: int, Y_ptr: int, ldy: int, k: int,
+                         stream: Optional[int] = None) -> None:
+    """Y = A X for k column-major right-hand sides (vector j at X + j*ldx)."""
+    _check(_load().hbdia_spmm_device_colmajor(matrix.handle, ctypes.c_void_p(X_ptr), ldx, ctypes.c_void_p(Y_ptr),
+                                              ldy, k, _stream_arg(stream)))
+
+
 def spmv_host(matrix: HBDIA, x: np.ndarray, y: np.ndarray) -> None:
     """End-to-end y = A x on host arrays (copies in, SpMV, copies out, sync)."""
     _check(_load().hbdia_spmv_host(matrix.handle, ctypes.c_void_p(x.ctypes.data), ctypes.c_void_p(y.ctypes.data)))
@@ -372,10 +379,12 @@ def generate_banded(n: int, offsets: Sequence[int], lo: float = 0.5, hi: float =
     return _two_call(_load().hbdia_generate_banded, n, _vp(o), len(o), lo, hi, drop, scatter, seed)
 
 
-def generate_stencil27_spd(nx: int, ny: int, nz: int, shift: float = 1e-3, seed: int = 7):
+def generate_stencil27_spd(nx: int, ny: int, nz: int, shift: float = 1e-3, seed: int = 7,
+                           extra_fraction: float = 0.0):
     """SPD symmetrised 27-point stencil (symmetric random off-diagonals -(0.5 + u),
-    diagonal (1 + shift) * row |sum|)."""
-    return _two_call(_load().hbdia_generate_stencil27_spd, nx, ny, nz, float(shift), seed)
+    plus symmetric off-pattern pairs making up ``extra_fraction`` of the
+    stencil's entries, diagonal (1 + shift) * row |sum|)."""
+    return _two_call(_load().hbdia_generate_stencil27_spd, nx, ny, nz, float(shift), float(extra_fraction), seed)
 
 
 def cg_solve(matrix: HBDIA, b_ptr: int, x_ptr: int, tol: float = 1e-10, inner_storage: int = STORE_F32,
@@ -468,3 +477,65 @@ def fill_uniform(n: int, lo: float, hi: float, seed: int) -> np.ndarray:
     out = np.empty(n, np.float64)
     _check(_load().hbdia_fill_uniform(_vp(out), n, lo, hi, seed))
     return out
+
+
+class Server:
+    """Resident matrices and a request queue (hbdia_server_*): SpMV requests
+    served with continuous batching (same-matrix requests become one SpMM per
+    step), CG requests on a pool of solver threads.  ``options`` overrides
+    fields of hbdia_server_default_options (memoryBudget, batching, maxRhs,
+    spmvStorage, cgInnerStorage, cgWorkers, cgTol, cgInnerTol, ...)."""
+
+    def __init__(self, **options):
+        o = _lib.ServerOptions()
+        _load().hbdia_server_default_options(ctypes.byref(o))
+        for k, v in options.items():
+            if not hasattr(o, k):
+                raise TypeError(f"unknown server option {k}")
+            setattr(o, k, v)
+        h = ctypes.c_void_p()
+        _check(_load().hbdia_server_create(ctypes.byref(o), ctypes.byref(h)))
+        self.handle = h
+        self.options = o
+        self._live = {}  # ticket -> (x, y): keeps the host arrays alive until collected
+
+    def close(self) -> None:
+        h = getattr(self, "handle", None)
+        if h is not None and h.value:
+            _load().hbdia_server_destroy(h)
+            self.handle = None
+            self._live.clear()
+
+    def __del__(self):
+        self.close()
+
+    def add_matrix(self, matrix: HBDIA) -> int:
+        mid = ctypes.c_int32(0)
+        _check(_load().hbdia_server_add_matrix(self.handle, matrix.handle, ctypes.byref(mid)))
+        return mid.value
+
+    def submit(self, matrix_id: int, kind: int, x: np.ndarray, y: np.ndarray) -> int:
+        """x: float64 right-hand side (numCols), y: float64 output (numRows);
+        both must stay untouched until wait(ticket) returns."""
+        if x.dtype != np.float64 or y.dtype != np.float64 or not x.flags.c_contiguous or not y.flags.c_contiguous:
+            raise ValueError("request vectors must be contiguous float64 arrays")
+        t = ctypes.c_uint64(0)
+        _check(_load().hbdia_server_submit(self.handle, matrix_id, kind, _vp(x), _vp(y), ctypes.byref(t)))
+        self._live[t.value] = (x, y)
+        return t.value
+
+    def pause(self, paused: bool = True) -> None:
+        """Hold (True) or release (False) the queues; released backlogs are
+        batched together."""
+        _check(_load().hbdia_server_pause(self.handle, 1 if paused else 0))
+
+    def wait(self, ticket: int) -> "_lib.RequestInfo":
+        info = _lib.RequestInfo()
+        _check(_load().hbdia_server_wait(self.handle, ticket, ctypes.byref(info)))
+        self._live.pop(ticket, None)
+        return info
+
+    def stats(self) -> "_lib.ServerStats":
+        s = _lib.ServerStats()
+        _check(_load().hbdia_server_get_stats(self.handle, ctypes.byref(s)))
+        return s

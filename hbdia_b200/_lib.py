@@ -31,6 +31,7 @@ TUNE_UNROLL, TUNE_SPMM_TILE = 1, 2
 
 HBDIA_F64, HBDIA_F32 = 0, 1
 BATCH_CONCURRENT, BATCH_QUEUE = 0, 1
+REQ_SPMV, REQ_CG = 0, 1
 STORE_NATIVE, STORE_F32, STORE_BF16_SCALED = 0, 1, 2
 
 
@@ -63,6 +64,23 @@ class CgResult(ctypes.Structure):
 class BatchConfig(ctypes.Structure):
     _fields_ = [("schedule", c_i32), ("streams", c_i32), ("threadsPerBlock", c_i32), ("tilesPerGrab", c_i32),
                 ("rhsTile", c_i32), ("useGraph", c_i32)]
+
+
+class ServerOptions(ctypes.Structure):
+    _fields_ = [("memoryBudget", c_i64), ("batching", c_i32), ("maxRhs", c_i32), ("spmvStorage", c_i32),
+                ("cgInnerStorage", c_i32), ("cgWorkers", c_i32), ("cgMaxOuter", c_i32), ("cgMaxInner", c_i32),
+                ("cgCheckEvery", c_i32), ("cgTol", c_dbl), ("cgInnerTol", c_dbl)]
+
+
+class RequestInfo(ctypes.Structure):
+    _fields_ = [("status", c_i32), ("kind", c_i32), ("matrix", c_i32), ("batchRhs", c_i32),
+                ("submitted", c_dbl), ("started", c_dbl), ("finished", c_dbl),
+                ("cgOuter", c_i32), ("cgInner", c_i32), ("cgRelResidual", c_dbl)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("completed", c_i64), ("spmvRequests", c_i64), ("cgRequests", c_i64), ("spmvSteps", c_i64),
+                ("spmvLaunches", c_i64), ("deviceBytes", c_i64), ("matrices", c_i32)]
 
 
 class HBDIACudaError(RuntimeError):
@@ -123,6 +141,7 @@ _SIGS = [
     ("hbdia_spmv", ctypes.c_int, [c_vp, c_vp, c_vp, c_i32, c_i32]),
     ("hbdia_spmv_device", ctypes.c_int, [c_vp, c_vp, c_vp, c_vp]),
     ("hbdia_spmm_device", ctypes.c_int, [c_vp, c_vp, c_i64, c_vp, c_i64, c_i32, c_vp]),
+    ("hbdia_spmm_device_colmajor", ctypes.c_int, [c_vp, c_vp, c_i64, c_vp, c_i64, c_i32, c_vp]),
     ("hbdia_spmv_host", ctypes.c_int, [c_vp, c_vp, c_vp]),
     ("hbdia_spmv_host_noalloc", ctypes.c_int, [c_vp, c_vp, c_vp]),
     ("hbdia_generate_stencil27", ctypes.c_int,
@@ -131,7 +150,8 @@ _SIGS = [
     ("hbdia_generate_banded", ctypes.c_int,
      [c_i32, c_vp, c_i32, c_dbl, c_dbl, c_dbl, c_dbl, c_u64, c_i64p, c_vp, c_vp, c_vp]),
     ("hbdia_fill_uniform", ctypes.c_int, [c_vp, c_i64, c_dbl, c_dbl, c_u64]),
-    ("hbdia_generate_stencil27_spd", ctypes.c_int, [c_i32, c_i32, c_i32, c_dbl, c_u64, c_i64p, c_vp, c_vp, c_vp]),
+    ("hbdia_generate_stencil27_spd", ctypes.c_int,
+     [c_i32, c_i32, c_i32, c_dbl, c_dbl, c_u64, c_i64p, c_vp, c_vp, c_vp]),
     ("hbdia_cg_solve", ctypes.c_int, [c_vp, c_vp, c_vp, ctypes.POINTER(CgOptions), c_vp, ctypes.POINTER(CgResult)]),
     ("hbdia_batch_create", ctypes.c_int, [c_vpp, c_i32, c_vpp]),
     ("hbdia_batch_destroy", None, [c_vp]),
@@ -142,6 +162,14 @@ _SIGS = [
     ("hbdia_batch_autotune", ctypes.c_int, [c_vp, c_vp, ctypes.POINTER(ctypes.c_float), c_i32p]),
     ("hbdia_batch_info", ctypes.c_int, [c_vp, c_i32p, c_i32p, c_i64p]),
     ("hbdia_batch_stream", ctypes.c_int, [c_vp, c_vpp]),
+    ("hbdia_server_default_options", None, [ctypes.POINTER(ServerOptions)]),
+    ("hbdia_server_create", ctypes.c_int, [ctypes.POINTER(ServerOptions), c_vpp]),
+    ("hbdia_server_destroy", None, [c_vp]),
+    ("hbdia_server_add_matrix", ctypes.c_int, [c_vp, c_vp, c_i32p]),
+    ("hbdia_server_submit", ctypes.c_int, [c_vp, c_i32, c_i32, c_vp, c_vp, ctypes.POINTER(ctypes.c_uint64)]),
+    ("hbdia_server_pause", ctypes.c_int, [c_vp, c_i32]),
+    ("hbdia_server_wait", ctypes.c_int, [c_vp, ctypes.c_uint64, ctypes.POINTER(RequestInfo)]),
+    ("hbdia_server_get_stats", ctypes.c_int, [c_vp, ctypes.POINTER(ServerStats)]),
 ]
 
 # every C-ABI entry point (the exported-symbol check in the tests uses this list)

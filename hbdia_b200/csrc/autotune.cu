@@ -119,7 +119,7 @@ void autotune(DevicePlan &P, const void *X, int64_t ldx, void *Y, int64_t ldy, i
                 cand.push_back(c);
             }
         } else {
-            for (int32_t t : {4, 8, 16, 32}) {
+            for (int32_t t : {2, 4, 8, 16, 32}) {
                 if (t > 4 && t / 2 >= k) break;  // a tile twice as wide as k only adds idle work
                 Choice c;
                 c.tile = t;

@@ -11,35 +11,17 @@
 #include <new>
 #include <string>
 
+#include "handles.hpp"
 #include "hbdia_internal.hpp"
 
 using hbdia::Error;
 
-struct hbdia_vector {
-    int32_t dtype = HBDIA_F64;
-    int64_t n = 0;
-    void *d = nullptr;
-};
-
-struct hbdia_matrix {
-    int32_t dtype = HBDIA_F64;
-    bool hasCOO = false;
-    bool hasHBDIA = false;
-    bool hostLayout = false;  // host layout materialised
-    hbdia::Coo<double> c64;
-    hbdia::Coo<float> c32;
-    hbdia::HostLayout<double> L64;
-    hbdia::HostLayout<float> L32;
-    hbdia::DevicePlan plan;
-    hbdia::DevicePlan innerPlan;        // reduced-storage copy for the CG inner iterations
-    hbdia::CgWork *cg = nullptr;        // CG workspace
-    int32_t blockWidth = 0, threshold = 0;
-    int64_t maxCoo = 0;
-    std::mutex hostMu;  // serialises hbdia_spmv_host's scratch buffers
-};
-
 struct hbdia_batch {
     hbdia::Batch *B = nullptr;
+};
+
+struct hbdia_server {
+    hbdia::Server *S = nullptr;
 };
 
 namespace {
@@ -430,8 +412,8 @@ int hbdia_matrix_set_tuning(hbdia_matrix *m, int32_t key, int32_t value) {
             return;
         }
         if (key == HBDIA_TUNE_SPMM_TILE) {
-            need(value == 0 || value == 4 || value == 8 || value == 16 || value == 32, HBDIA_ERR_INVALID_ARGUMENT,
-                 "SpMM tile must be 0, 4, 8, 16 or 32");
+            need(value == 0 || value == 2 || value == 4 || value == 8 || value == 16 || value == 32,
+                 HBDIA_ERR_INVALID_ARGUMENT, "SpMM tile must be 0, 2, 4, 8, 16 or 32");
             m->plan.spmmTileForced = value;
             return;
         }
@@ -569,6 +551,15 @@ int hbdia_spmm_device(const hbdia_matrix *m, const void *X, int64_t ldx, void *Y
     });
 }
 
+int hbdia_spmm_device_colmajor(const hbdia_matrix *m, const void *X, int64_t ldx, void *Y, int64_t ldy, int32_t k,
+                               void *stream) {
+    return guarded([&] {
+        need(m != nullptr, HBDIA_ERR_INVALID_ARGUMENT, "null matrix");
+        need(m->plan.base != nullptr, HBDIA_ERR_NOT_CONVERTED, "matrix has no device layout");
+        hbdia::launch_spmm(m->plan, X, ldx, Y, ldy, k, stream, true);
+    });
+}
+
 int hbdia_spmv_host(hbdia_matrix *m, const void *xh, void *yh) {
     return guarded([&] {
         need(m && xh && yh, HBDIA_ERR_INVALID_ARGUMENT, "null argument");
@@ -619,6 +610,65 @@ int hbdia_cg_solve(hbdia_matrix *m, const double *b, double *x, const hbdia_cg_o
         r.converged = r.relResidual <= opt->tol;
         throw_if_timeout(read_status(m, true));
         if (out) *out = r;
+    });
+}
+
+// ---------------------------------------------------------------- serving
+void hbdia_server_default_options(hbdia_server_options *o) {
+    if (o) hbdia::server_default_options(o);
+}
+
+int hbdia_server_create(const hbdia_server_options *o, hbdia_server **out) {
+    return guarded([&] {
+        need(out != nullptr, HBDIA_ERR_INVALID_ARGUMENT, "null argument");
+        *out = nullptr;
+        hbdia_server_options d;
+        hbdia::server_default_options(&d);
+        auto s = std::make_unique<hbdia_server>();
+        s->S = hbdia::server_create(o ? *o : d);
+        *out = s.release();
+    });
+}
+
+void hbdia_server_destroy(hbdia_server *s) {
+    if (!s) return;
+    hbdia::server_destroy(s->S);
+    delete s;
+}
+
+int hbdia_server_add_matrix(hbdia_server *s, const hbdia_matrix *m, int32_t *id) {
+    return guarded([&] {
+        need(s && m && id, HBDIA_ERR_INVALID_ARGUMENT, "null argument");
+        *id = hbdia::server_add_matrix(s->S, m);
+    });
+}
+
+int hbdia_server_submit(hbdia_server *s, int32_t matrix, int32_t kind, const double *x, double *y,
+                        uint64_t *ticket) {
+    return guarded([&] {
+        need(s && ticket, HBDIA_ERR_INVALID_ARGUMENT, "null argument");
+        *ticket = hbdia::server_submit(s->S, matrix, kind, x, y);
+    });
+}
+
+int hbdia_server_pause(hbdia_server *s, int32_t paused) {
+    return guarded([&] {
+        need(s != nullptr, HBDIA_ERR_INVALID_ARGUMENT, "null server");
+        hbdia::server_pause(s->S, paused != 0);
+    });
+}
+
+int hbdia_server_wait(hbdia_server *s, uint64_t ticket, hbdia_request_info *info) {
+    return guarded([&] {
+        need(s != nullptr, HBDIA_ERR_INVALID_ARGUMENT, "null server");
+        hbdia::server_wait(s->S, ticket, info);
+    });
+}
+
+int hbdia_server_get_stats(hbdia_server *s, hbdia_server_stats *out) {
+    return guarded([&] {
+        need(s && out, HBDIA_ERR_INVALID_ARGUMENT, "null argument");
+        hbdia::server_stats(s->S, out);
     });
 }
 
@@ -720,9 +770,11 @@ int hbdia_generate_banded(int32_t n, const int32_t *offsets, int32_t numOffsets,
     });
 }
 
-int hbdia_generate_stencil27_spd(int32_t nx, int32_t ny, int32_t nz, double shift, uint64_t seed, int64_t *nnz,
-                                 int32_t *rows, int32_t *cols, double *values) {
-    return guarded([&] { hbdia::generate_stencil27_spd(nx, ny, nz, shift, seed, nnz, rows, cols, values); });
+int hbdia_generate_stencil27_spd(int32_t nx, int32_t ny, int32_t nz, double shift, double extraFraction,
+                                 uint64_t seed, int64_t *nnz, int32_t *rows, int32_t *cols, double *values) {
+    return guarded([&] {
+        hbdia::generate_stencil27_spd(nx, ny, nz, shift, extraFraction, seed, nnz, rows, cols, values);
+    });
 }
 
 int hbdia_fill_uniform(double *out, int64_t n, double lo, double hi, uint64_t seed) {

@@ -163,7 +163,7 @@ void cg_free(CgWork *w) {
 }
 
 CgWork *cg_work(CgWork *w, int64_t n) {
-    if (w && w->n == n) return w;
+    if (w && w->n >= n) return w;  // a larger workspace serves smaller systems
     cg_free(w);
     w = new CgWork();
     w->n = n;
@@ -195,7 +195,10 @@ void cg_solve(const DevicePlan &A64, const DevicePlan &Ainner, CgWork *w, const 
     const auto t0 = std::chrono::steady_clock::now();
     cudaStream_t s = static_cast<cudaStream_t>(stream ? stream : A64.stream);
     const int64_t n = A64.n;
-    const int G = w->nparts;
+    if (n > w->n) throw Error(HBDIA_ERR_INVALID_ARGUMENT, "CG workspace smaller than the system");
+    // reduction partitions from n alone (what a workspace sized to n has), so
+    // the result does not depend on the workspace's size
+    const int G = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(w->nparts, (n + kThreads - 1) / kThreads)));
     std::vector<double> tmp;
     // ||b||
     dot_partial<<<G, kThreads, 0, s>>>(b, b, n, w->nPart);

@@ -6,6 +6,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <fstream>
 #include <iostream>
@@ -433,20 +434,68 @@ inline uint64_t splitmix(uint64_t z) {
 }
 }  // namespace
 
-int generate_stencil27_spd(int32_t nx, int32_t ny, int32_t nz, double shift, uint64_t seed, int64_t *nnzOut,
-                           int32_t *rows, int32_t *cols, double *vals) {
-    if (nx <= 0 || ny <= 0 || nz <= 0 || !nnzOut || shift < 0)
+int generate_stencil27_spd(int32_t nx, int32_t ny, int32_t nz, double shift, double extraFraction, uint64_t seed,
+                           int64_t *nnzOut, int32_t *rows, int32_t *cols, double *vals) {
+    if (nx <= 0 || ny <= 0 || nz <= 0 || !nnzOut || shift < 0 || extraFraction < 0 || extraFraction > 1)
         throw Error(HBDIA_ERR_INVALID_ARGUMENT, "bad SPD stencil arguments");
     const int64_t n = static_cast<int64_t>(nx) * ny * nz;
     if (n > 2147483647LL) throw Error(HBDIA_ERR_INVALID_ARGUMENT, "grid too large for int32 indices");
-    *nnzOut = (3LL * nx - 2) * (3LL * ny - 2) * (3LL * nz - 2);
-    if (!rows) return HBDIA_OK;
+    const int64_t stencilNnz = (3LL * nx - 2) * (3LL * ny - 2) * (3LL * nz - 2);
     const int64_t plane = static_cast<int64_t>(nx) * ny;
+    // Symmetric off-pattern pairs (i < j, j outside i's 27-point neighbourhood,
+    // no pair twice): floor(extraFraction * stencil nnz / 2) of them, each
+    // stored as (i, j) and (j, i), drawn from a splitmix sequence of the seed.
+    const int64_t pairs = static_cast<int64_t>(std::floor(extraFraction * static_cast<double>(stencilNnz) / 2.0));
+    // unordered pairs outside the pattern: all pairs minus the stencil's off-diagonal ones
+    const int64_t farPairs = n * (n - 1) / 2 - (stencilNnz - n) / 2;
+    if (pairs > farPairs / 2)
+        throw Error(HBDIA_ERR_INVALID_ARGUMENT, "grid too small for that many off-pattern entries");
+    std::vector<std::pair<int32_t, int32_t>> extra;
+    extra.reserve(static_cast<size_t>(pairs));
+    {
+        std::unordered_set<uint64_t> seen;
+        uint64_t state = seed ^ 0x5bd1e9955bd1e995ULL;
+        auto near = [&](int64_t a, int64_t b) {
+            const int64_t ax = a % nx, ay = (a / nx) % ny, az = a / plane;
+            const int64_t bx = b % nx, by = (b / nx) % ny, bz = b / plane;
+            return std::llabs(ax - bx) <= 1 && std::llabs(ay - by) <= 1 && std::llabs(az - bz) <= 1;
+        };
+        while (static_cast<int64_t>(extra.size()) < pairs) {
+            state = splitmix(state);
+            int64_t a = static_cast<int64_t>(state % static_cast<uint64_t>(n));
+            state = splitmix(state);
+            int64_t b = static_cast<int64_t>(state % static_cast<uint64_t>(n));
+            if (a == b || near(a, b)) continue;
+            if (a > b) std::swap(a, b);
+            if (!seen.insert(static_cast<uint64_t>(a) * static_cast<uint64_t>(n) + static_cast<uint64_t>(b)).second)
+                continue;
+            extra.emplace_back(static_cast<int32_t>(a), static_cast<int32_t>(b));
+        }
+    }
+    *nnzOut = stencilNnz + 2 * pairs;
+    if (!rows) return HBDIA_OK;
+    // per-row extra columns, ascending
+    std::vector<int64_t> xstart(static_cast<size_t>(n) + 1, 0);
+    for (const auto &e : extra) {
+        ++xstart[e.first + 1];
+        ++xstart[e.second + 1];
+    }
+    for (int64_t r = 0; r < n; ++r) xstart[r + 1] += xstart[r];
+    std::vector<int32_t> xcol(static_cast<size_t>(2 * pairs));
+    {
+        std::vector<int64_t> fill(xstart.begin(), xstart.end() - 1);
+        for (const auto &e : extra) {
+            xcol[fill[e.first]++] = e.second;
+            xcol[fill[e.second]++] = e.first;
+        }
+    }
+#pragma omp parallel for schedule(static)
+    for (int64_t r = 0; r < n; ++r) std::sort(xcol.begin() + xstart[r], xcol.begin() + xstart[r + 1]);
     auto span = [](int64_t c, int64_t len) { return 1 + (c > 0) + (c < len - 1); };
     std::vector<int64_t> rstart(static_cast<size_t>(n) + 1, 0);
 #pragma omp parallel for schedule(static)
     for (int64_t r = 0; r < n; ++r)
-        rstart[r + 1] = span(r % nx, nx) * span((r / nx) % ny, ny) * span(r / plane, nz);
+        rstart[r + 1] = span(r % nx, nx) * span((r / nx) % ny, ny) * span(r / plane, nz) + (xstart[r + 1] - xstart[r]);
     for (int64_t r = 0; r < n; ++r) rstart[r + 1] += rstart[r];
     // symmetric weights: -(0.5 + u), u from a hash of the unordered pair
     auto weight = [&](int64_t i, int64_t j) {
@@ -458,7 +507,21 @@ int generate_stencil27_spd(int32_t nx, int32_t ny, int32_t nz, double shift, uin
     for (int64_t r = 0; r < n; ++r) {
         const int64_t x = r % nx, y = (r / nx) % ny, z = r / plane;
         int64_t p = rstart[r], diagPos = -1;
+        int64_t xe = xstart[r];
+        const int64_t xend = xstart[r + 1];
         double absSum = 0.0;
+        auto put = [&](int64_t c) {
+            rows[p] = static_cast<int32_t>(r);
+            cols[p] = static_cast<int32_t>(c);
+            if (c == r) {
+                diagPos = p;
+                vals[p] = 0.0;
+            } else {
+                vals[p] = weight(r, c);
+                absSum += -vals[p];
+            }
+            ++p;
+        };
         for (int dz = -1; dz <= 1; ++dz) {
             if (z + dz < 0 || z + dz >= nz) continue;
             for (int dy = -1; dy <= 1; ++dy) {
@@ -466,19 +529,12 @@ int generate_stencil27_spd(int32_t nx, int32_t ny, int32_t nz, double shift, uin
                 for (int dx = -1; dx <= 1; ++dx) {
                     if (x + dx < 0 || x + dx >= nx) continue;
                     const int64_t c = r + dz * plane + dy * nx + dx;
-                    rows[p] = static_cast<int32_t>(r);
-                    cols[p] = static_cast<int32_t>(c);
-                    if (c == r) {
-                        diagPos = p;
-                        vals[p] = 0.0;
-                    } else {
-                        vals[p] = weight(r, c);
-                        absSum += -vals[p];
-                    }
-                    ++p;
+                    while (xe < xend && xcol[xe] < c) put(xcol[xe++]);  // keep columns ascending
+                    put(c);
                 }
             }
         }
+        while (xe < xend) put(xcol[xe++]);
         vals[diagPos] = (1.0 + shift) * absSum;
     }
     return HBDIA_OK;

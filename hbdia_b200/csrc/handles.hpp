@@ -1,0 +1,30 @@
+// The C ABI's matrix and vector handles (shared by the C ABI and the server).
+#pragma once
+
+#include <cstdint>
+#include <mutex>
+
+#include "hbdia_internal.hpp"
+
+struct hbdia_vector {
+    int32_t dtype = HBDIA_F64;
+    int64_t n = 0;
+    void *d = nullptr;
+};
+
+struct hbdia_matrix {
+    int32_t dtype = HBDIA_F64;
+    bool hasCOO = false;
+    bool hasHBDIA = false;
+    bool hostLayout = false;  // host layout materialised
+    hbdia::Coo<double> c64;
+    hbdia::Coo<float> c32;
+    hbdia::HostLayout<double> L64;
+    hbdia::HostLayout<float> L32;
+    hbdia::DevicePlan plan;
+    hbdia::DevicePlan innerPlan;        // reduced-storage copy for the CG inner iterations
+    hbdia::CgWork *cg = nullptr;        // CG workspace
+    int32_t blockWidth = 0, threshold = 0;
+    int64_t maxCoo = 0;
+    std::mutex hostMu;  // serialises hbdia_spmv_host's scratch buffers
+};

@@ -110,11 +110,13 @@ void build_plan(const HostLayout<T> &L, int storage, DevicePlan &P);
 void free_plan(DevicePlan &P);
 // y = A x on `stream` (a cudaStream_t; nullptr -> the plan's stream)
 void launch_spmv(const DevicePlan &P, const void *x, void *y, void *stream);
+// Y = A X for k right-hand sides: row-major blocks (element (i, j) at
+// X[i * ldx + j]) or, with colMajor, column-major ones (X[j * ldx + i]).
 void launch_spmm(const DevicePlan &P, const void *X, int64_t ldx, void *Y, int64_t ldy, int32_t k,
-                 void *stream);
+                 void *stream, bool colMajor = false);
 void launch_spmm_tile(const DevicePlan &P, const void *X, int64_t ldx, void *Y, int64_t ldy, int32_t k,
-                      int32_t tile, void *stream);
-int32_t default_spmm_tile(int32_t k);
+                      int32_t tile, void *stream, bool colMajor = false);
+int32_t default_spmm_tile(int32_t k, bool colMajor = false);
 void autotune(DevicePlan &P, const void *X, int64_t ldx, void *Y, int64_t ldy, int32_t k, void *stream, bool force,
               int32_t *kernel, int32_t *unroll, int32_t *tile, int32_t *fromCache, float *ms);
 void autotune_clear_cache();
@@ -139,6 +141,17 @@ void batch_autotune(Batch *b, void *stream, float *ms, int32_t *candidates);
 void batch_info(const Batch *b, int32_t *count, int32_t *totalTiles, int64_t *bytesPerRun);
 void *batch_stream(const Batch *b);
 
+// Serving engine (serve.cpp)
+struct Server;
+void server_default_options(hbdia_server_options *o);
+Server *server_create(const hbdia_server_options &o);
+void server_destroy(Server *S);
+int32_t server_add_matrix(Server *S, const hbdia_matrix *m);
+uint64_t server_submit(Server *S, int32_t matrix, int32_t kind, const double *x, double *y);
+void server_wait(Server *S, uint64_t ticket, hbdia_request_info *info);
+void server_pause(Server *S, bool paused);
+void server_stats(Server *S, hbdia_server_stats *out);
+
 // throws Error(HBDIA_ERR_CUDA) with the CUDA error string
 void check_cuda(int err, const char *what);
 // Sets the message hbdia_last_error() reports on this thread; returns status.
@@ -151,7 +164,7 @@ int generate_banded(int32_t n, const int32_t *offs, int32_t noffs, double lo, do
                     double scatter, uint64_t seed, int64_t *nnzOut, int32_t *rows, int32_t *cols,
                     double *vals);
 void fill_uniform(double *out, int64_t n, double lo, double hi, uint64_t seed);
-int generate_stencil27_spd(int32_t nx, int32_t ny, int32_t nz, double shift, uint64_t seed, int64_t *nnzOut,
-                           int32_t *rows, int32_t *cols, double *vals);
+int generate_stencil27_spd(int32_t nx, int32_t ny, int32_t nz, double shift, double extraFraction, uint64_t seed,
+                           int64_t *nnzOut, int32_t *rows, int32_t *cols, double *vals);
 
 }  // namespace hbdia

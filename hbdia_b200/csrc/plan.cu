@@ -253,16 +253,17 @@ void launch_staged(const dev::TmaArgs<VT, XT> &T, int32_t numChunks, const XT *x
 // warps then walk the tiles grid-stride).
 template <typename VT, typename XT, typename Kernel>
 void launch_pipe(Kernel kernel, const dev::SpmvArgs<VT, XT> &a, int32_t numTiles, const XT *x, XT *y,
-                 cudaStream_t s) {
+                 cudaStream_t s, int threads = 256) {
     int dev = 0, sms = 0, perSm = 0;
     check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
     check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "cudaDeviceGetAttribute");
-    check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kernel, 256, 0),
+    check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kernel, threads, 0),
                "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
-    const int64_t ctasNeeded = (static_cast<int64_t>(numTiles) + 7) / 8;
+    const int64_t warpsPerCta = threads / 32;
+    const int64_t ctasNeeded = (static_cast<int64_t>(numTiles) + warpsPerCta - 1) / warpsPerCta;
     const unsigned grid = static_cast<unsigned>(std::max<int64_t>(1, std::min<int64_t>(ctasNeeded,
                                                                                        int64_t(sms) * std::max(1, perSm))));
-    kernel<<<grid, 256, 0, s>>>(a, x, y);
+    kernel<<<grid, threads, 0, s>>>(a, x, y);
 }
 
 template <typename VT, typename XT>
@@ -292,6 +293,7 @@ void launch_typed(const DevicePlan &P, const void *x, void *y, cudaStream_t s) {
         else launch_staged<VT, XT, kUnroll>(T, P.numChunks, xp, yp, s);
     } else if (kern == HBDIA_KERNEL_PIPE) {
         launch_pipe_tuned<VT, XT>(P, a, xp, yp, s);
+
     } else if (kern == HBDIA_KERNEL_WARP) {
         const int64_t warpsPerCta = 8;
         const unsigned grid = static_cast<unsigned>((P.numTiles + warpsPerCta - 1) / warpsPerCta);
@@ -343,62 +345,91 @@ void launch_spmv(const DevicePlan &P, const void *x, void *y, void *stream) {
 
 namespace {
 
-template <typename VT, typename XT, int KT>
+template <typename VT, typename XT, int KT, bool CM>
 void launch_spmm_kt(const DevicePlan &P, const dev::SpmvArgs<VT, XT> &a, const XT *X, int64_t ldx, XT *Y,
                     int64_t ldy, int32_t k, cudaStream_t s) {
     if (P.bw == 32) {
         const unsigned grid = static_cast<unsigned>((static_cast<int64_t>(P.numTiles) + 7) / 8);
-        dev::spmm_bw32<VT, XT, KT><<<grid, 256, 0, s>>>(a, X, ldx, Y, ldy, k);
+        // The full passes in one launch, a partial last pass (k not a multiple
+        // of KT) in a second one on the remaining columns; 32-bit gather
+        // indices when every pass's block has fewer than 2^31 elements.
+        const int64_t rowsX = std::max(P.n, P.numCols);
+        const bool i32 = (CM ? int64_t(KT) * ldx + rowsX : rowsX * ldx + KT) < (int64_t(1) << 31);
+        const int32_t kfull = k - k % KT, krest = k % KT;
+        const XT *Xr = CM ? X + static_cast<int64_t>(kfull) * ldx : X + kfull;
+        XT *Yr = CM ? Y + static_cast<int64_t>(kfull) * ldy : Y + kfull;
+        if (i32) {
+            if (kfull) dev::spmm_bw32<VT, XT, KT, CM, int32_t, true><<<grid, 256, 0, s>>>(a, X, ldx, Y, ldy, kfull);
+            if (krest) dev::spmm_bw32<VT, XT, KT, CM, int32_t, false><<<grid, 256, 0, s>>>(a, Xr, ldx, Yr, ldy, krest);
+        } else {
+            if (kfull) dev::spmm_bw32<VT, XT, KT, CM, int64_t, true><<<grid, 256, 0, s>>>(a, X, ldx, Y, ldy, kfull);
+            if (krest) dev::spmm_bw32<VT, XT, KT, CM, int64_t, false><<<grid, 256, 0, s>>>(a, Xr, ldx, Yr, ldy, krest);
+        }
     } else {
         const unsigned grid = static_cast<unsigned>((static_cast<int64_t>(P.n) + 255) / 256);
-        dev::spmm_rowwise<VT, XT, KT><<<grid, 256, 0, s>>>(a, X, ldx, Y, ldy, k);
+        dev::spmm_rowwise<VT, XT, KT, CM><<<grid, 256, 0, s>>>(a, X, ldx, Y, ldy, k);
+    }
+}
+
+template <typename VT, typename XT, bool CM>
+void launch_spmm_layout(const DevicePlan &P, const dev::SpmvArgs<VT, XT> &a, const XT *xp, int64_t ldx, XT *yp,
+                        int64_t ldy, int32_t k, int32_t tile, cudaStream_t s) {
+    switch (tile) {
+        case 2: launch_spmm_kt<VT, XT, 2, CM>(P, a, xp, ldx, yp, ldy, k, s); break;
+        case 4: launch_spmm_kt<VT, XT, 4, CM>(P, a, xp, ldx, yp, ldy, k, s); break;
+        case 8: launch_spmm_kt<VT, XT, 8, CM>(P, a, xp, ldx, yp, ldy, k, s); break;
+        case 16: launch_spmm_kt<VT, XT, 16, CM>(P, a, xp, ldx, yp, ldy, k, s); break;
+        default: launch_spmm_kt<VT, XT, 32, CM>(P, a, xp, ldx, yp, ldy, k, s); break;
     }
 }
 
 template <typename VT, typename XT>
 void launch_spmm_typed(const DevicePlan &P, const void *X, int64_t ldx, void *Y, int64_t ldy, int32_t k,
-                       int32_t tile, cudaStream_t s) {
+                       int32_t tile, bool colMajor, cudaStream_t s) {
     dev::SpmvArgs<VT, XT> a = make_args<VT, XT>(P);
     const XT *xp = static_cast<const XT *>(X);
     XT *yp = static_cast<XT *>(Y);
-    switch (tile) {
-        case 4: launch_spmm_kt<VT, XT, 4>(P, a, xp, ldx, yp, ldy, k, s); break;
-        case 8: launch_spmm_kt<VT, XT, 8>(P, a, xp, ldx, yp, ldy, k, s); break;
-        case 16: launch_spmm_kt<VT, XT, 16>(P, a, xp, ldx, yp, ldy, k, s); break;
-        default: launch_spmm_kt<VT, XT, 32>(P, a, xp, ldx, yp, ldy, k, s); break;
-    }
+    if (colMajor) launch_spmm_layout<VT, XT, true>(P, a, xp, ldx, yp, ldy, k, tile, s);
+    else launch_spmm_layout<VT, XT, false>(P, a, xp, ldx, yp, ldy, k, tile, s);
     check_cuda(cudaGetLastError(), "SpMM launch");
 }
 
 }  // namespace
 
-int32_t default_spmm_tile(int32_t k) {
-    // smallest supported tile covering k, at most 16 (32 costs occupancy)
-    if (k <= 4) return 4;
-    if (k <= 8) return 8;
-    return 16;
+int32_t default_spmm_tile(int32_t k, bool colMajor) {
+    // Measured on B200 (27-point stencil 256^3): column-major blocks are
+    // fastest in passes of 4 for every k >= 3 (each column a separate
+    // coalesced gather); row-major ones in the smallest tile covering k up to
+    // 8 (wider passes re-fetch the same lines of X in every pass).
+    if (k <= 2) return 2;
+    if (colMajor || k <= 4) return 4;
+    return 8;
 }
 
 void launch_spmm_tile(const DevicePlan &P, const void *X, int64_t ldx, void *Y, int64_t ldy, int32_t k,
-                      int32_t tile, void *stream) {
+                      int32_t tile, void *stream, bool colMajor) {
     if (!P.base) throw Error(HBDIA_ERR_NOT_CONVERTED, "matrix has no device layout");
     if (!X || !Y) throw Error(HBDIA_ERR_INVALID_ARGUMENT, "null matrix pointer");
-    if (k <= 0 || ldx < k || ldy < k) throw Error(HBDIA_ERR_INVALID_ARGUMENT, "need k > 0 and ldx, ldy >= k");
+    if (k <= 0) throw Error(HBDIA_ERR_INVALID_ARGUMENT, "need k > 0");
+    if (!colMajor && (ldx < k || ldy < k)) throw Error(HBDIA_ERR_INVALID_ARGUMENT, "need ldx, ldy >= k");
+    if (colMajor && (ldx < std::max(P.n, P.numCols) || ldy < P.n))
+        throw Error(HBDIA_ERR_INVALID_ARGUMENT, "column-major blocks need ldx >= max(numRows, numCols), ldy >= numRows");
     cudaStream_t s = static_cast<cudaStream_t>(stream ? stream : P.stream);
-    if (P.dtype == HBDIA_F32) launch_spmm_typed<float, float>(P, X, ldx, Y, ldy, k, tile, s);
-    else if (P.storage == HBDIA_STORE_F32) launch_spmm_typed<float, double>(P, X, ldx, Y, ldy, k, tile, s);
+    if (P.dtype == HBDIA_F32) launch_spmm_typed<float, float>(P, X, ldx, Y, ldy, k, tile, colMajor, s);
+    else if (P.storage == HBDIA_STORE_F32) launch_spmm_typed<float, double>(P, X, ldx, Y, ldy, k, tile, colMajor, s);
     else if (P.storage == HBDIA_STORE_BF16_SCALED)
-        launch_spmm_typed<__nv_bfloat16, double>(P, X, ldx, Y, ldy, k, tile, s);
-    else launch_spmm_typed<double, double>(P, X, ldx, Y, ldy, k, tile, s);
+        launch_spmm_typed<__nv_bfloat16, double>(P, X, ldx, Y, ldy, k, tile, colMajor, s);
+    else launch_spmm_typed<double, double>(P, X, ldx, Y, ldy, k, tile, colMajor, s);
 }
 
-void launch_spmm(const DevicePlan &P, const void *X, int64_t ldx, void *Y, int64_t ldy, int32_t k, void *stream) {
+void launch_spmm(const DevicePlan &P, const void *X, int64_t ldx, void *Y, int64_t ldy, int32_t k, void *stream,
+                 bool colMajor) {
     int32_t tile = P.spmmTileForced;
-    if (!tile) {
-        auto it = P.spmmTile.find(k);
-        tile = it != P.spmmTile.end() ? it->second : default_spmm_tile(k);
+    if (!tile) {  // the autotuner's table is measured on row-major blocks
+        auto it = colMajor ? P.spmmTile.end() : P.spmmTile.find(k);
+        tile = it != P.spmmTile.end() ? it->second : default_spmm_tile(k, colMajor);
     }
-    launch_spmm_tile(P, X, ldx, Y, ldy, k, tile, stream);
+    launch_spmm_tile(P, X, ldx, Y, ldy, k, tile, stream, colMajor);
 }
 
 }  // namespace hbdia

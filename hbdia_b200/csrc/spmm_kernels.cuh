@@ -1,8 +1,10 @@
 // Multi-RHS product Y = A X on the HBDIA layout (sm_100a).
 //
-// X (n x k) and Y are row-major with leading dimensions ldx, ldy.  Column j of
-// Y is computed with exactly the SpMV's arithmetic (ascending-offset FMA chain
-// over the blocked-DIA values, sequential multiply-then-add over the row's COO
+// X (n x k) and Y are row-major with leading dimensions ldx, ldy (CM = false:
+// element (i, j) at X[i * ldx + j]) or column-major (CM = true: X[j * ldx + i],
+// each right-hand side a contiguous vector).  Column j of Y is computed with
+// exactly the SpMV's arithmetic (ascending-offset FMA chain over the
+// blocked-DIA values, sequential multiply-then-add over the row's COO
 // entries, one final add), so it equals hbdia_spmv(A, X[:, j]) bit for bit.
 //
 // Each stored value is fetched from HBM once and used for every right-hand
@@ -22,10 +24,12 @@ __device__ __forceinline__ void load_x_row(const XT *__restrict__ p, int kc, boo
     if (sizeof(XT) == 8 && vec2) {
 #pragma unroll
         for (int q = 0; q < KT; q += 2) {
-            if (q < kc) {
+            if (q + 1 < kc) {  // both elements of the pair are in the block
                 const double2 d = __ldg(reinterpret_cast<const double2 *>(p) + q / 2);
                 xv[q] = static_cast<XT>(d.x);
-                if (q + 1 < KT) xv[q + 1] = static_cast<XT>(d.y);
+                xv[q + 1] = static_cast<XT>(d.y);
+            } else if (q < kc) {  // odd last column: never read past it
+                xv[q] = __ldg(p + q);
             }
         }
     } else {
@@ -35,11 +39,78 @@ __device__ __forceinline__ void load_x_row(const XT *__restrict__ p, int kc, boo
     }
 }
 
-// blockWidth 32: one warp per 32-row block, lane = row.
-template <typename VT, typename XT, int KT>
-__device__ __forceinline__ void bw32_spmm_tile(const SpmvArgs<VT, XT> &a, const XT *__restrict__ X, int64_t ldx,
-                                               XT *__restrict__ Y, int64_t ldy, int32_t k, int32_t tile,
-                                               int lane) {
+// Offset of element (row i, column j) of an X or Y block.
+template <bool CM>
+__device__ __forceinline__ int64_t blk(int64_t i, int64_t j, int64_t ld) {
+    return CM ? j * ld + i : i * ld + j;
+}
+
+// U offsets of one row block for the KT right-hand sides of one pass: the U
+// values and all U x KT x gathers are issued before any product is formed, so
+// a group costs one memory round trip.  Column q's products are added in
+// ascending offset order.  Xp is the pass's first column (column-major) or
+// X + r0 (row-major); IT is the element-index type (32-bit whenever the
+// pass's block fits, which keeps the address arithmetic to one instruction
+// per gather); FULL means all KT columns of the pass are used.
+template <typename VT, typename XT, int KT, bool CM, int U, typename IT, bool FULL>
+__device__ __forceinline__ void spmm_group(const SpmvArgs<VT, XT> &a, const XT *__restrict__ Xp, IT ld,
+                                           const VT *vp, int32_t myoff, int j, int64_t row, int kc, bool vec2,
+                                           float s, XT (&acc)[KT]) {
+    VT v[U];
+    bool ok[U];
+    XT xv[U][KT];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        const int64_t col = row + __shfl_sync(kFull, myoff, j + u);
+        ok[u] = static_cast<uint64_t>(col) < static_cast<uint64_t>(a.n);
+        v[u] = __ldg(vp + (j + u) * 32);
+        const IT c = ok[u] ? static_cast<IT>(col) : IT(0);
+        if (CM) {
+#pragma unroll
+            for (int q = 0; q < KT; ++q)
+                xv[u][q] = (FULL || q < kc) ? __ldg(Xp + (static_cast<IT>(q) * ld + c)) : XT(0);
+        } else {
+            load_x_row<XT, KT>(Xp + c * ld, FULL ? KT : kc, vec2, xv[u]);
+        }
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        const XT vv = widen<XT>(v[u], s);
+        const bool use = ok[u] && vv != XT(0);
+#pragma unroll
+        for (int q = 0; q < KT; ++q)
+            if (FULL || q < kc) acc[q] = use ? fma_rn(vv, xv[u][q], acc[q]) : acc[q];
+    }
+}
+
+// The offsets of one row block for one pass, in groups of U = 16 / KT (at
+// least 1), so about 16 x gathers per lane are in flight (32 measured slower
+// on B200 at every tile width).
+template <typename VT, typename XT, int KT, bool CM, typename IT, bool FULL>
+__device__ __forceinline__ void spmm_pass(const SpmvArgs<VT, XT> &a, const XT *__restrict__ Xp, IT ld, int32_t k0,
+                                          int32_t k1, int64_t row, int lane, int kc, bool vec2, float s,
+                                          XT (&acc)[KT]) {
+    constexpr int U = KT >= 16 ? 1 : 16 / KT;
+    for (int32_t kb = k0; kb < k1; kb += 32) {
+        const int cnt = min(32, k1 - kb);
+        const int32_t myoff = lane < cnt ? __ldg(a.offs + kb + lane) : 0;
+        const VT *vp = a.vals + static_cast<int64_t>(kb) * 32 + lane;
+        int j = 0;
+        for (; j + U <= cnt; j += U)
+            spmm_group<VT, XT, KT, CM, U, IT, FULL>(a, Xp, ld, vp, myoff, j, row, kc, vec2, s, acc);
+        for (; j < cnt; ++j)  // warp-uniform tail
+            spmm_group<VT, XT, KT, CM, 1, IT, FULL>(a, Xp, ld, vp, myoff, j, row, kc, vec2, s, acc);
+    }
+}
+
+// blockWidth 32: one warp per 32-row block, lane = row, k right-hand sides in
+// passes of KT.  IT: element-index type of the gathers (int32_t only when
+// every pass's block has fewer than 2^31 elements); FULL: k is a multiple of
+// KT (no partial pass).
+template <typename VT, typename XT, int KT, bool CM, typename IT, bool FULL>
+__device__ __forceinline__ void bw32_spmm_tile_t(const SpmvArgs<VT, XT> &a, const XT *__restrict__ X, int64_t ldx,
+                                                 XT *__restrict__ Y, int64_t ldy, int32_t k, int32_t tile,
+                                                 int lane) {
     const int64_t row0 = static_cast<int64_t>(tile) * 32;
     const int64_t row = row0 + lane;
     int32_t k0 = 0, k1 = 0;
@@ -50,74 +121,76 @@ __device__ __forceinline__ void bw32_spmm_tile(const SpmvArgs<VT, XT> &a, const 
     const int32_t c0 = a.hasCoo ? __ldg(a.cooTile + tile) : 0;
     const int32_t c1 = a.hasCoo ? __ldg(a.cooTile + tile + 1) : 0;
     const float s = (a.scale && tile < a.numBlocks) ? __ldg(a.scale + tile) : 1.0f;
-    const bool xAligned = (reinterpret_cast<uintptr_t>(X) & 15) == 0 && (ldx & 1) == 0;
+    const bool xAligned = !CM && (reinterpret_cast<uintptr_t>(X) & 15) == 0 && (ldx & 1) == 0;
     for (int32_t r0 = 0; r0 < k; r0 += KT) {
         const int kc = min(KT, k - r0);
         const bool vec2 = xAligned && (r0 & 1) == 0;
+        const XT *Xp = CM ? X + static_cast<int64_t>(r0) * ldx : X + r0;
         XT acc[KT];
 #pragma unroll
         for (int q = 0; q < KT; ++q) acc[q] = XT(0);
-        for (int32_t kb = k0; kb < k1; kb += 32) {
-            const int cnt = min(32, k1 - kb);
-            const int32_t myoff = lane < cnt ? __ldg(a.offs + kb + lane) : 0;
-            const VT *vp = a.vals + static_cast<int64_t>(kb) * 32 + lane;
-            for (int j = 0; j < cnt; ++j) {
-                const int64_t col = row + __shfl_sync(kFull, myoff, j);
-                const XT vv = widen<XT>(__ldg(vp + j * 32), s);
-                if (static_cast<uint64_t>(col) < static_cast<uint64_t>(a.n) && vv != XT(0)) {
-                    XT xv[KT];
-                    load_x_row<XT, KT>(X + col * ldx + r0, kc, vec2, xv);
+        spmm_pass<VT, XT, KT, CM, IT, FULL>(a, Xp, static_cast<IT>(ldx), k0, k1, row, lane, kc, vec2, s, acc);
+        if (a.hasCoo) {
+            // per column: the row's COO entries in list order, then one add;
+            // each batch of 32 entries is loaded once for all columns
+            XT c[KT];
+#pragma unroll
+            for (int q = 0; q < KT; ++q) c[q] = XT(0);
+            for (int32_t base = c0; base < c1; base += 32) {
+                const int32_t e = base + lane;
+                int lr = -1;
+                XT p[KT];
+#pragma unroll
+                for (int q = 0; q < KT; ++q) p[q] = XT(0);
+                if (e < c1) {
+                    lr = static_cast<int>(__ldg(a.cooRow + e) - row0);
+                    const int64_t cc = __ldg(a.cooCol + e);
+                    const XT cv = __ldg(a.cooVal + e);
 #pragma unroll
                     for (int q = 0; q < KT; ++q)
-                        if (q < kc) acc[q] = fma_rn(vv, xv[q], acc[q]);
+                        if (q < kc) p[q] = mul_rn(cv, __ldg(X + blk<CM>(cc, r0 + q, ldx)));
                 }
-            }
-        }
-        if (a.hasCoo) {
-            // per column: the row's COO entries in list order, then one add
+                const int m = min(32, c1 - base);
+                for (int t = 0; t < m; ++t) {
+                    const int rt = __shfl_sync(kFull, lr, t);
 #pragma unroll
-            for (int q = 0; q < KT; ++q) {
-                if (q >= kc) break;
-                XT c = XT(0);
-                for (int32_t base = c0; base < c1; base += 32) {
-                    const int32_t e = base + lane;
-                    int lr = -1;
-                    XT p = XT(0);
-                    if (e < c1) {
-                        lr = static_cast<int>(__ldg(a.cooRow + e) - row0);
-                        p = mul_rn(__ldg(a.cooVal + e), __ldg(X + static_cast<int64_t>(__ldg(a.cooCol + e)) * ldx + r0 + q));
-                    }
-                    const int m = min(32, c1 - base);
-                    for (int t = 0; t < m; ++t) {
-                        const int rt = __shfl_sync(kFull, lr, t);
-                        const XT pt = __shfl_sync(kFull, p, t);
-                        if (rt == lane) c = add_rn(c, pt);
+                    for (int q = 0; q < KT; ++q) {
+                        const XT pt = __shfl_sync(kFull, p[q], t);
+                        if (rt == lane) c[q] = add_rn(c[q], pt);
                     }
                 }
-                acc[q] = add_rn(acc[q], c);
             }
+#pragma unroll
+            for (int q = 0; q < KT; ++q) acc[q] = add_rn(acc[q], c[q]);
         }
         if (row < a.n) {
-            XT *yp = Y + row * ldy + r0;
 #pragma unroll
             for (int q = 0; q < KT; ++q)
-                if (q < kc) yp[q] = acc[q];
+                if (q < kc) Y[blk<CM>(row, r0 + q, ldy)] = acc[q];
         }
     }
 }
 
-template <typename VT, typename XT, int KT>
+// Any k, any size (the batch kernel's form).
+template <typename VT, typename XT, int KT, bool CM = false>
+__device__ __forceinline__ void bw32_spmm_tile(const SpmvArgs<VT, XT> &a, const XT *__restrict__ X, int64_t ldx,
+                                               XT *__restrict__ Y, int64_t ldy, int32_t k, int32_t tile,
+                                               int lane) {
+    bw32_spmm_tile_t<VT, XT, KT, CM, int64_t, false>(a, X, ldx, Y, ldy, k, tile, lane);
+}
+
+template <typename VT, typename XT, int KT, bool CM, typename IT, bool FULL>
 __global__ void __launch_bounds__(256)
 spmm_bw32(const SpmvArgs<VT, XT> a, const XT *__restrict__ X, int64_t ldx, XT *__restrict__ Y, int64_t ldy,
           int32_t k) {
     const int lane = threadIdx.x & 31;
     const int32_t tile = static_cast<int32_t>((static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5);
     if (tile >= a.numTiles) return;  // warp-uniform
-    bw32_spmm_tile<VT, XT, KT>(a, X, ldx, Y, ldy, k, tile, lane);
+    bw32_spmm_tile_t<VT, XT, KT, CM, IT, FULL>(a, X, ldx, Y, ldy, k, tile, lane);
 }
 
 // Any block width: one thread per row (the reference's mapping).
-template <typename VT, typename XT, int KT>
+template <typename VT, typename XT, int KT, bool CM>
 __global__ void __launch_bounds__(256)
 spmm_rowwise(const SpmvArgs<VT, XT> a, const XT *__restrict__ X, int64_t ldx, XT *__restrict__ Y, int64_t ldy,
              int32_t k) {
@@ -142,7 +215,7 @@ spmm_rowwise(const SpmvArgs<VT, XT> a, const XT *__restrict__ X, int64_t ldx, XT
             if (vv == XT(0) || col < 0 || col >= a.n) continue;
 #pragma unroll
             for (int q = 0; q < KT; ++q)
-                if (q < kc) acc[q] = fma_rn(vv, __ldg(X + col * ldx + r0 + q), acc[q]);
+                if (q < kc) acc[q] = fma_rn(vv, __ldg(X + blk<CM>(col, r0 + q, ldx)), acc[q]);
         }
         if (a.hasCoo) {
             const int32_t e0 = __ldg(a.cooRowPtr + row), e1 = __ldg(a.cooRowPtr + row + 1);
@@ -151,14 +224,13 @@ spmm_rowwise(const SpmvArgs<VT, XT> a, const XT *__restrict__ X, int64_t ldx, XT
                 if (q >= kc) break;
                 XT c = XT(0);
                 for (int32_t e = e0; e < e1; ++e)
-                    c = add_rn(c, mul_rn(__ldg(a.cooVal + e),
-                                         __ldg(X + static_cast<int64_t>(__ldg(a.cooCol + e)) * ldx + r0 + q)));
+                    c = add_rn(c, mul_rn(__ldg(a.cooVal + e), __ldg(X + blk<CM>(__ldg(a.cooCol + e), r0 + q, ldx))));
                 acc[q] = add_rn(acc[q], c);
             }
         }
 #pragma unroll
         for (int q = 0; q < KT; ++q)
-            if (q < kc) Y[row * ldy + r0 + q] = acc[q];
+            if (q < kc) Y[blk<CM>(row, r0 + q, ldy)] = acc[q];
     }
 }
 

@@ -4,6 +4,7 @@
     python -m hbdia_b200.suite spmm        # 7-point Laplacian 128^3, k in {4, 16, 32}, FP64 and FP32 storage
     python -m hbdia_b200.suite cg          # SPD 27-point 128^3: mixed-precision vs plain FP64 CG
     python -m hbdia_b200.suite batched     # 64 stencils of edge U[16,96]: separate launches vs one batched launch
+    python -m hbdia_b200.suite serve       # 32 resident matrices, Poisson arrivals: batched server vs plain FP64
 
 Each measurement prints one JSON line.  Times are CUDA-event device times on
 a dedicated stream after warm-up; inputs exceed L2 unless stated.  Accuracy
@@ -212,9 +213,154 @@ def batched(args):
             "candidates": ncand, "bit_identical_to_single": same})
 
 
+def _serve_run(hb, srv, ids, mats_n, kinds, mids, xbuf, ybuf, rate, seed):
+    """Submits the request list (kinds[i] on matrix mids[i]) -- all at once
+    (rate None: closed loop, the server paused until all are queued) or with
+    Poisson arrivals at `rate` requests/s -- and collects them.  Returns
+    (wall seconds from first submit to last completion, latencies in seconds,
+    SpMV batch widths, worst submit lag behind the arrival schedule)."""
+    import threading
+    import time
+    n_req = len(kinds)
+    tickets = [None] * n_req
+    ready = threading.Semaphore(0)
+    lag = [0.0]
+
+    def submit_all():
+        arrivals = np.cumsum(np.random.default_rng(seed).exponential(1.0 / rate, n_req)) if rate else None
+        t0 = time.perf_counter()
+        for i in range(n_req):
+            if arrivals is not None:
+                while True:
+                    d = arrivals[i] - (time.perf_counter() - t0)
+                    if d <= 0:
+                        break
+                    if d > 2e-4:
+                        time.sleep(d - 1e-4)
+                lag[0] = max(lag[0], (time.perf_counter() - t0) - arrivals[i])
+            m = mids[i]
+            tickets[i] = srv.submit(ids[m], kinds[i], xbuf[m][i % len(xbuf[m])], ybuf[m][i % len(ybuf[m])])
+            ready.release()
+
+    if rate is None:
+        srv.pause(True)
+    th = threading.Thread(target=submit_all)
+    th.start()
+    if rate is None:
+        th.join()
+        srv.pause(False)
+    lat, widths, first, last = [], [], None, 0.0
+    for i in range(n_req):
+        ready.acquire()
+        info = srv.wait(tickets[i])
+        if info.status != 0:
+            raise RuntimeError(f"request {i} failed with status {info.status}")
+        lat.append(info.finished - info.submitted)
+        if kinds[i] == hb.REQ_SPMV:
+            widths.append(info.batchRhs)
+        first = info.submitted if first is None else min(first, info.submitted)
+        last = max(last, info.finished)
+    th.join()
+    return last - first, np.array(lat), np.array(widths), lag[0]
+
+
+def serve(args):
+    """Config 5: resident matrices, Poisson arrivals, continuous batching.
+
+    32 SPD 27-point stencils of edge U[32, 160] (numpy default_rng(5)), each
+    with 0.5 % symmetric off-pattern entries (seed 50 + i), resident in a
+    server with a 150 GB admission budget.  Requests: 80 % SpMV, 20 % CG
+    (to ||b - A y|| / ||b|| <= 1e-10), matrix uniform (default_rng(6)), x / b
+    from a pool of pinned host vectors per matrix.  Two servers:
+      * batched: continuous batching, FP32-stored values (FP64 accumulation),
+        mixed-precision CG (FP32 inner, FP64 refinement), 4 CG solvers;
+      * plain: FP64 values, one request per launch, plain FP64 CG, 1 solver.
+    Each is first driven closed-loop (all requests queued, then released) to
+    measure its capacity, then open-loop with Poisson arrivals at
+    `--load` x its capacity, and the plain one also at the batched one's
+    rate when it can carry it.  Latency = completion - submission, measured
+    by the server's clock.  Output buffers are shared round-robin (results
+    are checked by the tests, not here)."""
+    import torch
+    import hbdia_b200 as hb
+    edges = np.random.default_rng(5).integers(args.edge_min, args.edge_max + 1, args.matrices)
+    mats, ns = [], []
+    for i, e in enumerate(edges.tolist()):
+        r, c, v = hb.generate_stencil27_spd(e, e, e, 1e-3, 50 + i, extra_fraction=0.005)
+        n = e ** 3
+        m = hb.HBDIA(r, c, v, n, n)
+        del r, c, v
+        m.convertToHBDIAFormat(32, 2, upload=False)
+        mats.append(m)
+        ns.append(n)
+    rng = np.random.default_rng(6)
+    n_req = args.requests
+    mids = rng.integers(0, len(mats), n_req)
+    kinds = np.where(rng.random(n_req) < args.cg_fraction, hb.REQ_CG, hb.REQ_SPMV)
+    pins = []
+
+    def pinned(n, fill):
+        t = torch.empty(n, dtype=torch.float64).pin_memory()
+        a = t.numpy()
+        a[:] = fill(n)
+        pins.append(t)
+        return a
+
+    xbuf = [[pinned(n, lambda k: rng.uniform(-1, 1, k)) for _ in range(2)] for n in ns]
+    ybuf = [[pinned(n, np.zeros) for _ in range(8)] for n in ns]
+    servers = {
+        "batched": hb.Server(),
+        "plain": hb.Server(batching=0, spmvStorage=hb.STORE_NATIVE, cgInnerStorage=hb.STORE_NATIVE,
+                           cgInnerTol=1e-11, cgWorkers=1),
+    }
+    ids = {k: [s.add_matrix(m) for m in mats] for k, s in servers.items()}
+    del mats
+    rows = int(sum(ns))
+    results = {}
+    for name, srv in servers.items():
+        # warm-up: every matrix once, both kinds
+        w_k = np.array([hb.REQ_SPMV] * len(ns) + [hb.REQ_CG] * min(4, len(ns)))
+        w_m = np.concatenate([np.arange(len(ns)), np.arange(min(4, len(ns)))])
+        _serve_run(hb, srv, ids[name], ns, w_k, w_m, xbuf, ybuf, None, 0)
+        wall, lat, widths, _ = _serve_run(hb, srv, ids[name], ns, kinds, mids, xbuf, ybuf, None, 0)
+        results[name] = {"capacity_req_s": n_req / wall}
+    rates = {"batched": args.load * results["batched"]["capacity_req_s"],
+             "plain": args.load * results["plain"]["capacity_req_s"]}
+    runs = [("batched", rates["batched"], "own"), ("plain", rates["plain"], "own")]
+    if results["plain"]["capacity_req_s"] > rates["batched"]:
+        runs.append(("plain", rates["batched"], "batched server's rate"))
+    runs.append(("batched", rates["plain"], "plain server's rate"))
+    for name, rate, which in runs:
+        srv = servers[name]
+        wall, lat, widths, lag = _serve_run(hb, srv, ids[name], ns, kinds, mids, xbuf, ybuf, rate, 7)
+        st = srv.stats()
+        is_cg = kinds == hb.REQ_CG
+        print(json.dumps({
+            "suite": "serve", "server": name, "arrivals": f"Poisson at {rate:.1f} req/s ({which} {args.load:g} x capacity)",
+            "workload": f"{len(ns)} SPD 27-point stencils, edge U[{args.edge_min},{args.edge_max}] seed 5, 0.5% "
+                        f"symmetric extras, {rows} rows; {n_req} requests, {args.cg_fraction:.0%} CG",
+            "capacity_req_s": results[name]["capacity_req_s"], "throughput_req_s": n_req / wall,
+            "p50_ms": 1e3 * float(np.percentile(lat, 50)), "p99_ms": 1e3 * float(np.percentile(lat, 99)),
+            "spmv_p50_ms": 1e3 * float(np.percentile(lat[~is_cg], 50)),
+            "spmv_p99_ms": 1e3 * float(np.percentile(lat[~is_cg], 99)),
+            "cg_p50_ms": 1e3 * float(np.percentile(lat[is_cg], 50)) if is_cg.any() else None,
+            "cg_p99_ms": 1e3 * float(np.percentile(lat[is_cg], 99)) if is_cg.any() else None,
+            "mean_spmv_batch": float(widths.mean()) if len(widths) else None,
+            "max_submit_lag_ms": 1e3 * lag, "device_bytes": int(st.deviceBytes),
+            "memory_budget_bytes": int(srv.options.memoryBudget)}), flush=True)
+    for s in servers.values():
+        s.close()
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("what", choices=["precision", "spmm", "cg", "batched"])
+    ap.add_argument("what", choices=["precision", "spmm", "cg", "batched", "serve"])
+    ap.add_argument("--requests", type=int, default=10000)
+    ap.add_argument("--matrices", type=int, default=32)
+    ap.add_argument("--edge-min", type=int, default=32)
+    ap.add_argument("--edge-max", type=int, default=160)
+    ap.add_argument("--cg-fraction", type=float, default=0.2)
+    ap.add_argument("--load", type=float, default=0.7)
     ap.add_argument("--count", type=int, default=64)
     ap.add_argument("--storage", type=int, default=0)
     ap.add_argument("--n", type=int, default=8 * 1024 * 1024)
@@ -222,7 +368,7 @@ def main(argv=None):
     args = ap.parse_args(argv)
     import torch
     torch.cuda.set_device(0)
-    {"precision": precision, "spmm": spmm, "cg": cg, "batched": batched}[args.what](args)
+    {"precision": precision, "spmm": spmm, "cg": cg, "batched": batched, "serve": serve}[args.what](args)
     return 0
 
 

@@ -220,6 +220,15 @@ int hbdia_spmv_device(const hbdia_matrix *m, const void *x, void *y, void *strea
 int hbdia_spmm_device(const hbdia_matrix *m, const void *X, int64_t ldx, void *Y, int64_t ldy,
                       int32_t k, void *stream);
 
+/* The same product on column-major blocks: right-hand side j is the
+ * contiguous vector X + j * ldx (ldx >= max(numRows, numCols)), result j is
+ * Y + j * ldy (ldy >= numRows).  For callers whose right-hand sides arrive
+ * as separate vectors (a server's requests).  Column j equals
+ * hbdia_spmv_device of that vector bit for bit.  No counterpart in the
+ * reference. */
+int hbdia_spmm_device_colmajor(const hbdia_matrix *m, const void *X, int64_t ldx, void *Y, int64_t ldy,
+                               int32_t k, void *stream);
+
 /* End-to-end form on HOST buffers: copies x to the device, runs the SpMV,
  * copies y back and synchronizes.  Page-locked host buffers are fastest. */
 int hbdia_spmv_host(hbdia_matrix *m, const void *xHost, void *yHost);
@@ -256,7 +265,7 @@ int hbdia_matrix_selected_kernel(const hbdia_matrix *m, const void *x, int32_t *
  * HBDIA_TUNE_UNROLL: offsets in flight per lane in the staged and pipelined
  * kernels (0 = default 9, or 27).
  * HBDIA_TUNE_SPMM_TILE: right-hand sides per pass of the SpMM kernels for
- * every k (0 = autotuned / default, or 4, 8, 16, 32). */
+ * every k (0 = autotuned / default, or 2, 4, 8, 16, 32). */
 typedef enum hbdia_tuning_key { HBDIA_TUNE_UNROLL = 1, HBDIA_TUNE_SPMM_TILE = 2 } hbdia_tuning_key;
 int hbdia_matrix_set_tuning(hbdia_matrix *m, int32_t key, int32_t value);
 
@@ -380,6 +389,78 @@ int hbdia_batch_autotune(hbdia_batch *b, void *stream, float *msPerRun, int32_t 
 int hbdia_batch_info(const hbdia_batch *b, int32_t *count, int32_t *totalTiles, int64_t *bytesPerRun);
 int hbdia_batch_stream(const hbdia_batch *b, void **stream);
 
+/* ---------------------------------------------------------------- serving */
+
+/* A server holds resident matrices and serves requests submitted from any
+ * host thread.  No counterpart in the reference.
+ *  - SpMV requests (y = A x) are served in steps by continuous batching:
+ *    each step takes all pending requests (up to maxRhs per matrix, oldest
+ *    first); the requests of one matrix become one SpMM over the matrix's
+ *    spmvStorage values (each x copied into its column, each y out of it),
+ *    the matrices of a step run concurrently; requests arriving during a
+ *    step join the next.  batching = 0 serves one request per launch in
+ *    arrival order.
+ *  - CG requests (solve A y = x, A symmetric positive definite) run on
+ *    cgWorkers worker threads: mixed-precision CG (hbdia_cg_solve) with
+ *    cgInnerStorage inner iterations, refined to cgTol.
+ * A request's result does not depend on the requests it is served with.
+ * Admission: hbdia_server_add_matrix returns HBDIA_ERR_NO_MEMORY when the
+ * matrix's plans, staging blocks and CG workspace growth would take the
+ * server's device memory past memoryBudget.  Host vectors must stay valid
+ * until the request is collected; page-locked memory is fastest. */
+typedef struct hbdia_server hbdia_server;
+typedef enum hbdia_request_kind { HBDIA_REQ_SPMV = 0, HBDIA_REQ_CG = 1 } hbdia_request_kind;
+
+typedef struct hbdia_server_options {
+    int64_t memoryBudget;   /* device bytes the server may hold (default 150e9)             */
+    int32_t batching;       /* continuous batching of SpMVs (default 1)                     */
+    int32_t maxRhs;         /* SpMV requests of one matrix per step, 1-64 (default 16)     */
+    int32_t spmvStorage;    /* hbdia_value_storage of SpMVs (default HBDIA_STORE_F32)       */
+    int32_t cgInnerStorage; /* storage of the CG inner iterations (default HBDIA_STORE_F32) */
+    int32_t cgWorkers;      /* concurrent CG solves, 1-64 (default 4)                       */
+    int32_t cgMaxOuter;     /* refinement steps (default 50)                                */
+    int32_t cgMaxInner;     /* inner iterations per step (default 5000)                     */
+    int32_t cgCheckEvery;   /* inner iterations per graph replay (default 10)               */
+    double cgTol;           /* target ||b - A y|| / ||b|| (default 1e-10)                   */
+    double cgInnerTol;      /* inner relative tolerance (default 1e-6)                      */
+} hbdia_server_options;
+
+typedef struct hbdia_request_info {
+    int32_t status;         /* hbdia_status of the request (CG: RUNTIME if not converged) */
+    int32_t kind, matrix;
+    int32_t batchRhs;       /* SpMV: requests of its matrix in its step                  */
+    double submitted, started, finished; /* seconds since the server was created         */
+    int32_t cgOuter, cgInner;
+    double cgRelResidual;
+} hbdia_request_info;
+
+typedef struct hbdia_server_stats {
+    int64_t completed, spmvRequests, cgRequests;
+    int64_t spmvSteps, spmvLaunches;
+    int64_t deviceBytes;    /* held under the budget */
+    int32_t matrices;
+} hbdia_server_stats;
+
+void hbdia_server_default_options(hbdia_server_options *options);
+int hbdia_server_create(const hbdia_server_options *options, hbdia_server **out);
+/* Serves everything pending, then stops. */
+void hbdia_server_destroy(hbdia_server *s);
+/* Makes a converted double matrix (host layout present) resident; the
+ * server builds its own device copies, so the matrix may be destroyed
+ * afterwards. */
+int hbdia_server_add_matrix(hbdia_server *s, const hbdia_matrix *m, int32_t *id);
+/* x: numCols doubles (the right-hand side b for CG); y: numRows doubles. */
+int hbdia_server_submit(hbdia_server *s, int32_t matrix, int32_t kind, const double *xHost, double *yHost,
+                        uint64_t *ticket);
+/* paused != 0: requests queue up but no SpMV step or CG solve starts (work
+ * already running finishes); 0 resumes, and everything queued is served --
+ * the SpMVs of the backlog batched together.  Waiting on an unfinished
+ * request while paused fails with HBDIA_ERR_RUNTIME. */
+int hbdia_server_pause(hbdia_server *s, int32_t paused);
+/* Blocks until the request is done and collects it (once per ticket). */
+int hbdia_server_wait(hbdia_server *s, uint64_t ticket, hbdia_request_info *info);
+int hbdia_server_get_stats(hbdia_server *s, hbdia_server_stats *stats);
+
 /* ---------------------------------------------------------------- workloads */
 
 /* Seeded synthetic 27-point stencil on an nx*ny*nz grid (Dirichlet boundary,
@@ -408,10 +489,12 @@ int hbdia_generate_banded(int32_t n, const int32_t *offsets, int32_t numOffsets,
 
 /* Symmetric positive definite 27-point stencil: off-diagonal a_ij = a_ji =
  * -(0.5 + u), u in [0, 1) drawn from a hash of the unordered pair (i, j) and
- * the seed, diagonal (1 + shift) * sum_j |a_ij| (shift >= 0).  Row-sorted,
- * ascending columns.  Two-call protocol as above. */
-int hbdia_generate_stencil27_spd(int32_t nx, int32_t ny, int32_t nz, double shift, uint64_t seed, int64_t *nnz,
-                                 int32_t *rows, int32_t *cols, double *values);
+ * the seed, plus floor(extraFraction * stencil_nnz / 2) symmetric pairs
+ * outside the 27-point pattern (distinct, seeded), diagonal
+ * (1 + shift) * sum_j |a_ij| (shift >= 0): diagonally dominant, so SPD.
+ * Row-sorted, ascending columns.  Two-call protocol as above. */
+int hbdia_generate_stencil27_spd(int32_t nx, int32_t ny, int32_t nz, double shift, double extraFraction,
+                                 uint64_t seed, int64_t *nnz, int32_t *rows, int32_t *cols, double *values);
 
 /* n doubles uniform in [lo, hi) from the library's seeded generator. */
 int hbdia_fill_uniform(double *out, int64_t n, double lo, double hi, uint64_t seed);

@@ -1,0 +1,220 @@
+"""Serving engine (hbdia_server_*): a request's result is the same whether it
+is served alone or batched with others (bit for bit), SpMV results equal the
+single-matrix entry points on the same value storage, CG results reach the
+FP64 tolerance (checked on the host) and equal hbdia_cg_solve, and admission
+keeps the device memory the server holds within its budget."""
+import numpy as np
+import pytest
+
+from conftest import bits_equal
+
+pytestmark = pytest.mark.gpu
+
+
+def _spd(lib, e, seed):
+    rows, cols, vals = lib.generate_stencil27_spd(e, e, e, 1e-3, seed, extra_fraction=0.005)
+    n = e ** 3
+    m = lib.HBDIA(rows, cols, vals, n, n)
+    m.convertToHBDIAFormat(32, 2, upload=False)
+    return m, (rows, cols, vals), n
+
+
+@pytest.fixture(scope="module")
+def mats(lib):
+    return [_spd(lib, e, 5 + e) for e in (10, 14, 18)]
+
+
+def _host_residual(rcv, x, b):
+    rows, cols, vals = rcv
+    ax = np.zeros(len(b))
+    np.add.at(ax, rows, vals * x[cols])
+    return np.linalg.norm(b - ax) / np.linalg.norm(b)
+
+
+def _pinned(n, rng=None):
+    import torch
+    t = torch.empty(n, dtype=torch.float64).pin_memory()
+    a = t.numpy()
+    if rng is not None:
+        a[:] = rng.uniform(-1, 1, n)
+    else:
+        a[:] = np.nan
+    return t, a
+
+
+@pytest.mark.parametrize("batching", [1, 0])
+def test_same_alone_and_in_mix(lib, mats, batching):
+    srv = lib.Server(batching=batching)
+    ids = [srv.add_matrix(m) for m, _, _ in mats]
+    rng = np.random.default_rng(1)
+    keep = []
+    # alone: one SpMV and one CG per matrix, each waited for before the next
+    alone = []
+    for mid, (m, rcv, n) in zip(ids, mats):
+        tx, x = _pinned(n, rng)
+        ty, y = _pinned(n)
+        info = srv.wait(srv.submit(mid, lib.REQ_SPMV, x, y))
+        assert info.status == 0 and info.batchRhs == 1
+        tb, b = _pinned(n, rng)
+        tc, c = _pinned(n)
+        info = srv.wait(srv.submit(mid, lib.REQ_CG, b, c))
+        assert info.status == 0 and info.cgRelResidual <= 1e-10
+        assert _host_residual(rcv, c, b) <= 2e-10
+        keep += [tx, ty, tb, tc]
+        alone.append((x.copy(), y.copy(), b.copy(), c.copy()))
+    # mix: a burst of SpMVs on every matrix (the alone x among them) and CGs,
+    # queued while the server is paused so that they are served together
+    srv.pause(True)
+    pending = []
+    for rep in range(8):
+        for j, (mid, (m, rcv, n)) in enumerate(zip(ids, mats)):
+            x0, y0, b0, c0 = alone[j]
+            tx, x = _pinned(n, rng)
+            if rep in (2, 5):
+                x[:] = x0
+            ty, y = _pinned(n)
+            keep += [tx, ty]
+            pending.append(("spmv", j, rep, x, y, srv.submit(mid, lib.REQ_SPMV, x, y)))
+            if rep == 3:
+                tb, b = _pinned(n)
+                b[:] = b0
+                tc, c = _pinned(n)
+                keep += [tb, tc]
+                pending.append(("cg", j, rep, b, c, srv.submit(mid, lib.REQ_CG, b, c)))
+    with pytest.raises(RuntimeError, match="paused"):
+        srv.wait(pending[0][-1])
+    srv.pause(False)
+    widest = 1
+    for kind, j, rep, x, y, t in pending:
+        info = srv.wait(t)
+        assert info.status == 0
+        x0, y0, b0, c0 = alone[j]
+        if kind == "spmv":
+            widest = max(widest, info.batchRhs)
+            if rep in (2, 5):
+                assert bits_equal(y, y0)
+            if batching == 0:
+                assert info.batchRhs == 1
+        else:
+            assert bits_equal(y, c0)
+    if batching:
+        assert widest == 8  # each matrix's 8 queued SpMVs went as one SpMM
+    st = srv.stats()
+    assert st.completed == len(pending) + 2 * len(mats) and st.matrices == 3
+    srv.close()
+
+
+def test_spmv_matches_entry_points_and_fp64(lib, mats):
+    import torch
+    m, rcv, n = mats[1]
+    rows, cols, vals = rcv
+    rng = np.random.default_rng(4)
+    x = rng.uniform(-1, 1, n)
+    res = {}
+    for storage in (lib.STORE_F32, lib.STORE_NATIVE):
+        srv = lib.Server(spmvStorage=storage)
+        mid = srv.add_matrix(m)
+        y = np.full(n, np.nan)
+        assert srv.wait(srv.submit(mid, lib.REQ_SPMV, x, y)).status == 0
+        srv.close()
+        ref = lib.HBDIA(rows, cols, vals, n, n)
+        ref.convertToHBDIAFormat(32, 2, upload=False)
+        ref.prepareForGPU(storage)
+        xt = torch.from_numpy(x).cuda()
+        yt = torch.zeros(n, dtype=torch.float64, device="cuda")
+        lib.spmv_device(ref, xt.data_ptr(), yt.data_ptr(), 0)
+        torch.cuda.synchronize()
+        assert bits_equal(y, yt.cpu().numpy())
+        res[storage] = y
+    scale = np.zeros(n)
+    np.add.at(scale, rows, np.abs(vals * x[cols]))
+    assert np.max(np.abs(res[lib.STORE_F32] - res[lib.STORE_NATIVE]) / scale) <= 1e-6
+
+
+def test_cg_matches_cg_solve(lib, mats):
+    import torch
+    m, rcv, n = mats[0]
+    rows, cols, vals = rcv
+    b = np.random.default_rng(9).uniform(-1, 1, n)
+    srv = lib.Server()
+    mid = srv.add_matrix(m)
+    y = np.zeros(n)
+    info = srv.wait(srv.submit(mid, lib.REQ_CG, b, y))
+    srv.close()
+    assert info.status == 0 and info.cgOuter >= 2
+    ref = lib.HBDIA(rows, cols, vals, n, n)
+    ref.convertToHBDIAFormat(32, 2)
+    bt = torch.from_numpy(b).cuda()
+    xt = torch.zeros(n, dtype=torch.float64, device="cuda")
+    r = lib.cg_solve(ref, bt.data_ptr(), xt.data_ptr(), tol=1e-10, inner_storage=lib.STORE_F32, inner_tol=1e-6)
+    assert r.innerIterations == info.cgInner
+    assert bits_equal(xt.cpu().numpy(), y)
+
+
+def test_admission_budget(lib, mats):
+    m0, _, _ = mats[0]
+    with pytest.raises(MemoryError, match="admission"):
+        lib.Server(memoryBudget=1 << 16).add_matrix(m0)  # the 1000-row matrix needs about 1 MB
+    big = lib.Server()
+    big.add_matrix(m0)
+    need = big.stats().deviceBytes
+    big.close()
+    srv = lib.Server(memoryBudget=int(need * 2.2))  # two copies fit (the CG workspace share counts once), not three
+    srv.add_matrix(m0)
+    srv.add_matrix(m0)
+    with pytest.raises(MemoryError):
+        srv.add_matrix(m0)
+    assert srv.stats().deviceBytes <= int(need * 2.2)
+    srv.close()
+
+
+def test_server_rejections(lib, mats):
+    m0, _, n = mats[0]
+    srv = lib.Server()
+    mid = srv.add_matrix(m0)
+    x, y = np.zeros(n), np.zeros(n)
+    with pytest.raises(IndexError):
+        srv.submit(mid + 5, lib.REQ_SPMV, x, y)
+    with pytest.raises(ValueError):
+        srv.submit(mid, 7, x, y)
+    t = srv.submit(mid, lib.REQ_SPMV, x, y)
+    srv.wait(t)
+    with pytest.raises(ValueError):
+        srv.wait(t)  # collected already
+    with pytest.raises(TypeError):
+        lib.Server(noSuchOption=1)
+    with pytest.raises(ValueError):
+        lib.Server(maxRhs=0)
+    host_only = lib.HBDIA(np.array([0], np.int32), np.array([0], np.int32), np.array([1.0]), 1, 1)
+    with pytest.raises(RuntimeError):
+        srv.add_matrix(host_only)  # not converted
+    srv.close()
+
+
+def test_step_with_more_matrices_than_streams(lib):
+    """One step spanning 20 matrices (the SpMV stream ring has 16 streams)."""
+    srv = lib.Server()
+    rng = np.random.default_rng(12)
+    mats = []
+    for i in range(20):
+        m, rcv, n = _spd(lib, 4 + i % 4, 30 + i)
+        mats.append((srv.add_matrix(m), n))
+    alone = []
+    for mid, n in mats:
+        x = rng.uniform(-1, 1, n)
+        y = np.full(n, np.nan)
+        srv.wait(srv.submit(mid, lib.REQ_SPMV, x, y))
+        alone.append((x, y))
+    srv.pause(True)
+    pend = []
+    for (mid, n), (x, y0) in zip(mats, alone):
+        for _ in range(2):
+            y = np.full(n, np.nan)
+            pend.append((srv.submit(mid, lib.REQ_SPMV, x, y), y, y0))
+    srv.pause(False)
+    for t, y, y0 in pend:
+        info = srv.wait(t)
+        assert info.status == 0 and info.batchRhs == 2
+        assert bits_equal(y, y0)
+    assert srv.stats().spmvSteps == 21  # 20 alone + one step for the whole burst
+    srv.close()

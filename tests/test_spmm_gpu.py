@@ -29,7 +29,7 @@ def _expected(orc, rows, cols, vals, n, bw, thr, X):
     return np.stack([om.spmv(np.ascontiguousarray(X[:, j])) for j in range(X.shape[1])], axis=1)
 
 
-@pytest.mark.parametrize("tile", [4, 8, 16, 32])
+@pytest.mark.parametrize("tile", [2, 4, 8, 16, 32])
 @pytest.mark.parametrize("k", [1, 3, 4, 9, 16, 33])
 def test_spmm_columns_equal_spmv(lib, orc, tile, k):
     rng = np.random.default_rng(300 + k)
@@ -101,8 +101,38 @@ def test_autotune_spmv_and_spmm(lib, orc):
     X = torch.from_numpy(np.random.default_rng(4).uniform(-1, 1, (n, k))).cuda().contiguous()
     Y = torch.zeros((n, k), dtype=torch.float64, device="cuda")
     r3 = m.autotune(X.data_ptr(), Y.data_ptr(), k=k)
-    assert r3.spmmTile in (4, 8, 16, 32)
+    assert r3.spmmTile in (2, 4, 8, 16, 32)
     lib.spmm_device(m, X.data_ptr(), k, Y.data_ptr(), k, k)
     m.synchronize()
     want = _expected(orc, rows, cols, vals, n, 32, 2, X.cpu().numpy()[:, :2])
     assert bits_equal(np.ascontiguousarray(Y.cpu().numpy()[:, :2]), want)
+
+
+@pytest.mark.parametrize("bw", [32, 16])
+@pytest.mark.parametrize("tile", [2, 4, 16])
+@pytest.mark.parametrize("k", [1, 5, 17])
+def test_spmm_colmajor_equals_spmv(lib, orc, bw, tile, k):
+    """Column-major blocks (each right-hand side a contiguous vector, leading
+    dimension larger than n): column j equals the SpMV of vector j."""
+    import torch
+    rng = np.random.default_rng(900 + k + bw)
+    n = 2500
+    rows, cols, vals = random_coo(rng, n, n, 26000)
+    m = lib.HBDIA(rows, cols, vals, n, n)
+    m.convertToHBDIAFormat(bw, 2)
+    m.setTuning(lib.TUNE_SPMM_TILE, tile)
+    ld = n + 37
+    X = rng.uniform(-1, 1, (k, n))
+    Xt = torch.zeros((k, ld), dtype=torch.float64, device="cuda")
+    Xt[:, :n] = torch.from_numpy(X).cuda()
+    Yt = torch.full((k, ld + 3), float("nan"), dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    lib.spmm_device_colmajor(m, Xt.data_ptr(), ld, Yt.data_ptr(), ld + 3, k)
+    m.synchronize()
+    Y = Yt.cpu().numpy()
+    om = orc.convert(rows, cols, vals, n, n, bw, 2)
+    for j in range(k):
+        assert bits_equal(Y[j, :n], om.spmv(np.ascontiguousarray(X[j])))
+    assert np.isnan(Y[:, n:]).all()  # nothing outside the columns written
+    with pytest.raises(ValueError):
+        lib.spmm_device_colmajor(m, Xt.data_ptr(), n - 1, Yt.data_ptr(), ld, k)
