@@ -117,6 +117,11 @@ class HBDIA:
         _check(_load().hbdia_matrix_convert(self._h, blockWidth, threshold, int(max_coo_entries),
                                             int(bool(COOisUnique)), int(execMode), int(bool(upload))))
 
+    def convertOnDevice(self, blockWidth: int = DEFAULT_BLOCK_WIDTH, threshold: int = DEFAULT_THRESHOLD,
+                        max_coo_entries: int = MAX_COO_ENTRIES, storage: int = STORE_NATIVE) -> None:
+        """convertToHBDIAFormat + prepareForGPU on the GPU (row-sorted COO)."""
+        _check(_load().hbdia_matrix_convert_on_device(self._h, blockWidth, threshold, int(max_coo_entries), storage))
+
     def prepareForGPU(self, storage: int = STORE_NATIVE) -> None:
         _check(_load().hbdia_matrix_prepare_gpu(self._h, storage))
 

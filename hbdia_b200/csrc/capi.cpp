@@ -251,8 +251,22 @@ int hbdia_matrix_prepare_gpu(hbdia_matrix *m, int32_t storage) {
     });
 }
 
-int hbdia_matrix_convert_on_device(hbdia_matrix *, int32_t, int32_t, int64_t, int32_t) {
-    return guarded([&] { throw Error(HBDIA_ERR_UNSUPPORTED, "device converter not built yet"); });
+int hbdia_matrix_convert_on_device(hbdia_matrix *m, int32_t blockWidth, int32_t threshold, int64_t maxCoo,
+                                   int32_t storage) {
+    return guarded([&] {
+        need(m != nullptr, HBDIA_ERR_INVALID_ARGUMENT, "null matrix");
+        // the same early returns as convertToHBDIAFormat (src/Format/HBDIA.cpp:511-524)
+        if (m->hasHBDIA || !m->hasCOO || coo_nnz(m) == 0) return;
+        need(blockWidth > 0, HBDIA_ERR_INVALID_ARGUMENT, "blockWidth must be positive");
+        if (m->dtype == HBDIA_F32)
+            hbdia::convert_on_device(m->c32, blockWidth, threshold, maxCoo, storage, m->plan, m->devMeta);
+        else hbdia::convert_on_device(m->c64, blockWidth, threshold, maxCoo, storage, m->plan, m->devMeta);
+        m->hasHBDIA = true;
+        m->hostLayout = false;
+        m->blockWidth = blockWidth;
+        m->threshold = threshold;
+        m->maxCoo = maxCoo;
+    });
 }
 
 int hbdia_matrix_get_info(const hbdia_matrix *m, hbdia_matrix_info *info) {
@@ -289,6 +303,8 @@ int hbdia_matrix_get_info(const hbdia_matrix *m, hbdia_matrix_info *info) {
             I.totalOffsets = m->plan.totalOffsets;
             I.numSlots = m->plan.slots;
             I.numCoo = m->plan.nCoo;
+            I.numberDiagonals = m->devMeta.numberDiagonals;
+            I.histogramLength = static_cast<int32_t>(m->devMeta.histBlocks.size());
         }
         *info = I;
     });
@@ -299,10 +315,31 @@ int hbdia_matrix_export_layout(const hbdia_matrix *m, int32_t *offsets, int32_t 
                                int32_t *histBlocks, int32_t *histNnz) {
     return guarded([&] {
         need(m != nullptr, HBDIA_ERR_INVALID_ARGUMENT, "null matrix");
-        need(m->hasHBDIA && m->hostLayout, HBDIA_ERR_NOT_CONVERTED, "no host HBDIA layout");
+        need(m->hasHBDIA, HBDIA_ERR_NOT_CONVERTED, "no HBDIA layout");
         auto cp = [](void *dst, const auto &v) {
             if (dst && !v.empty()) std::memcpy(dst, v.data(), v.size() * sizeof(v[0]));
         };
+        if (!m->hostLayout) {
+            // a layout the GPU converter built: read it back from the device
+            const hbdia::DevicePlan &P = m->plan;
+            need(P.base != nullptr, HBDIA_ERR_NOT_CONVERTED, "no HBDIA layout");
+            need(P.storage == HBDIA_STORE_NATIVE, HBDIA_ERR_UNSUPPORTED,
+                 "a reduced-storage device layout has no exact values to export");
+            const size_t es = esize(m->dtype);
+            auto down = [](void *dst, const void *src, size_t bytes) {
+                if (dst && bytes) hbdia::check_cuda(cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost), "cudaMemcpy(export)");
+            };
+            down(offsets, P.offs, sizeof(int32_t) * P.totalOffsets);
+            down(blockStart, P.blkOff, sizeof(int32_t) * (static_cast<size_t>(P.numBlocks) + 1));
+            down(data, P.vals, es * P.slots);
+            down(cooRow, P.cooRow, sizeof(int32_t) * P.nCoo);
+            down(cooCol, P.cooCol, sizeof(int32_t) * P.nCoo);
+            down(cooVal, P.cooVal, es * P.nCoo);
+            down(cooRowPtr, P.cooRowPtr, sizeof(int32_t) * (static_cast<size_t>(P.n) + 1));
+            cp(histBlocks, m->devMeta.histBlocks);
+            cp(histNnz, m->devMeta.histNnz);
+            return;
+        }
         auto go = [&](const auto &L) {
             cp(offsets, L.offsets);
             cp(blockStart, L.blockStart);

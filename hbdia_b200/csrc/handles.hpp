@@ -22,6 +22,7 @@ struct hbdia_matrix {
     hbdia::HostLayout<double> L64;
     hbdia::HostLayout<float> L32;
     hbdia::DevicePlan plan;
+    hbdia::DeviceLayoutMeta devMeta;    // layout facts when the GPU converter built the plan
     hbdia::DevicePlan innerPlan;        // reduced-storage copy for the CG inner iterations
     hbdia::CgWork *cg = nullptr;        // CG workspace
     int32_t blockWidth = 0, threshold = 0;

@@ -99,6 +99,18 @@ struct DevicePlan {
     int32_t spmmTileForced = 0;          // HBDIA_TUNE_SPMM_TILE (0: autotuned / default)
 };
 
+// Host-side facts of a layout built on the device (convert_gpu.cu).
+struct DeviceLayoutMeta {
+    int32_t numberDiagonals = 0;
+    std::vector<int32_t> histBlocks, histNnz;
+};
+// COO -> device plan on the GPU; row-sorted COO only (HBDIA_ERR_UNSUPPORTED
+// otherwise); the same layout as convert_to_hbdia + build_plan, without the
+// staged kernel's schedule.
+template <typename T>
+void convert_on_device(const Coo<T> &coo, int32_t blockWidth, int32_t threshold, int64_t maxCoo, int storage,
+                       DevicePlan &P, DeviceLayoutMeta &meta);
+
 void build_chunk_schedule(int32_t n, int32_t numBlocks, int32_t numTiles, const int32_t *blkOff,
                           const int32_t *offs, const int32_t *cooTile, int vrows, int xcap,
                           int xElemBytes, std::vector<int32_t> &rec, std::vector<XWindow> &win);

@@ -132,9 +132,15 @@ int hbdia_matrix_convert(hbdia_matrix *m, int32_t blockWidth, int32_t threshold,
  * the matrix's stream.  storage selects the device value format. */
 int hbdia_matrix_prepare_gpu(hbdia_matrix *m, int32_t storage);
 
-/* Builds the device layout straight from COO with the GPU converter (same
- * layout as hbdia_matrix_convert + prepare_gpu, but the host layout is not
- * materialised).  Requires row-sorted COO; otherwise HBDIA_ERR_UNSUPPORTED. */
+/* convertToHBDIAFormat (src/Format/HBDIA.cpp:507-718) + prepareForGPU done
+ * on the GPU: the same device layout (and the same offsets, values, COO
+ * remainder, histograms and numberDiagonals) as hbdia_matrix_convert +
+ * hbdia_matrix_prepare_gpu(storage), without the host pass over the
+ * entries; the host layout is not materialised (hbdia_matrix_export_layout
+ * reads the device copy back, for NATIVE storage).  Requires row-sorted COO
+ * (HBDIA_ERR_UNSUPPORTED otherwise).  The staged kernel's schedule is not
+ * built, so HBDIA_KERNEL_STAGED runs the warp kernel on such a matrix.  A
+ * no-op on an already converted or empty matrix, like the reference. */
 int hbdia_matrix_convert_on_device(hbdia_matrix *m, int32_t blockWidth, int32_t threshold,
                                    int64_t maxCooEntries, int32_t storage);
 
