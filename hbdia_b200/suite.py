@@ -5,6 +5,7 @@
     python -m hbdia_b200.suite cg          # SPD 27-point 128^3: mixed-precision vs plain FP64 CG
     python -m hbdia_b200.suite batched     # 64 stencils of edge U[16,96]: separate launches vs one batched launch
     python -m hbdia_b200.suite serve       # 32 resident matrices, Poisson arrivals: batched server vs plain FP64
+    python -m hbdia_b200.suite convert --grid 256   # host vs GPU converter, COO -> device layout
 
 Each measurement prints one JSON line.  Times are CUDA-event device times on
 a dedicated stream after warm-up; inputs exceed L2 unless stated.  Accuracy
@@ -98,21 +99,29 @@ def spmm(args):
         m.prepareForGPU(st)
         info = m.info()
         vbytes = info.numSlots * (8 if st == hb.STORE_NATIVE else 4) + 4 * info.totalOffsets + 4 * (info.numBlocks + 1)
+        x1 = torch.from_numpy(np.random.default_rng(3).uniform(-1, 1, n)).cuda()
+        y1 = torch.zeros(n, dtype=torch.float64, device="cuda")
+        ms1 = _time(lambda: hb.spmv_device(m, x1.data_ptr(), y1.data_ptr(), stream.cuda_stream), stream)
+        if stname == "fp64":
+            ms_plain = ms1
         for k in (4, 16, 32):
             X = torch.from_numpy(np.random.default_rng(3).uniform(-1, 1, (n, k))).cuda().contiguous()
             Y = torch.zeros((n, k), dtype=torch.float64, device="cuda")
             tune = m.autotune(X.data_ptr(), Y.data_ptr(), k=k, stream=stream.cuda_stream)
             ms = _time(lambda: hb.spmm_device(m, X.data_ptr(), k, Y.data_ptr(), k, k, stream.cuda_stream), stream)
-            x1 = X[:, 0].contiguous()
-            y1 = torch.zeros(n, dtype=torch.float64, device="cuda")
-            ms1 = _time(lambda: hb.spmv_device(m, x1.data_ptr(), y1.data_ptr(), stream.cuda_stream), stream)
+            Xc = X.t().contiguous()  # column-major: each right-hand side contiguous
+            Yc = torch.zeros((k, n), dtype=torch.float64, device="cuda")
+            msc = _time(lambda: hb.spmm_device_colmajor(m, Xc.data_ptr(), n, Yc.data_ptr(), n, k, stream.cuda_stream),
+                        stream)
             m.synchronize()
             b = vbytes + k * 16 * n
-            print(json.dumps({"suite": "spmm", "workload": f"7-point Laplacian {g}^3 (centre 6, -1)",
-                              "storage": stname, "k": k, "rhs_tile": tune.spmmTile, "ms": ms,
-                              "ms_k_spmv": k * ms1, "speedup_vs_k_spmv": k * ms1 / ms,
-                              "bytes": b, "gbs": b / (ms / 1e3) / 1e9,
-                              "frac_of_peak": b / (ms / 1e3) / 1e9 / _peak()}), flush=True)
+            for layout, t, tile in (("row-major (autotuned tile)", ms, tune.spmmTile), ("column-major (default tile)", msc, 4)):
+                print(json.dumps({"suite": "spmm", "workload": f"7-point Laplacian {g}^3 (centre 6, -1)",
+                                  "storage": stname, "k": k, "layout": layout, "rhs_tile": tile, "ms": t,
+                                  "ms_k_spmv": k * ms1, "speedup_vs_k_spmv": k * ms1 / t,
+                                  "spmv_per_s_vs_plain_fp64_spmv": k * ms_plain / t,
+                                  "bytes": b, "gbs": b / (t / 1e3) / 1e9,
+                                  "frac_of_peak": b / (t / 1e3) / 1e9 / _peak()}), flush=True)
         del m
 
 
@@ -352,9 +361,37 @@ def serve(args):
         s.close()
 
 
+def convert(args):
+    """convertToHBDIAFormat + prepareForGPU on the host (OpenMP, all cores)
+    against the GPU converter, on the bench workload (27-point stencil
+    256^3, 1 % extras, blockWidth 32, threshold 2); wall-clock seconds from
+    the COO arrays to a device layout ready for SpMV."""
+    import os
+    import time
+    import torch
+    import hbdia_b200 as hb
+    g = args.grid
+    n = g ** 3
+    r, c, v = hb.generate_stencil27(g, g, g, extra_fraction=0.01, seed=1)
+    for name in ("host", "gpu", "gpu"):  # the second GPU run is warm
+        m = hb.HBDIA(r, c, v, n, n)
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        if name == "host":
+            m.convertToHBDIAFormat(32, 2)
+        else:
+            m.convertOnDevice(32, 2)
+        m.synchronize()
+        dt = time.perf_counter() - t
+        print(json.dumps({"suite": "convert", "workload": f"27-point stencil {g}^3 + 1% extras, blockWidth 32, threshold 2",
+                          "converter": name, "seconds": dt, "nnz": int(len(v)), "host_threads": os.cpu_count(),
+                          "device_bytes": int(m.info().deviceBytes)}), flush=True)
+        del m
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("what", choices=["precision", "spmm", "cg", "batched", "serve"])
+    ap.add_argument("what", choices=["precision", "spmm", "cg", "batched", "serve", "convert"])
     ap.add_argument("--requests", type=int, default=10000)
     ap.add_argument("--matrices", type=int, default=32)
     ap.add_argument("--edge-min", type=int, default=32)
@@ -368,7 +405,8 @@ def main(argv=None):
     args = ap.parse_args(argv)
     import torch
     torch.cuda.set_device(0)
-    {"precision": precision, "spmm": spmm, "cg": cg, "batched": batched, "serve": serve}[args.what](args)
+    {"precision": precision, "spmm": spmm, "cg": cg, "batched": batched, "serve": serve,
+     "convert": convert}[args.what](args)
     return 0
 
 
