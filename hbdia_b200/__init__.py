@@ -148,6 +148,50 @@ class HBDIA:
     isCOOFormat = getHasCOO
     isHBDIAFormat = getHasHBDIA
 
+    # ---- DIA format (src/Format/HBDIA.cpp:372-505)
+    def removeCOODuplicates(self) -> None:
+        _check(_load().hbdia_matrix_remove_duplicates(self._h))
+
+    def convertToDIAFormat(self, COOisUnique: bool = False) -> None:
+        _check(_load().hbdia_matrix_convert_dia(self._h, int(bool(COOisUnique))))
+
+    def _dia_info(self):
+        h, nd, ln = ctypes.c_int32(0), ctypes.c_int32(0), ctypes.c_int32(0)
+        _check(_load().hbdia_matrix_dia_info(self._h, ctypes.byref(h), ctypes.byref(nd), ctypes.byref(ln)))
+        return bool(h.value), nd.value, ln.value
+
+    def isDIAFormat(self) -> bool:
+        return self._dia_info()[0]
+
+    getHasDIA = isDIAFormat
+
+    def getOffsets(self) -> np.ndarray:
+        _, nd, _ = self._dia_info()
+        out = np.zeros(nd, np.int32)
+        _check(_load().hbdia_matrix_export_dia(self._h, _vp(out), None))
+        return out
+
+    def getDiagonals(self) -> np.ndarray:
+        """[numDiagonals, min(numRows, numCols)]"""
+        _, nd, ln = self._dia_info()
+        out = np.zeros((nd, ln), self.dtype)
+        _check(_load().hbdia_matrix_export_dia(self._h, None, _vp(out)))
+        return out
+
+    def coo(self):
+        """The COO arrays (rows, cols, values) as the matrix holds them now."""
+        n = self.getNumNonZeros()
+        r, c, v = np.zeros(n, np.int32), np.zeros(n, np.int32), np.zeros(n, self.dtype)
+        _check(_load().hbdia_matrix_export_coo(self._h, _vp(r), _vp(c), _vp(v)))
+        return r, c, v
+
+    def storageCosts(self) -> dict:
+        """Bytes of HBDIA, COO, DIA, SELL and CSR storage
+        (benchmarking/benchmark.cpp:171-215)."""
+        s = _lib.StorageCosts()
+        _check(_load().hbdia_matrix_storage_costs(self._h, ctypes.byref(s)))
+        return {k: getattr(s, k) for k in ("hbdia", "coo", "dia", "sell", "csr")}
+
     def layout(self) -> dict:
         """The host layout as numpy arrays: offsets/block_start (flattened
         offsetsPerBlock), data, coo_row/coo_col/coo_val, coo_row_ptr, hist_blocks,
@@ -544,3 +588,41 @@ class Server:
         s = _lib.ServerStats()
         _check(_load().hbdia_server_get_stats(self.handle, ctypes.byref(s)))
         return s
+
+
+def write_storage_report(matrix: HBDIA, folder: str, name: str, nx: int = 0, ny: int = 0, nz: int = 0,
+                         noise: float = 0.0, execCOOCPU: bool = False, execCOOGPU: bool = True) -> None:
+    """matrix_info.csv and histogram.csv with the columns of the reference's
+    benchmark (benchmarking/benchmark.cpp:236-305) for a converted matrix.
+    The unified-memory columns of the reference are written as 0 (this
+    library keeps the matrix in device memory)."""
+    import csv
+    import os
+    i = matrix.info()
+    c = matrix.storageCosts()
+    os.makedirs(folder, exist_ok=True)
+    lay = matrix.layout() if i.storage == STORE_NATIVE or matrix.info().numSlots == 0 else None
+    hist_b = lay["hist_blocks"] if lay is not None else np.zeros(0, np.int32)
+    hist_n = lay["hist_nnz"] if lay is not None else np.zeros(0, np.int32)
+    header = ["name", "nx", "ny", "nz", "noise", "rows", "cols", "nnz", "num_diagonals",
+              "num_blocks", "block_width", "threshold", "max_coo_entries", "coo_fallback_entries",
+              "hbdia_data_size", "hbdia_cost_bytes", "coo_cost_bytes", "dia_cost_bytes",
+              "sell_cost_bytes", "csr_cost_bytes", "hbdia_vs_coo", "dia_vs_coo", "csr_vs_coo", "sell_vs_coo",
+              "execCOOCPU", "execCOOGPU", "unifiedMemory", "unifiedMemory_malloc",
+              "unifiedMemory_managedMalloc", "unifiedMemory_NumaAllocOnNode"]
+    row = [name, nx, ny, nz, f"{noise:.6f}", i.numRows, i.numCols, i.numNonZeros, i.numberDiagonals,
+           i.numBlocks, i.blockWidth, i.threshold, i.maxCooEntries, i.numCoo, i.numSlots,
+           c["hbdia"], c["coo"], c["dia"], c["sell"], c["csr"],
+           f"{c['hbdia'] / c['coo']:.6f}", f"{c['dia'] / c['coo']:.6f}", f"{c['csr'] / c['coo']:.6f}",
+           f"{c['sell'] / c['coo']:.6f}", int(execCOOCPU), int(execCOOGPU), 0, 0, 0, 0]
+    with open(os.path.join(folder, "matrix_info.csv"), "w", newline="") as f:
+        w = csv.writer(f)
+        w.writerow(header)
+        w.writerow(row)
+    with open(os.path.join(folder, "histogram.csv"), "w", newline="") as f:
+        w = csv.writer(f)
+        w.writerow(["diagonal_count", "blocks_with_diagonals", "nnz_in_blocks"])
+        for d in range(len(hist_b)):
+            nnzd = int(hist_n[d]) if d < len(hist_n) else 0
+            if hist_b[d] > 0 or nnzd > 0:
+                w.writerow([d, int(hist_b[d]), nnzd])

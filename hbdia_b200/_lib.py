@@ -83,6 +83,10 @@ class ServerStats(ctypes.Structure):
                 ("spmvLaunches", c_i64), ("deviceBytes", c_i64), ("matrices", c_i32)]
 
 
+class StorageCosts(ctypes.Structure):
+    _fields_ = [("hbdia", c_i64), ("coo", c_i64), ("dia", c_i64), ("sell", c_i64), ("csr", c_i64)]
+
+
 class HBDIACudaError(RuntimeError):
     """A CUDA runtime call inside the library failed."""
 
@@ -117,6 +121,11 @@ _SIGS = [
     ("hbdia_matrix_convert", ctypes.c_int, [c_vp, c_i32, c_i32, c_i64, c_i32, c_i32, c_i32]),
     ("hbdia_matrix_prepare_gpu", ctypes.c_int, [c_vp, c_i32]),
     ("hbdia_matrix_convert_on_device", ctypes.c_int, [c_vp, c_i32, c_i32, c_i64, c_i32]),
+    ("hbdia_matrix_remove_duplicates", ctypes.c_int, [c_vp]),
+    ("hbdia_matrix_convert_dia", ctypes.c_int, [c_vp, c_i32]),
+    ("hbdia_matrix_dia_info", ctypes.c_int, [c_vp, c_i32p, c_i32p, c_i32p]),
+    ("hbdia_matrix_export_dia", ctypes.c_int, [c_vp, c_vp, c_vp]),
+    ("hbdia_matrix_storage_costs", ctypes.c_int, [c_vp, ctypes.POINTER(StorageCosts)]),
     ("hbdia_matrix_get_info", ctypes.c_int, [c_vp, ctypes.POINTER(MatrixInfo)]),
     ("hbdia_matrix_export_layout", ctypes.c_int, [c_vp] * 10),
     ("hbdia_matrix_export_coo", ctypes.c_int, [c_vp, c_vp, c_vp, c_vp]),

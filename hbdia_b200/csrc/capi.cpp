@@ -251,6 +251,76 @@ int hbdia_matrix_prepare_gpu(hbdia_matrix *m, int32_t storage) {
     });
 }
 
+int hbdia_matrix_remove_duplicates(hbdia_matrix *m) {
+    return guarded([&] {
+        need(m != nullptr, HBDIA_ERR_INVALID_ARGUMENT, "null matrix");
+        if (!m->hasCOO) return;  // "No COO format available" (src/Format/HBDIA.cpp:374-377)
+        if (m->dtype == HBDIA_F32) hbdia::remove_coo_duplicates(m->c32);
+        else hbdia::remove_coo_duplicates(m->c64);
+    });
+}
+
+int hbdia_matrix_convert_dia(hbdia_matrix *m, int32_t cooIsUnique) {
+    return guarded([&] {
+        need(m != nullptr, HBDIA_ERR_INVALID_ARGUMENT, "null matrix");
+        // early returns of src/Format/HBDIA.cpp:416-429
+        if (m->hasDIA || !m->hasCOO) return;
+        if (coo_nnz(m) == 0) {
+            m->hasDIA = true;
+            return;
+        }
+        if (m->dtype == HBDIA_F32) hbdia::convert_to_dia(m->c32, cooIsUnique != 0, m->diaOffsets, m->dia32, m->diaLength);
+        else hbdia::convert_to_dia(m->c64, cooIsUnique != 0, m->diaOffsets, m->dia64, m->diaLength);
+        m->hasDIA = true;
+    });
+}
+
+int hbdia_matrix_dia_info(const hbdia_matrix *m, int32_t *hasDIA, int32_t *numDiagonals, int32_t *diagLength) {
+    return guarded([&] {
+        need(m && hasDIA && numDiagonals && diagLength, HBDIA_ERR_INVALID_ARGUMENT, "null argument");
+        *hasDIA = m->hasDIA;
+        *numDiagonals = static_cast<int32_t>(m->diaOffsets.size());
+        *diagLength = m->diaLength;
+    });
+}
+
+int hbdia_matrix_export_dia(const hbdia_matrix *m, int32_t *offsets, void *diagonals) {
+    return guarded([&] {
+        need(m != nullptr, HBDIA_ERR_INVALID_ARGUMENT, "null matrix");
+        need(m->hasDIA, HBDIA_ERR_NOT_CONVERTED, "matrix is not in DIA format");
+        if (offsets && !m->diaOffsets.empty())
+            std::memcpy(offsets, m->diaOffsets.data(), m->diaOffsets.size() * sizeof(int32_t));
+        if (diagonals) {
+            if (m->dtype == HBDIA_F32 && !m->dia32.empty())
+                std::memcpy(diagonals, m->dia32.data(), m->dia32.size() * sizeof(float));
+            else if (m->dtype == HBDIA_F64 && !m->dia64.empty())
+                std::memcpy(diagonals, m->dia64.data(), m->dia64.size() * sizeof(double));
+        }
+    });
+}
+
+int hbdia_matrix_storage_costs(const hbdia_matrix *m, hbdia_storage_costs *out) {
+    return guarded([&] {
+        need(m && out, HBDIA_ERR_INVALID_ARGUMENT, "null argument");
+        need(m->hasHBDIA, HBDIA_ERR_NOT_CONVERTED, "matrix is not in HBDIA format");
+        const int64_t vb = static_cast<int64_t>(esize(m->dtype));
+        const auto &npr = m->dtype == HBDIA_F32 ? m->c32.nnzPerRow : m->c64.nnzPerRow;
+        if (m->hostLayout) {
+            auto go = [&](const auto &L) {
+                hbdia::storage_costs(vb, L.numRows, L.numCols, coo_nnz(m), L.numberDiagonals, L.numBlocks,
+                                     L.blockWidth, static_cast<int64_t>(L.data.size()),
+                                     static_cast<int64_t>(L.cooRow.size()), L.histBlocks, npr, *out);
+            };
+            if (m->dtype == HBDIA_F32) go(m->L32);
+            else go(m->L64);
+        } else {
+            const hbdia::DevicePlan &P = m->plan;
+            hbdia::storage_costs(vb, P.n, P.numCols, coo_nnz(m), m->devMeta.numberDiagonals, P.numBlocks, P.bw,
+                                 P.slots, P.nCoo, m->devMeta.histBlocks, npr, *out);
+        }
+    });
+}
+
 int hbdia_matrix_convert_on_device(hbdia_matrix *m, int32_t blockWidth, int32_t threshold, int64_t maxCoo,
                                    int32_t storage) {
     return guarded([&] {

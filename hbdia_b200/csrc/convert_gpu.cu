@@ -85,6 +85,19 @@ T device_sum(const T *in, int64_t n, Scratch &S) {
 }
 
 // ---------------------------------------------------------------- kernels
+// Bit 0: rows not sorted; bit 1: an index outside the matrix.
+__global__ void validate_coo(const int32_t *__restrict__ R, const int32_t *__restrict__ C, int64_t nnz, int32_t nR,
+                             int32_t nC, int32_t *__restrict__ flags) {
+    int32_t f = 0;
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < nnz;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int32_t r = R[i], c = C[i];
+        if (r < 0 || r >= nR || c < 0 || c >= nC) f |= 2;
+        if (i > 0 && R[i - 1] > r) f |= 1;
+    }
+    if (f) atomicOr(flags, f);
+}
+
 __global__ void row_starts(const int32_t *__restrict__ R, int64_t nnz, int32_t nR, int64_t *__restrict__ rs) {
     const int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (r > nR) return;
@@ -339,9 +352,6 @@ void convert_on_device(const Coo<T> &coo, int32_t bw, int32_t thr, int64_t maxCo
     const int64_t nnz = static_cast<int64_t>(coo.vals.size());
     const int32_t nR = coo.numRows, nC = coo.numCols;
     if (nR <= 0 || nC <= 0) throw Error(HBDIA_ERR_INVALID_ARGUMENT, "empty matrix");
-    for (int64_t i = 1; i < nnz; ++i)
-        if (coo.rows[i - 1] > coo.rows[i])
-            throw Error(HBDIA_ERR_UNSUPPORTED, "the device converter needs row-sorted COO input");
     if (nnz > INT32_MAX) throw Error(HBDIA_ERR_UNSUPPORTED, "more than 2^31-1 entries");
     const int dtype = std::is_same<T, float>::value ? HBDIA_F32 : HBDIA_F64;
     if (storage != HBDIA_STORE_NATIVE && dtype != HBDIA_F64)
@@ -356,9 +366,15 @@ void convert_on_device(const Coo<T> &coo, int32_t bw, int32_t thr, int64_t maxCo
     check_cuda(cudaMemcpy(R, coo.rows.data(), sizeof(int32_t) * nnz, cudaMemcpyHostToDevice), "cudaMemcpy(rows)");
     check_cuda(cudaMemcpy(C, coo.cols.data(), sizeof(int32_t) * nnz, cudaMemcpyHostToDevice), "cudaMemcpy(cols)");
     check_cuda(cudaMemcpy(V, coo.vals.data(), sizeof(T) * nnz, cudaMemcpyHostToDevice), "cudaMemcpy(vals)");
-    for (int64_t i = 0; i < nnz; ++i)  // index bounds (checked again by the constructor; cheap)
-        if (coo.cols[i] < 0 || coo.cols[i] >= nC || coo.rows[i] < 0 || coo.rows[i] >= nR)
-            throw Error(HBDIA_ERR_OUT_OF_RANGE, "entry outside the matrix");
+    {
+        int32_t *flags = S.get<int32_t>(1);
+        check_cuda(cudaMemset(flags, 0, sizeof(int32_t)), "cudaMemset(flags)");
+        validate_coo<<<1184, 256>>>(R, C, nnz, nR, nC, flags);
+        int32_t f = 0;
+        check_cuda(cudaMemcpy(&f, flags, sizeof(int32_t), cudaMemcpyDeviceToHost), "cudaMemcpy(flags)");
+        if (f & 2) throw Error(HBDIA_ERR_OUT_OF_RANGE, "entry outside the matrix");
+        if (f & 1) throw Error(HBDIA_ERR_UNSUPPORTED, "the device converter needs row-sorted COO input");
+    }
 
     // 1. row starts
     int64_t *rs = S.get<int64_t>(static_cast<size_t>(nR) + 1);

@@ -23,6 +23,11 @@ struct hbdia_matrix {
     hbdia::HostLayout<float> L32;
     hbdia::DevicePlan plan;
     hbdia::DeviceLayoutMeta devMeta;    // layout facts when the GPU converter built the plan
+    bool hasDIA = false;                // DIA format (host data)
+    std::vector<int32_t> diaOffsets;
+    std::vector<double> dia64;
+    std::vector<float> dia32;
+    int32_t diaLength = 0;
     hbdia::DevicePlan innerPlan;        // reduced-storage copy for the CG inner iterations
     hbdia::CgWork *cg = nullptr;        // CG workspace
     int32_t blockWidth = 0, threshold = 0;

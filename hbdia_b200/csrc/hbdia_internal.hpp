@@ -52,6 +52,17 @@ template <typename T>
 void convert_to_hbdia(const Coo<T> &coo, int32_t blockWidth, int32_t threshold, int64_t maxCoo,
                       HostLayout<T> &out);
 
+// DIA format and storage costs (dia.cpp)
+template <typename T>
+void remove_coo_duplicates(Coo<T> &c);
+template <typename T>
+void convert_to_dia(Coo<T> &c, bool cooIsUnique, std::vector<int32_t> &offsets, std::vector<T> &diagonals,
+                    int32_t &diagLength);
+void storage_costs(int64_t valueBytes, int32_t numRows, int32_t numCols, int64_t numNonZeros,
+                   int32_t numberDiagonals, int32_t numBlocks, int32_t blockWidth, int64_t hbdiaSlots,
+                   int64_t cooEntries, const std::vector<int32_t> &histBlocks, const std::vector<int32_t> &nnzPerRow,
+                   hbdia_storage_costs &out);
+
 // Generators (generate.cpp)
 template <typename T>
 void reference_stencil27(int nx, int ny, int nz, double noise, int iteration, Coo<T> &out);

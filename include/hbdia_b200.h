@@ -132,6 +132,34 @@ int hbdia_matrix_convert(hbdia_matrix *m, int32_t blockWidth, int32_t threshold,
  * the matrix's stream.  storage selects the device value format. */
 int hbdia_matrix_prepare_gpu(hbdia_matrix *m, int32_t storage);
 
+/* removeCOODuplicates (src/Format/HBDIA.cpp:372-412): entries with the same
+ * (row, col) are summed (0 + v1 + v2 + ... in input order) and the COO is
+ * left sorted by (row, col). */
+int hbdia_matrix_remove_duplicates(hbdia_matrix *m);
+
+/* convertToDIAFormat(COOisUnique) (src/Format/HBDIA.cpp:414-505): unless
+ * cooIsUnique, removes duplicates first (changing the COO, as the reference
+ * does); then one diagonal of min(numRows, numCols) values per distinct
+ * offset col - row, ascending.  Host data only (the reference uploads DIA
+ * data to no device).  No-op when converted already or without COO. */
+int hbdia_matrix_convert_dia(hbdia_matrix *m, int32_t cooIsUnique);
+/* isDIAFormat, getOffsets().size(), diagonal length */
+int hbdia_matrix_dia_info(const hbdia_matrix *m, int32_t *hasDIA, int32_t *numDiagonals, int32_t *diagLength);
+/* getOffsets (numDiagonals int32) and getDiagonals flattened [diagonal][position]
+ * (include/Format/HBDIA.hpp:89-90). */
+int hbdia_matrix_export_dia(const hbdia_matrix *m, int32_t *offsets, void *diagonals);
+
+/* Storage costs in bytes of the matrix held as HBDIA (its values, block
+ * pointers, stored offsets and COO remainder), COO, DIA, SELL-C (C =
+ * blockWidth, from the per-row counts the 27-point stencil generator
+ * records; meaningful for threshold 1) and CSR -- the figures the
+ * reference's benchmark prints and saves (benchmarking/benchmark.cpp:171-215).
+ * Needs the HBDIA conversion. */
+typedef struct hbdia_storage_costs {
+    int64_t hbdia, coo, dia, sell, csr;
+} hbdia_storage_costs;
+int hbdia_matrix_storage_costs(const hbdia_matrix *m, hbdia_storage_costs *costs);
+
 /* convertToHBDIAFormat (src/Format/HBDIA.cpp:507-718) + prepareForGPU done
  * on the GPU: the same device layout (and the same offsets, values, COO
  * remainder, histograms and numberDiagonals) as hbdia_matrix_convert +

@@ -207,6 +207,10 @@ class Reference:
             f.restype = _vp
             getattr(lib, f"ref_cpu_coo_spmv_{t}").argtypes = [_vp, _vp, ctypes.c_int, _vp]
             getattr(lib, f"ref_cpu_coo_destroy_{t}").argtypes = [_vp]
+        lib.ref_matrix_remove_dups_f64.argtypes = [_vp]
+        lib.ref_matrix_convert_dia_f64.argtypes = [_vp, ctypes.c_int]
+        lib.ref_matrix_dia_sizes_f64.argtypes = [_vp, _vp]
+        lib.ref_matrix_export_dia_f64.argtypes = [_vp] * 6
         lib.ref_coo_sizes_f64.argtypes = [_vp, _i64p]
         lib.ref_coo_export_f64.argtypes = [_vp, _vp, _vp, _vp]
         lib.ref_stencil27_f64.argtypes = [ctypes.c_int] * 3 + [ctypes.c_double, ctypes.c_int]
@@ -223,6 +227,31 @@ class Reference:
     @staticmethod
     def available(path: str = _REF_SO) -> bool:
         return os.path.exists(path)
+
+    def dia(self, rows, cols, vals, num_rows, num_cols, coo_unique=False, remove_first=False):
+        """The reference's convertToDIAFormat on a float64 matrix: (offsets,
+        diagonals [numDiagonals, length], (rows, cols, vals) of its COO after
+        the call, numNonZeros)."""
+        rows = np.ascontiguousarray(rows, np.int32)
+        cols = np.ascontiguousarray(cols, np.int32)
+        vals = np.ascontiguousarray(vals, np.float64)
+        h = self.lib.ref_matrix_create_f64(_ptr(rows), _ptr(cols), _ptr(vals), len(vals), num_rows, num_cols, 1)
+        if not h:
+            raise ValueError("reference constructor rejected the input")
+        try:
+            if remove_first:
+                self.lib.ref_matrix_remove_dups_f64(h)
+            self.lib.ref_matrix_convert_dia_f64(h, int(bool(coo_unique)))
+            s = np.zeros(5, np.int64)
+            self.lib.ref_matrix_dia_sizes_f64(h, _ptr(s))
+            nd, ln, nnz, ncoo = int(s[0]), int(s[1]), int(s[2]), int(s[3])
+            off = np.zeros(nd, np.int32)
+            diag = np.zeros((nd, ln), np.float64)
+            r, c, v = np.zeros(ncoo, np.int32), np.zeros(ncoo, np.int32), np.zeros(ncoo, np.float64)
+            self.lib.ref_matrix_export_dia_f64(h, _ptr(off), _ptr(diag), _ptr(r), _ptr(c), _ptr(v))
+            return off, diag, (r, c, v), nnz
+        finally:
+            self.lib.ref_matrix_destroy_f64(h)
 
     # convertToHBDIAFormat through the partial-matrix constructor (no GPU needed)
     def convert(self, rows, cols, vals, num_rows, num_cols, bw=32, thr=1, max_coo=1_000_000_000,
@@ -315,3 +344,24 @@ class _RefCoo:
         if getattr(self, "_h", None):
             getattr(self._o.lib, f"ref_cpu_coo_destroy_{self.t}")(self._h)
             self._h = None
+
+
+def storage_costs(value_bytes, num_rows, num_cols, nnz, number_diagonals, num_blocks, block_width, hbdia_slots,
+                  coo_entries, hist_blocks, nnz_per_row):
+    """The storage-cost arithmetic of the reference's benchmark
+    (benchmarking/benchmark.cpp:171-215), restated: HBDIA, COO, DIA, SELL-C
+    (C = block width) and CSR bytes of one matrix.  Test infrastructure."""
+    sum_hist = sum(i * int(h) for i, h in enumerate(hist_blocks))
+    hbdia = hbdia_slots * value_bytes + (num_blocks + 1) * 4 + sum_hist * 4 + coo_entries * 4 * 2 + coo_entries * value_bytes
+    coo = nnz * 4 * 2 + nnz * value_bytes
+    dia = number_diagonals * min(num_rows, num_cols) * value_bytes + number_diagonals * 4
+    sell, mx = 0, 0
+    for i, c in enumerate(nnz_per_row):
+        if i % block_width == 0 and i > 0:
+            sell += mx * block_width * value_bytes + mx * block_width * 4
+            mx = 0
+        mx = max(mx, int(c))
+    sell += mx * block_width * value_bytes + mx * block_width * 4
+    sell += ((num_rows + block_width - 1) // block_width) * 4
+    csr = nnz * value_bytes + nnz * 4 + (num_rows + 1) * 4
+    return {"hbdia": hbdia, "coo": coo, "dia": dia, "sell": sell, "csr": csr}

@@ -146,6 +146,33 @@ void ref_matrix_export_f32(void *h, int *offsets, int *blockStart, float *data, 
     export_layout(static_cast<HBDIA<float> *>(h), offsets, blockStart, data, cooRow, cooCol,
                   cooVal, cooRowPtr, histBlocks, histNnz);
 }
+// ---- convertToDIAFormat / removeCOODuplicates (src/Format/HBDIA.cpp:372-505)
+void ref_matrix_remove_dups_f64(void *h) { static_cast<HBDIA<double> *>(h)->removeCOODuplicates(); }
+void ref_matrix_convert_dia_f64(void *h, int cooUnique) {
+    static_cast<HBDIA<double> *>(h)->convertToDIAFormat(cooUnique != 0);
+}
+// out: numDiagonals, diagonal length, numNonZeros, COO entries, isDIAFormat
+void ref_matrix_dia_sizes_f64(void *h, int64_t *out) {
+    auto *m = static_cast<HBDIA<double> *>(h);
+    const auto &d = m->getDiagonals();
+    out[0] = static_cast<int64_t>(m->getOffsets().size());
+    out[1] = d.empty() ? 0 : static_cast<int64_t>(d[0].size());
+    out[2] = m->getNumNonZeros();
+    out[3] = static_cast<int64_t>(m->getValues().size());
+    out[4] = m->getHasDIA() ? 1 : 0;
+}
+void ref_matrix_export_dia_f64(void *h, int *offsets, double *diagonals, int *rows, int *cols, double *vals) {
+    auto *m = static_cast<HBDIA<double> *>(h);
+    const auto &o = m->getOffsets();
+    const auto &d = m->getDiagonals();
+    std::copy(o.begin(), o.end(), offsets);
+    size_t p = 0;
+    for (const auto &diag : d)
+        for (double v : diag) diagonals[p++] = v;
+    std::copy(m->getRowIndices().begin(), m->getRowIndices().end(), rows);
+    std::copy(m->getColIndices().begin(), m->getColIndices().end(), cols);
+    std::copy(m->getValues().begin(), m->getValues().end(), vals);
+}
 void ref_matrix_destroy_f64(void *h) { delete static_cast<HBDIA<double> *>(h); }
 void ref_matrix_destroy_f32(void *h) { delete static_cast<HBDIA<float> *>(h); }
 

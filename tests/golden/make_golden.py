@@ -3,7 +3,8 @@
 Runs only where the reference tree exists: it builds oracle/_ref from the
 reference sources (oracle/Makefile) and records, for small fixed inputs, the
 exact outputs of the reference's convertToHBDIAFormat
-(src/Format/HBDIA.cpp:507-718), create3DStencil27Point
+(src/Format/HBDIA.cpp:507-718), convertToDIAFormat and removeCOODuplicates
+(src/Format/HBDIA.cpp:372-505), create3DStencil27Point
 (src/Format/HBDIA.cpp:1416-1607) and cpu_coo_spmv_kernel
 (src/Operations/HBDIASpMV.cpp:36-99).  With --gpu (on a CUDA machine) it also
 records the reference's full hbdiaSpMV result (its blocked-DIA kernel,
@@ -99,14 +100,56 @@ def save_layout(path, rows, cols, vals, nr, nc, bw, thr, mc, L: oracle.Layout, *
                         has_hbdia=int(L.has_hbdia), **{k: getattr(L, k) for k in LAYOUT_KEYS}, **extra)
 
 
+def dia_cases():
+    """Inputs of the DIA fixtures: (rows, cols, vals, numRows, numCols,
+    COOisUnique, removeCOODuplicates first)."""
+    rng = np.random.default_rng(42)
+    out = []
+    r, c, v = print_test_3x3()
+    out.append((r, c, v, 3, 3, False, False))
+    for nr, nc, nnz in ((40, 30, 300), (30, 45, 260)):
+        r = np.sort(rng.integers(0, nr, nnz)).astype(np.int32)
+        c = rng.integers(0, nc, nnz).astype(np.int32)
+        v = rng.standard_normal(nnz)
+        dup = rng.integers(0, nnz, 40)  # repeated positions with other values
+        r = np.concatenate([r, r[dup]])
+        c = np.concatenate([c, c[dup]])
+        v = np.concatenate([v, rng.standard_normal(40)])
+        v[rng.random(len(v)) < 0.05] = -0.0
+        out.append((r, c, v, nr, nc, False, False))
+        out.append((r, c, v, nr, nc, True, False))   # duplicates kept: last one wins in DIA
+        out.append((r, c, v, nr, nc, False, True))   # removeCOODuplicates, then the conversion
+    return out
+
+
+def save_dia(path, R):
+    out = {}
+    cases = dia_cases()
+    r, c, v, nr, nc = R.stencil27(6, 6, 6, 0.05, 1)
+    cases.append((r, c, v, nr, nc, False, False))
+    for k, (r, c, v, nr, nc, uniq, first) in enumerate(cases):
+        off, diag, (orr, occ, ovv), nnz = R.dia(r, c, v, nr, nc, coo_unique=uniq, remove_first=first)
+        out.update({f"c{k}_rows": r, f"c{k}_cols": c, f"c{k}_vals": v,
+                    f"c{k}_params": np.array([nr, nc, int(uniq), int(first), nnz], np.int64),
+                    f"c{k}_offsets": off, f"c{k}_diag": diag, f"c{k}_out_rows": orr, f"c{k}_out_cols": occ,
+                    f"c{k}_out_vals": ovv})
+    np.savez_compressed(path, ncase=len(cases), **out)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpu", action="store_true")
+    ap.add_argument("--dia-only", action="store_true", help="write dia_reference.npz only")
     ap.add_argument("--out", default=HERE)
     a = ap.parse_args()
     if not oracle.Reference.available():
         oracle.build()
     R = oracle.Reference()
+    # the reference's convertToDIAFormat / removeCOODuplicates (src/Format/HBDIA.cpp:372-505)
+    save_dia(os.path.join(a.out, "dia_reference.npz"), R)
+    if a.dia_only:
+        print("golden fixtures written to", a.out)
+        return
 
     r, c, v = print_test_3x3()
     save_layout(os.path.join(a.out, "print_test_3x3.npz"), r, c, v, 3, 3, 4, 2, 10 ** 9,
