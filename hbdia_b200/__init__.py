@@ -291,6 +291,105 @@ class HBDIA:
         """Test hook: the staged kernel never publishes `chunk` (-1: off)."""
         _check(_load().hbdia_matrix_test_skip_chunk(self._h, int(chunk)))
 
+    # ---- partial matrices: one rank's rows (include/Format/HBDIA.hpp:37-39, 77-79, 117-136)
+    @classmethod
+    def _adopt(cls, handle: ctypes.c_void_p, dtype) -> "HBDIA":
+        m = cls.__new__(cls)
+        m.dtype = np.dtype(dtype)
+        m._h = handle
+        return m
+
+    @classmethod
+    def partial(cls, rowIndices, colIndices, values, numRows: int, numCols: int, globalRowMapping,
+                partialMatrix: bool = True, numGlobalRows: Optional[int] = None,
+                numGlobalCols: Optional[int] = None, numGlobalNonZeros: int = 0, rank: int = 0, size: int = 1,
+                dtype=np.float64) -> "HBDIA":
+        """``HBDIA(rows, cols, vals, numRows, numCols, globalRowMapping, partialMatrix,
+        numGlobalRows, numGlobalCols, numGlobalNonZeros, rank, size)``
+        (src/Format/HBDIA.cpp:118-154): local rows, global columns.  The global
+        row mapping must be contiguous (the one BasicExtractor builds)."""
+        if not partialMatrix:
+            return cls(rowIndices, colIndices, values, numRows, numCols, dtype=dtype)
+        mapping = np.asarray(globalRowMapping, np.int64)
+        if len(mapping) != numRows:
+            raise ValueError("Global row mapping size must match number of rows")
+        if np.any(np.diff(mapping) != 1):
+            raise NotImplementedError("only contiguous global row mappings (the row-wise partition's)")
+        r = np.ascontiguousarray(rowIndices, np.int32)
+        c = np.ascontiguousarray(colIndices, np.int32)
+        v = np.ascontiguousarray(values, np.dtype(dtype))
+        if not (len(r) == len(c) == len(v)):
+            raise ValueError("Row indices, column indices, and values vectors must have the same size")
+        h = ctypes.c_void_p()
+        _check(_load().hbdia_matrix_create_partial(
+            _dtype_code(np.dtype(dtype)), _vp(r), _vp(c), _vp(v), len(v), int(numRows),
+            int(numGlobalRows if numGlobalRows is not None else numCols),
+            int(numGlobalCols if numGlobalCols is not None else numCols), int(numGlobalNonZeros),
+            int(mapping[0]) if len(mapping) else 0, int(rank), int(size), ctypes.byref(h)))
+        return cls._adopt(h, dtype)
+
+    def partition(self, numProcesses: int, part: int) -> "HBDIA":
+        """Partition ``part`` of BasicExtractor's row-wise partitioning
+        (src/DataExchange/BasicExtractor.cpp:124-234) as a partial matrix."""
+        h = ctypes.c_void_p()
+        _check(_load().hbdia_matrix_partition(self._h, int(numProcesses), int(part), ctypes.byref(h)))
+        return HBDIA._adopt(h, self.dtype)
+
+    def partialInfo(self) -> "_lib.PartialInfo":
+        i = _lib.PartialInfo()
+        _check(_load().hbdia_matrix_partial_info(self._h, ctypes.byref(i)))
+        return i
+
+    def isPartialMatrix(self) -> bool: return bool(self.partialInfo().isPartial)
+    def getNumGlobalRows(self) -> int: return self.partialInfo().numGlobalRows
+    def getNumGlobalCols(self) -> int: return self.partialInfo().numGlobalCols
+    def getNumGlobalNonZeros(self) -> int: return self.partialInfo().numGlobalNonZeros
+
+    def getGlobalRowMapping(self) -> np.ndarray:
+        i = self.partialInfo()
+        if not i.isPartial:
+            return np.zeros(0, np.int32)
+        return np.arange(i.globalRowStart, i.globalRowStart + self.getNumRows(), dtype=np.int32)
+
+    def getGlobalRowIndex(self, localRowIndex: int) -> int:
+        i = self.partialInfo()
+        return int(localRowIndex) + (i.globalRowStart if i.isPartial else 0)
+
+    def _ranges(self):
+        i = self.partialInfo()
+        d = np.zeros((i.numDataRanges, 2), np.int32)
+        p = np.zeros((i.numProcessRanges, 3), np.int32)
+        _check(_load().hbdia_matrix_export_ranges(self._h, _vp(d), _vp(p)))
+        return i, d, p
+
+    def analyzeDataRanges(self) -> None:
+        """Kept for the reference's call sequence: a partial matrix's data
+        ranges are computed by convertToHBDIAFormat."""
+
+    def getDataRanges(self) -> List[tuple]:
+        """analyzeDataRanges (src/Format/HBDIA.cpp:1333-1414): merged [start, end)
+        ranges of the global columns this rank's rows read."""
+        return [tuple(int(v) for v in r) for r in self._ranges()[1]]
+
+    def hasPartialMatrixMetadata(self) -> bool:
+        i = self.partialInfo()
+        return bool(i.isPartial and i.hasMetadata and i.totalBufferSize > 0)
+
+    def getPartialMatrixMetadata(self) -> dict:
+        """PartialMatrixMetadata (include/Format/HBDIA.hpp:18-22): dataRanges,
+        processDataRanges[p] (the ranges process p provides) and totalBufferSize."""
+        i, d, p = self._ranges()
+        per = [[] for _ in range(max(i.size, 1))]
+        for q, s, e in p:
+            per[int(q)].append((int(s), int(e)))
+        return {"dataRanges": [tuple(int(v) for v in r) for r in d], "processDataRanges": per,
+                "totalBufferSize": int(i.totalBufferSize)}
+
+    def window(self) -> tuple:
+        """(first global column, length) of the x window the plan reads."""
+        i = self.partialInfo()
+        return int(i.windowStart), int(i.windowLength)
+
 
 class HBDIAVector:
     """``HBDIAVector<T>`` on one GPU: a device buffer (no halos)."""

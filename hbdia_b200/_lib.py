@@ -87,6 +87,14 @@ class StorageCosts(ctypes.Structure):
     _fields_ = [("hbdia", c_i64), ("coo", c_i64), ("dia", c_i64), ("sell", c_i64), ("csr", c_i64)]
 
 
+class PartialInfo(ctypes.Structure):
+    _fields_ = [("isPartial", c_i32), ("hasMetadata", c_i32), ("globalRowStart", c_i32),
+                ("numGlobalRows", c_i32), ("numGlobalCols", c_i32), ("rank", c_i32), ("size", c_i32),
+                ("numGlobalNonZeros", c_i64), ("numDataRanges", c_i64), ("numProcessRanges", c_i64),
+                ("totalBufferSize", c_i64), ("leftBufferSize", c_i64), ("rightBufferSize", c_i64),
+                ("windowStart", c_i32), ("windowLength", c_i32)]
+
+
 class HBDIACudaError(RuntimeError):
     """A CUDA runtime call inside the library failed."""
 
@@ -179,6 +187,15 @@ _SIGS = [
     ("hbdia_server_pause", ctypes.c_int, [c_vp, c_i32]),
     ("hbdia_server_wait", ctypes.c_int, [c_vp, ctypes.c_uint64, ctypes.POINTER(RequestInfo)]),
     ("hbdia_server_get_stats", ctypes.c_int, [c_vp, ctypes.POINTER(ServerStats)]),
+    ("hbdia_matrix_create_partial", ctypes.c_int, [c_i32, c_vp, c_vp, c_vp, c_i64, c_i32, c_i32, c_i32, c_i64,
+                                                   c_i32, c_i32, c_i32, c_vpp]),
+    ("hbdia_matrix_partition", ctypes.c_int, [c_vp, c_i32, c_i32, c_vpp]),
+    ("hbdia_matrix_partial_info", ctypes.c_int, [c_vp, ctypes.POINTER(PartialInfo)]),
+    ("hbdia_matrix_export_ranges", ctypes.c_int, [c_vp, c_vp, c_vp]),
+    ("hbdia_halo_create", ctypes.c_int, [c_i32, c_vp, c_vp, c_vp, c_i32, c_i64, c_i64, c_vpp]),
+    ("hbdia_halo_copy", ctypes.c_int, [c_vp, c_vp, c_vp, c_vp]),
+    ("hbdia_halo_elements", c_i64, [c_vp]),
+    ("hbdia_halo_destroy", None, [c_vp]),
 ]
 
 # every C-ABI entry point (the exported-symbol check in the tests uses this list)

@@ -19,6 +19,7 @@ inline dev::SpmvArgs<VT, XT> make_args(const DevicePlan &P) {
     a.cooRowPtr = P.cooRowPtr;
     a.cooTile = P.cooTile;
     a.n = P.n;
+    a.xn = P.xn;
     a.bw = P.bw;
     a.numBlocks = P.numBlocks;
     a.numTiles = P.numTiles;

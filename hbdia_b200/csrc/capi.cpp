@@ -24,6 +24,10 @@ struct hbdia_server {
     hbdia::Server *S = nullptr;
 };
 
+struct hbdia_halo {
+    hbdia::Halo *H = nullptr;
+};
+
 namespace {
 
 thread_local std::string g_err;
@@ -110,13 +114,21 @@ void reset_hbdia(hbdia_matrix *m) {
     m->L32 = hbdia::HostLayout<float>();
     m->hasHBDIA = false;
     m->hostLayout = false;
+    m->part.hasMetadata = false;
 }
 
 void prepare(hbdia_matrix *m, int32_t storage) {
     need(m->hasHBDIA, HBDIA_ERR_NOT_CONVERTED, "matrix is not in HBDIA format");
     need(m->hostLayout, HBDIA_ERR_NOT_CONVERTED, "no host layout to upload");
-    if (m->dtype == HBDIA_F32) hbdia::build_plan(m->L32, storage, m->plan);
-    else hbdia::build_plan(m->L64, storage, m->plan);
+    hbdia::ColumnWindow w, *W = nullptr;
+    if (m->part.partial) {  // the plan reads x through the rank's window
+        w.lo = m->part.windowLo;
+        w.len = m->part.windowLen;
+        w.rowBase = m->dtype == HBDIA_F32 ? m->c32.rowBase : m->c64.rowBase;
+        W = &w;
+    }
+    if (m->dtype == HBDIA_F32) hbdia::build_plan(m->L32, storage, m->plan, W);
+    else hbdia::build_plan(m->L64, storage, m->plan, W);
 }
 
 void ensure_device(hbdia_matrix *m) {
@@ -235,6 +247,10 @@ int hbdia_matrix_convert(hbdia_matrix *m, int32_t blockWidth, int32_t threshold,
         need(blockWidth > 0, HBDIA_ERR_INVALID_ARGUMENT, "blockWidth must be positive");
         if (m->dtype == HBDIA_F32) hbdia::convert_to_hbdia(m->c32, blockWidth, threshold, maxCoo, m->L32);
         else hbdia::convert_to_hbdia(m->c64, blockWidth, threshold, maxCoo, m->L64);
+        if (m->part.partial) {  // BasicDistributor::receiveMatrix's analyzeDataRanges + metadata
+            if (m->dtype == HBDIA_F32) hbdia::partial_metadata(m->c32, m->L32, m->part);
+            else hbdia::partial_metadata(m->c64, m->L64, m->part);
+        }
         m->hasHBDIA = true;
         m->hostLayout = true;
         m->blockWidth = blockWidth;
@@ -328,6 +344,7 @@ int hbdia_matrix_convert_on_device(hbdia_matrix *m, int32_t blockWidth, int32_t 
         // the same early returns as convertToHBDIAFormat (src/Format/HBDIA.cpp:511-524)
         if (m->hasHBDIA || !m->hasCOO || coo_nnz(m) == 0) return;
         need(blockWidth > 0, HBDIA_ERR_INVALID_ARGUMENT, "blockWidth must be positive");
+        need(!m->part.partial, HBDIA_ERR_UNSUPPORTED, "partial matrices convert on the host (hbdia_matrix_convert)");
         if (m->dtype == HBDIA_F32)
             hbdia::convert_on_device(m->c32, blockWidth, threshold, maxCoo, storage, m->plan, m->devMeta);
         else hbdia::convert_on_device(m->c64, blockWidth, threshold, maxCoo, storage, m->plan, m->devMeta);
@@ -696,6 +713,7 @@ int hbdia_cg_solve(hbdia_matrix *m, const double *b, double *x, const hbdia_cg_o
         need(m->dtype == HBDIA_F64, HBDIA_ERR_UNSUPPORTED, "the CG solver needs a double matrix");
         need(m->hasHBDIA, HBDIA_ERR_NOT_CONVERTED, "matrix is not in HBDIA format");
         need(num_rows(m) == num_cols(m), HBDIA_ERR_INVALID_ARGUMENT, "CG needs a square matrix");
+        need(!m->part.partial, HBDIA_ERR_UNSUPPORTED, "CG runs on whole matrices, not on one rank's rows");
         need(opt->tol > 0 && opt->innerTol > 0 && opt->maxOuter >= 0 && opt->maxInner > 0 && opt->checkEvery > 0,
              HBDIA_ERR_INVALID_ARGUMENT, "bad CG options");
         ensure_device(m);
@@ -746,6 +764,7 @@ void hbdia_server_destroy(hbdia_server *s) {
 int hbdia_server_add_matrix(hbdia_server *s, const hbdia_matrix *m, int32_t *id) {
     return guarded([&] {
         need(s && m && id, HBDIA_ERR_INVALID_ARGUMENT, "null argument");
+        need(!m->part.partial, HBDIA_ERR_UNSUPPORTED, "the server serves whole matrices");
         *id = hbdia::server_add_matrix(s->S, m);
     });
 }
@@ -892,3 +911,134 @@ int hbdia_fill_uniform(double *out, int64_t n, double lo, double hi, uint64_t se
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------- row partitioning
+int hbdia_matrix_create_partial(hbdia_dtype dtype, const int32_t *rows, const int32_t *cols, const void *values,
+                                int64_t nnz, int32_t numLocalRows, int32_t numGlobalRows, int32_t numGlobalCols,
+                                int64_t numGlobalNonZeros, int32_t globalRowStart, int32_t rank, int32_t size,
+                                hbdia_matrix **out) {
+    return guarded([&] {
+        need(out != nullptr, HBDIA_ERR_INVALID_ARGUMENT, "null output handle");
+        need(dtype == HBDIA_F64 || dtype == HBDIA_F32, HBDIA_ERR_INVALID_ARGUMENT, "unknown dtype");
+        need(numLocalRows > 0 && numGlobalRows > 0 && numGlobalCols > 0, HBDIA_ERR_INVALID_ARGUMENT,
+             "Matrix dimensions must be positive");
+        need(numGlobalRows == numGlobalCols, HBDIA_ERR_UNSUPPORTED,
+             "row partitioning needs a square matrix (x is partitioned like the rows)");
+        need(globalRowStart >= 0 && static_cast<int64_t>(globalRowStart) + numLocalRows <= numGlobalRows,
+             HBDIA_ERR_OUT_OF_RANGE, "the local rows lie outside the global matrix");
+        need(size >= 1 && rank >= 0 && rank < size, HBDIA_ERR_INVALID_ARGUMENT, "bad rank / size");
+        need(numGlobalRows / size >= 1, HBDIA_ERR_INVALID_ARGUMENT, "more processes than rows");
+        std::unique_ptr<hbdia_matrix> m(new hbdia_matrix());
+        m->dtype = dtype;
+        // the partial constructor validates against numRows = numLocalRows and
+        // numCols = numLocalCols = numGlobalCols (src/Format/HBDIA.cpp:140-153)
+        if (dtype == HBDIA_F32) {
+            fill_coo(m->c32, rows, cols, values, nnz, numLocalRows, numGlobalCols);
+            m->c32.rowBase = globalRowStart;
+        } else {
+            fill_coo(m->c64, rows, cols, values, nnz, numLocalRows, numGlobalCols);
+            m->c64.rowBase = globalRowStart;
+        }
+        m->hasCOO = true;
+        m->part.partial = true;
+        m->part.numGlobalRows = numGlobalRows;
+        m->part.numGlobalCols = numGlobalCols;
+        m->part.numGlobalNonZeros = numGlobalNonZeros;
+        m->part.rank = rank;
+        m->part.size = size;
+        m->part.windowLo = globalRowStart;
+        m->part.windowLen = numLocalRows;
+        *out = m.release();
+    });
+}
+
+int hbdia_matrix_partition(const hbdia_matrix *g, int32_t numProcesses, int32_t part, hbdia_matrix **out) {
+    return guarded([&] {
+        need(g && out, HBDIA_ERR_INVALID_ARGUMENT, "null argument");
+        need(g->hasCOO, HBDIA_ERR_INVALID_ARGUMENT, "Matrix must be in COO format for partitioning");
+        need(!g->part.partial, HBDIA_ERR_UNSUPPORTED, "the matrix is a partition already");
+        std::unique_ptr<hbdia_matrix> m(new hbdia_matrix());
+        m->dtype = g->dtype;
+        int32_t nLocal, rb;
+        if (g->dtype == HBDIA_F32) {
+            hbdia::partition_rows(g->c32, numProcesses, part, m->c32);
+            nLocal = m->c32.numRows;
+            rb = m->c32.rowBase;
+        } else {
+            hbdia::partition_rows(g->c64, numProcesses, part, m->c64);
+            nLocal = m->c64.numRows;
+            rb = m->c64.rowBase;
+        }
+        m->hasCOO = true;
+        m->part.partial = true;
+        m->part.numGlobalRows = num_rows(g);
+        m->part.numGlobalCols = num_cols(g);
+        m->part.numGlobalNonZeros = coo_nnz(g);
+        m->part.rank = part;
+        m->part.size = numProcesses;
+        m->part.windowLo = rb;
+        m->part.windowLen = nLocal;
+        *out = m.release();
+    });
+}
+
+int hbdia_matrix_partial_info(const hbdia_matrix *m, hbdia_partial_info *info) {
+    return guarded([&] {
+        need(m && info, HBDIA_ERR_INVALID_ARGUMENT, "null argument");
+        const hbdia::PartialMeta &p = m->part;
+        hbdia_partial_info I;
+        std::memset(&I, 0, sizeof(I));
+        I.isPartial = p.partial;
+        I.hasMetadata = p.hasMetadata;
+        I.globalRowStart = m->dtype == HBDIA_F32 ? m->c32.rowBase : m->c64.rowBase;
+        I.numGlobalRows = p.partial ? p.numGlobalRows : num_rows(m);
+        I.numGlobalCols = p.partial ? p.numGlobalCols : num_cols(m);
+        I.numGlobalNonZeros = p.partial ? p.numGlobalNonZeros : coo_nnz(m);
+        I.rank = p.rank;
+        I.size = p.size;
+        I.numDataRanges = static_cast<int64_t>(p.dataRanges.size() / 2);
+        I.numProcessRanges = static_cast<int64_t>(p.processRanges.size() / 3);
+        I.totalBufferSize = p.totalBufferSize;
+        I.leftBufferSize = p.leftBufferSize;
+        I.rightBufferSize = p.rightBufferSize;
+        I.windowStart = p.partial ? p.windowLo : 0;
+        I.windowLength = p.partial ? p.windowLen : num_cols(m);
+        *info = I;
+    });
+}
+
+int hbdia_matrix_export_ranges(const hbdia_matrix *m, int32_t *dataRanges, int32_t *processRanges) {
+    return guarded([&] {
+        need(m != nullptr, HBDIA_ERR_INVALID_ARGUMENT, "null matrix");
+        const hbdia::PartialMeta &p = m->part;
+        if (dataRanges && !p.dataRanges.empty())
+            std::memcpy(dataRanges, p.dataRanges.data(), p.dataRanges.size() * sizeof(int32_t));
+        if (processRanges && !p.processRanges.empty())
+            std::memcpy(processRanges, p.processRanges.data(), p.processRanges.size() * sizeof(int32_t));
+    });
+}
+
+int hbdia_halo_create(int32_t elemBytes, const int64_t *srcOffset, const int64_t *dstOffset, const int64_t *length,
+                      int32_t numSegments, int64_t srcLength, int64_t dstLength, hbdia_halo **out) {
+    return guarded([&] {
+        need(out != nullptr, HBDIA_ERR_INVALID_ARGUMENT, "null output handle");
+        std::unique_ptr<hbdia_halo> h(new hbdia_halo());
+        h->H = hbdia::halo_create(elemBytes, srcOffset, dstOffset, length, numSegments, srcLength, dstLength);
+        *out = h.release();
+    });
+}
+
+int hbdia_halo_copy(const hbdia_halo *h, const void *src, void *dst, void *stream) {
+    return guarded([&] {
+        need(h != nullptr, HBDIA_ERR_INVALID_ARGUMENT, "null halo");
+        hbdia::halo_copy(h->H, src, dst, stream);
+    });
+}
+
+int64_t hbdia_halo_elements(const hbdia_halo *h) { return h ? hbdia::halo_elements(h->H) : 0; }
+
+void hbdia_halo_destroy(hbdia_halo *h) {
+    if (!h) return;
+    hbdia::halo_free(h->H);
+    delete h;
+}

@@ -53,14 +53,14 @@ inline int64_t find_with_cursor(const int32_t *list, int64_t n, int32_t key, int
 
 // Distinct (offset, count) of one block's entries, ascending by offset.
 template <typename EntryFn>
-void block_histogram(int64_t j0, int64_t j1, const int32_t *R, const int32_t *C, EntryFn entry,
+void block_histogram(int64_t j0, int64_t j1, const int32_t *R, const int32_t *C, int32_t rb, EntryFn entry,
                      std::vector<OffCount> &list, std::vector<int32_t> &scratch) {
     list.clear();
     size_t cursor = 0;
     bool overflow = false;
     for (int64_t j = j0; j < j1; ++j) {
         const int64_t i = entry(j);
-        const int32_t off = C[i] - R[i];
+        const int32_t off = C[i] - R[i] - rb;
         if (cursor < list.size() && list[cursor].off == off) {
             list[cursor++].cnt++;
             continue;
@@ -82,7 +82,7 @@ void block_histogram(int64_t j0, int64_t j1, const int32_t *R, const int32_t *C,
     scratch.clear();
     for (int64_t j = j0; j < j1; ++j) {
         const int64_t i = entry(j);
-        scratch.push_back(C[i] - R[i]);
+        scratch.push_back(C[i] - R[i] - rb);
     }
     std::sort(scratch.begin(), scratch.end());
     list.clear();
@@ -102,6 +102,7 @@ void convert_to_hbdia(const Coo<T> &coo, int32_t bw, int32_t thr, int64_t maxCoo
     if (bw <= 0) throw Error(HBDIA_ERR_INVALID_ARGUMENT, "blockWidth must be positive");
     const int64_t nnz = static_cast<int64_t>(coo.vals.size());
     const int32_t nR = coo.numRows, nC = coo.numCols;
+    const int32_t rb = coo.rowBase;  // 0 unless a partial matrix
     const int32_t *R = coo.rows.data();
     const int32_t *C = coo.cols.data();
     const T *V = coo.vals.data();
@@ -112,6 +113,7 @@ void convert_to_hbdia(const Coo<T> &coo, int32_t bw, int32_t thr, int64_t maxCoo
     L.blockWidth = bw;
     L.threshold = thr;
     L.maxCoo = maxCoo;
+    L.rowBase = rb;
     // maxNumBlocks = ceil(min(numRows, numCols) / blockWidth)   (HBDIA.cpp:537)
     const int32_t nb = static_cast<int32_t>((static_cast<int64_t>(std::min(nR, nC)) + bw - 1) / bw);
     L.numBlocks = nb;
@@ -158,7 +160,7 @@ void convert_to_hbdia(const Coo<T> &coo, int32_t bw, int32_t thr, int64_t maxCoo
         list.reserve(64);
 #pragma omp for schedule(dynamic, 256)
         for (int64_t b = 0; b < nb; ++b) {
-            block_histogram(bstart[b], bstart[b + 1], R, C, entry, list, scratch);
+            block_histogram(bstart[b], bstart[b + 1], R, C, rb, entry, list, scratch);
             for (size_t u = 0; u < list.size(); ++u) {
                 uoff[bstart[b] + u] = list[u].off;
                 ucnt[bstart[b] + u] = list[u].cnt;
@@ -193,12 +195,13 @@ void convert_to_hbdia(const Coo<T> &coo, int32_t bw, int32_t thr, int64_t maxCoo
 
     // numberDiagonals: distinct offsets over all blocks (HBDIA.cpp:563,585)
     {
-        const int64_t span = static_cast<int64_t>(nR) + nC;  // offsets in [-(nR-1), nC-1]
+        // offsets in [-(rb+nR-1), nC-1]
+        const int64_t span = static_cast<int64_t>(rb) + nR + nC;
         std::vector<uint64_t> bits(static_cast<size_t>((span + 63) / 64), 0);
 #pragma omp parallel for schedule(dynamic, 1024)
         for (int64_t b = 0; b < nb; ++b)
             for (int32_t u = 0; u < ndist[b]; ++u) {
-                const int64_t k = static_cast<int64_t>(uoff[bstart[b] + u]) + (nR - 1);
+                const int64_t k = static_cast<int64_t>(uoff[bstart[b] + u]) + rb + (nR - 1);
                 __atomic_fetch_or(&bits[k >> 6], uint64_t(1) << (k & 63), __ATOMIC_RELAXED);
             }
         int64_t nd = 0;
@@ -262,7 +265,7 @@ void convert_to_hbdia(const Coo<T> &coo, int32_t bw, int32_t thr, int64_t maxCoo
                 const int64_t nk = KS[b + 1] - KS[b];
                 int64_t cursor = 0, ncoo = 0;
                 for (int64_t i = bstart[b]; i < bstart[b + 1]; ++i) {
-                    const int64_t idx = nk ? find_with_cursor(KO + KS[b], nk, C[i] - R[i], cursor) : -1;
+                    const int64_t idx = nk ? find_with_cursor(KO + KS[b], nk, C[i] - R[i] - rb, cursor) : -1;
                     if (idx >= 0) {
                         D[(static_cast<int64_t>(KS[b]) + idx) * bw + (R[i] % bw)] = V[i];
                         h[nk]++;
@@ -287,7 +290,7 @@ void convert_to_hbdia(const Coo<T> &coo, int32_t bw, int32_t thr, int64_t maxCoo
             const int64_t nk = KS[b + 1] - KS[b];
             int64_t cursor = 0, p = cooCount[b];
             for (int64_t i = bstart[b]; i < bstart[b + 1]; ++i) {
-                const int64_t idx = nk ? find_with_cursor(KO + KS[b], nk, C[i] - R[i], cursor) : -1;
+                const int64_t idx = nk ? find_with_cursor(KO + KS[b], nk, C[i] - R[i] - rb, cursor) : -1;
                 if (idx < 0) {
                     L.cooRow[p] = R[i];
                     L.cooCol[p] = C[i];
@@ -307,7 +310,7 @@ void convert_to_hbdia(const Coo<T> &coo, int32_t bw, int32_t thr, int64_t maxCoo
             int64_t idx = -1, nk = 0, cursor = 0;
             if (b < nb) {
                 nk = KS[b + 1] - KS[b];
-                if (nk) idx = find_with_cursor(KO + KS[b], nk, C[i] - R[i], cursor);
+                if (nk) idx = find_with_cursor(KO + KS[b], nk, C[i] - R[i] - rb, cursor);
             }
             if (idx >= 0) {
                 D[(static_cast<int64_t>(KS[b]) + idx) * bw + (R[i] % bw)] = V[i];

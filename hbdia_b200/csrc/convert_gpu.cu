@@ -446,6 +446,7 @@ void convert_on_device(const Coo<T> &coo, int32_t bw, int32_t thr, int64_t maxCo
     Q.dtype = dtype;
     Q.storage = storage;
     Q.n = nR;
+    Q.xn = nR;
     Q.numCols = nC;
     Q.bw = bw;
     Q.numBlocks = nb;

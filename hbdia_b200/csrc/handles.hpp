@@ -32,5 +32,6 @@ struct hbdia_matrix {
     hbdia::CgWork *cg = nullptr;        // CG workspace
     int32_t blockWidth = 0, threshold = 0;
     int64_t maxCoo = 0;
+    hbdia::PartialMeta part;            // partial matrix (one rank's rows) and its metadata
     std::mutex hostMu;  // serialises hbdia_spmv_host's scratch buffers
 };

@@ -26,6 +26,10 @@ struct Coo {
     std::vector<T> vals;
     int32_t numRows = 0, numCols = 0;
     std::vector<int32_t> nnzPerRow;  // filled by the stencil generator only
+    // Partial matrix (one rank's rows): global row of local row 0.  Offsets
+    // are col - (row + rowBase), as the reference computes them from its
+    // global row mapping (src/Format/HBDIA.cpp:546-552).
+    int32_t rowBase = 0;
 };
 
 // Host HBDIA layout: exactly the reference's host-side members after
@@ -35,6 +39,7 @@ template <typename T>
 struct HostLayout {
     int32_t numRows = 0, numCols = 0, blockWidth = 0, threshold = 0;
     int64_t maxCoo = 0;
+    int32_t rowBase = 0;                   // partial matrices: global row of local row 0
     int32_t numBlocks = 0;                 // maxNumBlocks
     std::vector<int32_t> offsets;          // kept offsets, ascending per block
     std::vector<int32_t> blockStart;       // numBlocks + 1, offset units
@@ -46,6 +51,31 @@ struct HostLayout {
     std::vector<int32_t> histBlocks, histNnz;
     bool cooRowSorted = true;              // COO rows non-decreasing
 };
+
+// Partial matrix (one rank's rows, partition.cpp): the reference's
+// PartialMatrixMetadata plus this library's x window.
+struct PartialMeta {
+    bool partial = false, hasMetadata = false;
+    int32_t numGlobalRows = 0, numGlobalCols = 0, rank = 0, size = 1;
+    int64_t numGlobalNonZeros = 0;
+    std::vector<int32_t> dataRanges;      // pairs [start, end), ascending
+    std::vector<int32_t> processRanges;   // triples (process, start, end)
+    int64_t totalBufferSize = 0, leftBufferSize = 0, rightBufferSize = 0;
+    int32_t windowLo = 0, windowLen = 0;
+};
+template <typename T>
+void partition_rows(const Coo<T> &g, int32_t numProcesses, int32_t part, Coo<T> &local);
+template <typename T>
+void partial_metadata(const Coo<T> &c, const HostLayout<T> &L, PartialMeta &m);
+
+// Halo copies (halo.cu): a fixed list of (src, dst, len) element segments
+// between two device buffers, copied by one kernel.
+struct Halo;
+Halo *halo_create(int32_t elemBytes, const int64_t *srcOff, const int64_t *dstOff, const int64_t *len,
+                  int32_t numSegments, int64_t srcLen, int64_t dstLen);
+void halo_copy(const Halo *h, const void *src, void *dst, void *stream);
+void halo_free(Halo *h);
+int64_t halo_elements(const Halo *h);
 
 // Converter: convertToHBDIAFormat restated for speed (OpenMP), bit-exact.
 template <typename T>
@@ -84,6 +114,7 @@ struct DevicePlan {
     int32_t dtype = HBDIA_F64;          // T of x, y and the COO values
     int32_t storage = HBDIA_STORE_NATIVE;
     int32_t n = 0, numCols = 0, bw = 0, numBlocks = 0, numTiles = 0;
+    int32_t xn = 0;  // DIA column bound: n, or a partial matrix's x-window length
     int64_t totalOffsets = 0, slots = 0, nCoo = 0;
     void *base = nullptr;
     size_t bytes = 0;
@@ -128,8 +159,14 @@ void build_chunk_schedule(int32_t n, int32_t numBlocks, int32_t numTiles, const 
 // kernel that launch_spmv would use for x (HBDIA_KERNEL_*)
 int32_t select_kernel(const DevicePlan &P, const void *x);
 
+// The x window of a partial matrix's plan: global column c is read at
+// x[c - lo], lo <= c < lo + len; the rank's rows start at global row rowBase.
+struct ColumnWindow {
+    int32_t lo = 0, len = 0, rowBase = 0;
+};
+
 template <typename T>
-void build_plan(const HostLayout<T> &L, int storage, DevicePlan &P);
+void build_plan(const HostLayout<T> &L, int storage, DevicePlan &P, const ColumnWindow *W = nullptr);
 void free_plan(DevicePlan &P);
 // y = A x on `stream` (a cudaStream_t; nullptr -> the plan's stream)
 void launch_spmv(const DevicePlan &P, const void *x, void *y, void *stream);

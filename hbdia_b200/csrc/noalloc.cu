@@ -77,6 +77,11 @@ extern "C" int hbdia_spmv_host_noalloc(hbdia_matrix *m, const void *xHost, void 
         int st = hbdia_matrix_get_info(m, &info);
         if (st != HBDIA_OK) return st;
         if (!info.hasHBDIA) return hbdia::record_error(HBDIA_ERR_NOT_CONVERTED, "matrix is not in HBDIA format");
+        hbdia_partial_info pinfo;
+        st = hbdia_matrix_partial_info(m, &pinfo);
+        if (st != HBDIA_OK) return st;
+        if (pinfo.isPartial)
+            return hbdia::record_error(HBDIA_ERR_UNSUPPORTED, "partial matrices use hbdia_spmv_host or _device");
         if (!info.onDevice)
             return hbdia::record_error(HBDIA_ERR_NOT_CONVERTED,
                                        "matrix has no device layout: call hbdia_matrix_prepare_gpu first "

@@ -62,7 +62,7 @@ void free_plan(DevicePlan &P) {
 }
 
 template <typename T>
-void build_plan(const HostLayout<T> &L, int storage, DevicePlan &P) {
+void build_plan(const HostLayout<T> &L, int storage, DevicePlan &P, const ColumnWindow *W) {
     DevicePlan Q;
     Q.kernel = P.kernel;  // settings survive a rebuild
     Q.waitTimeoutNs = P.waitTimeoutNs;
@@ -76,7 +76,8 @@ void build_plan(const HostLayout<T> &L, int storage, DevicePlan &P) {
         throw Error(HBDIA_ERR_INVALID_ARGUMENT, "unknown value storage");
     Q.storage = storage;
     Q.n = L.numRows;
-    Q.numCols = L.numCols;
+    Q.numCols = W ? W->len : L.numCols;
+    Q.xn = W ? W->len : L.numRows;
     Q.bw = L.blockWidth;
     Q.numBlocks = L.numBlocks;
     Q.numTiles = static_cast<int32_t>((static_cast<int64_t>(L.numRows) + 31) / 32);
@@ -90,6 +91,18 @@ void build_plan(const HostLayout<T> &L, int storage, DevicePlan &P) {
     const int32_t *cr = L.cooRow.data(), *cc = L.cooCol.data();
     const T *cv = L.cooVal.data();
     const int32_t *crp = L.cooRowPtr.data();
+    // a partial matrix's plan works in x-window coordinates: offsets become
+    // col - lo - localRow, COO columns col - lo
+    const int32_t *ko = L.offsets.data();
+    std::vector<int32_t> wOffs, wCols;
+    if (W) {
+        wOffs.resize(L.offsets.size());
+        for (size_t k = 0; k < wOffs.size(); ++k) wOffs[k] = L.offsets[k] + (W->rowBase - W->lo);
+        wCols.resize(L.cooCol.size());
+        for (size_t e = 0; e < wCols.size(); ++e) wCols[e] = L.cooCol[e] - W->lo;
+        ko = wOffs.data();
+        cc = wCols.data();
+    }
     std::vector<int32_t> sr, sc, srp;
     std::vector<T> sv;
     for (int64_t e = 0; e < Q.nCoo; ++e) {
@@ -121,9 +134,9 @@ void build_plan(const HostLayout<T> &L, int storage, DevicePlan &P) {
     // chunk schedule of the staged kernel (blockWidth 32)
     std::vector<int32_t> rec;
     std::vector<XWindow> win;
-    if (Q.bw == 32) {
+    if (Q.bw == 32 && !W) {  // (the schedule's x ranges assume x holds numRows entries)
         // x windows are prefetched into L2, not staged: no capacity limit
-        build_chunk_schedule(Q.n, Q.numBlocks, Q.numTiles, L.blockStart.data(), L.offsets.data(), tile.data(),
+        build_chunk_schedule(Q.n, Q.numBlocks, Q.numTiles, L.blockStart.data(), ko, tile.data(),
                              dev::kVRows, 1 << 30, static_cast<int>(sizeof(T)), rec, win);
         Q.numChunks = static_cast<int32_t>(rec.size() / kRecInts);
         Q.numWindows = static_cast<int64_t>(win.size());
@@ -195,7 +208,7 @@ void build_plan(const HostLayout<T> &L, int storage, DevicePlan &P) {
         };
         up(Q.vals, valSrc, Q.slots * vsz);
         if (Q.scale) up(Q.scale, sf.data(), Q.numBlocks * sizeof(float));
-        up(Q.offs, L.offsets.data(), Q.totalOffsets * sizeof(int32_t));
+        up(Q.offs, ko, Q.totalOffsets * sizeof(int32_t));
         up(Q.blkOff, L.blockStart.data(), (static_cast<size_t>(Q.numBlocks) + 1) * sizeof(int32_t));
         up(Q.cooRow, cr, Q.nCoo * sizeof(int32_t));
         up(Q.cooCol, cc, Q.nCoo * sizeof(int32_t));
@@ -225,8 +238,8 @@ void build_plan(const HostLayout<T> &L, int storage, DevicePlan &P) {
     P = Q;
 }
 
-template void build_plan<double>(const HostLayout<double> &, int, DevicePlan &);
-template void build_plan<float>(const HostLayout<float> &, int, DevicePlan &);
+template void build_plan<double>(const HostLayout<double> &, int, DevicePlan &, const ColumnWindow *);
+template void build_plan<float>(const HostLayout<float> &, int, DevicePlan &, const ColumnWindow *);
 
 namespace {
 

@@ -62,7 +62,7 @@ __device__ __forceinline__ void spmm_group(const SpmvArgs<VT, XT> &a, const XT *
 #pragma unroll
     for (int u = 0; u < U; ++u) {
         const int64_t col = row + __shfl_sync(kFull, myoff, j + u);
-        ok[u] = static_cast<uint64_t>(col) < static_cast<uint64_t>(a.n);
+        ok[u] = static_cast<uint64_t>(col) < static_cast<uint64_t>(a.xn);
         v[u] = __ldg(vp + (j + u) * 32);
         const IT c = ok[u] ? static_cast<IT>(col) : IT(0);
         if (CM) {
@@ -212,7 +212,7 @@ spmm_rowwise(const SpmvArgs<VT, XT> a, const XT *__restrict__ X, int64_t ldx, XT
         for (int32_t kk = k0; kk < k1; ++kk) {
             const XT vv = widen<XT>(__ldg(a.vals + static_cast<int64_t>(kk) * a.bw + lane), s);
             const int64_t col = row + __ldg(a.offs + kk);
-            if (vv == XT(0) || col < 0 || col >= a.n) continue;
+            if (vv == XT(0) || col < 0 || col >= a.xn) continue;
 #pragma unroll
             for (int q = 0; q < KT; ++q)
                 if (q < kc) acc[q] = fma_rn(vv, __ldg(X + blk<CM>(col, r0 + q, ldx)), acc[q]);

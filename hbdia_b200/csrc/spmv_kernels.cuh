@@ -40,6 +40,8 @@ struct SpmvArgs {
     const int32_t *cooRowPtr;  // numRows + 1 (row-per-thread kernel)
     const int32_t *cooTile;    // numTiles + 1 (warp kernels): COO range of each 32-row tile
     int32_t n;               // numRows
+    int32_t xn;              // DIA column bound: numRows (the reference's col < numRows),
+                             // or the x-window length of a partial matrix
     int32_t bw;              // blockWidth
     int32_t numBlocks;       // DIA blocks
     int32_t numTiles;        // ceil(n / 32)
@@ -89,7 +91,7 @@ spmv_rowwise(const SpmvArgs<VT, XT> a, const XT *__restrict__ x, XT *__restrict_
             const XT v = widen<XT>(ld_stream(a.vals + static_cast<int64_t>(k) * a.bw + lane), s);
             if (v == XT(0)) continue;
             const int64_t col = row + __ldg(a.offs + k);
-            if (col < 0 || col >= a.n) continue;
+            if (col < 0 || col >= a.xn) continue;
             sum = fma_rn(v, __ldg(x + col), sum);
         }
     }
@@ -162,7 +164,7 @@ __device__ __forceinline__ void bw32_tile(const SpmvArgs<VT, XT> &a, const XT *_
 #pragma unroll
                 for (int u = 0; u < U; ++u) {
                     col[u] = row + __shfl_sync(kFull, myoff, j + u);
-                    ok[u] = static_cast<uint64_t>(col[u]) < static_cast<uint64_t>(a.n);
+                    ok[u] = static_cast<uint64_t>(col[u]) < static_cast<uint64_t>(a.xn);
                     v[u] = ld_stream(vp + static_cast<int64_t>(j + u) * 32);
                     xv[u] = XT(0);
                 }
@@ -178,7 +180,7 @@ __device__ __forceinline__ void bw32_tile(const SpmvArgs<VT, XT> &a, const XT *_
             for (; j < cnt; ++j) {  // warp-uniform tail
                 const int64_t col = row + __shfl_sync(kFull, myoff, j);
                 const XT vv = widen<XT>(ld_stream(vp + static_cast<int64_t>(j) * 32), s);
-                if (static_cast<uint64_t>(col) < static_cast<uint64_t>(a.n) && vv != XT(0))
+                if (static_cast<uint64_t>(col) < static_cast<uint64_t>(a.xn) && vv != XT(0))
                     sum = fma_rn(vv, __ldg(x + col), sum);
             }
         }
@@ -232,7 +234,7 @@ spmv_bw32_pipe(const SpmvArgs<VT, XT> a, const XT *__restrict__ x, XT *__restric
     const int32_t W = static_cast<int32_t>((static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5);
     int32_t t = static_cast<int32_t>((static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5);
     if (t >= a.numTiles) return;  // warp-uniform
-    const uint32_t n = static_cast<uint32_t>(a.n);
+    const uint32_t n = static_cast<uint32_t>(a.xn);  // column bound
     TileMeta m = load_meta(a, t);
     int32_t offNext = (lane < m.k1 - m.k0) ? __ldg(a.offs + m.k0 + lane) : 0;
     while (t < a.numTiles) {

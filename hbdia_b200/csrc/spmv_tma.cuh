@@ -176,7 +176,7 @@ __device__ __forceinline__ XT tile_direct(const SpmvArgs<VT, XT> &a, int32_t til
         for (int32_t k = k0; k < k1; ++k) {
             const XT v = widen<XT>(ld_stream(a.vals + static_cast<int64_t>(k) * 32 + lane), s);
             const int64_t col = row + __ldg(a.offs + k);
-            if (v != XT(0) && col >= 0 && col < a.n) sum = fma_rn(v, __ldg(x + col), sum);
+            if (v != XT(0) && col >= 0 && col < a.xn) sum = fma_rn(v, __ldg(x + col), sum);
         }
     }
     if (a.hasCoo) {
@@ -203,7 +203,7 @@ __device__ __forceinline__ XT tile_staged(const SpmvArgs<VT, XT> &a, const Stage
     const int32_t *offs = S.offs + (kt0 - (k0c & ~3));
     const VT *vrow = S.vals + (kt0 - k0c) * 32 + lane;
     const int cnt = kt1 - kt0;
-    const uint32_t n = static_cast<uint32_t>(a.n);
+    const uint32_t n = static_cast<uint32_t>(a.xn);  // column bound
     XT sum = XT(0);
     int j = 0;
     // full groups of U offsets: U independent x loads in flight, then the

@@ -533,6 +533,79 @@ int hbdia_generate_stencil27_spd(int32_t nx, int32_t ny, int32_t nz, double shif
 /* n doubles uniform in [lo, hi) from the library's seeded generator. */
 int hbdia_fill_uniform(double *out, int64_t n, double lo, double hi, uint64_t seed);
 
+/* ---- Row-partitioned distribution (one rank per GPU) -------------------
+ *
+ * A partial matrix holds one rank's contiguous rows of a square matrix: local
+ * row indices, GLOBAL column indices, offsets col - globalRow.  After
+ * hbdia_matrix_convert it also holds the reference's partial-matrix metadata
+ * (the x ranges it reads and which rank owns each), and its device plan reads
+ * x through a dense window of global columns [windowStart, windowStart +
+ * windowLength): x_window[c - windowStart] = x[c].  The window holds the
+ * rank's own x entries at [globalRowStart - windowStart, ... + numRows) and
+ * the other ranks' entries at their data ranges; hbdia_spmv_device(m, x_window,
+ * y_local, stream) then computes the rank's rows of y. */
+
+/* HBDIA<T>(rows, cols, vals, numRows, numCols, globalRowMapping, partialMatrix=true,
+ * numGlobalRows, numGlobalCols, numGlobalNonZeros, rank, size)
+ * (src/Format/HBDIA.cpp:118-154) with the contiguous mapping global row =
+ * globalRowStart + local row (the mapping BasicExtractor builds).  rows are
+ * local (< numLocalRows), cols global (< numGlobalCols); the matrix must be
+ * square (numGlobalRows == numGlobalCols) and globalRowStart + numLocalRows
+ * <= numGlobalRows. */
+int hbdia_matrix_create_partial(hbdia_dtype dtype, const int32_t *rows, const int32_t *cols,
+                                const void *values, int64_t nnz, int32_t numLocalRows,
+                                int32_t numGlobalRows, int32_t numGlobalCols, int64_t numGlobalNonZeros,
+                                int32_t globalRowStart, int32_t rank, int32_t size, hbdia_matrix **out);
+
+/* BasicExtractor::createMatrixPartitions + partitionRowWise
+ * (src/DataExchange/BasicExtractor.cpp:16-45, 124-234) for one partition:
+ * rows [part * (n / numProcesses), ...), the last partition taking n %
+ * numProcesses more, entries in input order.  The result is a partial matrix
+ * (rank = part, size = numProcesses).  Needs a square matrix with entries and
+ * numProcesses <= numRows. */
+int hbdia_matrix_partition(const hbdia_matrix *global, int32_t numProcesses, int32_t part, hbdia_matrix **out);
+
+typedef struct hbdia_partial_info {
+    int32_t isPartial;          /* isPartialMatrix (include/Format/HBDIA.hpp:126)        */
+    int32_t hasMetadata;        /* metadata computed (after conversion)                  */
+    int32_t globalRowStart;     /* getGlobalRowIndex(0)                                  */
+    int32_t numGlobalRows;      /* getNumGlobalRows                                      */
+    int32_t numGlobalCols;      /* getNumGlobalCols                                      */
+    int32_t rank, size;
+    int64_t numGlobalNonZeros;  /* getNumGlobalNonZeros                                  */
+    int64_t numDataRanges;      /* getDataRanges().size() (analyzeDataRanges)           */
+    int64_t numProcessRanges;   /* segments of processDataRanges, all processes          */
+    int64_t totalBufferSize;    /* PartialMatrixMetadata::totalBufferSize                */
+    int64_t leftBufferSize;     /* HBDIAVector(localData, matrix, rank, size) receive    */
+    int64_t rightBufferSize;    /*   buffers (src/Format/HBDIAVector.cpp:39-66)          */
+    int32_t windowStart;        /* this library's x window                              */
+    int32_t windowLength;
+} hbdia_partial_info;
+int hbdia_matrix_partial_info(const hbdia_matrix *m, hbdia_partial_info *info);
+
+/* dataRanges: numDataRanges pairs [start, end) -- HBDIA::analyzeDataRanges
+ * (src/Format/HBDIA.cpp:1333-1414); processRanges: numProcessRanges triples
+ * (process, start, end) -- BasicExtractor::extractPartialMatrixMetadataRowWise
+ * (src/DataExchange/BasicExtractor.cpp:269-333), grouped by process in the
+ * reference's order.  Either pointer may be NULL. */
+int hbdia_matrix_export_ranges(const hbdia_matrix *m, int32_t *dataRanges, int32_t *processRanges);
+
+/* Halo copy plan: numSegments element segments (src[srcOffset .. +length) ->
+ * dst[dstOffset .. +length)) between a source buffer of srcLength and a
+ * destination of dstLength elements of elemBytes (4 or 8), validated and
+ * uploaded once.  hbdia_halo_copy runs them as one kernel on the stream:
+ * allocation-free, graph-capturable.  It replaces the per-range packing of
+ * MPICommunicator::exchangeData (src/DataExchange/MPICommunicator.cpp:253-412):
+ * the ranges a peer requested are packed into one send buffer, and the
+ * received buffer is unpacked into the x window. */
+typedef struct hbdia_halo hbdia_halo;
+int hbdia_halo_create(int32_t elemBytes, const int64_t *srcOffset, const int64_t *dstOffset,
+                      const int64_t *length, int32_t numSegments, int64_t srcLength, int64_t dstLength,
+                      hbdia_halo **out);
+int hbdia_halo_copy(const hbdia_halo *h, const void *src, void *dst, void *stream);
+int64_t hbdia_halo_elements(const hbdia_halo *h);
+void hbdia_halo_destroy(hbdia_halo *h);
+
 #ifdef __cplusplus
 }
 #endif

@@ -103,6 +103,11 @@ class Restated:
                                     ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                     ctypes.c_int64, ctypes.POINTER(_vp)]
         lib.orc_convert.restype = ctypes.c_int
+        lib.orc_convert_partial.argtypes = [_vp, _vp, _vp, ctypes.c_int, ctypes.c_int64, ctypes.c_int32,
+                                            ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                            ctypes.c_int64, ctypes.POINTER(_vp)]
+        lib.orc_convert_partial.restype = ctypes.c_int
+        lib.orc_spmv_partial_f64.argtypes = [_vp, ctypes.c_int32, _vp, _vp]
         lib.orc_sizes.argtypes = [_vp, _i64p]
         lib.orc_export.argtypes = [_vp] * 10
         lib.orc_destroy.argtypes = [_vp]
@@ -125,6 +130,25 @@ class Restated:
                 self.lib.orc_destroy(h)
             raise RuntimeError(f"orc_convert failed with {rc}")
         return _OracleMatrix(self, h, vals.dtype)
+
+    def convert_partial(self, rows, cols, vals, num_rows, num_cols, row_base, bw=32, thr=1,
+                        max_coo=1_000_000_000):
+        """A partial matrix (local rows, global columns, global row = row_base +
+        local row) converted as the reference's partial-matrix constructor
+        does (offsets col - globalRow)."""
+        rows = np.ascontiguousarray(rows, np.int32)
+        cols = np.ascontiguousarray(cols, np.int32)
+        vals = np.ascontiguousarray(vals, np.float64)
+        h = _vp()
+        rc = self.lib.orc_convert_partial(_ptr(rows), _ptr(cols), _ptr(vals), 0, len(vals), num_rows, num_cols,
+                                          row_base, bw, thr, max_coo, ctypes.byref(h))
+        if rc != 0:
+            if h:
+                self.lib.orc_destroy(h)
+            raise RuntimeError(f"orc_convert_partial failed with {rc}")
+        m = _OracleMatrix(self, h, np.float64)
+        m.num_rows = num_rows
+        return m
 
     def coo_spmv(self, rows, cols, vals, x, num_rows, y=None):
         y = np.zeros(num_rows, np.float64) if y is None else y
@@ -155,6 +179,13 @@ class _OracleMatrix:
         y = np.zeros_like(x)
         f = self._o.lib.orc_spmv_f32 if self.dtype == np.float32 else self._o.lib.orc_spmv_f64
         f(self._h, _ptr(x), _ptr(y))
+        return y
+
+    def spmv_partial(self, x_global: np.ndarray) -> np.ndarray:
+        """A partial matrix's rows of y over the global x."""
+        x = np.ascontiguousarray(x_global, np.float64)
+        y = np.zeros(self.num_rows, np.float64)
+        self._o.lib.orc_spmv_partial_f64(self._h, len(x), _ptr(x), _ptr(y))
         return y
 
     def spmv_with_values(self, values: np.ndarray, x: np.ndarray) -> np.ndarray:
@@ -211,6 +242,13 @@ class Reference:
         lib.ref_matrix_convert_dia_f64.argtypes = [_vp, ctypes.c_int]
         lib.ref_matrix_dia_sizes_f64.argtypes = [_vp, _vp]
         lib.ref_matrix_export_dia_f64.argtypes = [_vp] * 6
+        lib.ref_partition_f64.argtypes = [_vp, _vp, _vp, ctypes.c_int64] + [ctypes.c_int] * 5
+        lib.ref_partition_f64.restype = _vp
+        lib.ref_partition_sizes.argtypes = [_vp, _i64p]
+        lib.ref_partition_export.argtypes = [_vp] * 6
+        lib.ref_partition_matrix.argtypes = [_vp]
+        lib.ref_partition_matrix.restype = _vp
+        lib.ref_partition_destroy.argtypes = [_vp]
         lib.ref_coo_sizes_f64.argtypes = [_vp, _i64p]
         lib.ref_coo_export_f64.argtypes = [_vp, _vp, _vp, _vp]
         lib.ref_stencil27_f64.argtypes = [ctypes.c_int] * 3 + [ctypes.c_double, ctypes.c_int]
@@ -277,6 +315,40 @@ class Reference:
             return _to_layout(a)
         finally:
             getattr(self.lib, f"ref_matrix_destroy_{t}")(h)
+
+    def partition(self, rows, cols, vals, n, num_processes, part, bw=32, thr=1) -> dict:
+        """One rank's side of BasicDistributor::scatterMatrix / receiveMatrix
+        run on the reference's own code: its partition (local COO, first
+        global row), the partial matrix's HBDIA layout, dataRanges,
+        processDataRanges (triples process, start, end) and totalBufferSize."""
+        rows = np.ascontiguousarray(rows, np.int32)
+        cols = np.ascontiguousarray(cols, np.int32)
+        vals = np.ascontiguousarray(vals, np.float64)
+        h = self.lib.ref_partition_f64(_ptr(rows), _ptr(cols), _ptr(vals), len(vals), n, num_processes, part,
+                                       bw, thr)
+        if not h:
+            raise ValueError("reference partitioning failed")
+        try:
+            s = np.zeros(6, np.int64)
+            self.lib.ref_partition_sizes(h, s.ctypes.data_as(_i64p))
+            nnz, nd, npr = int(s[2]), int(s[3]), int(s[4])
+            r, c, v = np.zeros(nnz, np.int32), np.zeros(nnz, np.int32), np.zeros(nnz, np.float64)
+            data = np.zeros((nd, 2), np.int32)
+            proc = np.zeros((npr, 3), np.int32)
+            self.lib.ref_partition_export(h, _ptr(r), _ptr(c), _ptr(v), _ptr(data), _ptr(proc))
+            m = self.lib.ref_partition_matrix(h)
+            sizes = np.zeros(10, np.int64)
+            self.lib.ref_matrix_sizes_f64(m, sizes.ctypes.data_as(_i64p))
+            a = _alloc_layout(sizes, np.float64)
+            if a["has"]:
+                self.lib.ref_matrix_export_f64(m, *[_ptr(a[k]) for k in (
+                    "offsets", "block_start", "data", "coo_row", "coo_col", "coo_val", "coo_row_ptr",
+                    "hist_blocks", "hist_nnz")])
+            return {"row_start": int(s[0]), "num_local_rows": int(s[1]), "rows": r, "cols": c, "vals": v,
+                    "data_ranges": data, "process_ranges": proc, "total_buffer_size": int(s[5]),
+                    "layout": _to_layout(a)}
+        finally:
+            self.lib.ref_partition_destroy(h)
 
     def _export_coo(self, h):
         s = np.zeros(3, np.int64)

@@ -14,6 +14,7 @@
 
 struct orc_layout {
     int32_t numRows, numCols, bw, threshold;
+    int32_t rowBase;         /* partial matrix: global row of local row 0 */
     int64_t maxCoo;
     int is_f32;
     int has_hbdia;
@@ -52,12 +53,21 @@ static int64_t find_offset(const int32_t *list, int64_t n, int32_t key) {
 int orc_convert(const int32_t *rows, const int32_t *cols, const void *vals, int is_f32,
                 int64_t nnz, int32_t numRows, int32_t numCols, int32_t bw, int32_t threshold,
                 int64_t maxCoo, orc_layout **out) {
-    if (!out || bw <= 0 || numRows <= 0 || numCols <= 0 || nnz < 0) return -1;
+    return orc_convert_partial(rows, cols, vals, is_f32, nnz, numRows, numCols, 0, bw, threshold, maxCoo, out);
+}
+
+/* The partial-matrix form: offsets are col - (row + rowBase), the global row
+ * taken from a contiguous global row mapping (src/Format/HBDIA.cpp:546-552,
+ * 646-657); blocks, lanes and the COO remainder use local rows. */
+int orc_convert_partial(const int32_t *rows, const int32_t *cols, const void *vals, int is_f32,
+                        int64_t nnz, int32_t numRows, int32_t numCols, int32_t rowBase, int32_t bw,
+                        int32_t threshold, int64_t maxCoo, orc_layout **out) {
+    if (!out || bw <= 0 || numRows <= 0 || numCols <= 0 || nnz < 0 || rowBase < 0) return -1;
     orc_layout *h = (orc_layout *)calloc(1, sizeof(orc_layout));
     if (!h) return -1;
     const size_t esz = is_f32 ? sizeof(float) : sizeof(double);
     h->numRows = numRows; h->numCols = numCols; h->bw = bw; h->threshold = threshold;
-    h->maxCoo = maxCoo; h->is_f32 = is_f32;
+    h->maxCoo = maxCoo; h->is_f32 = is_f32; h->rowBase = rowBase;
     *out = h;
     /* Empty matrix: the reference returns without converting
      * (src/Format/HBDIA.cpp:521-524). */
@@ -82,7 +92,7 @@ int orc_convert(const int32_t *rows, const int32_t *cols, const void *vals, int 
     for (int32_t b = 0; b < nb; ++b) fillp[b] = bcount[b];
     for (int64_t i = 0; i < nnz; ++i) {
         int32_t b = rows[i] / bw;
-        if (b < nb) boffs[fillp[b]++] = cols[i] - rows[i];
+        if (b < nb) boffs[fillp[b]++] = cols[i] - rows[i] - rowBase;
     }
     free(fillp);
     /* distinct (offset,count) per block, in place: uniq[] holds offsets,
@@ -173,7 +183,7 @@ int orc_convert(const int32_t *rows, const int32_t *cols, const void *vals, int 
     int64_t nextOffset = 0;
     for (int64_t i = 0; i < nnz; ++i) {
         const int32_t r = rows[i], c = cols[i];
-        const int32_t b = r / bw, off = c - r, lane = r % bw;
+        const int32_t b = r / bw, off = c - r - rowBase, lane = r % bw;
         int64_t idx = -1;
         if (b < nb && h->blockStart[b + 1] > h->blockStart[b])
             idx = find_offset(h->offsets + h->blockStart[b],
@@ -274,6 +284,40 @@ void orc_spmv_f64_values(const orc_layout *h, const double *values, double *y, c
     orc_layout g = *h;
     g.data = (void *)values;
     orc_spmv_f64(&g, x, y);
+}
+
+/* A partial matrix's rows of y = A x over the GLOBAL x: the blocked-DIA
+ * column of local row r at offset o is rowBase + r + o, skipped outside
+ * [0, numGlobalCols); COO columns are global.  The operation order is
+ * orc_spmv_f64's (src/Operations/HBDIASpMV.cu:22-71, HBDIASpMV.cpp:76-92,
+ * HBDIASpMV.cu:77-88) -- the reference's kernel itself reads x at
+ * localRow + offset (HBDIASpMV.cu:53-58), so for partial matrices this is the
+ * arithmetic its distributed SpMV intends rather than what that kernel
+ * computes. */
+void orc_spmv_partial_f64(const orc_layout *h, int32_t numGlobalCols, const double *x, double *y) {
+    const int32_t n = h->numRows, bw = h->bw;
+    const double *data = (const double *)h->data;
+    const double *cv = (const double *)h->cooVal;
+    double *coo = (double *)calloc((size_t)n + 1, sizeof(double));
+    for (int64_t e = 0; e < h->nCoo; ++e) {
+        double p = cv[e] * x[h->cooCol[e]];
+        coo[h->cooRow[e]] = coo[h->cooRow[e]] + p;
+    }
+    for (int32_t row = 0; row < n; ++row) {
+        double sum = 0.0;
+        const int32_t b = row / bw, lane = row % bw;
+        if (h->has_hbdia && b < h->numBlocks) {
+            for (int32_t k = h->blockStart[b]; k < h->blockStart[b + 1]; ++k) {
+                double v = data[(int64_t)k * bw + lane];
+                if (v == 0.0) continue;
+                int64_t col = (int64_t)h->rowBase + row + h->offsets[k];
+                if (col < 0 || col >= numGlobalCols) continue;
+                sum = fma(v, x[col], sum);
+            }
+        }
+        y[row] = (h->nCoo > 0) ? sum + coo[row] : sum;
+    }
+    free(coo);
 }
 
 void orc_coo_spmv_f64(const int32_t *rows, const int32_t *cols, const double *vals,

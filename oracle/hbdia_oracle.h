@@ -27,6 +27,10 @@ enum { ORC_NSIZES = 10 };
 int orc_convert(const int32_t *rows, const int32_t *cols, const void *vals, int is_f32,
                 int64_t nnz, int32_t numRows, int32_t numCols, int32_t blockWidth,
                 int32_t threshold, int64_t maxCooEntries, orc_layout **out);
+/* The partial-matrix form: offsets col - (row + rowBase). */
+int orc_convert_partial(const int32_t *rows, const int32_t *cols, const void *vals, int is_f32,
+                        int64_t nnz, int32_t numRows, int32_t numCols, int32_t rowBase, int32_t blockWidth,
+                        int32_t threshold, int64_t maxCooEntries, orc_layout **out);
 void orc_sizes(const orc_layout *h, int64_t *sizes);
 void orc_export(const orc_layout *h, int32_t *offsets, int32_t *blockStart, void *data,
                 int32_t *cooRow, int32_t *cooCol, void *cooVal, int32_t *cooRowPtr,
@@ -38,6 +42,8 @@ void orc_destroy(orc_layout *h);
  * (src/Operations/HBDIASpMV.cu:77-88).  x and y hold numRows elements. */
 void orc_spmv_f64(const orc_layout *h, const double *x, double *y);
 void orc_spmv_f32(const orc_layout *h, const float *x, float *y);
+/* A partial matrix's rows of y over the global x (numGlobalCols elements). */
+void orc_spmv_partial_f64(const orc_layout *h, int32_t numGlobalCols, const double *x, double *y);
 /* orc_spmv_f64 with the blocked-DIA values taken from `values` instead. */
 void orc_spmv_f64_values(const orc_layout *h, const double *values, double *y, const double *x);
 

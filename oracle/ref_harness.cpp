@@ -4,7 +4,8 @@
 // reference's unmodified sources (src/Format/HBDIA.cpp, HBDIAPrinter.cpp,
 // HBDIAVector.cpp, src/Operations/HBDIASpMV.cu) into oracle/_ref/libhbdia_ref.so.
 // It includes src/Operations/HBDIASpMV.cpp so that the file-local template
-// cpu_coo_spmv_kernel (src/Operations/HBDIASpMV.cpp:36-99) is reachable.
+// cpu_coo_spmv_kernel (src/Operations/HBDIASpMV.cpp:36-99) is reachable, and
+// links src/DataExchange/BasicExtractor.cpp for the row partitioning.
 //
 // Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline / reference
 // arm load this library, and only as the checker or the timed CPU baseline.
@@ -19,6 +20,7 @@
 // empty), so the layout can be produced on a host without a GPU.
 
 #include "src/Operations/HBDIASpMV.cpp"
+#include "include/DataExchange/BasicExtractor.hpp"
 
 #include <cstring>
 #include <cstdint>
@@ -260,6 +262,94 @@ int ref_gpu_spmv_f64(const int *rows, const int *cols, const double *vals, int64
         std::fprintf(stderr, "oracle: reference hbdiaSpMV threw: %s\n", e.what());
         return -1;
     }
+}
+
+// ---- row partitioning, as BasicDistributor::scatterMatrix / receiveMatrix do
+// it for one rank (src/DataExchange/BasicDistributor.cpp:17-146): the
+// extractor's partition, the partial-matrix constructor, convertToHBDIAFormat,
+// analyzeDataRanges and extractPartialMatrixMetadata -- all host code.
+struct RefPartition {
+    HBDIA<double> *m = nullptr;
+    std::vector<int> rows, cols;
+    std::vector<double> vals;
+    int rowStart = 0, numLocalRows = 0;
+    std::vector<std::tuple<int, int>> data;
+    std::vector<std::vector<std::tuple<int, int>>> proc;
+    int total = 0;
+};
+
+void *ref_partition_f64(const int *rows, const int *cols, const double *vals, int64_t nnz, int n, int P,
+                        int part, int bw, int thr) {
+    try {
+        HBDIA<double> g(std::vector<int>(rows, rows + nnz), std::vector<int>(cols, cols + nnz),
+                        std::vector<double>(vals, vals + nnz), n, n);
+        BasicExtractor<double> ex;
+        if (!ex.createMatrixPartitions(g, P)) return nullptr;
+        const auto &pt = ex.getPartitions()[part];
+        const auto &md = ex.getMatrixData()[part];
+        auto *h = new RefPartition();
+        h->rows = pt.localRowIndices;
+        h->cols = pt.localColIndices;
+        h->vals = pt.localValues;
+        h->rowStart = pt.globalRowMapping.empty() ? 0 : pt.globalRowMapping[0];
+        h->numLocalRows = md.numLocalRows;
+        h->m = new HBDIA<double>(pt.localRowIndices, pt.localColIndices, pt.localValues, md.numLocalRows,
+                                 md.numLocalCols, pt.globalRowMapping, true, md.numGlobalRows, md.numGlobalCols,
+                                 md.numGlobalNonZeros, part, P);
+        h->m->convertToHBDIAFormat(bw, thr);
+        h->m->analyzeDataRanges();
+        ex.extractPartialMatrixMetadata(*h->m, P);
+        const auto &meta = h->m->getPartialMatrixMetadata();
+        h->data = meta.dataRanges;
+        h->proc = meta.processDataRanges;
+        h->total = meta.totalBufferSize;
+        return h;
+    } catch (const std::exception &e) {
+        std::fprintf(stderr, "oracle: reference partitioning threw: %s\n", e.what());
+        return nullptr;
+    }
+}
+
+// out: rowStart, numLocalRows, local nnz, #data ranges, #process segments, totalBufferSize
+void ref_partition_sizes(void *hp, int64_t *out) {
+    auto *h = static_cast<RefPartition *>(hp);
+    int64_t segs = 0;
+    for (const auto &v : h->proc) segs += static_cast<int64_t>(v.size());
+    out[0] = h->rowStart;
+    out[1] = h->numLocalRows;
+    out[2] = static_cast<int64_t>(h->vals.size());
+    out[3] = static_cast<int64_t>(h->data.size());
+    out[4] = segs;
+    out[5] = h->total;
+}
+
+void ref_partition_export(void *hp, int *rows, int *cols, double *vals, int *data, int *proc) {
+    auto *h = static_cast<RefPartition *>(hp);
+    if (!h->vals.empty()) {
+        std::memcpy(rows, h->rows.data(), h->rows.size() * sizeof(int));
+        std::memcpy(cols, h->cols.data(), h->cols.size() * sizeof(int));
+        std::memcpy(vals, h->vals.data(), h->vals.size() * sizeof(double));
+    }
+    for (size_t i = 0; i < h->data.size(); ++i) {
+        data[2 * i] = std::get<0>(h->data[i]);
+        data[2 * i + 1] = std::get<1>(h->data[i]);
+    }
+    size_t k = 0;
+    for (size_t p = 0; p < h->proc.size(); ++p)
+        for (const auto &t : h->proc[p]) {
+            proc[3 * k] = static_cast<int>(p);
+            proc[3 * k + 1] = std::get<0>(t);
+            proc[3 * k + 2] = std::get<1>(t);
+            ++k;
+        }
+}
+
+void *ref_partition_matrix(void *hp) { return static_cast<RefPartition *>(hp)->m; }
+
+void ref_partition_destroy(void *hp) {
+    auto *h = static_cast<RefPartition *>(hp);
+    delete h->m;
+    delete h;
 }
 
 }  // extern "C"
