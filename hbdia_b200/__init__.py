@@ -487,6 +487,18 @@ def spmm_device_colmajor(matrix: HBDIA, X_ptr: int, ldx: int, Y_ptr: int, ldy: i
                                               ldy, k, _stream_arg(stream)))
 
 
+def spmv_list_device(matrix: HBDIA, x_ptrs: Sequence[int], y_ptrs: Sequence[int],
+                     stream: Optional[int] = None) -> None:
+    """y_j = A x_j for separate device vectors, each stored value read once per
+    32 vectors; y_j equals spmv_device(matrix, x_j, y_j) bit for bit."""
+    k = len(x_ptrs)
+    if len(y_ptrs) != k:
+        raise ValueError("x and y lists differ in length")
+    xa = (ctypes.c_void_p * max(k, 1))(*x_ptrs)
+    ya = (ctypes.c_void_p * max(k, 1))(*y_ptrs)
+    _check(_load().hbdia_spmv_list_device(matrix.handle, xa, ya, k, _stream_arg(stream)))
+
+
 def spmv_host(matrix: HBDIA, x: np.ndarray, y: np.ndarray) -> None:
     """End-to-end y = A x on host arrays (copies in, SpMV, copies out, sync)."""
     _check(_load().hbdia_spmv_host(matrix.handle, ctypes.c_void_p(x.ctypes.data), ctypes.c_void_p(y.ctypes.data)))
@@ -669,6 +681,18 @@ class Server:
             raise ValueError("request vectors must be contiguous float64 arrays")
         t = ctypes.c_uint64(0)
         _check(_load().hbdia_server_submit(self.handle, matrix_id, kind, _vp(x), _vp(y), ctypes.byref(t)))
+        self._live[t.value] = (x, y)
+        return t.value
+
+    def submit_device(self, matrix_id: int, kind: int, x, y) -> int:
+        """The same request on CUDA tensors (float64, contiguous), read and
+        written in place; keep them untouched until wait(ticket) returns."""
+        for t in (x, y):
+            if not t.is_cuda or str(t.dtype) != "torch.float64" or not t.is_contiguous():
+                raise ValueError("device request vectors must be contiguous float64 CUDA tensors")
+        t = ctypes.c_uint64(0)
+        _check(_load().hbdia_server_submit_device(self.handle, matrix_id, kind, ctypes.c_void_p(x.data_ptr()),
+                                                  ctypes.c_void_p(y.data_ptr()), ctypes.byref(t)))
         self._live[t.value] = (x, y)
         return t.value
 

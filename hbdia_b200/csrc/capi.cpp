@@ -684,6 +684,14 @@ int hbdia_spmm_device_colmajor(const hbdia_matrix *m, const void *X, int64_t ldx
     });
 }
 
+int hbdia_spmv_list_device(const hbdia_matrix *m, const void *const *x, void *const *y, int32_t k, void *stream) {
+    return guarded([&] {
+        need(m != nullptr, HBDIA_ERR_INVALID_ARGUMENT, "null matrix");
+        need(m->plan.base != nullptr, HBDIA_ERR_NOT_CONVERTED, "matrix has no device layout");
+        hbdia::launch_spmv_list(m->plan, x, y, k, stream);
+    });
+}
+
 int hbdia_spmv_host(hbdia_matrix *m, const void *xh, void *yh) {
     return guarded([&] {
         need(m && xh && yh, HBDIA_ERR_INVALID_ARGUMENT, "null argument");
@@ -773,7 +781,15 @@ int hbdia_server_submit(hbdia_server *s, int32_t matrix, int32_t kind, const dou
                         uint64_t *ticket) {
     return guarded([&] {
         need(s && ticket, HBDIA_ERR_INVALID_ARGUMENT, "null argument");
-        *ticket = hbdia::server_submit(s->S, matrix, kind, x, y);
+        *ticket = hbdia::server_submit(s->S, matrix, kind, x, y, false);
+    });
+}
+
+int hbdia_server_submit_device(hbdia_server *s, int32_t matrix, int32_t kind, const double *xDevice, double *yDevice,
+                               uint64_t *ticket) {
+    return guarded([&] {
+        need(s && ticket, HBDIA_ERR_INVALID_ARGUMENT, "null argument");
+        *ticket = hbdia::server_submit(s->S, matrix, kind, xDevice, yDevice, true);
     });
 }
 

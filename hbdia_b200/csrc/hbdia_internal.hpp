@@ -177,6 +177,9 @@ void launch_spmm(const DevicePlan &P, const void *X, int64_t ldx, void *Y, int64
 void launch_spmm_tile(const DevicePlan &P, const void *X, int64_t ldx, void *Y, int64_t ldy, int32_t k,
                       int32_t tile, void *stream, bool colMajor = false);
 int32_t default_spmm_tile(int32_t k, bool colMajor = false);
+// k SpMVs of one matrix on separate device vectors (x[j] -> y[j]) as
+// vector-list SpMMs of up to 32 vectors per launch, bit-identical to k SpMVs.
+void launch_spmv_list(const DevicePlan &P, const void *const *x, void *const *y, int32_t k, void *stream);
 void autotune(DevicePlan &P, const void *X, int64_t ldx, void *Y, int64_t ldy, int32_t k, void *stream, bool force,
               int32_t *kernel, int32_t *unroll, int32_t *tile, int32_t *fromCache, float *ms);
 void autotune_clear_cache();
@@ -207,7 +210,7 @@ void server_default_options(hbdia_server_options *o);
 Server *server_create(const hbdia_server_options &o);
 void server_destroy(Server *S);
 int32_t server_add_matrix(Server *S, const hbdia_matrix *m);
-uint64_t server_submit(Server *S, int32_t matrix, int32_t kind, const double *x, double *y);
+uint64_t server_submit(Server *S, int32_t matrix, int32_t kind, const double *x, double *y, bool device);
 void server_wait(Server *S, uint64_t ticket, hbdia_request_info *info);
 void server_pause(Server *S, bool paused);
 void server_stats(Server *S, hbdia_server_stats *out);

@@ -435,6 +435,63 @@ void launch_spmm_tile(const DevicePlan &P, const void *X, int64_t ldx, void *Y, 
     else launch_spmm_typed<double, double>(P, X, ldx, Y, ldy, k, tile, colMajor, s);
 }
 
+namespace {
+
+template <typename VT, typename XT, int KT>
+void launch_list_kt(const DevicePlan &P, const dev::SpmvArgs<VT, XT> &a, const void *const *x, void *const *y,
+                    int32_t k, cudaStream_t s) {
+    // full passes in one launch, a partial last pass in a second
+    const unsigned grid = static_cast<unsigned>((static_cast<int64_t>(P.numTiles) + 7) / 8);
+    const int32_t kfull = k - k % KT, krest = k % KT;
+    auto fill = [&](int32_t j0, int32_t cnt) {
+        dev::VecList<XT> L{};
+        for (int32_t j = 0; j < cnt; ++j) {
+            L.x[j] = static_cast<const XT *>(x[j0 + j]);
+            L.y[j] = static_cast<XT *>(y[j0 + j]);
+        }
+        return L;
+    };
+    if (kfull) dev::spmm_bw32_list<VT, XT, KT, true><<<grid, 256, 0, s>>>(a, fill(0, kfull), kfull);
+    if (krest) dev::spmm_bw32_list<VT, XT, KT, false><<<grid, 256, 0, s>>>(a, fill(kfull, krest), krest);
+}
+
+template <typename VT, typename XT>
+void launch_list_typed(const DevicePlan &P, const void *const *x, void *const *y, int32_t k, int32_t tile,
+                       cudaStream_t s) {
+    const dev::SpmvArgs<VT, XT> a = make_args<VT, XT>(P);
+    switch (tile) {
+        case 2: launch_list_kt<VT, XT, 2>(P, a, x, y, k, s); break;
+        case 4: launch_list_kt<VT, XT, 4>(P, a, x, y, k, s); break;
+        case 8: launch_list_kt<VT, XT, 8>(P, a, x, y, k, s); break;
+        case 16: launch_list_kt<VT, XT, 16>(P, a, x, y, k, s); break;
+        default: launch_list_kt<VT, XT, 32>(P, a, x, y, k, s); break;
+    }
+    check_cuda(cudaGetLastError(), "SpMV list launch");
+}
+
+}  // namespace
+
+void launch_spmv_list(const DevicePlan &P, const void *const *x, void *const *y, int32_t k, void *stream) {
+    if (!P.base) throw Error(HBDIA_ERR_NOT_CONVERTED, "matrix has no device layout");
+    if (k < 0 || (k > 0 && (!x || !y))) throw Error(HBDIA_ERR_INVALID_ARGUMENT, "bad vector list");
+    for (int32_t j = 0; j < k; ++j)
+        if (!x[j] || !y[j]) throw Error(HBDIA_ERR_INVALID_ARGUMENT, "null vector in the list");
+    cudaStream_t s = static_cast<cudaStream_t>(stream ? stream : P.stream);
+    if (P.bw != 32) {  // one SpMV per vector (column j of an SpMM is that SpMV)
+        for (int32_t j = 0; j < k; ++j) launch_spmv(P, x[j], y[j], s);
+        return;
+    }
+    for (int32_t j0 = 0; j0 < k; j0 += dev::kVecListMax) {
+        const int32_t kk = std::min<int32_t>(dev::kVecListMax, k - j0);
+        const int32_t tile = P.spmmTileForced ? P.spmmTileForced : default_spmm_tile(kk, true);
+        if (P.dtype == HBDIA_F32) launch_list_typed<float, float>(P, x + j0, y + j0, kk, tile, s);
+        else if (P.storage == HBDIA_STORE_F32) launch_list_typed<float, double>(P, x + j0, y + j0, kk, tile, s);
+        else if (P.storage == HBDIA_STORE_BF16_SCALED)
+            launch_list_typed<__nv_bfloat16, double>(P, x + j0, y + j0, kk, tile, s);
+        else launch_list_typed<double, double>(P, x + j0, y + j0, kk, tile, s);
+    }
+}
+
 void launch_spmm(const DevicePlan &P, const void *X, int64_t ldx, void *Y, int64_t ldy, int32_t k, void *stream,
                  bool colMajor) {
     int32_t tile = P.spmmTileForced;

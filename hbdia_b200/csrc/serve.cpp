@@ -15,6 +15,11 @@
 //    against).
 //  * CG: solve A y = x to a relative residual, by the mixed-precision CG of
 //    cg.cu on one of cgWorkers worker threads (own stream, own workspace).
+// x and y are host buffers (hbdia_server_submit: copied in and out on the
+// server's streams) or device buffers (hbdia_server_submit_device: read and
+// written in place).  A step's device SpMV requests on one matrix become one
+// vector-list SpMM (each value read once for up to 32 requests, no staging
+// copies); its host requests one column-major SpMM over the staging block.
 // A request's result does not depend on what it was batched with: column j
 // of the SpMM equals the SpMV of x_j bit for bit, and a CG solve depends only
 // on its matrix and right-hand side.
@@ -63,6 +68,7 @@ struct Request {
     const ServedMatrix *m = nullptr;  // taken under the server lock at submit
     const double *x = nullptr;
     double *y = nullptr;
+    bool device = false;  // x, y in device memory
     hbdia_request_info info{};
     bool done = false;
 };
@@ -127,21 +133,35 @@ void serve_step(Server *S, std::vector<Request *> &step) {
             const ServedMatrix &M = *g[0]->m;
             cudaStream_t st = S->streams[gi % S->streams.size()];
             used = std::min(S->streams.size(), std::max(used, gi + 1));  // streams of the ring in use
-            const int32_t k = static_cast<int32_t>(g.size());
+            const DevicePlan &P = M.spmvPlan(S->opt.spmvStorage);
+            std::vector<Request *> host;
+            std::vector<const void *> dx;
+            std::vector<void *> dy;
+            for (Request *r : g) {
+                r->info.started = started;
+                if (r->device) {
+                    dx.push_back(r->x);
+                    dy.push_back(r->y);
+                } else {
+                    host.push_back(r);
+                }
+            }
+            for (Request *r : g) r->info.batchRhs = static_cast<int32_t>(r->device ? dx.size() : host.size());
+            // device requests: one vector-list SpMM, in place
+            if (dx.size() == 1) launch_spmv(P, dx[0], dy[0], st);
+            else if (!dx.empty()) launch_spmv_list(P, dx.data(), dy.data(), static_cast<int32_t>(dx.size()), st);
+            // host requests: through the staging block
+            const int32_t k = static_cast<int32_t>(host.size());
             const size_t xb = static_cast<size_t>(M.rowsX) * sizeof(double);
             const size_t yb = static_cast<size_t>(M.n) * sizeof(double);
-            for (int32_t j = 0; j < k; ++j) {
-                g[j]->info.started = started;
-                g[j]->info.batchRhs = k;
-                check_cuda(cudaMemcpyAsync(M.X + static_cast<int64_t>(j) * M.rowsX, g[j]->x, xb,
-                                           cudaMemcpyHostToDevice, st), "cudaMemcpyAsync(request x)");
-            }
-            const DevicePlan &P = M.spmvPlan(S->opt.spmvStorage);
-            if (k == 1) launch_spmv(P, M.X, M.Y, st);
-            else launch_spmm(P, M.X, M.rowsX, M.Y, M.n, k, st, true);
             for (int32_t j = 0; j < k; ++j)
-                check_cuda(cudaMemcpyAsync(g[j]->y, M.Y + static_cast<int64_t>(j) * M.n, yb, cudaMemcpyDeviceToHost,
-                                           st), "cudaMemcpyAsync(request y)");
+                check_cuda(cudaMemcpyAsync(M.X + static_cast<int64_t>(j) * M.rowsX, host[j]->x, xb,
+                                           cudaMemcpyHostToDevice, st), "cudaMemcpyAsync(request x)");
+            if (k == 1) launch_spmv(P, M.X, M.Y, st);
+            else if (k > 1) launch_spmm(P, M.X, M.rowsX, M.Y, M.n, k, st, true);
+            for (int32_t j = 0; j < k; ++j)
+                check_cuda(cudaMemcpyAsync(host[j]->y, M.Y + static_cast<int64_t>(j) * M.n, yb,
+                                           cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync(request y)");
         }
     } catch (const Error &e) {
         status = e.status;
@@ -211,22 +231,26 @@ void cg_worker(Server *S) {
         try {
             if (!ok) throw Error(HBDIA_ERR_CUDA, "CG worker stream");
             const ServedMatrix &M = *r->m;
-            if (M.n > cap) {
+            if (!r->device && M.n > cap) {
                 if (bx) cudaFree(bx);
                 bx = nullptr;
                 check_cuda(cudaMalloc(&bx, 2 * sizeof(double) * static_cast<size_t>(M.n)), "cudaMalloc(CG b, x)");
                 cap = M.n;
             }
             w = cg_work(w, M.n);
-            double *b = bx, *x = bx + cap;
+            // device requests solve in place: b = request x, solution into request y
+            const double *b = r->device ? r->x : bx;
+            double *x = r->device ? r->y : bx + cap;
             const size_t nb = sizeof(double) * static_cast<size_t>(M.n);
-            check_cuda(cudaMemcpyAsync(b, r->x, nb, cudaMemcpyHostToDevice, st), "cudaMemcpyAsync(CG b)");
+            if (!r->device)
+                check_cuda(cudaMemcpyAsync(bx, r->x, nb, cudaMemcpyHostToDevice, st), "cudaMemcpyAsync(CG b)");
             check_cuda(cudaMemsetAsync(x, 0, nb, st), "cudaMemsetAsync(CG x)");
             const hbdia_server_options &o = S->opt;
             double secs = 0.0;
             cg_solve(M.p64, M.cgInner(o.cgInnerStorage), w, b, x, o.cgTol, o.cgMaxOuter, o.cgMaxInner, o.cgInnerTol,
                      o.cgCheckEvery, st, &r->info.cgOuter, &r->info.cgInner, &r->info.cgRelResidual, &secs);
-            check_cuda(cudaMemcpyAsync(r->y, x, nb, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync(CG y)");
+            if (!r->device)
+                check_cuda(cudaMemcpyAsync(r->y, x, nb, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync(CG y)");
             check_cuda(cudaStreamSynchronize(st), "cudaStreamSynchronize(CG)");
             if (r->info.cgRelResidual > o.cgTol) status = HBDIA_ERR_RUNTIME;  // not converged
         } catch (const Error &e) {
@@ -350,7 +374,7 @@ int32_t server_add_matrix(Server *S, const hbdia_matrix *m) {
     }
 }
 
-uint64_t server_submit(Server *S, int32_t matrix, int32_t kind, const double *x, double *y) {
+uint64_t server_submit(Server *S, int32_t matrix, int32_t kind, const double *x, double *y, bool device) {
     if (!x || !y) throw Error(HBDIA_ERR_INVALID_ARGUMENT, "null request vector");
     if (kind != HBDIA_REQ_SPMV && kind != HBDIA_REQ_CG) throw Error(HBDIA_ERR_INVALID_ARGUMENT, "unknown request kind");
     std::lock_guard<std::mutex> lk(S->mu);
@@ -364,6 +388,7 @@ uint64_t server_submit(Server *S, int32_t matrix, int32_t kind, const double *x,
     r->kind = kind;
     r->x = x;
     r->y = y;
+    r->device = device;
     r->info.kind = kind;
     r->info.matrix = matrix;
     r->info.submitted = now_since(S->t0);

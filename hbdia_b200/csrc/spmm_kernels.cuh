@@ -45,17 +45,44 @@ __device__ __forceinline__ int64_t blk(int64_t i, int64_t j, int64_t ld) {
     return CM ? j * ld + i : i * ld + j;
 }
 
+// How one pass reads its KT right-hand sides at column c: from a block (X
+// row- or column-major with leading dimension ld; Xp is the pass's first
+// column, column-major, or X + r0, row-major; IT is the element-index type,
+// 32-bit whenever the pass's block fits, which keeps the address arithmetic
+// to one instruction per gather) ...
+template <typename XT, int KT, bool CM, typename IT, bool FULL>
+struct XBlock {
+    const XT *Xp;
+    IT ld;
+    bool vec2;
+    __device__ __forceinline__ void load(IT c, int kc, XT (&xv)[KT]) const {
+        if (CM) {
+#pragma unroll
+            for (int q = 0; q < KT; ++q)
+                xv[q] = (FULL || q < kc) ? __ldg(Xp + (static_cast<IT>(q) * ld + c)) : XT(0);
+        } else {
+            load_x_row<XT, KT>(Xp + c * ld, FULL ? KT : kc, vec2, xv);
+        }
+    }
+};
+
+// ... or from KT separate vectors (column q at p[q]).
+template <typename XT, int KT, bool FULL>
+struct XList {
+    const XT *p[KT];
+    __device__ __forceinline__ void load(int32_t c, int kc, XT (&xv)[KT]) const {
+#pragma unroll
+        for (int q = 0; q < KT; ++q) xv[q] = (FULL || q < kc) ? __ldg(p[q] + c) : XT(0);
+    }
+};
+
 // U offsets of one row block for the KT right-hand sides of one pass: the U
 // values and all U x KT x gathers are issued before any product is formed, so
 // a group costs one memory round trip.  Column q's products are added in
-// ascending offset order.  Xp is the pass's first column (column-major) or
-// X + r0 (row-major); IT is the element-index type (32-bit whenever the
-// pass's block fits, which keeps the address arithmetic to one instruction
-// per gather); FULL means all KT columns of the pass are used.
-template <typename VT, typename XT, int KT, bool CM, int U, typename IT, bool FULL>
-__device__ __forceinline__ void spmm_group(const SpmvArgs<VT, XT> &a, const XT *__restrict__ Xp, IT ld,
-                                           const VT *vp, int32_t myoff, int j, int64_t row, int kc, bool vec2,
-                                           float s, XT (&acc)[KT]) {
+// ascending offset order.
+template <typename VT, typename XT, int KT, int U, typename IT, bool FULL, typename XS>
+__device__ __forceinline__ void spmm_group(const SpmvArgs<VT, XT> &a, const XS &xs, const VT *vp, int32_t myoff, int j,
+                                           int64_t row, int kc, float s, XT (&acc)[KT]) {
     VT v[U];
     bool ok[U];
     XT xv[U][KT];
@@ -64,14 +91,7 @@ __device__ __forceinline__ void spmm_group(const SpmvArgs<VT, XT> &a, const XT *
         const int64_t col = row + __shfl_sync(kFull, myoff, j + u);
         ok[u] = static_cast<uint64_t>(col) < static_cast<uint64_t>(a.xn);
         v[u] = __ldg(vp + (j + u) * 32);
-        const IT c = ok[u] ? static_cast<IT>(col) : IT(0);
-        if (CM) {
-#pragma unroll
-            for (int q = 0; q < KT; ++q)
-                xv[u][q] = (FULL || q < kc) ? __ldg(Xp + (static_cast<IT>(q) * ld + c)) : XT(0);
-        } else {
-            load_x_row<XT, KT>(Xp + c * ld, FULL ? KT : kc, vec2, xv[u]);
-        }
+        xs.load(ok[u] ? static_cast<IT>(col) : IT(0), kc, xv[u]);
     }
 #pragma unroll
     for (int u = 0; u < U; ++u) {
@@ -86,10 +106,9 @@ __device__ __forceinline__ void spmm_group(const SpmvArgs<VT, XT> &a, const XT *
 // The offsets of one row block for one pass, in groups of U = 16 / KT (at
 // least 1), so about 16 x gathers per lane are in flight (32 measured slower
 // on B200 at every tile width).
-template <typename VT, typename XT, int KT, bool CM, typename IT, bool FULL>
-__device__ __forceinline__ void spmm_pass(const SpmvArgs<VT, XT> &a, const XT *__restrict__ Xp, IT ld, int32_t k0,
-                                          int32_t k1, int64_t row, int lane, int kc, bool vec2, float s,
-                                          XT (&acc)[KT]) {
+template <typename VT, typename XT, int KT, typename IT, bool FULL, typename XS>
+__device__ __forceinline__ void spmm_pass(const SpmvArgs<VT, XT> &a, const XS &xs, int32_t k0, int32_t k1,
+                                          int64_t row, int lane, int kc, float s, XT (&acc)[KT]) {
     constexpr int U = KT >= 16 ? 1 : 16 / KT;
     for (int32_t kb = k0; kb < k1; kb += 32) {
         const int cnt = min(32, k1 - kb);
@@ -97,10 +116,48 @@ __device__ __forceinline__ void spmm_pass(const SpmvArgs<VT, XT> &a, const XT *_
         const VT *vp = a.vals + static_cast<int64_t>(kb) * 32 + lane;
         int j = 0;
         for (; j + U <= cnt; j += U)
-            spmm_group<VT, XT, KT, CM, U, IT, FULL>(a, Xp, ld, vp, myoff, j, row, kc, vec2, s, acc);
+            spmm_group<VT, XT, KT, U, IT, FULL>(a, xs, vp, myoff, j, row, kc, s, acc);
         for (; j < cnt; ++j)  // warp-uniform tail
-            spmm_group<VT, XT, KT, CM, 1, IT, FULL>(a, Xp, ld, vp, myoff, j, row, kc, vec2, s, acc);
+            spmm_group<VT, XT, KT, 1, IT, FULL>(a, xs, vp, myoff, j, row, kc, s, acc);
     }
+}
+
+// The COO remainder of one 32-row tile for one pass of the vector-list form,
+// added to acc: per column, the row's COO entries in list order, then one
+// add; each batch of 32 entries is loaded once for all columns.  xat(cc, q)
+// reads x_q[cc].  (bw32_spmm_tile_t keeps the same steps inline.)
+template <typename XT, int KT, typename XAt>
+__device__ __forceinline__ void spmm_coo(const int32_t *cooRow, const int32_t *cooCol, const XT *cooVal, int32_t c0,
+                                         int32_t c1, int64_t row0, int lane, int kc, XAt xat, XT (&acc)[KT]) {
+    XT c[KT];
+#pragma unroll
+    for (int q = 0; q < KT; ++q) c[q] = XT(0);
+    for (int32_t base = c0; base < c1; base += 32) {
+        const int32_t e = base + lane;
+        int lr = -1;
+        XT p[KT];
+#pragma unroll
+        for (int q = 0; q < KT; ++q) p[q] = XT(0);
+        if (e < c1) {
+            lr = static_cast<int>(__ldg(cooRow + e) - row0);
+            const int64_t cc = __ldg(cooCol + e);
+            const XT cv = __ldg(cooVal + e);
+#pragma unroll
+            for (int q = 0; q < KT; ++q)
+                if (q < kc) p[q] = mul_rn(cv, xat(cc, q));
+        }
+        const int m = min(32, c1 - base);
+        for (int t = 0; t < m; ++t) {
+            const int rt = __shfl_sync(kFull, lr, t);
+#pragma unroll
+            for (int q = 0; q < KT; ++q) {
+                const XT pt = __shfl_sync(kFull, p[q], t);
+                if (rt == lane) c[q] = add_rn(c[q], pt);
+            }
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < KT; ++q) acc[q] = add_rn(acc[q], c[q]);
 }
 
 // blockWidth 32: one warp per 32-row block, lane = row, k right-hand sides in
@@ -124,12 +181,12 @@ __device__ __forceinline__ void bw32_spmm_tile_t(const SpmvArgs<VT, XT> &a, cons
     const bool xAligned = !CM && (reinterpret_cast<uintptr_t>(X) & 15) == 0 && (ldx & 1) == 0;
     for (int32_t r0 = 0; r0 < k; r0 += KT) {
         const int kc = min(KT, k - r0);
-        const bool vec2 = xAligned && (r0 & 1) == 0;
-        const XT *Xp = CM ? X + static_cast<int64_t>(r0) * ldx : X + r0;
+        const XBlock<XT, KT, CM, IT, FULL> xs{CM ? X + static_cast<int64_t>(r0) * ldx : X + r0,
+                                              static_cast<IT>(ldx), xAligned && (r0 & 1) == 0};
         XT acc[KT];
 #pragma unroll
         for (int q = 0; q < KT; ++q) acc[q] = XT(0);
-        spmm_pass<VT, XT, KT, CM, IT, FULL>(a, Xp, static_cast<IT>(ldx), k0, k1, row, lane, kc, vec2, s, acc);
+        spmm_pass<VT, XT, KT, IT, FULL>(a, xs, k0, k1, row, lane, kc, s, acc);
         if (a.hasCoo) {
             // per column: the row's COO entries in list order, then one add;
             // each batch of 32 entries is loaded once for all columns
@@ -171,6 +228,51 @@ __device__ __forceinline__ void bw32_spmm_tile_t(const SpmvArgs<VT, XT> &a, cons
     }
 }
 
+// k <= kVecListMax separate vectors: x_j and y_j anywhere in device memory,
+// passed by value in the kernel's parameter block (no table in memory, so a
+// launch allocates nothing and can be captured in a graph).
+constexpr int kVecListMax = 32;
+template <typename XT>
+struct VecList {
+    const XT *x[kVecListMax];
+    XT *y[kVecListMax];
+};
+
+// The vector-list form of bw32_spmm_tile_t (x_j read at x[j] + col, 32-bit
+// offsets: each vector has fewer than 2^31 elements).
+template <typename VT, typename XT, int KT, bool FULL>
+__device__ __forceinline__ void bw32_spmm_list_tile(const SpmvArgs<VT, XT> &a, const VecList<XT> &L, int32_t k,
+                                                    int32_t tile, int lane) {
+    const int64_t row0 = static_cast<int64_t>(tile) * 32;
+    const int64_t row = row0 + lane;
+    int32_t k0 = 0, k1 = 0;
+    if (tile < a.numBlocks) {
+        k0 = __ldg(a.blkOff + tile);
+        k1 = __ldg(a.blkOff + tile + 1);
+    }
+    const int32_t c0 = a.hasCoo ? __ldg(a.cooTile + tile) : 0;
+    const int32_t c1 = a.hasCoo ? __ldg(a.cooTile + tile + 1) : 0;
+    const float s = (a.scale && tile < a.numBlocks) ? __ldg(a.scale + tile) : 1.0f;
+    for (int32_t r0 = 0; r0 < k; r0 += KT) {
+        const int kc = min(KT, k - r0);
+        XList<XT, KT, FULL> xs;
+#pragma unroll
+        for (int q = 0; q < KT; ++q) xs.p[q] = (FULL || q < kc) ? L.x[r0 + q] : L.x[r0];
+        XT acc[KT];
+#pragma unroll
+        for (int q = 0; q < KT; ++q) acc[q] = XT(0);
+        spmm_pass<VT, XT, KT, int32_t, FULL>(a, xs, k0, k1, row, lane, kc, s, acc);
+        if (a.hasCoo)
+            spmm_coo<XT, KT>(a.cooRow, a.cooCol, a.cooVal, c0, c1, row0, lane, kc,
+                             [&](int64_t cc, int q) { return __ldg(xs.p[q] + cc); }, acc);
+        if (row < a.n) {
+#pragma unroll
+            for (int q = 0; q < KT; ++q)
+                if (q < kc) L.y[r0 + q][row] = acc[q];
+        }
+    }
+}
+
 // Any k, any size (the batch kernel's form).
 template <typename VT, typename XT, int KT, bool CM = false>
 __device__ __forceinline__ void bw32_spmm_tile(const SpmvArgs<VT, XT> &a, const XT *__restrict__ X, int64_t ldx,
@@ -187,6 +289,15 @@ spmm_bw32(const SpmvArgs<VT, XT> a, const XT *__restrict__ X, int64_t ldx, XT *_
     const int32_t tile = static_cast<int32_t>((static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5);
     if (tile >= a.numTiles) return;  // warp-uniform
     bw32_spmm_tile_t<VT, XT, KT, CM, IT, FULL>(a, X, ldx, Y, ldy, k, tile, lane);
+}
+
+template <typename VT, typename XT, int KT, bool FULL>
+__global__ void __launch_bounds__(256)
+spmm_bw32_list(const SpmvArgs<VT, XT> a, const __grid_constant__ VecList<XT> L, int32_t k) {
+    const int lane = threadIdx.x & 31;
+    const int32_t tile = static_cast<int32_t>((static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5);
+    if (tile >= a.numTiles) return;  // warp-uniform
+    bw32_spmm_list_tile<VT, XT, KT, FULL>(a, L, k, tile, lane);
 }
 
 // Any block width: one thread per row (the reference's mapping).

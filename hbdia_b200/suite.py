@@ -113,9 +113,15 @@ def spmm(args):
             Yc = torch.zeros((k, n), dtype=torch.float64, device="cuda")
             msc = _time(lambda: hb.spmm_device_colmajor(m, Xc.data_ptr(), n, Yc.data_ptr(), n, k, stream.cuda_stream),
                         stream)
+            # separate vectors (one allocation each): the vector-list form
+            xs = [torch.from_numpy(np.random.default_rng(3 + j).uniform(-1, 1, n)).cuda() for j in range(k)]
+            ys = [torch.zeros(n, dtype=torch.float64, device="cuda") for _ in range(k)]
+            xp, yp = [t.data_ptr() for t in xs], [t.data_ptr() for t in ys]
+            msl = _time(lambda: hb.spmv_list_device(m, xp, yp, stream.cuda_stream), stream)
             m.synchronize()
             b = vbytes + k * 16 * n
-            for layout, t, tile in (("row-major (autotuned tile)", ms, tune.spmmTile), ("column-major (default tile)", msc, 4)):
+            for layout, t, tile in (("row-major (autotuned tile)", ms, tune.spmmTile), ("column-major (default tile)", msc, 4),
+                                    ("vector list (default tile)", msl, 4)):
                 print(json.dumps({"suite": "spmm", "workload": f"7-point Laplacian {g}^3 (centre 6, -1)",
                                   "storage": stname, "k": k, "layout": layout, "rhs_tile": tile, "ms": t,
                                   "ms_k_spmv": k * ms1, "speedup_vs_k_spmv": k * ms1 / t,
@@ -235,6 +241,12 @@ def _serve_run(hb, srv, ids, mats_n, kinds, mids, xbuf, ybuf, rate, seed):
     ready = threading.Semaphore(0)
     lag = [0.0]
 
+    seq = np.zeros(n_req, np.int64)  # each request's number on its matrix: picks its buffers
+    cnt = {}
+    for i, m in enumerate(mids):
+        seq[i] = cnt.get(m, 0)
+        cnt[m] = seq[i] + 1
+
     def submit_all():
         arrivals = np.cumsum(np.random.default_rng(seed).exponential(1.0 / rate, n_req)) if rate else None
         t0 = time.perf_counter()
@@ -248,7 +260,11 @@ def _serve_run(hb, srv, ids, mats_n, kinds, mids, xbuf, ybuf, rate, seed):
                         time.sleep(d - 1e-4)
                 lag[0] = max(lag[0], (time.perf_counter() - t0) - arrivals[i])
             m = mids[i]
-            tickets[i] = srv.submit(ids[m], kinds[i], xbuf[m][i % len(xbuf[m])], ybuf[m][i % len(ybuf[m])])
+            x, y = xbuf[m][seq[i] % len(xbuf[m])], ybuf[m][seq[i] % len(ybuf[m])]
+            if isinstance(x, np.ndarray):
+                tickets[i] = srv.submit(ids[m], kinds[i], x, y)
+            else:  # CUDA tensors: a device request
+                tickets[i] = srv.submit_device(ids[m], kinds[i], x, y)
             ready.release()
 
     if rate is None:
@@ -280,7 +296,8 @@ def serve(args):
     with 0.5 % symmetric off-pattern entries (seed 50 + i), resident in a
     server with a 150 GB admission budget.  Requests: 80 % SpMV, 20 % CG
     (to ||b - A y|| / ||b|| <= 1e-10), matrix uniform (default_rng(6)), x / b
-    from a pool of pinned host vectors per matrix.  Two servers:
+    from a pool of pinned host vectors per matrix (--device: device vectors,
+    served in place).  Two servers:
       * batched: continuous batching, FP32-stored values (FP64 accumulation),
         mixed-precision CG (FP32 inner, FP64 refinement), 4 CG solvers;
       * plain: FP64 values, one request per launch, plain FP64 CG, 1 solver.
@@ -315,8 +332,12 @@ def serve(args):
         pins.append(t)
         return a
 
-    xbuf = [[pinned(n, lambda k: rng.uniform(-1, 1, k)) for _ in range(2)] for n in ns]
-    ybuf = [[pinned(n, np.zeros) for _ in range(8)] for n in ns]
+    if args.device:  # one output per request of a batch: no two writers of one y
+        xbuf = [[torch.from_numpy(rng.uniform(-1, 1, n)).cuda() for _ in range(2)] for n in ns]
+        ybuf = [[torch.zeros(n, dtype=torch.float64, device="cuda") for _ in range(40)] for n in ns]
+    else:
+        xbuf = [[pinned(n, lambda k: rng.uniform(-1, 1, k)) for _ in range(2)] for n in ns]
+        ybuf = [[pinned(n, np.zeros) for _ in range(8)] for n in ns]
     servers = {
         "batched": hb.Server(),
         "plain": hb.Server(batching=0, spmvStorage=hb.STORE_NATIVE, cgInnerStorage=hb.STORE_NATIVE,
@@ -345,7 +366,8 @@ def serve(args):
         st = srv.stats()
         is_cg = kinds == hb.REQ_CG
         print(json.dumps({
-            "suite": "serve", "server": name, "arrivals": f"Poisson at {rate:.1f} req/s ({which} {args.load:g} x capacity)",
+            "suite": "serve", "server": name, "vectors": "device" if args.device else "pinned host",
+            "arrivals": f"Poisson at {rate:.1f} req/s ({which} {args.load:g} x capacity)",
             "workload": f"{len(ns)} SPD 27-point stencils, edge U[{args.edge_min},{args.edge_max}] seed 5, 0.5% "
                         f"symmetric extras, {rows} rows; {n_req} requests, {args.cg_fraction:.0%} CG",
             "capacity_req_s": results[name]["capacity_req_s"], "throughput_req_s": n_req / wall,
@@ -402,6 +424,7 @@ def main(argv=None):
     ap.add_argument("--storage", type=int, default=0)
     ap.add_argument("--n", type=int, default=8 * 1024 * 1024)
     ap.add_argument("--grid", type=int, default=128)
+    ap.add_argument("--device", action="store_true", help="serve: request vectors in device memory")
     args = ap.parse_args(argv)
     import torch
     torch.cuda.set_device(0)

@@ -263,6 +263,14 @@ int hbdia_spmm_device(const hbdia_matrix *m, const void *X, int64_t ldx, void *Y
 int hbdia_spmm_device_colmajor(const hbdia_matrix *m, const void *X, int64_t ldx, void *Y, int64_t ldy,
                                int32_t k, void *stream);
 
+/* k SpMVs of one matrix over separate device vectors: y[j] = A x[j] for
+ * j < k (x[j] holding max(numRows, numCols) elements, y[j] numRows), with
+ * each stored value read once for up to 32 vectors (vector-list SpMMs; the
+ * pointer arrays are host arrays, passed to the kernel by value).  Each y[j]
+ * equals hbdia_spmv_device(m, x[j], y[j]) bit for bit.  Allocation-free and
+ * graph-capturable.  No counterpart in the reference. */
+int hbdia_spmv_list_device(const hbdia_matrix *m, const void *const *x, void *const *y, int32_t k, void *stream);
+
 /* End-to-end form on HOST buffers: copies x to the device, runs the SpMV,
  * copies y back and synchronizes.  Page-locked host buffers are fastest. */
 int hbdia_spmv_host(hbdia_matrix *m, const void *xHost, void *yHost);
@@ -486,6 +494,13 @@ int hbdia_server_add_matrix(hbdia_server *s, const hbdia_matrix *m, int32_t *id)
 /* x: numCols doubles (the right-hand side b for CG); y: numRows doubles. */
 int hbdia_server_submit(hbdia_server *s, int32_t matrix, int32_t kind, const double *xHost, double *yHost,
                         uint64_t *ticket);
+/* The same request on device buffers (this process's current device):
+ * read and written in place, no host copies.  A step's device SpMV requests
+ * on one matrix run as one vector-list SpMM (hbdia_spmv_list_device); a
+ * device CG request solves with b = xDevice into yDevice.  Both buffers must
+ * stay valid and untouched until hbdia_server_wait returns. */
+int hbdia_server_submit_device(hbdia_server *s, int32_t matrix, int32_t kind, const double *xDevice,
+                               double *yDevice, uint64_t *ticket);
 /* paused != 0: requests queue up but no SpMV step or CG solve starts (work
  * already running finishes); 0 resumes, and everything queued is served --
  * the SpMVs of the backlog batched together.  Waiting on an unfinished

@@ -218,3 +218,61 @@ def test_step_with_more_matrices_than_streams(lib):
         assert bits_equal(y, y0)
     assert srv.stats().spmvSteps == 21  # 20 alone + one step for the whole burst
     srv.close()
+
+
+def test_device_requests_equal_host_requests(lib, mats):
+    """Requests on device buffers (read and written in place) give the same
+    bits as the same requests on host buffers, batched or alone, mixed with
+    host requests in one step; device CG equals host CG."""
+    import torch
+    srv = lib.Server()
+    ids = [srv.add_matrix(m) for m, _, _ in mats]
+    rng = np.random.default_rng(3)
+    keep, host_y, dev = [], {}, []
+    # reference results: host requests served one at a time
+    for j, (mid, (m, rcv, n)) in enumerate(zip(ids, mats)):
+        for rep in range(3):
+            tx, x = _pinned(n, rng)
+            ty, y = _pinned(n)
+            keep += [tx, ty]
+            assert srv.wait(srv.submit(mid, lib.REQ_SPMV, x, y)).status == 0
+            host_y[(j, rep)] = (x.copy(), y.copy())
+        tb, b = _pinned(n, rng)
+        tc, c = _pinned(n)
+        keep += [tb, tc]
+        assert srv.wait(srv.submit(mid, lib.REQ_CG, b, c)).status == 0
+        host_y[(j, "cg")] = (b.copy(), c.copy())
+    # the same inputs as device requests, queued together with host requests
+    srv.pause(True)
+    pending = []
+    for rep in range(12):
+        for j, (mid, (m, rcv, n)) in enumerate(zip(ids, mats)):
+            x0, y0 = host_y[(j, rep % 3)]
+            xd = torch.from_numpy(x0).cuda()
+            yd = torch.full((n,), float("nan"), dtype=torch.float64, device="cuda")
+            pending.append((y0, yd, srv.submit_device(mid, lib.REQ_SPMV, xd, yd)))
+            keep.append(xd)
+            if rep % 4 == 1:  # a host request in the same step
+                tx, x = _pinned(n)
+                x[:] = x0
+                ty, y = _pinned(n)
+                keep += [tx, ty]
+                pending.append((y0, y, srv.submit(mid, lib.REQ_SPMV, x, y)))
+            if rep == 5:
+                b0, c0 = host_y[(j, "cg")]
+                bd = torch.from_numpy(b0).cuda()
+                cd = torch.full((n,), float("nan"), dtype=torch.float64, device="cuda")
+                keep.append(bd)
+                pending.append((c0, cd, srv.submit_device(mid, lib.REQ_CG, bd, cd)))
+    srv.pause(False)
+    widest = 0
+    for exp, got, t in pending:
+        info = srv.wait(t)
+        assert info.status == 0
+        widest = max(widest, info.batchRhs)
+        g = got.cpu().numpy() if hasattr(got, "is_cuda") else got
+        assert bits_equal(g, exp)
+    assert widest >= 12  # the paused backlog formed vector-list batches
+    with pytest.raises(ValueError):
+        srv.submit_device(ids[0], lib.REQ_SPMV, torch.zeros(4), torch.zeros(4))
+    srv.close()

@@ -136,3 +136,58 @@ def test_spmm_colmajor_equals_spmv(lib, orc, bw, tile, k):
     assert np.isnan(Y[:, n:]).all()  # nothing outside the columns written
     with pytest.raises(ValueError):
         lib.spmm_device_colmajor(m, Xt.data_ptr(), n - 1, Yt.data_ptr(), ld, k)
+
+
+@pytest.mark.parametrize("storage", [0, 1, 2])
+@pytest.mark.parametrize("k", [1, 3, 8, 13, 32, 45])
+def test_spmv_list_equals_spmv(lib, k, storage):
+    """Separate device vectors (scattered allocations) through the
+    vector-list SpMM: each y_j equals its own SpMV bit for bit, for every
+    value storage, k past one launch's 32, and tile widths forced."""
+    import torch
+    rng = np.random.default_rng(700 + k)
+    n = 2500
+    rows, cols, vals = random_coo(rng, n, n, 25000)
+    i = np.arange(n, dtype=np.int32)
+    rows = np.concatenate([rows, i, i[1:]]).astype(np.int32)
+    cols = np.concatenate([cols, i, i[:-1]]).astype(np.int32)
+    vals = np.concatenate([vals, rng.uniform(-1, 1, 2 * n - 1)])
+    o = np.argsort(rows, kind="stable")
+    m = lib.HBDIA(rows[o], cols[o], vals[o], n, n)
+    m.convertToHBDIAFormat(32, 2, upload=False)
+    m.prepareForGPU(storage)
+    xs = [torch.from_numpy(rng.uniform(-1, 1, n)).cuda() for _ in range(k)]
+    pad = [torch.empty(int(rng.integers(1, 100)), dtype=torch.float64, device="cuda") for _ in range(k)]
+    ys = [torch.full((n,), float("nan"), dtype=torch.float64, device="cuda") for _ in range(k)]
+    ref = [torch.empty(n, dtype=torch.float64, device="cuda") for _ in range(k)]
+    for x, r in zip(xs, ref):
+        lib.spmv_device(m, x.data_ptr(), r.data_ptr(), 0)
+    for tile in (0, 2, 4, 16):
+        m.setTuning(lib.TUNE_SPMM_TILE, tile)
+        for y in ys:
+            y.fill_(float("nan"))
+        lib.spmv_list_device(m, [x.data_ptr() for x in xs], [y.data_ptr() for y in ys], 0)
+        torch.cuda.synchronize()
+        for y, r in zip(ys, ref):
+            assert bits_equal(y.cpu().numpy(), r.cpu().numpy()), tile
+    del pad
+
+
+def test_spmv_list_other_block_widths_and_errors(lib, orc):
+    import torch
+    rng = np.random.default_rng(9)
+    n = 900
+    rows, cols, vals = random_coo(rng, n, n, 9000)
+    m = lib.HBDIA(rows, cols, vals, n, n)
+    m.convertToHBDIAFormat(16, 1)
+    xs = [rng.uniform(-1, 1, n) for _ in range(5)]
+    tx = [torch.from_numpy(x).cuda() for x in xs]
+    ty = [torch.zeros(n, dtype=torch.float64, device="cuda") for _ in xs]
+    lib.spmv_list_device(m, [t.data_ptr() for t in tx], [t.data_ptr() for t in ty], 0)
+    torch.cuda.synchronize()
+    om = orc.convert(rows, cols, vals, n, n, 16, 1)
+    for x, y in zip(xs, ty):
+        assert bits_equal(y.cpu().numpy(), om.spmv(x))
+    with pytest.raises(ValueError):
+        lib.spmv_list_device(m, [tx[0].data_ptr(), 0], [ty[0].data_ptr(), ty[1].data_ptr()], 0)
+    lib.spmv_list_device(m, [], [], 0)  # nothing to do
