@@ -535,6 +535,11 @@ int hbdia_matrix_set_tuning(hbdia_matrix *m, int32_t key, int32_t value) {
             m->plan.unroll = value;
             return;
         }
+        if (key == HBDIA_TUNE_PREFETCH) {
+            need(value == 0 || value == 1, HBDIA_ERR_INVALID_ARGUMENT, "prefetch must be 0 or 1");
+            m->plan.prefetchL2 = value;
+            return;
+        }
         if (key == HBDIA_TUNE_SPMM_TILE) {
             need(value == 0 || value == 2 || value == 4 || value == 8 || value == 16 || value == 32,
                  HBDIA_ERR_INVALID_ARGUMENT, "SpMM tile must be 0, 2, 4, 8, 16 or 32");

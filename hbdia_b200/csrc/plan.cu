@@ -68,6 +68,7 @@ void build_plan(const HostLayout<T> &L, int storage, DevicePlan &P, const Column
     Q.waitTimeoutNs = P.waitTimeoutNs;
     Q.skipChunk = P.skipChunk;
     Q.unroll = P.unroll;
+    Q.prefetchL2 = P.prefetchL2;
     free_plan(P);
     Q.dtype = std::is_same<T, float>::value ? HBDIA_F32 : HBDIA_F64;
     if (storage != HBDIA_STORE_NATIVE && Q.dtype != HBDIA_F64)
@@ -283,6 +284,10 @@ template <typename VT, typename XT>
 void launch_pipe_tuned(const DevicePlan &P, const dev::SpmvArgs<VT, XT> &a, const XT *x, XT *y, cudaStream_t s) {
     // Forcing 4-6 CTAs per SM through __launch_bounds__ made ptxas spill and
     // ran 3-45% slower on B200; the compiler's own register choice is kept.
+    if (P.prefetchL2) {
+        if (P.unroll == 27) return launch_pipe(dev::spmv_bw32_pipe<VT, XT, 27, true>, a, P.numTiles, x, y, s);
+        return launch_pipe(dev::spmv_bw32_pipe<VT, XT, kUnroll, true>, a, P.numTiles, x, y, s);
+    }
     if (P.unroll == 27) return launch_pipe(dev::spmv_bw32_pipe<VT, XT, 27>, a, P.numTiles, x, y, s);
     return launch_pipe(dev::spmv_bw32_pipe<VT, XT, kUnroll>, a, P.numTiles, x, y, s);
 }

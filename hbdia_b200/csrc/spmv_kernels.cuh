@@ -227,7 +227,15 @@ __device__ __forceinline__ TileMeta load_meta(const SpmvArgs<VT, XT> &a, int32_t
     return m;
 }
 
-template <typename VT, typename XT, int U>
+// Bulk prefetch of [p, p + bytes) into L2 (bytes a multiple of 16, p 16-byte
+// aligned): a hint, no registers, no completion to wait for.
+__device__ __forceinline__ void prefetch_l2_bulk(const void *p, uint32_t bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
+// PF: one lane also asks L2 for tile t+W's value rows (up to 32 KB) while tile
+// t is computed, so its value loads find them in L2.
+template <typename VT, typename XT, int U, bool PF = false>
 __global__ void __launch_bounds__(256)
 spmv_bw32_pipe(const SpmvArgs<VT, XT> a, const XT *__restrict__ x, XT *__restrict__ y) {
     const int lane = threadIdx.x & 31;
@@ -240,6 +248,11 @@ spmv_bw32_pipe(const SpmvArgs<VT, XT> a, const XT *__restrict__ x, XT *__restric
     while (t < a.numTiles) {
         const int32_t tn = t + W;
         const TileMeta mn = tn < a.numTiles ? load_meta(a, tn) : TileMeta{0, 0, 0, 0};
+        if (PF && lane == 0 && mn.k1 > mn.k0) {  // values of [k0, k1) are contiguous, 64-byte aligned
+            const int64_t bytes = static_cast<int64_t>(mn.k1 - mn.k0) * 32 * static_cast<int64_t>(sizeof(VT));
+            prefetch_l2_bulk(a.vals + static_cast<int64_t>(mn.k0) * 32,
+                             static_cast<uint32_t>(bytes < 32768 ? bytes : 32768));
+        }
         const int32_t row0 = t * 32;
         const int32_t row = row0 + lane;
         // first 32 COO entries of this tile and their x values, consumed at the end

@@ -31,7 +31,7 @@ import numpy as np
 import torch
 import torch.distributed as dist
 
-from . import HBDIA, _lib, spmv_device
+from . import HBDIA, _lib, set_device, spmv_device
 from ._lib import check as _check, load as _load
 
 __all__ = ["MatrixData", "Partition", "VectorPartition", "BasicExtractor", "PartialVector", "Distributor",
@@ -305,6 +305,8 @@ class Distributor:
         if device is None:
             device = torch.device("cuda", torch.cuda.current_device()) if backend == "nccl" else torch.device("cpu")
         self.device = torch.device(device)
+        if self.device.type == "cuda":  # the library's own runtime follows the rank's GPU
+            set_device(self.device.index if self.device.index is not None else torch.cuda.current_device())
         # NCCL moves device tensors only; gloo moves host tensors
         self._comm = self.device if backend == "nccl" else torch.device("cpu")
         self.blockWidth, self.threshold, self.maxCooEntries = blockWidth, threshold, maxCooEntries

@@ -296,3 +296,35 @@ def test_kernel_selection(lib):
     yv = lib.HBDIAVector(np.zeros(n))
     lib.hbdiaSpMV(m2, lib.HBDIAVector(x), yv, True, False)
     assert bits_equal(yt.cpu().numpy(), yv.toHost())
+
+
+@pytest.mark.parametrize("storage", [0, 1, 2])
+def test_pipe_prefetch_knob_bitequal(lib, storage):
+    """The pipelined kernel's L2 prefetch and unroll knobs change speed only."""
+    import torch
+    rng = np.random.default_rng(21)
+    n = 40000
+    rows, cols, vals = random_coo(rng, n, n, 300000)
+    i = np.arange(n, dtype=np.int32)
+    rows = np.concatenate([rows, i, i[1:], i[:-1]]).astype(np.int32)
+    cols = np.concatenate([cols, i, i[:-1], i[1:]]).astype(np.int32)
+    vals = np.concatenate([vals, rng.uniform(-1, 1, 3 * n - 2)])
+    o = np.argsort(rows, kind="stable")
+    m = lib.HBDIA(rows[o], cols[o], vals[o], n, n)
+    m.convertToHBDIAFormat(32, 2, upload=False)
+    m.prepareForGPU(storage)
+    m.setKernel(lib.KERNEL_PIPE)
+    x = torch.from_numpy(rng.uniform(-1, 1, n)).cuda()
+    out = []
+    for unroll in (0, 27):
+        for pf in (1, 0):
+            m.setTuning(lib.TUNE_UNROLL, unroll)
+            m.setTuning(lib.TUNE_PREFETCH, pf)
+            y = torch.full((n,), float("nan"), dtype=torch.float64, device="cuda")
+            lib.spmv_device(m, x.data_ptr(), y.data_ptr(), 0)
+            torch.cuda.synchronize()
+            out.append(y.cpu().numpy())
+    for y in out[1:]:
+        assert bits_equal(y, out[0])
+    with pytest.raises(ValueError):
+        m.setTuning(lib.TUNE_PREFETCH, 2)
