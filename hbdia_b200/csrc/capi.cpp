@@ -536,7 +536,7 @@ int hbdia_matrix_set_tuning(hbdia_matrix *m, int32_t key, int32_t value) {
             return;
         }
         if (key == HBDIA_TUNE_PREFETCH) {
-            need(value == 0 || value == 1, HBDIA_ERR_INVALID_ARGUMENT, "prefetch must be 0 or 1");
+            need(value >= -1 && value <= 1, HBDIA_ERR_INVALID_ARGUMENT, "prefetch must be -1, 0 or 1");
             m->plan.prefetchL2 = value;
             return;
         }

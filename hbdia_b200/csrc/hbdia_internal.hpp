@@ -139,7 +139,8 @@ struct DevicePlan {
     int32_t unroll = 0;                  // offsets in flight per lane (0: default)
     std::map<int32_t, int32_t> spmmTile; // autotuned RHS tile per k
     int32_t spmmTileForced = 0;          // HBDIA_TUNE_SPMM_TILE (0: autotuned / default)
-    int32_t prefetchL2 = 1;              // HBDIA_TUNE_PREFETCH: pipe kernel L2 prefetch of the next tile
+    int32_t prefetchL2 = -1;             // HBDIA_TUNE_PREFETCH: pipe kernel L2 prefetch of the next
+                                         // tile (-1: when x exceeds L2, 0: off, 1: on)
 };
 
 // Host-side facts of a layout built on the device (convert_gpu.cu).

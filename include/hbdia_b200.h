@@ -308,10 +308,11 @@ int hbdia_matrix_selected_kernel(const hbdia_matrix *m, const void *x, int32_t *
  * kernels (0 = default 9, or 27).
  * HBDIA_TUNE_SPMM_TILE: right-hand sides per pass of the SpMM kernels for
  * every k (0 = autotuned / default, or 2, 4, 8, 16, 32).
- * HBDIA_TUNE_PREFETCH: 1 (default) = the pipelined kernel asks L2 for the
- * next tile's value rows while computing the current one (bulk L2
- * prefetch; measured on B200 at 256^3: FP64 +1.5 %, FP32 storage +8 %),
- * 0 = off. */
+ * HBDIA_TUNE_PREFETCH: 1 = the pipelined kernel asks L2 for the next
+ * tile's value rows while computing the current one (bulk L2 prefetch),
+ * 0 = off, -1 (default) = on when the x vector is larger than the GPU's L2.
+ * Measured on B200: with a 134 MB x, FP64 +1.5 % and FP32 storage +8 %; with
+ * x in L2 (57 MB and below) -2 to -10 %, as the prefetched rows evict x. */
 typedef enum hbdia_tuning_key {
     HBDIA_TUNE_UNROLL = 1,
     HBDIA_TUNE_SPMM_TILE = 2,

@@ -317,7 +317,7 @@ def test_pipe_prefetch_knob_bitequal(lib, storage):
     x = torch.from_numpy(rng.uniform(-1, 1, n)).cuda()
     out = []
     for unroll in (0, 27):
-        for pf in (1, 0):
+        for pf in (1, 0, -1):
             m.setTuning(lib.TUNE_UNROLL, unroll)
             m.setTuning(lib.TUNE_PREFETCH, pf)
             y = torch.full((n,), float("nan"), dtype=torch.float64, device="cuda")
@@ -328,3 +328,4 @@ def test_pipe_prefetch_knob_bitequal(lib, storage):
         assert bits_equal(y, out[0])
     with pytest.raises(ValueError):
         m.setTuning(lib.TUNE_PREFETCH, 2)
+    m.setTuning(lib.TUNE_PREFETCH, -1)
