@@ -499,6 +499,22 @@ def spmv_list_device(matrix: HBDIA, x_ptrs: Sequence[int], y_ptrs: Sequence[int]
     _check(_load().hbdia_spmv_list_device(matrix.handle, xa, ya, k, _stream_arg(stream)))
 
 
+def spmv_host_many(matrix: HBDIA, xs: Sequence[np.ndarray], ys: Sequence[np.ndarray]) -> None:
+    """y_j = A x_j for host arrays, pipelined so that one step's upload
+    overlaps another's download (page-locked arrays for the overlap)."""
+    if len(xs) != len(ys):
+        raise ValueError("x and y lists differ in length")
+    nx = max(matrix.getNumRows(), matrix.getNumCols())
+    for x, y in zip(xs, ys):
+        if x.dtype != matrix.dtype or y.dtype != matrix.dtype or not x.flags.c_contiguous or not y.flags.c_contiguous \
+                or x.size < nx or y.size < matrix.getNumRows():
+            raise ValueError("vectors must be contiguous arrays of the matrix's type and size")
+    k = len(xs)
+    xa = (ctypes.c_void_p * max(k, 1))(*[x.ctypes.data for x in xs])
+    ya = (ctypes.c_void_p * max(k, 1))(*[y.ctypes.data for y in ys])
+    _check(_load().hbdia_spmv_host_many(matrix.handle, xa, ya, k))
+
+
 def spmv_host(matrix: HBDIA, x: np.ndarray, y: np.ndarray) -> None:
     """End-to-end y = A x on host arrays (copies in, SpMV, copies out, sync)."""
     _check(_load().hbdia_spmv_host(matrix.handle, ctypes.c_void_p(x.ctypes.data), ctypes.c_void_p(y.ctypes.data)))

@@ -197,6 +197,7 @@ _SIGS = [
     ("hbdia_halo_elements", c_i64, [c_vp]),
     ("hbdia_halo_destroy", None, [c_vp]),
     ("hbdia_spmv_list_device", ctypes.c_int, [c_vp, c_vpp, c_vpp, c_i32, c_vp]),
+    ("hbdia_spmv_host_many", ctypes.c_int, [c_vp, c_vpp, c_vpp, c_i32]),
     ("hbdia_server_submit_device", ctypes.c_int, [c_vp, c_i32, c_i32, c_vp, c_vp, ctypes.POINTER(ctypes.c_uint64)]),
 ]
 

@@ -105,7 +105,17 @@ void fill_coo(hbdia::Coo<T> &c, const int32_t *r, const int32_t *col, const void
     c.numCols = nC;
 }
 
+void free_host_pipeline(hbdia_matrix *m) {
+    for (int d = 0; d < hbdia_matrix::kHostDepth; ++d) {
+        if (m->pipeX[d]) cudaFree(m->pipeX[d]);
+        if (m->pipeY[d]) cudaFree(m->pipeY[d]);
+        if (m->pipeStream[d]) cudaStreamDestroy(static_cast<cudaStream_t>(m->pipeStream[d]));
+        m->pipeX[d] = m->pipeY[d] = m->pipeStream[d] = nullptr;
+    }
+}
+
 void reset_hbdia(hbdia_matrix *m) {
+    free_host_pipeline(m);
     hbdia::free_plan(m->plan);
     hbdia::free_plan(m->innerPlan);
     hbdia::cg_free(m->cg);
@@ -714,6 +724,62 @@ int hbdia_spmv_host(hbdia_matrix *m, const void *xh, void *yh) {
         hbdia::launch_spmv(P, P.xScratch, P.yScratch, s);
         hbdia::check_cuda(cudaMemcpyAsync(yh, P.yScratch, yb, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync(y)");
         hbdia::check_cuda(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+        throw_if_timeout(read_status(m, true));
+    });
+}
+
+int hbdia_spmv_host_many(hbdia_matrix *m, const void *const *xh, void *const *yh, int32_t count) {
+    return guarded([&] {
+        need(m != nullptr && count >= 0, HBDIA_ERR_INVALID_ARGUMENT, "bad argument");
+        need(count == 0 || (xh && yh), HBDIA_ERR_INVALID_ARGUMENT, "null vector list");
+        for (int32_t j = 0; j < count; ++j) need(xh[j] && yh[j], HBDIA_ERR_INVALID_ARGUMENT, "null vector");
+        need(m->hasHBDIA, HBDIA_ERR_NOT_CONVERTED, "matrix is not in HBDIA format");
+        if (count == 0) return;
+        ensure_device(m);
+        std::lock_guard<std::mutex> lk(m->hostMu);
+        hbdia::DevicePlan &P = m->plan;
+        const size_t es = esize(m->dtype);
+        const size_t xb = static_cast<size_t>(std::max(P.n, P.numCols)) * es;
+        const size_t yb = static_cast<size_t>(P.n) * es;
+        constexpr int D = hbdia_matrix::kHostDepth;
+        const int depth = std::min<int32_t>(D, count);
+        for (int d = 0; d < depth; ++d) {
+            if (!m->pipeStream[d]) {
+                cudaStream_t s = nullptr;
+                hbdia::check_cuda(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "cudaStreamCreate(pipeline)");
+                m->pipeStream[d] = s;
+            }
+            if (!m->pipeX[d]) hbdia::check_cuda(cudaMalloc(&m->pipeX[d], xb), "cudaMalloc(pipeline x)");
+            if (!m->pipeY[d]) hbdia::check_cuda(cudaMalloc(&m->pipeY[d], yb), "cudaMalloc(pipeline y)");
+        }
+        // step j on stage j % depth: its copy in, SpMV and copy out are ordered
+        // on that stage's stream (so the stage's buffers are free again when
+        // step j + depth starts), while different stages overlap -- one
+        // step's upload runs beside another's download and kernel
+        std::string err;
+        int status = HBDIA_OK;
+        try {
+            for (int32_t j = 0; j < count; ++j) {
+                const int d = j % depth;
+                cudaStream_t s = static_cast<cudaStream_t>(m->pipeStream[d]);
+                hbdia::check_cuda(cudaMemcpyAsync(m->pipeX[d], xh[j], xb, cudaMemcpyHostToDevice, s),
+                                  "cudaMemcpyAsync(x)");
+                hbdia::launch_spmv(P, m->pipeX[d], m->pipeY[d], s);
+                hbdia::check_cuda(cudaMemcpyAsync(yh[j], m->pipeY[d], yb, cudaMemcpyDeviceToHost, s),
+                                  "cudaMemcpyAsync(y)");
+            }
+        } catch (const hbdia::Error &e) {
+            status = e.status;
+            err = e.what();
+        }
+        for (int d = 0; d < depth; ++d) {  // always drain what was issued
+            const cudaError_t rc = cudaStreamSynchronize(static_cast<cudaStream_t>(m->pipeStream[d]));
+            if (rc != cudaSuccess && status == HBDIA_OK) {
+                status = HBDIA_ERR_CUDA;
+                err = cudaGetErrorString(rc);
+            }
+        }
+        if (status != HBDIA_OK) throw hbdia::Error(status, err);
         throw_if_timeout(read_status(m, true));
     });
 }

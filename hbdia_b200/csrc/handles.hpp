@@ -33,5 +33,8 @@ struct hbdia_matrix {
     int32_t blockWidth = 0, threshold = 0;
     int64_t maxCoo = 0;
     hbdia::PartialMeta part;            // partial matrix (one rank's rows) and its metadata
+    // hbdia_spmv_host_many: device staging pairs and streams of its pipeline
+    static constexpr int kHostDepth = 3;
+    void *pipeX[kHostDepth] = {}, *pipeY[kHostDepth] = {}, *pipeStream[kHostDepth] = {};
     std::mutex hostMu;  // serialises hbdia_spmv_host's scratch buffers
 };

@@ -275,6 +275,17 @@ int hbdia_spmv_list_device(const hbdia_matrix *m, const void *const *x, void *co
  * copies y back and synchronizes.  Page-locked host buffers are fastest. */
 int hbdia_spmv_host(hbdia_matrix *m, const void *xHost, void *yHost);
 
+/* count SpMVs on host buffers, y[j] = A x[j], pipelined three deep: step j's
+ * copy in, SpMV and copy out run in order on one of three streams (with its
+ * own device staging pair, allocated on the first call and kept until the
+ * matrix is destroyed or reconverted), so step j+1's upload overlaps step
+ * j's kernel and download on the two directions of the host link.  Each
+ * y[j] equals hbdia_spmv_host(m, x[j], y[j]) bit for bit; returns when all
+ * are done.  The overlap needs page-locked host buffers.  A y buffer may
+ * appear more than once only at least three steps apart.  No counterpart in
+ * the reference. */
+int hbdia_spmv_host_many(hbdia_matrix *m, const void *const *xHost, void *const *yHost, int32_t count);
+
 /* hbdia_spmv_host without any device allocation.  No counterpart in the
  * reference.  For callers whose device memory belongs to another allocator
  * or budget, where the cudaMalloc that hbdia_spmv_host makes on its first

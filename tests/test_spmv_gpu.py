@@ -329,3 +329,49 @@ def test_pipe_prefetch_knob_bitequal(lib, storage):
     with pytest.raises(ValueError):
         m.setTuning(lib.TUNE_PREFETCH, 2)
     m.setTuning(lib.TUNE_PREFETCH, -1)
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+@pytest.mark.parametrize("count", [1, 2, 5, 8])
+def test_spmv_host_many_equals_host(lib, dtype, count):
+    """The pipelined host form: each y_j equals the single-call host SpMV bit
+    for bit, with page-locked and pageable buffers and a y buffer reused three
+    steps apart."""
+    import torch
+    rng = np.random.default_rng(40 + count)
+    n = 30000
+    rows, cols, vals = random_coo(rng, n, n, 250000)
+    i = np.arange(n, dtype=np.int32)
+    rows = np.concatenate([rows, i, i[1:]]).astype(np.int32)
+    cols = np.concatenate([cols, i, i[:-1]]).astype(np.int32)
+    vals = np.concatenate([vals, rng.uniform(-1, 1, 2 * n - 1)]).astype(dtype)
+    o = np.argsort(rows, kind="stable")
+    m = lib.HBDIA(rows[o], cols[o], vals[o], n, n, dtype=dtype)
+    m.convertToHBDIAFormat(32, 2)
+    tdt = torch.float64 if dtype == np.float64 else torch.float32
+    keep = []
+
+    def pinned(a):
+        t = torch.from_numpy(a).pin_memory()
+        keep.append(t)
+        return t.numpy()
+
+    xs = [rng.uniform(-1, 1, n).astype(dtype) for _ in range(count)]
+    exp = []
+    for x in xs:
+        y = np.zeros(n, dtype)
+        lib.spmv_host(m, x, y)
+        exp.append(y)
+    for pin in (True, False):
+        xin = [pinned(x.copy()) if pin else x.copy() for x in xs]
+        ybufs = [pinned(np.full(n, np.nan, dtype)) if pin else np.full(n, np.nan, dtype) for _ in range(3)]
+        lib.spmv_host_many(m, xin, [ybufs[j % 3] for j in range(count)])
+        for j in range(max(0, count - 3), count):  # the last write of each buffer
+            assert bits_equal(ybufs[j % 3], exp[j]), (pin, j)
+        ys = [np.full(n, np.nan, dtype) for _ in range(count)]
+        lib.spmv_host_many(m, xin, ys)
+        for y, e in zip(ys, exp):
+            assert bits_equal(y, e)
+    lib.spmv_host_many(m, [], [])
+    with pytest.raises(ValueError):
+        lib.spmv_host_many(m, xs[:1], [np.zeros(n - 1, dtype)])
