@@ -499,6 +499,37 @@ def spmv_list_device(matrix: HBDIA, x_ptrs: Sequence[int], y_ptrs: Sequence[int]
     _check(_load().hbdia_spmv_list_device(matrix.handle, xa, ya, k, _stream_arg(stream)))
 
 
+class LayoutPlan:
+    """``hbdia_plan`` over HBDIA device arrays the caller owns (the arrays
+    prepareForGPU leaves on the device).  Pointers are device addresses
+    (ints); ``keep`` holds whatever owns them for the plan's lifetime."""
+
+    def __init__(self, *, dtype=np.float64, storage: int = STORE_NATIVE, numRows: int, numCols: int,
+                 blockWidth: int, numBlocks: int, totalOffsets: int, numCoo: int, values: int, offsets: int,
+                 blockStart: int, cooRow: int = 0, cooCol: int = 0, cooVal: int = 0, cooRowPtr: int = 0,
+                 scales: int = 0, keep=None):
+        d = _lib.LayoutDesc(_dtype_code(dtype), storage, numRows, numCols, blockWidth, numBlocks, totalOffsets,
+                            numCoo, values or None, scales or None, offsets or None, blockStart or None,
+                            cooRow or None, cooCol or None, cooVal or None, cooRowPtr or None)
+        self._h = ctypes.c_void_p()
+        self._keep = keep
+        self.numRows, self.numCols = numRows, numCols
+        _check(_load().hbdia_plan_create(ctypes.byref(d), ctypes.byref(self._h)))
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _load().hbdia_plan_destroy(h)
+            self._h = None
+
+    def spmv(self, x_ptr: int, y_ptr: int, stream: Optional[int] = None) -> None:
+        _check(_load().hbdia_plan_spmv(self._h, ctypes.c_void_p(x_ptr), ctypes.c_void_p(y_ptr), _stream_arg(stream)))
+
+    def spmm(self, X_ptr: int, ldx: int, Y_ptr: int, ldy: int, k: int, stream: Optional[int] = None) -> None:
+        _check(_load().hbdia_plan_spmm(self._h, ctypes.c_void_p(X_ptr), ldx, ctypes.c_void_p(Y_ptr), ldy, k,
+                                       _stream_arg(stream)))
+
+
 def spmv_host_many(matrix: HBDIA, xs: Sequence[np.ndarray], ys: Sequence[np.ndarray]) -> None:
     """y_j = A x_j for host arrays, pipelined so that one step's upload
     overlaps another's download (page-locked arrays for the overlap)."""

@@ -95,6 +95,13 @@ class PartialInfo(ctypes.Structure):
                 ("windowStart", c_i32), ("windowLength", c_i32)]
 
 
+class LayoutDesc(ctypes.Structure):
+    _fields_ = [("dtype", c_i32), ("storage", c_i32), ("numRows", c_i32), ("numCols", c_i32),
+                ("blockWidth", c_i32), ("numBlocks", c_i32), ("totalOffsets", c_i64), ("numCoo", c_i64),
+                ("values", c_vp), ("scales", c_vp), ("offsets", c_vp), ("blockStart", c_vp), ("cooRow", c_vp),
+                ("cooCol", c_vp), ("cooVal", c_vp), ("cooRowPtr", c_vp)]
+
+
 class HBDIACudaError(RuntimeError):
     """A CUDA runtime call inside the library failed."""
 
@@ -198,6 +205,10 @@ _SIGS = [
     ("hbdia_halo_destroy", None, [c_vp]),
     ("hbdia_spmv_list_device", ctypes.c_int, [c_vp, c_vpp, c_vpp, c_i32, c_vp]),
     ("hbdia_spmv_host_many", ctypes.c_int, [c_vp, c_vpp, c_vpp, c_i32]),
+    ("hbdia_plan_create", ctypes.c_int, [ctypes.POINTER(LayoutDesc), c_vpp]),
+    ("hbdia_plan_spmv", ctypes.c_int, [c_vp, c_vp, c_vp, c_vp]),
+    ("hbdia_plan_spmm", ctypes.c_int, [c_vp, c_vp, c_i64, c_vp, c_i64, c_i32, c_vp]),
+    ("hbdia_plan_destroy", None, [c_vp]),
     ("hbdia_server_submit_device", ctypes.c_int, [c_vp, c_i32, c_i32, c_vp, c_vp, ctypes.POINTER(ctypes.c_uint64)]),
 ]
 

@@ -28,6 +28,10 @@ struct hbdia_halo {
     hbdia::Halo *H = nullptr;
 };
 
+struct hbdia_plan {
+    hbdia::DevicePlan P;
+};
+
 namespace {
 
 thread_local std::string g_err;
@@ -1128,4 +1132,34 @@ void hbdia_halo_destroy(hbdia_halo *h) {
     if (!h) return;
     hbdia::halo_free(h->H);
     delete h;
+}
+
+// ---------------------------------------------------- borrowed device layouts
+int hbdia_plan_create(const hbdia_layout_desc *desc, hbdia_plan **out) {
+    return guarded([&] {
+        need(desc && out, HBDIA_ERR_INVALID_ARGUMENT, "null argument");
+        std::unique_ptr<hbdia_plan> p(new hbdia_plan());
+        hbdia::borrow_plan(*desc, p->P);
+        *out = p.release();
+    });
+}
+
+int hbdia_plan_spmv(const hbdia_plan *p, const void *x, void *y, void *stream) {
+    return guarded([&] {
+        need(p != nullptr, HBDIA_ERR_INVALID_ARGUMENT, "null plan");
+        hbdia::launch_spmv(p->P, x, y, stream);
+    });
+}
+
+int hbdia_plan_spmm(const hbdia_plan *p, const void *X, int64_t ldx, void *Y, int64_t ldy, int32_t k, void *stream) {
+    return guarded([&] {
+        need(p != nullptr, HBDIA_ERR_INVALID_ARGUMENT, "null plan");
+        hbdia::launch_spmm(p->P, X, ldx, Y, ldy, k, stream, false);
+    });
+}
+
+void hbdia_plan_destroy(hbdia_plan *p) {
+    if (!p) return;
+    hbdia::free_plan(p->P);
+    delete p;
 }

@@ -169,6 +169,8 @@ struct ColumnWindow {
 
 template <typename T>
 void build_plan(const HostLayout<T> &L, int storage, DevicePlan &P, const ColumnWindow *W = nullptr);
+// A plan over a caller-owned device layout (layout_plan.cu).
+void borrow_plan(const hbdia_layout_desc &d, DevicePlan &P);
 void free_plan(DevicePlan &P);
 // y = A x on `stream` (a cudaStream_t; nullptr -> the plan's stream)
 void launch_spmv(const DevicePlan &P, const void *x, void *y, void *stream);

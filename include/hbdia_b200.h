@@ -286,6 +286,50 @@ int hbdia_spmv_host(hbdia_matrix *m, const void *xHost, void *yHost);
  * the reference. */
 int hbdia_spmv_host_many(hbdia_matrix *m, const void *const *xHost, void *const *yHost, int32_t count);
 
+/* ---- Plans over a device layout the caller owns ------------------------
+ *
+ * The arrays prepareForGPU leaves on the device (src/Format/HBDIA.cpp:720-816),
+ * read through the reference's getters (include/Format/HBDIA.hpp:155-165):
+ *   values      getHBDIADataDevice()          totalOffsets * blockWidth, [block][offsetIdx][lane]
+ *   offsets     getFlattenedOffsetsDevice()   totalOffsets, ascending within each block
+ *   blockStart  getBlockStartIndicesDevice()  numBlocks + 1, offset units
+ *   cooRow, cooCol, cooVal, cooRowPtr         getCpuRowIndicesDevice() ... getCpuRowPtrDevice():
+ *                                             numCoo entries, row-sorted; numRows + 1 row pointer
+ * numBlocks = ceil(min(numRows, numCols) / blockWidth) as convertToHBDIAFormat
+ * makes it.  storage F32 / BF16_SCALED describe float / bfloat16 values of a
+ * double layout (with one float scale per block for BF16: value = stored *
+ * scale). */
+typedef struct hbdia_layout_desc {
+    int32_t dtype;          /* hbdia_dtype of x, y and the COO values            */
+    int32_t storage;        /* hbdia_value_storage of `values`                   */
+    int32_t numRows, numCols, blockWidth, numBlocks;
+    int64_t totalOffsets;   /* = blockStart[numBlocks]                           */
+    int64_t numCoo;         /* COO remainder entries (0: the COO arrays unused)  */
+    const void *values;
+    const float *scales;    /* numBlocks, BF16_SCALED only                       */
+    const int32_t *offsets;
+    const int32_t *blockStart;
+    const int32_t *cooRow, *cooCol;
+    const void *cooVal;
+    const int32_t *cooRowPtr;
+} hbdia_layout_desc;
+typedef struct hbdia_plan hbdia_plan;
+
+/* A plan over the described device arrays, which it BORROWS: they must stay
+ * valid and unchanged until hbdia_plan_destroy.  The arrays are checked on
+ * the device first (block starts, row pointer, COO rows and columns);
+ * HBDIA_ERR_INVALID_ARGUMENT / _OUT_OF_RANGE name what is malformed.  The
+ * plan allocates only its per-tile COO ranges and a status word. */
+int hbdia_plan_create(const hbdia_layout_desc *desc, hbdia_plan **out);
+/* hbdiaSpMV on the plan (the same fused kernels and bit-identical y as
+ * hbdia_spmv_device on the matrix the layout came from); x holds
+ * max(numRows, numCols) elements. */
+int hbdia_plan_spmv(const hbdia_plan *p, const void *x, void *y, void *stream);
+/* Y = A X, row-major blocks (as hbdia_spmm_device). */
+int hbdia_plan_spmm(const hbdia_plan *p, const void *X, int64_t ldx, void *Y, int64_t ldy, int32_t k,
+                    void *stream);
+void hbdia_plan_destroy(hbdia_plan *p);
+
 /* hbdia_spmv_host without any device allocation.  No counterpart in the
  * reference.  For callers whose device memory belongs to another allocator
  * or budget, where the cudaMalloc that hbdia_spmv_host makes on its first
