@@ -242,6 +242,11 @@ class Reference:
         lib.ref_matrix_convert_dia_f64.argtypes = [_vp, ctypes.c_int]
         lib.ref_matrix_dia_sizes_f64.argtypes = [_vp, _vp]
         lib.ref_matrix_export_dia_f64.argtypes = [_vp] * 6
+        lib.ref_gpu_matrix_f64.argtypes = [_vp, _vp, _vp, ctypes.c_int64] + [ctypes.c_int] * 4
+        lib.ref_gpu_matrix_f64.restype = _vp
+        lib.ref_gpu_matrix_arrays_f64.argtypes = [_vp, _i64p, _vp]
+        lib.ref_gpu_matrix_spmv_f64.argtypes = [_vp, _vp, _vp, ctypes.c_int]
+        lib.ref_gpu_matrix_spmv_f64.restype = ctypes.c_int
         lib.ref_partition_f64.argtypes = [_vp, _vp, _vp, ctypes.c_int64] + [ctypes.c_int] * 5
         lib.ref_partition_f64.restype = _vp
         lib.ref_partition_sizes.argtypes = [_vp, _i64p]
@@ -315,6 +320,17 @@ class Reference:
             return _to_layout(a)
         finally:
             getattr(self.lib, f"ref_matrix_destroy_{t}")(h)
+
+    def gpu_matrix(self, rows, cols, vals, num_rows, num_cols, bw, thr) -> "_RefGpuMatrix":
+        """A float64 matrix converted by the reference on the GPU (its
+        prepareForGPU device arrays stay alive with the returned object)."""
+        rows = np.ascontiguousarray(rows, np.int32)
+        cols = np.ascontiguousarray(cols, np.int32)
+        vals = np.ascontiguousarray(vals, np.float64)
+        h = self.lib.ref_gpu_matrix_f64(_ptr(rows), _ptr(cols), _ptr(vals), len(vals), num_rows, num_cols, bw, thr)
+        if not h:
+            raise RuntimeError("reference conversion failed")
+        return _RefGpuMatrix(self, h, num_rows)
 
     def partition(self, rows, cols, vals, n, num_processes, part, bw=32, thr=1) -> dict:
         """One rank's side of BasicDistributor::scatterMatrix / receiveMatrix
@@ -392,6 +408,35 @@ class Reference:
         if rc != 0:
             raise RuntimeError(f"reference hbdiaSpMV failed with {rc}")
         return y
+
+
+class _RefGpuMatrix:
+    def __init__(self, owner: Reference, h, n):
+        self._o, self._h, self.n = owner, h, n
+
+    def arrays(self) -> dict:
+        """numBlocks, totalOffsets, numCoo and the device addresses of its
+        prepareForGPU arrays (getHBDIADataDevice() ... getCpuRowPtrDevice())."""
+        s = np.zeros(3, np.int64)
+        p = (ctypes.c_void_p * 7)()
+        self._o.lib.ref_gpu_matrix_arrays_f64(self._h, s.ctypes.data_as(_i64p), p)
+        names = ("values", "offsets", "blockStart", "cooRow", "cooCol", "cooVal", "cooRowPtr")
+        return {"numBlocks": int(s[0]), "totalOffsets": int(s[1]), "numCoo": int(s[2]),
+                **{k: (v or 0) for k, v in zip(names, p)}}
+
+    def spmv(self, x: np.ndarray, exec_cpu: bool = True) -> np.ndarray:
+        """The reference's own hbdiaSpMV on this matrix."""
+        x = np.ascontiguousarray(x, np.float64)
+        y = np.zeros(self.n, np.float64)
+        rc = self._o.lib.ref_gpu_matrix_spmv_f64(self._h, _ptr(x), _ptr(y), int(exec_cpu))
+        if rc != 0:
+            raise RuntimeError(f"reference hbdiaSpMV failed ({rc})")
+        return y
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            self._o.lib.ref_matrix_destroy_f64(self._h)
+            self._h = None
 
 
 class _RefCoo:

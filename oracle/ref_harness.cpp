@@ -264,6 +264,56 @@ int ref_gpu_spmv_f64(const int *rows, const int *cols, const double *vals, int64
     }
 }
 
+// ---- a matrix converted by the reference on a GPU (convertToHBDIAFormat ends in
+// prepareForGPU for non-partial matrices, src/Format/HBDIA.cpp:715-717): its own
+// device arrays, and its own hbdiaSpMV on them
+void *ref_gpu_matrix_f64(const int *rows, const int *cols, const double *vals, int64_t nnz, int numRows,
+                         int numCols, int bw, int thr) {
+    try {
+        auto *m = new HBDIA<double>(std::vector<int>(rows, rows + nnz), std::vector<int>(cols, cols + nnz),
+                                    std::vector<double>(vals, vals + nnz), numRows, numCols);
+        m->convertToHBDIAFormat(bw, thr);
+        return m;
+    } catch (const std::exception &e) {
+        std::fprintf(stderr, "oracle: reference conversion threw: %s\n", e.what());
+        return nullptr;
+    }
+}
+
+// sizes: numBlocks, totalOffsets, numCoo; ptrs: values, offsets, blockStart, cooRow, cooCol, cooVal, cooRowPtr
+void ref_gpu_matrix_arrays_f64(void *h, int64_t *sizes, const void **ptrs) {
+    const auto *m = static_cast<const HBDIA<double> *>(h);
+    int64_t total = 0;
+    for (const auto &b : m->getOffsetsPerBlock()) total += static_cast<int64_t>(b.size());
+    sizes[0] = m->getNumBlocks();
+    sizes[1] = total;
+    sizes[2] = static_cast<int64_t>(m->getCpuValues().size());
+    ptrs[0] = m->getHBDIADataDevice();
+    ptrs[1] = m->getFlattenedOffsetsDevice();
+    ptrs[2] = m->getBlockStartIndicesDevice();
+    ptrs[3] = m->getCpuRowIndicesDevice();
+    ptrs[4] = m->getCpuColIndicesDevice();
+    ptrs[5] = m->getCpuValuesDevice();
+    ptrs[6] = m->getCpuRowPtrDevice();
+}
+
+int ref_gpu_matrix_spmv_f64(void *h, const double *x, double *y, int execCOOCPU) {
+    try {
+        auto &m = *static_cast<HBDIA<double> *>(h);
+        const int n = m.getNumRows();
+        HBDIAVector<double> vx(std::vector<double>(x, x + n));
+        HBDIAVector<double> vy(std::vector<double>(n, 0.0));
+        hbdiaSpMV<double>(m, vx, vy, execCOOCPU != 0, false);
+        if (cudaDeviceSynchronize() != cudaSuccess) return -3;
+        if (cudaMemcpy(y, vy.getDeviceLocalPtr(), sizeof(double) * n, cudaMemcpyDeviceToHost) != cudaSuccess)
+            return -3;
+        return 0;
+    } catch (const std::exception &e) {
+        std::fprintf(stderr, "oracle: reference hbdiaSpMV threw: %s\n", e.what());
+        return -1;
+    }
+}
+
 // ---- row partitioning, as BasicDistributor::scatterMatrix / receiveMatrix do
 // it for one rank (src/DataExchange/BasicDistributor.cpp:17-146): the
 // extractor's partition, the partial-matrix constructor, convertToHBDIAFormat,

@@ -147,3 +147,23 @@ def test_malformed_layouts_refused(lib):
     plan = _plan(lib, L, n, n, 32)
     x = rng.uniform(-1, 1, n)
     assert np.all(np.isfinite(_run(plan, x, n)))
+
+
+@pytest.mark.parametrize("case", ["stencil", "random"])
+def test_reference_device_arrays(lib, ref, case):
+    """The reference converts on the GPU (its prepareForGPU allocates and fills
+    its device arrays); a plan over THOSE arrays, no copy, gives the same y as
+    the reference's own hbdiaSpMV on them, bit for bit."""
+    rng = np.random.default_rng(8)
+    if case == "stencil":
+        rows, cols, vals, nr, nc = ref.stencil27(16, 16, 16, 0.01, 2)
+    else:
+        nr = nc = 5000
+        rows, cols, vals = random_coo(rng, nr, nc, 60000)
+    g = ref.gpu_matrix(rows, cols, vals, nr, nc, 32, 2)
+    a = g.arrays()
+    assert a["numCoo"] > 0 and a["values"] and a["cooRowPtr"]
+    plan = lib.LayoutPlan(numRows=nr, numCols=nc, blockWidth=32, keep=g, **a)
+    x = rng.uniform(-1, 1, max(nr, nc))
+    assert bits_equal(_run(plan, x, nr), g.spmv(x))
+    del plan
