@@ -1,5 +1,6 @@
 """Benchmark suite for the configurations beside the headline SpMV.
 
+    python -m hbdia_b200.suite small       # 27-point 64^3: launch-bound; separate launches vs one CUDA graph
     python -m hbdia_b200.suite precision   # banded n = 8M, FP64 / FP32 / BF16-scaled value storage
     python -m hbdia_b200.suite spmm        # 7-point Laplacian 128^3, k in {4, 16, 32}, FP64 and FP32 storage
     python -m hbdia_b200.suite cg          # SPD 27-point 128^3: mixed-precision vs plain FP64 CG
@@ -129,6 +130,55 @@ def spmm(args):
                                   "bytes": b, "gbs": b / (t / 1e3) / 1e9,
                                   "frac_of_peak": b / (t / 1e3) / 1e9 / _peak()}), flush=True)
         del m
+
+
+def small(args):
+    """Config 1: the 27-point stencil on 64^3 (centre 26, neighbours -1) with
+    0.5 % extras U(0.1, 1) (seed 0), blockWidth 32, threshold 2, x_i = i + 1.
+    One SpMV is ~61 MB, so a lone launch is launch-bound: timed as separate
+    launches on a stream and as 100 SpMVs replayed from one CUDA graph, and
+    through the host entry points (one call per SpMV; pipelined)."""
+    import time
+    import torch
+    import hbdia_b200 as hb
+    g = args.grid if args.grid != 128 else 64
+    n = g ** 3
+    rows, cols, vals = hb.generate_stencil27(g, g, g, 26.0, -1.0, 0.005, 0.1, 1.0, 0)
+    m = hb.HBDIA(rows, cols, vals, n, n)
+    m.convertToHBDIAFormat(32, 2)
+    b = m.bytesPerSpmv()
+    x = torch.arange(1, n + 1, dtype=torch.float64, device="cuda")
+    y = torch.zeros(n, dtype=torch.float64, device="cuda")
+    stream = torch.cuda.Stream()
+    sp = stream.cuda_stream
+    ms_launch = _time(lambda: hb.spmv_device(m, x.data_ptr(), y.data_ptr(), sp), stream, reps=200)
+    reps = 100
+    gr = torch.cuda.CUDAGraph()
+    with torch.cuda.stream(stream):
+        hb.spmv_device(m, x.data_ptr(), y.data_ptr(), sp)  # warm outside capture
+        torch.cuda.synchronize()
+        with torch.cuda.graph(gr, stream=stream):
+            for _ in range(reps):
+                hb.spmv_device(m, x.data_ptr(), y.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    with torch.cuda.stream(stream):
+        ms_graph = _time(gr.replay, stream, reps=10) / reps
+    xh = torch.arange(1, n + 1, dtype=torch.float64).pin_memory().numpy()
+    yh = [torch.zeros(n, dtype=torch.float64).pin_memory().numpy() for _ in range(3)]
+    hb.spmv_host(m, xh, yh[0])
+    t = time.perf_counter()
+    for _ in range(50):
+        hb.spmv_host(m, xh, yh[0])
+    ms_host = 1e3 * (time.perf_counter() - t) / 50
+    hb.spmv_host_many(m, [xh] * 3, yh)
+    t = time.perf_counter()
+    hb.spmv_host_many(m, [xh] * 60, [yh[j % 3] for j in range(60)])
+    ms_many = 1e3 * (time.perf_counter() - t) / 60
+    for name, ms in (("device, separate launches", ms_launch), ("device, 100 SpMVs in one CUDA graph", ms_graph),
+                     ("host buffers, hbdia_spmv_host per SpMV", ms_host),
+                     ("host buffers, hbdia_spmv_host_many (pipelined)", ms_many)):
+        print(json.dumps({"suite": "small", "workload": f"27-point stencil {g}^3 + 0.5% extras, x_i = i + 1",
+                          "path": name, "ms_per_spmv": ms, "bytes_per_spmv": b, "gbs": b / (ms / 1e3) / 1e9,
+                          "frac_of_peak": b / (ms / 1e3) / 1e9 / _peak()}), flush=True)
 
 
 def cg(args):
@@ -413,7 +463,7 @@ def convert(args):
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("what", choices=["precision", "spmm", "cg", "batched", "serve", "convert"])
+    ap.add_argument("what", choices=["precision", "spmm", "cg", "batched", "serve", "convert", "small"])
     ap.add_argument("--requests", type=int, default=10000)
     ap.add_argument("--matrices", type=int, default=32)
     ap.add_argument("--edge-min", type=int, default=32)
@@ -429,7 +479,7 @@ def main(argv=None):
     import torch
     torch.cuda.set_device(0)
     {"precision": precision, "spmm": spmm, "cg": cg, "batched": batched, "serve": serve,
-     "convert": convert}[args.what](args)
+     "convert": convert, "small": small}[args.what](args)
     return 0
 
 
