@@ -7,6 +7,7 @@
     python -m hbdia_b200.suite batched     # 64 stencils of edge U[16,96]: separate launches vs one batched launch
     python -m hbdia_b200.suite serve       # 32 resident matrices, Poisson arrivals: batched server vs plain FP64
     python -m hbdia_b200.suite convert --grid 256   # host vs GPU converter, COO -> device layout
+    python -m hbdia_b200.suite partition   # 256^3 cut into 2/4/8 row partitions: per-rank SpMV and halo
 
 Each measurement prints one JSON line.  Times are CUDA-event device times on
 a dedicated stream after warm-up; inputs exceed L2 unless stated.  Accuracy
@@ -433,6 +434,67 @@ def serve(args):
         s.close()
 
 
+def partition(args):
+    """Row-partitioned SpMV, measured part by part on one GPU: the bench
+    workload (27-point stencil {grid}^3, 1 % extras, blockWidth 32, threshold 2)
+    cut into P row partitions (P = 2, 4, 8), each with its own x-window plan.
+    Per rank: the window SpMV (CUDA events), the halo it receives from the
+    other ranks (bytes) and the time of the halo-copy kernel that unpacks it
+    (the sender's pack copies the same segments).  The step of a P-GPU run is
+    then modelled -- not measured, one GPU here -- as the slowest rank's pack +
+    unpack + transfer at the measured 770 GB/s per direction per GPU of NVLink
+    5 + SpMV, against the whole matrix's SpMV on one GPU."""
+    import torch
+    import hbdia_b200 as hb
+    from hbdia_b200.distributed import _HaloPlan
+    g = args.grid if args.grid != 128 else 256
+    n = g ** 3
+    r, c, v = hb.generate_stencil27(g, g, g, 26.0, -1.0, 0.01, 0.1, 1.0, 1)
+    x = torch.from_numpy(hb.fill_uniform(n, -1.0, 1.0, 1)).cuda()
+    stream = torch.cuda.Stream()
+    sp = stream.cuda_stream
+    whole = hb.HBDIA(r, c, v, n, n)
+    whole.convertToHBDIAFormat(32, 2)
+    y = torch.zeros(n, dtype=torch.float64, device="cuda")
+    ms_whole = _time(lambda: hb.spmv_device(whole, x.data_ptr(), y.data_ptr(), sp), stream)
+    del whole
+    glob = hb.HBDIA(r, c, v, n, n)
+    link_gbs = 770.0
+    for P in (2, 4, 8):
+        ranks = []
+        for p in range(P):
+            m = glob.partition(P, p)
+            m.convertToHBDIAFormat(32, 2)
+            w0, wl = m.window()
+            win = x[w0:w0 + wl].clone()
+            yl = torch.zeros(m.getNumRows(), dtype=torch.float64, device="cuda")
+            ms = _time(lambda: hb.spmv_device(m, win.data_ptr(), yl.data_ptr(), sp), stream)
+            meta = m.getPartialMatrixMetadata()
+            segs = [(s0, e0) for q, rs in enumerate(meta["processDataRanges"]) if q != p for s0, e0 in rs]
+            total = sum(e0 - s0 for s0, e0 in segs)
+            ms_unpack = 0.0
+            if total:
+                off = np.cumsum([0] + [e0 - s0 for s0, e0 in segs])[:-1]
+                buf = torch.empty(total, dtype=torch.float64, device="cuda")
+                unpack = _HaloPlan(off, [s0 - w0 for s0, _ in segs], [e0 - s0 for s0, e0 in segs], total, wl, 8,
+                                   torch.device("cuda"))
+                with torch.cuda.stream(stream):
+                    ms_unpack = _time(lambda: unpack(buf, win), stream)
+            ranks.append({"rank": p, "rows": m.getNumRows(), "spmv_ms": ms, "halo_bytes": 8 * total,
+                          "halo_segments": len(segs), "unpack_ms": ms_unpack,
+                          "window_rows": wl, "spmv_gbs": m.bytesPerSpmv() / ms / 1e6})
+            del m, win, yl
+        step = max(rk["spmv_ms"] + 2 * rk["unpack_ms"] + rk["halo_bytes"] / (link_gbs * 1e6) for rk in ranks)
+        print(json.dumps({"suite": "partition", "workload": f"27-point stencil {g}^3 + 1% extras, bw 32, thr 2",
+                          "ranks": P, "whole_matrix_spmv_ms": ms_whole,
+                          "max_rank_spmv_ms": max(rk["spmv_ms"] for rk in ranks),
+                          "max_halo_bytes": max(rk["halo_bytes"] for rk in ranks),
+                          "max_halo_segments": max(rk["halo_segments"] for rk in ranks),
+                          "max_unpack_ms": max(rk["unpack_ms"] for rk in ranks),
+                          "modelled_step_ms": step, "modelled_speedup": ms_whole / step,
+                          "per_rank": ranks}), flush=True)
+
+
 def convert(args):
     """convertToHBDIAFormat + prepareForGPU on the host (OpenMP, all cores)
     against the GPU converter, on the bench workload (27-point stencil
@@ -463,7 +525,7 @@ def convert(args):
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("what", choices=["precision", "spmm", "cg", "batched", "serve", "convert", "small"])
+    ap.add_argument("what", choices=["precision", "spmm", "cg", "batched", "serve", "convert", "small", "partition"])
     ap.add_argument("--requests", type=int, default=10000)
     ap.add_argument("--matrices", type=int, default=32)
     ap.add_argument("--edge-min", type=int, default=32)
@@ -479,7 +541,7 @@ def main(argv=None):
     import torch
     torch.cuda.set_device(0)
     {"precision": precision, "spmm": spmm, "cg": cg, "batched": batched, "serve": serve,
-     "convert": convert, "small": small}[args.what](args)
+     "convert": convert, "small": small, "partition": partition}[args.what](args)
     return 0
 
 
