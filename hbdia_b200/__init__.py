@@ -18,7 +18,7 @@ from typing import List, Optional, Sequence
 import numpy as np
 
 from . import _lib
-from ._lib import (BATCH_CONCURRENT, BATCH_QUEUE, REQ_CG, REQ_SPMV, KERNEL_AUTO, KERNEL_PIPE, KERNEL_ROWWISE, KERNEL_STAGED, KERNEL_WARP, TUNE_PREFETCH, TUNE_SPMM_TILE,
+from ._lib import (BATCH_CONCURRENT, BATCH_QUEUE, REQ_CG, REQ_SPMV, KERNEL_AUTO, KERNEL_PIPE, KERNEL_ROWWISE, KERNEL_STAGED, KERNEL_WARP, TUNE_PREFETCH, TUNE_SPMM_TILE, TUNE_TAIL,
                    TUNE_UNROLL, HBDIACudaError,
                    HBDIADeviceTimeout, STORE_BF16_SCALED, STORE_F32, STORE_NATIVE, MatrixInfo,
                    check as _check, load as _load)

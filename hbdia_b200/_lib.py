@@ -27,7 +27,7 @@ HBDIA_ERR_UNSUPPORTED = -7
 HBDIA_ERR_DEVICE_TIMEOUT = -8
 
 KERNEL_AUTO, KERNEL_ROWWISE, KERNEL_WARP, KERNEL_STAGED, KERNEL_PIPE = 0, 1, 2, 3, 4
-TUNE_UNROLL, TUNE_SPMM_TILE, TUNE_PREFETCH = 1, 2, 3
+TUNE_UNROLL, TUNE_SPMM_TILE, TUNE_PREFETCH, TUNE_TAIL = 1, 2, 3, 4
 
 HBDIA_F64, HBDIA_F32 = 0, 1
 BATCH_CONCURRENT, BATCH_QUEUE = 0, 1

@@ -554,6 +554,11 @@ int hbdia_matrix_set_tuning(hbdia_matrix *m, int32_t key, int32_t value) {
             m->plan.prefetchL2 = value;
             return;
         }
+        if (key == HBDIA_TUNE_TAIL) {
+            need(value >= -1 && value <= 1, HBDIA_ERR_INVALID_ARGUMENT, "tail must be -1, 0 or 1");
+            m->plan.maskedTail = value;
+            return;
+        }
         if (key == HBDIA_TUNE_SPMM_TILE) {
             need(value == 0 || value == 2 || value == 4 || value == 8 || value == 16 || value == 32,
                  HBDIA_ERR_INVALID_ARGUMENT, "SpMM tile must be 0, 2, 4, 8, 16 or 32");

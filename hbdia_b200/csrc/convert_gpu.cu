@@ -544,6 +544,7 @@ void convert_on_device(const Coo<T> &coo, int32_t bw, int32_t thr, int64_t maxCo
     if (Q.scale) bytes += 4 * static_cast<int64_t>(nb);
     if (Q.nCoo > 0) bytes += bw == 32 ? 4 * (static_cast<int64_t>(Q.numTiles) + 1) : 4 * (static_cast<int64_t>(nR) + 1);
     Q.bytesPerSpmv = bytes;
+    Q.tailHeavy = tail_heavy(meta.histBlocks);
     P = Q;
 }
 

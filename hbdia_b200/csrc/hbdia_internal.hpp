@@ -141,6 +141,9 @@ struct DevicePlan {
     int32_t spmmTileForced = 0;          // HBDIA_TUNE_SPMM_TILE (0: autotuned / default)
     int32_t prefetchL2 = -1;             // HBDIA_TUNE_PREFETCH: pipe kernel L2 prefetch of the next
                                          // tile (-1: when x exceeds L2, 0: off, 1: on)
+    int32_t maskedTail = -1;             // HBDIA_TUNE_TAIL: the pipe kernel's offsets past its last full
+                                         // group in masked groups (-1: when tailHeavy, 0: off, 1: on)
+    bool tailHeavy = false;              // at least half the stored offsets lie past full groups
 };
 
 // Host-side facts of a layout built on the device (convert_gpu.cu).
@@ -172,6 +175,9 @@ void build_plan(const HostLayout<T> &L, int storage, DevicePlan &P, const Column
 // A plan over a caller-owned device layout (layout_plan.cu).
 void borrow_plan(const hbdia_layout_desc &d, DevicePlan &P);
 void free_plan(DevicePlan &P);
+// True when at least half of the stored offsets fall past the last full group
+// of the pipe kernel (histBlocks[d] = blocks with d offsets).
+bool tail_heavy(const std::vector<int32_t> &histBlocks);
 // y = A x on `stream` (a cudaStream_t; nullptr -> the plan's stream)
 void launch_spmv(const DevicePlan &P, const void *x, void *y, void *stream);
 // Y = A X for k right-hand sides: row-major blocks (element (i, j) at

@@ -50,6 +50,17 @@ size_t storage_bytes(int storage, int dtype) {
 
 }  // namespace
 
+bool tail_heavy(const std::vector<int32_t> &hist) {
+    // a block's offsets go in chunks of 32, each in groups of kUnroll
+    int64_t tail = 0, total = 0;
+    for (size_t d = 0; d < hist.size(); ++d) {
+        const int64_t dd = static_cast<int64_t>(d);
+        tail += hist[d] * ((dd / 32) * (32 % kUnroll) + (dd % 32) % kUnroll);
+        total += hist[d] * dd;
+    }
+    return total > 0 && 2 * tail >= total;
+}
+
 void free_plan(DevicePlan &P) {
     if (P.stream) {
         cudaStreamSynchronize(static_cast<cudaStream_t>(P.stream));
@@ -69,6 +80,8 @@ void build_plan(const HostLayout<T> &L, int storage, DevicePlan &P, const Column
     Q.skipChunk = P.skipChunk;
     Q.unroll = P.unroll;
     Q.prefetchL2 = P.prefetchL2;
+    Q.maskedTail = P.maskedTail;
+    Q.tailHeavy = tail_heavy(L.histBlocks);
     free_plan(P);
     Q.dtype = std::is_same<T, float>::value ? HBDIA_F32 : HBDIA_F64;
     if (storage != HBDIA_STORE_NATIVE && Q.dtype != HBDIA_F64)
@@ -294,6 +307,10 @@ void launch_pipe_tuned(const DevicePlan &P, const dev::SpmvArgs<VT, XT> &a, cons
         check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
         check_cuda(cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, dev), "cudaDeviceGetAttribute(L2)");
         pf = static_cast<int64_t>(std::max(P.n, P.numCols)) * static_cast<int64_t>(sizeof(XT)) > l2;
+    }
+    if (P.unroll != 27 && (P.maskedTail > 0 || (P.maskedTail < 0 && P.tailHeavy))) {
+        if (pf) return launch_pipe(dev::spmv_bw32_pipe<VT, XT, kUnroll, true, true>, a, P.numTiles, x, y, s);
+        return launch_pipe(dev::spmv_bw32_pipe<VT, XT, kUnroll, false, true>, a, P.numTiles, x, y, s);
     }
     if (pf) {
         if (P.unroll == 27) return launch_pipe(dev::spmv_bw32_pipe<VT, XT, 27, true>, a, P.numTiles, x, y, s);

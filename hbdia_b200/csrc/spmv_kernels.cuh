@@ -235,7 +235,9 @@ __device__ __forceinline__ void prefetch_l2_bulk(const void *p, uint32_t bytes) 
 
 // PF: one lane also asks L2 for tile t+W's value rows (up to 32 KB) while tile
 // t is computed, so its value loads find them in L2.
-template <typename VT, typename XT, int U, bool PF = false>
+// MT: the offsets after the last full group of U run as masked groups of 4
+// (their loads in flight together) instead of one at a time.
+template <typename VT, typename XT, int U, bool PF = false, bool MT = false>
 __global__ void __launch_bounds__(256)
 spmv_bw32_pipe(const SpmvArgs<VT, XT> a, const XT *__restrict__ x, XT *__restrict__ y) {
     const int lane = threadIdx.x & 31;
@@ -300,10 +302,37 @@ spmv_bw32_pipe(const SpmvArgs<VT, XT> a, const XT *__restrict__ x, XT *__restric
                     if (ok[u] && vv != XT(0)) sum = fma_rn(vv, xv[u], sum);
                 }
             }
-            for (; j < cnt; ++j) {
-                const int32_t col = row + __shfl_sync(kFull, myoff, j);
-                const XT vv = widen<XT>(ld_stream(vp + j * 32), s);
-                if (static_cast<uint32_t>(col) < n && vv != XT(0)) sum = fma_rn(vv, __ldg(x + col), sum);
+            if (MT) {
+                // the last cnt - j < U offsets in masked groups of 4 (loads in flight together)
+                for (; j < cnt; j += 4) {
+                    const int rem = cnt - j;
+                    VT v[4];
+                    XT xv[4];
+                    bool ok[4];
+                    int32_t col[4];
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        const bool in = u < rem;  // warp-uniform
+                        col[u] = row + __shfl_sync(kFull, myoff, in ? j + u : j);
+                        ok[u] = in && static_cast<uint32_t>(col[u]) < n;
+                        v[u] = in ? ld_stream(vp + (j + u) * 32) : VT(0);
+                        xv[u] = XT(0);
+                    }
+#pragma unroll
+                    for (int u = 0; u < 4; ++u)
+                        if (ok[u]) xv[u] = __ldg(x + col[u]);
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        const XT vv = widen<XT>(v[u], s);
+                        if (ok[u] && vv != XT(0)) sum = fma_rn(vv, xv[u], sum);
+                    }
+                }
+            } else {
+                for (; j < cnt; ++j) {
+                    const int32_t col = row + __shfl_sync(kFull, myoff, j);
+                    const XT vv = widen<XT>(ld_stream(vp + j * 32), s);
+                    if (static_cast<uint32_t>(col) < n && vv != XT(0)) sum = fma_rn(vv, __ldg(x + col), sum);
+                }
             }
         }
         // next tile's first offsets (its pointers arrived during this tile)

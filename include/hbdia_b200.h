@@ -367,11 +367,19 @@ int hbdia_matrix_selected_kernel(const hbdia_matrix *m, const void *x, int32_t *
  * tile's value rows while computing the current one (bulk L2 prefetch),
  * 0 = off, -1 (default) = on when the x vector is larger than the GPU's L2.
  * Measured on B200: with a 134 MB x, FP64 +1.5 % and FP32 storage +8 %; with
- * x in L2 (57 MB and below) -2 to -10 %, as the prefetched rows evict x. */
+ * x in L2 (57 MB and below) -2 to -10 %, as the prefetched rows evict x.
+ * HBDIA_TUNE_TAIL: the pipelined kernel takes a block's offsets in groups of
+ * 9 (all loads of a group in flight); 1 = the offsets past the last full
+ * group go in masked groups of 4 instead of one at a time, 0 = one at a time,
+ * -1 (default) = masked when at least half of the stored offsets lie past
+ * full groups (e.g. 7-point stencils: 7 offsets per block).  Measured on
+ * B200: 7-point stencil +13-20 % (FP64), +40-49 % (FP32 storage); the masked
+ * form costs 80 registers in FP64 and 14-26 % where there is no tail. */
 typedef enum hbdia_tuning_key {
     HBDIA_TUNE_UNROLL = 1,
     HBDIA_TUNE_SPMM_TILE = 2,
-    HBDIA_TUNE_PREFETCH = 3
+    HBDIA_TUNE_PREFETCH = 3,
+    HBDIA_TUNE_TAIL = 4
 } hbdia_tuning_key;
 int hbdia_matrix_set_tuning(hbdia_matrix *m, int32_t key, int32_t value);
 

@@ -316,9 +316,10 @@ def test_pipe_prefetch_knob_bitequal(lib, storage):
     m.setKernel(lib.KERNEL_PIPE)
     x = torch.from_numpy(rng.uniform(-1, 1, n)).cuda()
     out = []
-    for unroll in (0, 27):
+    for unroll, tail in ((0, -1), (0, 1), (0, 0), (27, -1)):
         for pf in (1, 0, -1):
             m.setTuning(lib.TUNE_UNROLL, unroll)
+            m.setTuning(lib.TUNE_TAIL, tail)
             m.setTuning(lib.TUNE_PREFETCH, pf)
             y = torch.full((n,), float("nan"), dtype=torch.float64, device="cuda")
             lib.spmv_device(m, x.data_ptr(), y.data_ptr(), 0)
