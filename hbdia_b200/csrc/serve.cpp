@@ -3,16 +3,17 @@
 //
 // Requests come from any host thread (hbdia_server_submit) and complete in
 // the background (hbdia_server_wait).  Two kinds:
-//  * SpMV: y = A x.  A scheduler thread serves them in steps.  With batching
-//    on, a step takes every pending request (up to maxRhs per matrix, oldest
-//    first; the rest wait for the next step): the requests of one matrix
-//    become one column-major SpMM -- each x copied straight into its column
-//    of the matrix's staging block, each y copied straight out of its column
-//    -- so the matrix's values cross HBM once for all of them, and the
-//    matrices of a step run concurrently on a ring of streams.  Requests
-//    that arrive during a step join the next one.  With batching off, one
-//    request per launch in arrival order (the plain form it is measured
-//    against).
+//  * SpMV: y = A x.  Each resident matrix has its own queue and its own
+//    stream.  Whenever a matrix has pending requests and fewer than
+//    maxInFlight batches running, the scheduler thread takes up to maxRhs of
+//    them (oldest first; with batching off, one) and issues them as one SpMM
+//    -- device vectors as a vector-list SpMM read and written in place, host
+//    vectors through the matrix's column-major staging block -- so the
+//    matrix's values cross HBM once for all of them.  A completer thread
+//    completes a batch the moment the event behind its work fires, so a
+//    request waits only for its own matrix, never for a global step; requests that arrive while a batch runs form the next one
+//    (continuous batching).  With batching off, one request per launch (the
+//    plain form it is measured against).
 //  * CG: solve A y = x to a relative residual, by the mixed-precision CG of
 //    cg.cu on one of cgWorkers worker threads (own stream, own workspace).
 // x and y are host buffers (hbdia_server_submit: copied in and out on the
@@ -50,7 +51,6 @@ namespace hbdia {
 
 namespace {
 
-constexpr int kSpmvStreams = 16;
 
 struct ServedMatrix {
     DevicePlan p64;   // FP64 values: CG outer residual; SpMVs when spmvStorage is NATIVE
@@ -58,6 +58,9 @@ struct ServedMatrix {
     int32_t n = 0, rowsX = 0;
     double *X = nullptr, *Y = nullptr;  // column-major staging blocks, maxRhs columns
     int64_t bytes = 0;
+    cudaStream_t stream = nullptr;      // this matrix's SpMV batches, in order
+    std::deque<struct Request *> pending;  // SpMV requests not yet issued (server lock)
+    int32_t inFlight = 0;               // batches issued and not completed (server lock)
     const DevicePlan &spmvPlan(int32_t storage) const { return storage == HBDIA_STORE_NATIVE ? p64 : pLow; }
     const DevicePlan &cgInner(int32_t storage) const { return storage == HBDIA_STORE_NATIVE ? p64 : pLow; }
 };
@@ -73,6 +76,13 @@ struct Request {
     bool done = false;
 };
 
+// An SpMV batch in flight: its requests and the event recorded behind its work.
+struct SpmvBatch {
+    ServedMatrix *M = nullptr;
+    std::vector<Request *> reqs;
+    cudaEvent_t done = nullptr;
+};
+
 double now_since(std::chrono::steady_clock::time_point t0) {
     return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 }
@@ -84,18 +94,20 @@ struct Server {
     int device = 0;
     std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
     std::mutex mu;
-    std::condition_variable cvWork, cvDone, cvCg;
+    std::condition_variable cvWork, cvDone, cvCg, cvActive;
     std::vector<std::unique_ptr<ServedMatrix>> mats;
     int64_t used = 0;  // device bytes held
     int32_t maxN = 0;
     std::unordered_map<uint64_t, std::unique_ptr<Request>> reqs;
-    std::deque<Request *> spmvQ, cgQ;
+    std::deque<Request *> cgQ;
+    int64_t spmvPending = 0;  // SpMV requests queued on the matrices
     uint64_t nextTicket = 1;
     bool stop = false;
     bool paused = false;  // requests queue up; no step or solve starts
     hbdia_server_stats stats{};
-    std::vector<cudaStream_t> streams;
-    std::thread sched;
+    std::thread sched, completerThread;
+    std::vector<SpmvBatch> active;  // issued batches not yet taken by the completer
+    bool schedDone = false;
     std::vector<std::thread> cgThreads;
 };
 
@@ -112,100 +124,150 @@ void complete(Server *S, const std::vector<Request *> &rs, int status, double fi
     S->cvDone.notify_all();
 }
 
-// One scheduler step: the requests in `step`, grouped by matrix in order of
-// first arrival.
-void serve_step(Server *S, std::vector<Request *> &step) {
-    std::vector<int32_t> order;
-    std::map<int32_t, std::vector<Request *>> groups;
-    for (Request *r : step) {
-        auto &g = groups[r->matrix];
-        if (g.empty()) order.push_back(r->matrix);
-        g.push_back(r);
-    }
+// Issues one matrix's batch on its stream and hands it to the completer.
+void issue_batch(Server *S, ServedMatrix *M, std::vector<Request *> &reqs) {
     const double started = now_since(S->t0);
-    int status = HBDIA_OK;
-    std::string err;
-    size_t used = 0;
+    cudaStream_t st = M->stream;
     try {
-        for (size_t gi = 0; gi < order.size(); ++gi) {
-            const int32_t mid = order[gi];
-            auto &g = groups[mid];
-            const ServedMatrix &M = *g[0]->m;
-            cudaStream_t st = S->streams[gi % S->streams.size()];
-            used = std::min(S->streams.size(), std::max(used, gi + 1));  // streams of the ring in use
-            const DevicePlan &P = M.spmvPlan(S->opt.spmvStorage);
-            std::vector<Request *> host;
-            std::vector<const void *> dx;
-            std::vector<void *> dy;
-            for (Request *r : g) {
-                r->info.started = started;
-                if (r->device) {
-                    dx.push_back(r->x);
-                    dy.push_back(r->y);
-                } else {
-                    host.push_back(r);
-                }
+        const DevicePlan &P = M->spmvPlan(S->opt.spmvStorage);
+        std::vector<Request *> host;
+        std::vector<const void *> dx;
+        std::vector<void *> dy;
+        for (Request *r : reqs) {
+            r->info.started = started;
+            r->info.status = HBDIA_OK;
+            if (r->device) {
+                dx.push_back(r->x);
+                dy.push_back(r->y);
+            } else {
+                host.push_back(r);
             }
-            for (Request *r : g) r->info.batchRhs = static_cast<int32_t>(r->device ? dx.size() : host.size());
-            // device requests: one vector-list SpMM, in place
-            if (dx.size() == 1) launch_spmv(P, dx[0], dy[0], st);
-            else if (!dx.empty()) launch_spmv_list(P, dx.data(), dy.data(), static_cast<int32_t>(dx.size()), st);
-            // host requests: through the staging block
-            const int32_t k = static_cast<int32_t>(host.size());
-            const size_t xb = static_cast<size_t>(M.rowsX) * sizeof(double);
-            const size_t yb = static_cast<size_t>(M.n) * sizeof(double);
-            for (int32_t j = 0; j < k; ++j)
-                check_cuda(cudaMemcpyAsync(M.X + static_cast<int64_t>(j) * M.rowsX, host[j]->x, xb,
-                                           cudaMemcpyHostToDevice, st), "cudaMemcpyAsync(request x)");
-            if (k == 1) launch_spmv(P, M.X, M.Y, st);
-            else if (k > 1) launch_spmm(P, M.X, M.rowsX, M.Y, M.n, k, st, true);
-            for (int32_t j = 0; j < k; ++j)
-                check_cuda(cudaMemcpyAsync(host[j]->y, M.Y + static_cast<int64_t>(j) * M.n, yb,
-                                           cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync(request y)");
         }
+        for (Request *r : reqs) r->info.batchRhs = static_cast<int32_t>(r->device ? dx.size() : host.size());
+        // device requests: one vector-list SpMM, in place
+        if (dx.size() == 1) launch_spmv(P, dx[0], dy[0], st);
+        else if (!dx.empty()) launch_spmv_list(P, dx.data(), dy.data(), static_cast<int32_t>(dx.size()), st);
+        // host requests: through the staging block
+        const int32_t k = static_cast<int32_t>(host.size());
+        const size_t xb = static_cast<size_t>(M->rowsX) * sizeof(double);
+        const size_t yb = static_cast<size_t>(M->n) * sizeof(double);
+        for (int32_t j = 0; j < k; ++j)
+            check_cuda(cudaMemcpyAsync(M->X + static_cast<int64_t>(j) * M->rowsX, host[j]->x, xb,
+                                       cudaMemcpyHostToDevice, st), "cudaMemcpyAsync(request x)");
+        if (k == 1) launch_spmv(P, M->X, M->Y, st);
+        else if (k > 1) launch_spmm(P, M->X, M->rowsX, M->Y, M->n, k, st, true);
+        for (int32_t j = 0; j < k; ++j)
+            check_cuda(cudaMemcpyAsync(host[j]->y, M->Y + static_cast<int64_t>(j) * M->n, yb,
+                                       cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync(request y)");
+        SpmvBatch b;
+        b.M = M;
+        b.reqs = reqs;
+        check_cuda(cudaEventCreateWithFlags(&b.done, cudaEventDisableTiming), "cudaEventCreate(batch)");
+        const cudaError_t rc = cudaEventRecord(b.done, st);
+        if (rc != cudaSuccess) {
+            cudaEventDestroy(b.done);
+            check_cuda(rc, "cudaEventRecord(batch)");
+        }
+        {
+            std::lock_guard<std::mutex> lk(S->mu);
+            S->active.push_back(std::move(b));
+        }
+        S->cvActive.notify_one();
     } catch (const Error &e) {
-        status = e.status;
-        err = e.what();
+        cudaStreamSynchronize(st);  // nothing issued may still touch the request buffers
+        complete(S, reqs, e.status, now_since(S->t0));
+        {
+            std::lock_guard<std::mutex> lk(S->mu);
+            M->inFlight -= 1;
+        }
+        S->cvWork.notify_all();
     }
-    for (size_t j = 0; j < used; ++j) {
-        const cudaError_t rc = cudaStreamSynchronize(S->streams[j]);
-        if (rc != cudaSuccess && status == HBDIA_OK) status = HBDIA_ERR_CUDA;
-    }
-    {
-        std::lock_guard<std::mutex> lk(S->mu);
-        S->stats.spmvSteps += 1;
-        S->stats.spmvLaunches += static_cast<int64_t>(order.size());
-    }
-    complete(S, step, status, now_since(S->t0));
 }
 
+// Forms per-matrix batches whenever a matrix with pending requests has a
+// free slot, and issues them.
 void scheduler(Server *S) {
     cudaSetDevice(S->device);
+    const int32_t perBatch = S->opt.batching ? S->opt.maxRhs : 1;
     for (;;) {
-        std::vector<Request *> step;
+        std::vector<std::pair<ServedMatrix *, std::vector<Request *>>> batches;
         {
             std::unique_lock<std::mutex> lk(S->mu);
-            S->cvWork.wait(lk, [&] { return S->stop || (!S->paused && !S->spmvQ.empty()); });
-            if (S->spmvQ.empty()) return;  // stopping and drained
-            if (!S->opt.batching) {
-                step.push_back(S->spmvQ.front());
-                S->spmvQ.pop_front();
-            } else {
-                std::map<int32_t, int32_t> taken;
-                std::deque<Request *> rest;
-                for (Request *r : S->spmvQ) {
-                    int32_t &c = taken[r->matrix];
-                    if (c < S->opt.maxRhs) {
-                        ++c;
-                        step.push_back(r);
-                    } else {
-                        rest.push_back(r);
-                    }
-                }
-                S->spmvQ.swap(rest);
+            auto ready = [&] {
+                if (S->spmvPending == 0) return false;
+                if (S->paused && !S->stop) return false;  // stopping drains even while paused
+                for (auto &m : S->mats)
+                    if (!m->pending.empty() && m->inFlight < S->opt.maxInFlight) return true;
+                return false;
+            };
+            S->cvWork.wait(lk, [&] { return (S->stop && S->spmvPending == 0) || ready(); });
+            if (S->spmvPending == 0) {  // stopping and drained
+                S->schedDone = true;
+                S->cvActive.notify_all();
+                return;
             }
+            for (auto &m : S->mats) {
+                if (m->pending.empty() || m->inFlight >= S->opt.maxInFlight) continue;
+                std::vector<Request *> b;
+                while (!m->pending.empty() && static_cast<int32_t>(b.size()) < perBatch) {
+                    b.push_back(m->pending.front());
+                    m->pending.pop_front();
+                }
+                S->spmvPending -= static_cast<int64_t>(b.size());
+                m->inFlight += 1;
+                batches.emplace_back(m.get(), std::move(b));
+            }
+            S->stats.spmvSteps += 1;
+            S->stats.spmvLaunches += static_cast<int64_t>(batches.size());
         }
-        serve_step(S, step);
+        for (auto &b : batches) issue_batch(S, b.first, b.second);
+    }
+}
+
+// Completes batches the moment their events fire, in whatever order the
+// matrices finish: polls the events of the batches in flight (yielding between
+// passes) and sleeps while none is in flight.
+void completer(Server *S) {
+    cudaSetDevice(S->device);
+    std::vector<SpmvBatch> mine;
+    for (;;) {
+        {
+            std::unique_lock<std::mutex> lk(S->mu);
+            S->cvActive.wait(lk, [&] { return !S->active.empty() || !mine.empty() || S->schedDone; });
+            for (auto &b : S->active) mine.push_back(std::move(b));
+            S->active.clear();
+            if (mine.empty() && S->schedDone) return;
+        }
+        bool any = false;
+        for (size_t k = 0; k < mine.size();) {
+            const cudaError_t q = cudaEventQuery(mine[k].done);
+            if (q == cudaErrorNotReady) {
+                ++k;
+                continue;
+            }
+            const int status = q == cudaSuccess ? HBDIA_OK : HBDIA_ERR_CUDA;
+            cudaEventDestroy(mine[k].done);
+            const double t = now_since(S->t0);
+            {
+                std::lock_guard<std::mutex> lk(S->mu);
+                for (Request *r : mine[k].reqs) {
+                    r->info.status = status;
+                    r->info.finished = t;
+                    r->done = true;
+                    S->stats.completed += 1;
+                }
+                mine[k].M->inFlight -= 1;
+            }
+            mine[k] = std::move(mine.back());
+            mine.pop_back();
+            any = true;
+        }
+        if (any) {
+            S->cvDone.notify_all();
+            S->cvWork.notify_all();  // those matrices may take their next batch
+        } else {
+            std::this_thread::yield();
+        }
     }
 }
 
@@ -270,7 +332,9 @@ void free_matrix(ServedMatrix &M) {
     free_plan(M.pLow);
     if (M.X) cudaFree(M.X);
     if (M.Y) cudaFree(M.Y);
+    if (M.stream) cudaStreamDestroy(M.stream);
     M.X = M.Y = nullptr;
+    M.stream = nullptr;
 }
 
 }  // namespace
@@ -288,11 +352,13 @@ void server_default_options(hbdia_server_options *o) {
     o->cgMaxOuter = 50;
     o->cgMaxInner = 5000;
     o->cgCheckEvery = 10;
+    o->maxInFlight = 1;
 }
 
 Server *server_create(const hbdia_server_options &o) {
     if (o.memoryBudget <= 0 || o.maxRhs < 1 || o.maxRhs > 64 || o.cgWorkers < 1 || o.cgWorkers > 64 ||
-        o.cgTol <= 0 || o.cgInnerTol <= 0 || o.cgMaxOuter < 1 || o.cgMaxInner < 1 || o.cgCheckEvery < 1)
+        o.cgTol <= 0 || o.cgInnerTol <= 0 || o.cgMaxOuter < 1 || o.cgMaxInner < 1 || o.cgCheckEvery < 1 ||
+        o.maxInFlight < 1 || o.maxInFlight > 8)
         throw Error(HBDIA_ERR_INVALID_ARGUMENT, "bad server options");
     for (int32_t st : {o.spmvStorage, o.cgInnerStorage})
         if (st != HBDIA_STORE_NATIVE && st != HBDIA_STORE_F32 && st != HBDIA_STORE_BF16_SCALED)
@@ -303,13 +369,9 @@ Server *server_create(const hbdia_server_options &o) {
     auto S = std::make_unique<Server>();
     S->opt = o;
     check_cuda(cudaGetDevice(&S->device), "cudaGetDevice");
-    for (int i = 0; i < kSpmvStreams; ++i) {
-        cudaStream_t st = nullptr;
-        check_cuda(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "cudaStreamCreate(server)");
-        S->streams.push_back(st);
-    }
     Server *raw = S.get();
     S->sched = std::thread(scheduler, raw);
+    S->completerThread = std::thread(completer, raw);
     for (int32_t i = 0; i < o.cgWorkers; ++i) S->cgThreads.emplace_back(cg_worker, raw);
     return S.release();
 }
@@ -323,9 +385,10 @@ void server_destroy(Server *S) {
     S->cvWork.notify_all();
     S->cvCg.notify_all();
     if (S->sched.joinable()) S->sched.join();
+    S->cvActive.notify_all();
+    if (S->completerThread.joinable()) S->completerThread.join();
     for (auto &t : S->cgThreads)
         if (t.joinable()) t.join();
-    for (cudaStream_t st : S->streams) cudaStreamDestroy(st);
     for (auto &m : S->mats) free_matrix(*m);
     delete S;
 }
@@ -362,6 +425,7 @@ int32_t server_add_matrix(Server *S, const hbdia_matrix *m) {
                    "cudaMalloc(server staging x)");
         check_cuda(cudaMalloc(&M->Y, sizeof(double) * static_cast<size_t>(S->opt.maxRhs) * M->n),
                    "cudaMalloc(server staging y)");
+        check_cuda(cudaStreamCreateWithFlags(&M->stream, cudaStreamNonBlocking), "cudaStreamCreate(server)");
         std::lock_guard<std::mutex> lk(S->mu);
         S->used += M->bytes + cgGrow;
         S->maxN = std::max(S->maxN, M->n);
@@ -396,7 +460,8 @@ uint64_t server_submit(Server *S, int32_t matrix, int32_t kind, const double *x,
     Request *raw = r.get();
     S->reqs.emplace(raw->ticket, std::move(r));
     if (kind == HBDIA_REQ_SPMV) {
-        S->spmvQ.push_back(raw);
+        S->mats[matrix]->pending.push_back(raw);
+        S->spmvPending += 1;
         S->stats.spmvRequests += 1;
         S->cvWork.notify_one();
     } else {

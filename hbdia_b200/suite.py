@@ -352,12 +352,14 @@ def serve(args):
       * batched: continuous batching, FP32-stored values (FP64 accumulation),
         mixed-precision CG (FP32 inner, FP64 refinement), 4 CG solvers;
       * plain: FP64 values, one request per launch, plain FP64 CG, 1 solver.
+    (--serial-too adds the batched server with two batches per matrix in flight.)
     Each is first driven closed-loop (all requests queued, then released) to
-    measure its capacity, then open-loop with Poisson arrivals at
-    `--load` x its capacity, and the plain one also at the batched one's
-    rate when it can carry it.  Latency = completion - submission, measured
-    by the server's clock.  Output buffers are shared round-robin (results
-    are checked by the tests, not here)."""
+    measure its capacity; then every server takes the same open-loop Poisson
+    arrivals at each of --loads x the batched server's capacity, and reports
+    its completed rate beside the offered one (below it: saturated, the queue
+    grows over the run) with p50 / p99 latency = completion - submission on
+    the server's clock.  Output buffers are picked per request on its matrix
+    (results are checked by the tests, not here)."""
     import torch
     import hbdia_b200 as hb
     edges = np.random.default_rng(5).integers(args.edge_min, args.edge_max + 1, args.matrices)
@@ -394,6 +396,8 @@ def serve(args):
         "plain": hb.Server(batching=0, spmvStorage=hb.STORE_NATIVE, cgInnerStorage=hb.STORE_NATIVE,
                            cgInnerTol=1e-11, cgWorkers=1),
     }
+    if args.serial_too:
+        servers["batched, 2 batches in flight"] = hb.Server(maxInFlight=2)
     ids = {k: [s.add_matrix(m) for m in mats] for k, s in servers.items()}
     del mats
     rows = int(sum(ns))
@@ -405,31 +409,29 @@ def serve(args):
         _serve_run(hb, srv, ids[name], ns, w_k, w_m, xbuf, ybuf, None, 0)
         wall, lat, widths, _ = _serve_run(hb, srv, ids[name], ns, kinds, mids, xbuf, ybuf, None, 0)
         results[name] = {"capacity_req_s": n_req / wall}
-    rates = {"batched": args.load * results["batched"]["capacity_req_s"],
-             "plain": args.load * results["plain"]["capacity_req_s"]}
-    runs = [("batched", rates["batched"], "own"), ("plain", rates["plain"], "own")]
-    if results["plain"]["capacity_req_s"] > rates["batched"]:
-        runs.append(("plain", rates["batched"], "batched server's rate"))
-    runs.append(("batched", rates["plain"], "plain server's rate"))
-    for name, rate, which in runs:
-        srv = servers[name]
-        wall, lat, widths, lag = _serve_run(hb, srv, ids[name], ns, kinds, mids, xbuf, ybuf, rate, 7)
-        st = srv.stats()
-        is_cg = kinds == hb.REQ_CG
-        print(json.dumps({
-            "suite": "serve", "server": name, "vectors": "device" if args.device else "pinned host",
-            "arrivals": f"Poisson at {rate:.1f} req/s ({which} {args.load:g} x capacity)",
-            "workload": f"{len(ns)} SPD 27-point stencils, edge U[{args.edge_min},{args.edge_max}] seed 5, 0.5% "
-                        f"symmetric extras, {rows} rows; {n_req} requests, {args.cg_fraction:.0%} CG",
-            "capacity_req_s": results[name]["capacity_req_s"], "throughput_req_s": n_req / wall,
-            "p50_ms": 1e3 * float(np.percentile(lat, 50)), "p99_ms": 1e3 * float(np.percentile(lat, 99)),
-            "spmv_p50_ms": 1e3 * float(np.percentile(lat[~is_cg], 50)),
-            "spmv_p99_ms": 1e3 * float(np.percentile(lat[~is_cg], 99)),
-            "cg_p50_ms": 1e3 * float(np.percentile(lat[is_cg], 50)) if is_cg.any() else None,
-            "cg_p99_ms": 1e3 * float(np.percentile(lat[is_cg], 99)) if is_cg.any() else None,
-            "mean_spmv_batch": float(widths.mean()) if len(widths) else None,
-            "max_submit_lag_ms": 1e3 * lag, "device_bytes": int(st.deviceBytes),
-            "memory_budget_bytes": int(srv.options.memoryBudget)}), flush=True)
+    cap = results["batched"]["capacity_req_s"]
+    for load in [float(v) for v in args.loads.split(",")]:
+        rate = load * cap
+        for name, srv in servers.items():
+            wall, lat, widths, lag = _serve_run(hb, srv, ids[name], ns, kinds, mids, xbuf, ybuf, rate, 7)
+            st = srv.stats()
+            is_cg = kinds == hb.REQ_CG
+            thr = n_req / wall
+            print(json.dumps({
+                "suite": "serve", "server": name, "vectors": "device" if args.device else "pinned host",
+                "arrivals": f"Poisson at {rate:.1f} req/s ({load:g} x the batched server's capacity)",
+                "workload": f"{len(ns)} SPD 27-point stencils, edge U[{args.edge_min},{args.edge_max}] seed 5, 0.5% "
+                            f"symmetric extras, {rows} rows; {n_req} requests, {args.cg_fraction:.0%} CG",
+                "offered_req_s": rate, "capacity_req_s": results[name]["capacity_req_s"], "throughput_req_s": thr,
+                "saturated": bool(thr < 0.97 * rate),
+                "p50_ms": 1e3 * float(np.percentile(lat, 50)), "p99_ms": 1e3 * float(np.percentile(lat, 99)),
+                "spmv_p50_ms": 1e3 * float(np.percentile(lat[~is_cg], 50)) if (~is_cg).any() else None,
+                "spmv_p99_ms": 1e3 * float(np.percentile(lat[~is_cg], 99)) if (~is_cg).any() else None,
+                "cg_p50_ms": 1e3 * float(np.percentile(lat[is_cg], 50)) if is_cg.any() else None,
+                "cg_p99_ms": 1e3 * float(np.percentile(lat[is_cg], 99)) if is_cg.any() else None,
+                "mean_spmv_batch": float(widths.mean()) if len(widths) else None,
+                "max_submit_lag_ms": 1e3 * lag, "device_bytes": int(st.deviceBytes),
+                "memory_budget_bytes": int(srv.options.memoryBudget)}), flush=True)
     for s in servers.values():
         s.close()
 
@@ -531,7 +533,8 @@ def main(argv=None):
     ap.add_argument("--edge-min", type=int, default=32)
     ap.add_argument("--edge-max", type=int, default=160)
     ap.add_argument("--cg-fraction", type=float, default=0.2)
-    ap.add_argument("--load", type=float, default=0.7)
+    ap.add_argument("--loads", default="0.25,0.5,0.7,0.9", help="serve: offered rates, x batched capacity")
+    ap.add_argument("--serial-too", action="store_true", help="serve: also the batched server, 1 step in flight")
     ap.add_argument("--count", type=int, default=64)
     ap.add_argument("--storage", type=int, default=0)
     ap.add_argument("--n", type=int, default=8 * 1024 * 1024)

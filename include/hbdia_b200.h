@@ -537,6 +537,8 @@ typedef struct hbdia_server_options {
     int32_t cgCheckEvery;   /* inner iterations per graph replay (default 10)               */
     double cgTol;           /* target ||b - A y|| / ||b|| (default 1e-10)                   */
     double cgInnerTol;      /* inner relative tolerance (default 1e-6)                      */
+    int32_t maxInFlight;    /* SpMV batches of one matrix issued and not yet completed,     */
+                            /* 1-8 (default 1: the next batch forms while one runs)         */
 } hbdia_server_options;
 
 typedef struct hbdia_request_info {
