@@ -688,10 +688,10 @@ def fill_uniform(n: int, lo: float, hi: float, seed: int) -> np.ndarray:
 
 class Server:
     """Resident matrices and a request queue (hbdia_server_*): SpMV requests
-    served with continuous batching (same-matrix requests become one SpMM per
-    step), CG requests on a pool of solver threads.  ``options`` overrides
+    served with continuous batching (each matrix's pending requests become one
+    SpMM whenever the matrix is free), CG requests on a pool of solver threads.  ``options`` overrides
     fields of hbdia_server_default_options (memoryBudget, batching, maxRhs,
-    spmvStorage, cgInnerStorage, cgWorkers, cgTol, cgInnerTol, ...)."""
+    spmvStorage, cgInnerStorage, cgWorkers, cgTol, cgInnerTol, maxInFlight, ...)."""
 
     def __init__(self, **options):
         o = _lib.ServerOptions()

@@ -138,12 +138,15 @@ __global__ void __launch_bounds__(kThreads) add_into(double *__restrict__ x, con
 
 __global__ void copy_scalar(const double *__restrict__ src, double *__restrict__ dst) { dst[0] = src[0]; }
 
-double host_sum(const double *dpart, int nparts, cudaStream_t s, std::vector<double> &tmp) {
-    tmp.resize(nparts);
-    check_cuda(cudaMemcpyAsync(tmp.data(), dpart, sizeof(double) * nparts, cudaMemcpyDeviceToHost, s), "copy partials");
+// The partials land in page-locked memory: a copy into pageable memory is
+// synchronous inside the driver, and with several solvers on their own
+// threads those waits starved every other thread's CUDA calls (measured on a
+// served mix: SpMV requests beside 4 solvers held back for up to 0.4 s).
+double host_sum(const double *dpart, int nparts, cudaStream_t s, double *pinned) {
+    check_cuda(cudaMemcpyAsync(pinned, dpart, sizeof(double) * nparts, cudaMemcpyDeviceToHost, s), "copy partials");
     check_cuda(cudaStreamSynchronize(s), "cudaStreamSynchronize");
     double t = 0.0;
-    for (int i = 0; i < nparts; ++i) t += tmp[i];
+    for (int i = 0; i < nparts; ++i) t += pinned[i];
     return t;
 }
 
@@ -154,11 +157,13 @@ struct CgWork {
     int nparts = 0;
     double *buf = nullptr;  // r, p, q, d, tmp (n each) + 3 partial arrays + scalars
     double *r, *p, *q, *d, *tmp, *pqPart, *rrPart, *nPart, *scal;
+    double *host = nullptr;  // page-locked: nparts partial sums, then r.r
 };
 
 void cg_free(CgWork *w) {
     if (!w) return;
     if (w->buf) cudaFree(w->buf);
+    if (w->host) cudaFreeHost(w->host);
     delete w;
 }
 
@@ -173,7 +178,14 @@ CgWork *cg_work(CgWork *w, int64_t n) {
     w->nparts = static_cast<int>(std::min<int64_t>(int64_t(sms) * 4, (n + kThreads - 1) / kThreads));
     if (w->nparts < 1) w->nparts = 1;
     const size_t words = 5 * static_cast<size_t>(n) + 3 * static_cast<size_t>(w->nparts) + 8;
-    check_cuda(cudaMalloc(&w->buf, words * sizeof(double)), "cudaMalloc(CG workspace)");
+    try {
+        check_cuda(cudaMalloc(&w->buf, words * sizeof(double)), "cudaMalloc(CG workspace)");
+        check_cuda(cudaMallocHost(&w->host, (static_cast<size_t>(w->nparts) + 1) * sizeof(double)),
+                   "cudaMallocHost(CG partials)");
+    } catch (...) {
+        cg_free(w);
+        throw;
+    }
     double *b = w->buf;
     w->r = b; b += n;
     w->p = b; b += n;
@@ -199,10 +211,9 @@ void cg_solve(const DevicePlan &A64, const DevicePlan &Ainner, CgWork *w, const 
     // reduction partitions from n alone (what a workspace sized to n has), so
     // the result does not depend on the workspace's size
     const int G = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(w->nparts, (n + kThreads - 1) / kThreads)));
-    std::vector<double> tmp;
     // ||b||
     dot_partial<<<G, kThreads, 0, s>>>(b, b, n, w->nPart);
-    const double bnorm = std::sqrt(host_sum(w->nPart, G, s, tmp));
+    const double bnorm = std::sqrt(host_sum(w->nPart, G, s, w->host));
     int outer = 0, inner = 0;
     double rel = 0.0;
     cudaGraphExec_t exec = nullptr;
@@ -224,7 +235,7 @@ void cg_solve(const DevicePlan &A64, const DevicePlan &Ainner, CgWork *w, const 
             // outer residual in FP64
             launch_spmv(A64, x, w->tmp, s);
             residual<<<G, kThreads, 0, s>>>(b, w->tmp, w->r, n, w->nPart);
-            const double rnorm = std::sqrt(host_sum(w->nPart, G, s, tmp));
+            const double rnorm = std::sqrt(host_sum(w->nPart, G, s, w->host));
             rel = bnorm > 0 ? rnorm / bnorm : rnorm;
             if (rel <= tol || outer >= maxOuter || !std::isfinite(rel)) break;
             ++outer;
@@ -242,9 +253,10 @@ void cg_solve(const DevicePlan &A64, const DevicePlan &Ainner, CgWork *w, const 
             while (it < maxInner) {
                 check_cuda(cudaGraphLaunch(exec, s), "cudaGraphLaunch");
                 it += checkEvery;
-                double rr = 0.0;
-                check_cuda(cudaMemcpyAsync(&rr, w->scal, sizeof(double), cudaMemcpyDeviceToHost, s), "copy r.r");
+                double *rrHost = w->host + w->nparts;
+                check_cuda(cudaMemcpyAsync(rrHost, w->scal, sizeof(double), cudaMemcpyDeviceToHost, s), "copy r.r");
                 check_cuda(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+                const double rr = *rrHost;
                 if (!(std::sqrt(rr) > target)) break;  // converged (or not finite)
             }
             inner += it;

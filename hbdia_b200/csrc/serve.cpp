@@ -9,16 +9,18 @@
 //    them (oldest first; with batching off, one) and issues them as one SpMM
 //    -- device vectors as a vector-list SpMM read and written in place, host
 //    vectors through the matrix's column-major staging block -- so the
-//    matrix's values cross HBM once for all of them.  A completer thread
-//    completes a batch the moment the event behind its work fires, so a
-//    request waits only for its own matrix, never for a global step; requests that arrive while a batch runs form the next one
-//    (continuous batching).  With batching off, one request per launch (the
-//    plain form it is measured against).
+//    matrix's values cross HBM once for all of them.  A host function queued
+//    behind each batch wakes the same thread, which completes the batch and
+//    issues the matrix's next one, so a request waits only for its own
+//    matrix, never for a global step; requests that arrive while a batch runs
+//    form the next one (continuous batching).  No thread polls the GPU.  With
+//    batching off, one request per launch (the plain form it is measured
+//    against).
 //  * CG: solve A y = x to a relative residual, by the mixed-precision CG of
 //    cg.cu on one of cgWorkers worker threads (own stream, own workspace).
 // x and y are host buffers (hbdia_server_submit: copied in and out on the
 // server's streams) or device buffers (hbdia_server_submit_device: read and
-// written in place).  A step's device SpMV requests on one matrix become one
+// written in place).  A batch's device SpMV requests on one matrix become one
 // vector-list SpMM (each value read once for up to 32 requests, no staging
 // copies); its host requests one column-major SpMM over the staging block.
 // A request's result does not depend on what it was batched with: column j
@@ -52,15 +54,26 @@ namespace hbdia {
 namespace {
 
 
+struct Request;
+
+// An SpMV batch on its matrix's stream: its requests and the event (from the
+// matrix's pool) recorded behind its work.
+struct SpmvBatch {
+    std::vector<Request *> reqs;
+    cudaEvent_t done = nullptr;
+};
+
 struct ServedMatrix {
     DevicePlan p64;   // FP64 values: CG outer residual; SpMVs when spmvStorage is NATIVE
     DevicePlan pLow;  // reduced storage (when one is asked for)
     int32_t n = 0, rowsX = 0;
     double *X = nullptr, *Y = nullptr;  // column-major staging blocks, maxRhs columns
     int64_t bytes = 0;
-    cudaStream_t stream = nullptr;      // this matrix's SpMV batches, in order
-    std::deque<struct Request *> pending;  // SpMV requests not yet issued (server lock)
-    int32_t inFlight = 0;               // batches issued and not completed (server lock)
+    Server *server = nullptr;
+    cudaStream_t stream = nullptr;         // this matrix's SpMV batches, in order
+    std::vector<cudaEvent_t> freeEvents;   // maxInFlight events, reused (scheduler thread)
+    std::deque<SpmvBatch> running;         // issued, in stream order (scheduler thread)
+    std::deque<Request *> pending;         // SpMV requests not yet issued (server lock)
     const DevicePlan &spmvPlan(int32_t storage) const { return storage == HBDIA_STORE_NATIVE ? p64 : pLow; }
     const DevicePlan &cgInner(int32_t storage) const { return storage == HBDIA_STORE_NATIVE ? p64 : pLow; }
 };
@@ -76,16 +89,14 @@ struct Request {
     bool done = false;
 };
 
-// An SpMV batch in flight: its requests and the event recorded behind its work.
-struct SpmvBatch {
-    ServedMatrix *M = nullptr;
-    std::vector<Request *> reqs;
-    cudaEvent_t done = nullptr;
-};
-
 double now_since(std::chrono::steady_clock::time_point t0) {
     return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 }
+
+// With batches in flight and no doorbell, the scheduler queries every running
+// batch's event this often (a batch whose doorbell never runs -- a failed
+// host-function launch, a context error -- still completes).
+constexpr int kSweepMs = 50;
 
 }  // namespace
 
@@ -94,20 +105,19 @@ struct Server {
     int device = 0;
     std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
     std::mutex mu;
-    std::condition_variable cvWork, cvDone, cvCg, cvActive;
+    std::condition_variable cvWork, cvDone, cvCg;
     std::vector<std::unique_ptr<ServedMatrix>> mats;
     int64_t used = 0;  // device bytes held
     int32_t maxN = 0;
     std::unordered_map<uint64_t, std::unique_ptr<Request>> reqs;
     std::deque<Request *> cgQ;
     int64_t spmvPending = 0;  // SpMV requests queued on the matrices
+    std::vector<ServedMatrix *> rung;  // matrices whose doorbell rang since the scheduler last looked
     uint64_t nextTicket = 1;
     bool stop = false;
-    bool paused = false;  // requests queue up; no step or solve starts
+    bool paused = false;  // requests queue up; no batch or solve starts
     hbdia_server_stats stats{};
-    std::thread sched, completerThread;
-    std::vector<SpmvBatch> active;  // issued batches not yet taken by the completer
-    bool schedDone = false;
+    std::thread sched;
     std::vector<std::thread> cgThreads;
 };
 
@@ -124,7 +134,22 @@ void complete(Server *S, const std::vector<Request *> &rs, int status, double fi
     S->cvDone.notify_all();
 }
 
-// Issues one matrix's batch on its stream and hands it to the completer.
+// Host function queued behind every batch: tells the scheduler that work on
+// this matrix's stream has finished.  It makes no CUDA call (a host function
+// must not), and no thread holds the server lock across a CUDA call, so it
+// cannot deadlock against one.
+void CUDART_CB doorbell(void *p) {
+    ServedMatrix *M = static_cast<ServedMatrix *>(p);
+    Server *S = M->server;
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        S->rung.push_back(M);
+    }
+    S->cvWork.notify_one();
+}
+
+// Issues one matrix's batch on its stream (scheduler thread, no lock held).
+// On a failure the requests complete with its status at once.
 void issue_batch(Server *S, ServedMatrix *M, std::vector<Request *> &reqs) {
     const double started = now_since(S->t0);
     cudaStream_t st = M->stream;
@@ -160,113 +185,108 @@ void issue_batch(Server *S, ServedMatrix *M, std::vector<Request *> &reqs) {
             check_cuda(cudaMemcpyAsync(host[j]->y, M->Y + static_cast<int64_t>(j) * M->n, yb,
                                        cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync(request y)");
         SpmvBatch b;
-        b.M = M;
         b.reqs = reqs;
-        check_cuda(cudaEventCreateWithFlags(&b.done, cudaEventDisableTiming), "cudaEventCreate(batch)");
-        const cudaError_t rc = cudaEventRecord(b.done, st);
-        if (rc != cudaSuccess) {
-            cudaEventDestroy(b.done);
-            check_cuda(rc, "cudaEventRecord(batch)");
-        }
-        {
-            std::lock_guard<std::mutex> lk(S->mu);
-            S->active.push_back(std::move(b));
-        }
-        S->cvActive.notify_one();
+        b.done = M->freeEvents.back();
+        check_cuda(cudaEventRecord(b.done, st), "cudaEventRecord(batch)");
+        M->freeEvents.pop_back();
+        M->running.push_back(std::move(b));
+        // without the doorbell the periodic sweep still completes the batch
+        if (cudaLaunchHostFunc(st, doorbell, M) != cudaSuccess) cudaGetLastError();
     } catch (const Error &e) {
         cudaStreamSynchronize(st);  // nothing issued may still touch the request buffers
         complete(S, reqs, e.status, now_since(S->t0));
-        {
-            std::lock_guard<std::mutex> lk(S->mu);
-            M->inFlight -= 1;
-        }
-        S->cvWork.notify_all();
     }
 }
 
-// Forms per-matrix batches whenever a matrix with pending requests has a
-// free slot, and issues them.
+// The SpMV scheduler: one thread issues every batch and completes it.  It
+// sleeps until a request arrives or a doorbell rings; then it completes the
+// batches whose events have fired (front of each rung matrix's queue, which
+// its stream runs in order), and issues a new batch on every matrix with
+// pending requests and fewer than maxInFlight batches running -- up to maxRhs
+// requests, oldest first (with batching off, one).  Requests that arrive
+// while their matrix's batch runs form its next batch (continuous batching);
+// a request waits only for its own matrix.  No thread polls the GPU.
 void scheduler(Server *S) {
     cudaSetDevice(S->device);
     const int32_t perBatch = S->opt.batching ? S->opt.maxRhs : 1;
+    int64_t running = 0;  // batches in flight over all matrices
+    std::vector<ServedMatrix *> rung;
+    std::vector<std::pair<std::vector<Request *>, int>> finished;  // requests, status
+    std::vector<std::pair<ServedMatrix *, std::vector<Request *>>> batches;
     for (;;) {
-        std::vector<std::pair<ServedMatrix *, std::vector<Request *>>> batches;
+        bool sweep = false;
+        rung.clear();
         {
             std::unique_lock<std::mutex> lk(S->mu);
+            auto drained = [&] { return S->stop && S->spmvPending == 0 && running == 0; };
             auto ready = [&] {
-                if (S->spmvPending == 0) return false;
-                if (S->paused && !S->stop) return false;  // stopping drains even while paused
+                if (!S->rung.empty()) return true;
+                if (S->spmvPending == 0 || (S->paused && !S->stop)) return false;  // stopping drains
                 for (auto &m : S->mats)
-                    if (!m->pending.empty() && m->inFlight < S->opt.maxInFlight) return true;
+                    if (!m->pending.empty() && static_cast<int32_t>(m->running.size()) < S->opt.maxInFlight)
+                        return true;
                 return false;
             };
-            S->cvWork.wait(lk, [&] { return (S->stop && S->spmvPending == 0) || ready(); });
-            if (S->spmvPending == 0) {  // stopping and drained
-                S->schedDone = true;
-                S->cvActive.notify_all();
-                return;
+            auto pred = [&] { return drained() || ready(); };
+            if (running > 0) {
+                if (!S->cvWork.wait_for(lk, std::chrono::milliseconds(kSweepMs), pred)) sweep = true;
+            } else {
+                S->cvWork.wait(lk, pred);
             }
-            for (auto &m : S->mats) {
-                if (m->pending.empty() || m->inFlight >= S->opt.maxInFlight) continue;
-                std::vector<Request *> b;
-                while (!m->pending.empty() && static_cast<int32_t>(b.size()) < perBatch) {
-                    b.push_back(m->pending.front());
-                    m->pending.pop_front();
-                }
-                S->spmvPending -= static_cast<int64_t>(b.size());
-                m->inFlight += 1;
-                batches.emplace_back(m.get(), std::move(b));
-            }
-            S->stats.spmvSteps += 1;
-            S->stats.spmvLaunches += static_cast<int64_t>(batches.size());
+            if (drained()) return;
+            rung.swap(S->rung);
+            if (sweep)
+                for (auto &m : S->mats)
+                    if (!m->running.empty()) rung.push_back(m.get());
         }
-        for (auto &b : batches) issue_batch(S, b.first, b.second);
-    }
-}
-
-// Completes batches the moment their events fire, in whatever order the
-// matrices finish: polls the events of the batches in flight (yielding between
-// passes) and sleeps while none is in flight.
-void completer(Server *S) {
-    cudaSetDevice(S->device);
-    std::vector<SpmvBatch> mine;
-    for (;;) {
+        // completions (CUDA queries outside the lock)
+        finished.clear();
+        auto retire = [&](ServedMatrix *M) {
+            while (!M->running.empty()) {
+                SpmvBatch &b = M->running.front();
+                const cudaError_t q = cudaEventQuery(b.done);
+                if (q == cudaErrorNotReady) break;
+                finished.emplace_back(std::move(b.reqs), q == cudaSuccess ? HBDIA_OK : HBDIA_ERR_CUDA);
+                M->freeEvents.push_back(b.done);
+                M->running.pop_front();
+                running -= 1;
+            }
+        };
+        for (ServedMatrix *M : rung) retire(M);
+        batches.clear();
         {
-            std::unique_lock<std::mutex> lk(S->mu);
-            S->cvActive.wait(lk, [&] { return !S->active.empty() || !mine.empty() || S->schedDone; });
-            for (auto &b : S->active) mine.push_back(std::move(b));
-            S->active.clear();
-            if (mine.empty() && S->schedDone) return;
-        }
-        bool any = false;
-        for (size_t k = 0; k < mine.size();) {
-            const cudaError_t q = cudaEventQuery(mine[k].done);
-            if (q == cudaErrorNotReady) {
-                ++k;
-                continue;
-            }
-            const int status = q == cudaSuccess ? HBDIA_OK : HBDIA_ERR_CUDA;
-            cudaEventDestroy(mine[k].done);
+            std::lock_guard<std::mutex> lk(S->mu);
             const double t = now_since(S->t0);
-            {
-                std::lock_guard<std::mutex> lk(S->mu);
-                for (Request *r : mine[k].reqs) {
-                    r->info.status = status;
+            for (auto &f : finished)
+                for (Request *r : f.first) {
+                    r->info.status = f.second;
                     r->info.finished = t;
                     r->done = true;
                     S->stats.completed += 1;
                 }
-                mine[k].M->inFlight -= 1;
+            if (!(S->paused && !S->stop) && S->spmvPending > 0) {
+                for (auto &m : S->mats) {
+                    if (m->pending.empty() || static_cast<int32_t>(m->running.size()) >= S->opt.maxInFlight)
+                        continue;
+                    std::vector<Request *> b;
+                    while (!m->pending.empty() && static_cast<int32_t>(b.size()) < perBatch) {
+                        b.push_back(m->pending.front());
+                        m->pending.pop_front();
+                    }
+                    S->spmvPending -= static_cast<int64_t>(b.size());
+                    batches.emplace_back(m.get(), std::move(b));
+                }
+                if (!batches.empty()) {
+                    S->stats.spmvSteps += 1;
+                    S->stats.spmvLaunches += static_cast<int64_t>(batches.size());
+                }
             }
-            mine[k] = std::move(mine.back());
-            mine.pop_back();
-            any = true;
         }
-        if (any) {
-            S->cvDone.notify_all();
-            S->cvWork.notify_all();  // those matrices may take their next batch
-        } else {
-            std::this_thread::yield();
+        if (!finished.empty()) S->cvDone.notify_all();
+        for (auto &b : batches) {
+            const size_t before = b.first->running.size();
+            issue_batch(S, b.first, b.second);
+            running += static_cast<int64_t>(b.first->running.size() - before);
         }
     }
 }
@@ -333,6 +353,8 @@ void free_matrix(ServedMatrix &M) {
     if (M.X) cudaFree(M.X);
     if (M.Y) cudaFree(M.Y);
     if (M.stream) cudaStreamDestroy(M.stream);
+    for (cudaEvent_t e : M.freeEvents) cudaEventDestroy(e);
+    M.freeEvents.clear();
     M.X = M.Y = nullptr;
     M.stream = nullptr;
 }
@@ -353,12 +375,13 @@ void server_default_options(hbdia_server_options *o) {
     o->cgMaxInner = 5000;
     o->cgCheckEvery = 10;
     o->maxInFlight = 1;
+    o->spmvPriority = 1;
 }
 
 Server *server_create(const hbdia_server_options &o) {
     if (o.memoryBudget <= 0 || o.maxRhs < 1 || o.maxRhs > 64 || o.cgWorkers < 1 || o.cgWorkers > 64 ||
         o.cgTol <= 0 || o.cgInnerTol <= 0 || o.cgMaxOuter < 1 || o.cgMaxInner < 1 || o.cgCheckEvery < 1 ||
-        o.maxInFlight < 1 || o.maxInFlight > 8)
+        o.maxInFlight < 1 || o.maxInFlight > 8 || o.spmvPriority < 0 || o.spmvPriority > 1)
         throw Error(HBDIA_ERR_INVALID_ARGUMENT, "bad server options");
     for (int32_t st : {o.spmvStorage, o.cgInnerStorage})
         if (st != HBDIA_STORE_NATIVE && st != HBDIA_STORE_F32 && st != HBDIA_STORE_BF16_SCALED)
@@ -371,7 +394,6 @@ Server *server_create(const hbdia_server_options &o) {
     check_cuda(cudaGetDevice(&S->device), "cudaGetDevice");
     Server *raw = S.get();
     S->sched = std::thread(scheduler, raw);
-    S->completerThread = std::thread(completer, raw);
     for (int32_t i = 0; i < o.cgWorkers; ++i) S->cgThreads.emplace_back(cg_worker, raw);
     return S.release();
 }
@@ -385,10 +407,12 @@ void server_destroy(Server *S) {
     S->cvWork.notify_all();
     S->cvCg.notify_all();
     if (S->sched.joinable()) S->sched.join();
-    S->cvActive.notify_all();
-    if (S->completerThread.joinable()) S->completerThread.join();
     for (auto &t : S->cgThreads)
         if (t.joinable()) t.join();
+    // a doorbell may still be queued behind the last batch's event: let it run
+    // before its matrix goes
+    for (auto &m : S->mats)
+        if (m->stream) cudaStreamSynchronize(m->stream);
     for (auto &m : S->mats) free_matrix(*m);
     delete S;
 }
@@ -425,7 +449,21 @@ int32_t server_add_matrix(Server *S, const hbdia_matrix *m) {
                    "cudaMalloc(server staging x)");
         check_cuda(cudaMalloc(&M->Y, sizeof(double) * static_cast<size_t>(S->opt.maxRhs) * M->n),
                    "cudaMalloc(server staging y)");
-        check_cuda(cudaStreamCreateWithFlags(&M->stream, cudaStreamNonBlocking), "cudaStreamCreate(server)");
+        // SpMV batches are short and latency-bound, CG solves long: with
+        // spmvPriority the block scheduler starts a waiting SpMV's CTAs before
+        // further CG CTAs (CG streams keep the default, lowest priority)
+        int leastPrio = 0, greatestPrio = 0;
+        if (S->opt.spmvPriority)
+            check_cuda(cudaDeviceGetStreamPriorityRange(&leastPrio, &greatestPrio), "cudaDeviceGetStreamPriorityRange");
+        check_cuda(cudaStreamCreateWithPriority(&M->stream, cudaStreamNonBlocking,
+                                                S->opt.spmvPriority ? greatestPrio : leastPrio),
+                   "cudaStreamCreate(server)");
+        for (int32_t i = 0; i < S->opt.maxInFlight; ++i) {
+            cudaEvent_t e = nullptr;
+            check_cuda(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate(server)");
+            M->freeEvents.push_back(e);
+        }
+        M->server = S;
         std::lock_guard<std::mutex> lk(S->mu);
         S->used += M->bytes + cgGrow;
         S->maxN = std::max(S->maxN, M->n);

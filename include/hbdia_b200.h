@@ -507,13 +507,14 @@ int hbdia_batch_stream(const hbdia_batch *b, void **stream);
 
 /* A server holds resident matrices and serves requests submitted from any
  * host thread.  No counterpart in the reference.
- *  - SpMV requests (y = A x) are served in steps by continuous batching:
- *    each step takes all pending requests (up to maxRhs per matrix, oldest
- *    first); the requests of one matrix become one SpMM over the matrix's
- *    spmvStorage values (each x copied into its column, each y out of it),
- *    the matrices of a step run concurrently; requests arriving during a
- *    step join the next.  batching = 0 serves one request per launch in
- *    arrival order.
+ *  - SpMV requests (y = A x) are served by continuous batching per matrix:
+ *    each matrix has its own queue and stream; whenever it has pending
+ *    requests and fewer than maxInFlight batches running, up to maxRhs of
+ *    them (oldest first) become one SpMM over the matrix's spmvStorage
+ *    values (host vectors copied into and out of its staging columns, device
+ *    vectors read and written in place); the matrices run concurrently, and
+ *    requests arriving while their matrix is busy join its next batch.
+ *    batching = 0 serves one request per launch in arrival order.
  *  - CG requests (solve A y = x, A symmetric positive definite) run on
  *    cgWorkers worker threads: mixed-precision CG (hbdia_cg_solve) with
  *    cgInnerStorage inner iterations, refined to cgTol.
@@ -528,7 +529,7 @@ typedef enum hbdia_request_kind { HBDIA_REQ_SPMV = 0, HBDIA_REQ_CG = 1 } hbdia_r
 typedef struct hbdia_server_options {
     int64_t memoryBudget;   /* device bytes the server may hold (default 150e9)             */
     int32_t batching;       /* continuous batching of SpMVs (default 1)                     */
-    int32_t maxRhs;         /* SpMV requests of one matrix per step, 1-64 (default 16)     */
+    int32_t maxRhs;         /* SpMV requests of one matrix per batch, 1-64 (default 16)    */
     int32_t spmvStorage;    /* hbdia_value_storage of SpMVs (default HBDIA_STORE_F32)       */
     int32_t cgInnerStorage; /* storage of the CG inner iterations (default HBDIA_STORE_F32) */
     int32_t cgWorkers;      /* concurrent CG solves, 1-64 (default 4)                       */
@@ -539,12 +540,14 @@ typedef struct hbdia_server_options {
     double cgInnerTol;      /* inner relative tolerance (default 1e-6)                      */
     int32_t maxInFlight;    /* SpMV batches of one matrix issued and not yet completed,     */
                             /* 1-8 (default 1: the next batch forms while one runs)         */
+    int32_t spmvPriority;   /* 1: SpMV streams at the device's greatest stream priority,    */
+                            /* CG at the default one (default 1); 0: all default            */
 } hbdia_server_options;
 
 typedef struct hbdia_request_info {
     int32_t status;         /* hbdia_status of the request (CG: RUNTIME if not converged) */
     int32_t kind, matrix;
-    int32_t batchRhs;       /* SpMV: requests of its matrix in its step                  */
+    int32_t batchRhs;       /* SpMV: requests in its batch                               */
     double submitted, started, finished; /* seconds since the server was created         */
     int32_t cgOuter, cgInner;
     double cgRelResidual;
@@ -552,7 +555,7 @@ typedef struct hbdia_request_info {
 
 typedef struct hbdia_server_stats {
     int64_t completed, spmvRequests, cgRequests;
-    int64_t spmvSteps, spmvLaunches;
+    int64_t spmvSteps, spmvLaunches; /* scheduler passes that issued batches; batches */
     int64_t deviceBytes;    /* held under the budget */
     int32_t matrices;
 } hbdia_server_stats;

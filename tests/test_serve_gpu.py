@@ -191,8 +191,10 @@ def test_server_rejections(lib, mats):
     srv.close()
 
 
-def test_step_with_more_matrices_than_streams(lib):
-    """One step spanning 20 matrices (the SpMV stream ring has 16 streams)."""
+def test_burst_over_many_matrices(lib):
+    """A burst over 20 matrices, queued while paused, is issued in one
+    scheduler pass (each matrix's two requests as one batch on its own
+    stream) and gives the bits of the requests served alone."""
     srv = lib.Server()
     rng = np.random.default_rng(12)
     mats = []
@@ -216,7 +218,7 @@ def test_step_with_more_matrices_than_streams(lib):
         info = srv.wait(t)
         assert info.status == 0 and info.batchRhs == 2
         assert bits_equal(y, y0)
-    assert srv.stats().spmvSteps == 21  # 20 alone + one step for the whole burst
+    assert srv.stats().spmvSteps == 21  # 20 alone + one pass for the whole burst
     srv.close()
 
 
