@@ -69,8 +69,7 @@ class BatchConfig(ctypes.Structure):
 class ServerOptions(ctypes.Structure):
     _fields_ = [("memoryBudget", c_i64), ("batching", c_i32), ("maxRhs", c_i32), ("spmvStorage", c_i32),
                 ("cgInnerStorage", c_i32), ("cgWorkers", c_i32), ("cgMaxOuter", c_i32), ("cgMaxInner", c_i32),
-                ("cgCheckEvery", c_i32), ("cgTol", c_dbl), ("cgInnerTol", c_dbl), ("maxInFlight", c_i32),
-                ("spmvPriority", c_i32)]
+                ("cgCheckEvery", c_i32), ("cgTol", c_dbl), ("cgInnerTol", c_dbl), ("maxInFlight", c_i32)]
 
 
 class RequestInfo(ctypes.Structure):

@@ -375,13 +375,12 @@ void server_default_options(hbdia_server_options *o) {
     o->cgMaxInner = 5000;
     o->cgCheckEvery = 10;
     o->maxInFlight = 1;
-    o->spmvPriority = 1;
 }
 
 Server *server_create(const hbdia_server_options &o) {
     if (o.memoryBudget <= 0 || o.maxRhs < 1 || o.maxRhs > 64 || o.cgWorkers < 1 || o.cgWorkers > 64 ||
         o.cgTol <= 0 || o.cgInnerTol <= 0 || o.cgMaxOuter < 1 || o.cgMaxInner < 1 || o.cgCheckEvery < 1 ||
-        o.maxInFlight < 1 || o.maxInFlight > 8 || o.spmvPriority < 0 || o.spmvPriority > 1)
+        o.maxInFlight < 1 || o.maxInFlight > 8)
         throw Error(HBDIA_ERR_INVALID_ARGUMENT, "bad server options");
     for (int32_t st : {o.spmvStorage, o.cgInnerStorage})
         if (st != HBDIA_STORE_NATIVE && st != HBDIA_STORE_F32 && st != HBDIA_STORE_BF16_SCALED)
@@ -449,15 +448,7 @@ int32_t server_add_matrix(Server *S, const hbdia_matrix *m) {
                    "cudaMalloc(server staging x)");
         check_cuda(cudaMalloc(&M->Y, sizeof(double) * static_cast<size_t>(S->opt.maxRhs) * M->n),
                    "cudaMalloc(server staging y)");
-        // SpMV batches are short and latency-bound, CG solves long: with
-        // spmvPriority the block scheduler starts a waiting SpMV's CTAs before
-        // further CG CTAs (CG streams keep the default, lowest priority)
-        int leastPrio = 0, greatestPrio = 0;
-        if (S->opt.spmvPriority)
-            check_cuda(cudaDeviceGetStreamPriorityRange(&leastPrio, &greatestPrio), "cudaDeviceGetStreamPriorityRange");
-        check_cuda(cudaStreamCreateWithPriority(&M->stream, cudaStreamNonBlocking,
-                                                S->opt.spmvPriority ? greatestPrio : leastPrio),
-                   "cudaStreamCreate(server)");
+        check_cuda(cudaStreamCreateWithFlags(&M->stream, cudaStreamNonBlocking), "cudaStreamCreate(server)");
         for (int32_t i = 0; i < S->opt.maxInFlight; ++i) {
             cudaEvent_t e = nullptr;
             check_cuda(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate(server)");

@@ -540,8 +540,6 @@ typedef struct hbdia_server_options {
     double cgInnerTol;      /* inner relative tolerance (default 1e-6)                      */
     int32_t maxInFlight;    /* SpMV batches of one matrix issued and not yet completed,     */
                             /* 1-8 (default 1: the next batch forms while one runs)         */
-    int32_t spmvPriority;   /* 1: SpMV streams at the device's greatest stream priority,    */
-                            /* CG at the default one (default 1); 0: all default            */
 } hbdia_server_options;
 
 typedef struct hbdia_request_info {
