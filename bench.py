@@ -81,11 +81,12 @@ def profiled_traffic():
 class ClockSampler:
     """Samples SM clock and throttle reasons through NVML while running."""
 
-    def __init__(self, device_index: int, period_s: float = 0.02):
+    def __init__(self, device_index: int, period_s: float = 0.005):
         self.idx, self.period = device_index, period_s
         self.samples, self.reasons, self.max_mhz = [], set(), None
         self._stop = threading.Event()
         self._t = None
+        self._nv = None
 
     def __enter__(self):
         try:
@@ -102,7 +103,7 @@ class ClockSampler:
         self._t.start()
         return self
 
-    def _run(self):
+    def _sample(self):
         nv = self._nv
         names = {
             "hw_slowdown": getattr(nv, "nvmlClocksThrottleReasonHwSlowdown", 0x8),
@@ -111,18 +112,26 @@ class ClockSampler:
             "sw_power_cap": getattr(nv, "nvmlClocksThrottleReasonSwPowerCap", 0x4),
             "hw_power_brake_slowdown": getattr(nv, "nvmlClocksThrottleReasonHwPowerBrakeSlowdown", 0x80),
         }
+        try:
+            self.samples.append(nv.nvmlDeviceGetClockInfo(self._h, nv.NVML_CLOCK_SM))
+            r = nv.nvmlDeviceGetCurrentClocksThrottleReasons(self._h)
+            for k, bit in names.items():
+                if r & bit:
+                    self.reasons.add(k)
+        except Exception:
+            pass
+
+    def _run(self):
         while not self._stop.is_set():
-            try:
-                self.samples.append(nv.nvmlDeviceGetClockInfo(self._h, nv.NVML_CLOCK_SM))
-                r = nv.nvmlDeviceGetCurrentClocksThrottleReasons(self._h)
-                for k, bit in names.items():
-                    if r & bit:
-                        self.reasons.add(k)
-            except Exception:
-                pass
+            self._sample()
             self._stop.wait(self.period)
 
     def __exit__(self, *exc):
+        # one more sample while the GPU is still warm from the region: the
+        # thread competes with the launch loop for the interpreter and may
+        # have taken few
+        if self._nv is not None:
+            self._sample()
         self._stop.set()
         if self._t:
             self._t.join(timeout=2)
