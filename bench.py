@@ -46,8 +46,9 @@ WORKLOAD = dict(nx=256, ny=256, nz=256, center=26.0, neighbor=-1.0, extra_fracti
 METRIC = "SpMV HBM GB/s"
 UNIT = "GB/s"
 KERNEL_NAMES = {1: "spmv_rowwise<double,double>", 2: "spmv_bw32<double,double>",
-                3: "spmv_bw32_tma<double,double> (TMA-staged)",
-                4: "spmv_bw32_pipe<double,double> (persistent, pipelined)"}
+                3: "spmv_bw32_xs<double,double> (x window staged by bulk copies)",
+                4: "spmv_bw32_pipe<double,double> (persistent, pipelined)",
+                5: "spmv_bw32_quad<double,double> (4 blocks per warp)"}
 
 
 def log(*a):
@@ -193,7 +194,7 @@ def cpu_reference_throughput(rows, cols, vals, n, x, bytes_per_spmv, budget_s, s
         med = statistics.median(times)
         return dict(value=bytes_per_spmv / med / 1e9, unit=UNIT, cores=ref.omp_max_threads(), kind="reference",
                     sample=f"whole {WORKLOAD['nx']}^3 matrix ({len(vals)} COO entries), {len(times)} SpMVs, median",
-                    spmv_per_s=1.0 / med, ms_per_spmv=med * 1e3)
+                    spmv_per_s=1.0 / med, ms_per_spmv=med * 1e3), y
     orc = oracle.Restated()
     # scalar port on the first rows (about 1/64 of the matrix), scaled by entries
     cut = int(np.searchsorted(rows, n // 64))
@@ -203,24 +204,55 @@ def cpu_reference_throughput(rows, cols, vals, n, x, bytes_per_spmv, budget_s, s
     dt = (time.perf_counter() - t) * len(vals) / max(cut, 1)
     return dict(value=bytes_per_spmv / dt / 1e9, unit=UNIT, cores=1, kind="port",
                 sample=f"rows 0..{n // 64} ({cut} entries) of the 256^3 matrix, scaled by entries",
-                spmv_per_s=1.0 / dt, ms_per_spmv=dt * 1e3)
+                spmv_per_s=1.0 / dt, ms_per_spmv=dt * 1e3), None
+
+
+def parity_report(rows, cols, vals, n, x, y_gpu, y_ref_coo, full_oracle=True):
+    """The GPU y of the timed SpMV against (1) the reference's own
+    cpu_coo_spmv_kernel over the whole matrix in row-sorted COO (a different
+    summation order: bounded by 1e-12 * sum_j |a_ij x_j| per row), and (2) the
+    oracle's restated HBDIA SpMV on its own conversion (same order: bit for
+    bit).  Outside every timed region."""
+    out = {"tolerance": "|y - y_ref| <= 1e-12 * sum_j |a_ij x_j| per row"}
+    absrow = np.bincount(rows, weights=np.abs(vals * x[cols]), minlength=n)
+    scale = np.maximum(absrow, np.finfo(np.float64).tiny)
+    if y_ref_coo is not None:
+        err = np.abs(y_gpu - y_ref_coo) / scale
+        out["reference_cpu_coo"] = {
+            "oracle": "the reference's cpu_coo_spmv_kernel (oracle/_ref), whole matrix in row-sorted COO",
+            "max_scaled_err": float(err.max()), "bitexact_frac": float(np.mean(y_gpu == y_ref_coo)),
+            "pass": bool(err.max() <= 1e-12)}
+    if full_oracle:
+        import oracle
+        t = time.time()
+        om = oracle.Restated().convert(rows, cols, vals, n, n, WORKLOAD["block_width"], WORKLOAD["threshold"])
+        y_orc = om.spmv(x)
+        del om
+        same = y_gpu.view(np.uint64) == y_orc.view(np.uint64)
+        out["oracle_hbdia"] = {
+            "oracle": "oracle/hbdia_oracle.c: convertToHBDIAFormat + hbdiaSpMV restated, same operation order",
+            "bitexact_frac": float(np.mean(same)), "max_scaled_err": float((np.abs(y_gpu - y_orc) / scale).max()),
+            "pass": bool(same.all()), "seconds": time.time() - t}
+    out["pass"] = all(v["pass"] for v in out.values() if isinstance(v, dict))
+    return out
 
 
 def run_reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    import hbdia_b200 as hb
+    # Everything here is the reference's code (oracle/_ref) or the oracle's
+    # restatement (oracle/hbdia_oracle.c): the product library is not loaded.
+    import oracle
     w = WORKLOAD
     n = w["nx"] * w["ny"] * w["nz"]
-    rows, cols, vals = hb.generate_stencil27(w["nx"], w["ny"], w["nz"], w["center"], w["neighbor"],
-                                             w["extra_fraction"], w["extra_lo"], w["extra_hi"], w["extra_seed"])
-    x = hb.fill_uniform(n, -1.0, 1.0, w["x_seed"])
-    m = hb.HBDIA(rows, cols, vals, n, n)
-    m.convertToHBDIAFormat(w["block_width"], w["threshold"], upload=False)
-    i = m.info()
-    bytes_per_spmv = hbm_bytes_model(i)
-    import oracle
+    orc = oracle.Restated()
+    rows, cols, vals = orc.workload_stencil27(w["nx"], w["ny"], w["nz"], w["center"], w["neighbor"],
+                                              w["extra_fraction"], w["extra_lo"], w["extra_hi"], w["extra_seed"])
+    x = orc.fill_uniform(n, -1.0, 1.0, w["x_seed"])
+    L = orc.convert(rows, cols, vals, n, n, w["block_width"], w["threshold"]).layout()
+    bytes_per_spmv = bytes_model(n, len(L.data), len(L.offsets), L.num_blocks, len(L.coo_row))
+    del L
     if not oracle.Reference.available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libhbdia_ref.so was not built"}))
         return 0
@@ -252,7 +284,7 @@ def run_reference_arm(args):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total / args.steps * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-        "config": workload_config(),
+        "config": dict(workload_config(), parallelism="replicas1"),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": ref.omp_max_threads(), "kind": "reference",
                          "sample": f"rows 0..{r1} of the 256^3 matrix ({cut} of {len(vals)} entries) per step; "
                                    f"value scaled to whole-matrix SpMV bytes by entries"},
@@ -263,16 +295,19 @@ def run_reference_arm(args):
     return 0
 
 
-def hbm_bytes_model(i):
+def bytes_model(n, slots, total_offsets, num_blocks, num_coo):
     """Algorithmic bytes of one plain-FP64 SpMV over the HBDIA layout (bw 32
     kernel): values 8*slots + offsets 4*totalOffsets + block pointers
     4*(numBlocks+1) + x read once 8n + y written once 8n + COO (row, col, value)
     16*nCoo + one x gather per COO entry 8*nCoo + COO tile pointers 4*(n/32+1)."""
-    n = i.numRows
-    b = 8 * i.numSlots + 4 * i.totalOffsets + 4 * (i.numBlocks + 1) + 16 * n + 24 * i.numCoo
-    if i.numCoo:
+    b = 8 * slots + 4 * total_offsets + 4 * (num_blocks + 1) + 16 * n + 24 * num_coo
+    if num_coo:
         b += 4 * ((n + 31) // 32 + 1)
     return b
+
+
+def hbm_bytes_model(i):
+    return bytes_model(i.numRows, i.numSlots, i.totalOffsets, i.numBlocks, i.numCoo)
 
 
 def workload_config():
@@ -292,9 +327,10 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--cpu-budget", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-parity", action="store_true", help="skip the full-size parity check against the oracles")
     ap.add_argument("--unroll", type=int, default=0, choices=[0, 9, 27],
                     help="offsets in flight per lane in the staged kernel (0: default)")
-    ap.add_argument("--kernel", default=None, choices=["pipe", "staged", "warp", "rowwise"],
+    ap.add_argument("--kernel", default=None, choices=["pipe", "quad", "staged", "warp", "rowwise"],
                     help="force one SpMV kernel (default: the library's choice)")
     ap.add_argument("--size", type=int, default=256,
                     help="grid edge of the stencil workload (256 is the benchmark; smaller sizes for profiling)")
@@ -325,7 +361,7 @@ def main():
     bytes_per_spmv = hbm_bytes_model(info)
     assert bytes_per_spmv == info.bytesPerSpmv, (bytes_per_spmv, info.bytesPerSpmv)
     if args.kernel:
-        m.setKernel({"pipe": hb.KERNEL_PIPE, "staged": hb.KERNEL_STAGED, "warp": hb.KERNEL_WARP,
+        m.setKernel({"pipe": hb.KERNEL_PIPE, "quad": hb.KERNEL_QUAD, "staged": hb.KERNEL_STAGED, "warp": hb.KERNEL_WARP,
                      "rowwise": hb.KERNEL_ROWWISE}[args.kernel])
     if args.unroll:
         m.setTuning(hb.TUNE_UNROLL, args.unroll)
@@ -404,8 +440,11 @@ def main():
     ok = ok and all(np.array_equal(y.view(np.uint64), ref_y) for y in ys)
 
     cpu = None
+    parity = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_reference_throughput(rows, cols, vals, n, x, bytes_per_spmv, args.cpu_budget)
+        cpu, y_ref = cpu_reference_throughput(rows, cols, vals, n, x, bytes_per_spmv, args.cpu_budget)
+        if not args.no_parity:
+            parity = parity_report(rows, cols, vals, n, x, yt.cpu().numpy(), y_ref)
 
     if rank == 0:
         cs = clk.summary()
@@ -416,6 +455,8 @@ def main():
             "config": dict(workload_config(), parallelism=f"replicas{world}"),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": profiled_traffic(), "peak_source": peak_kind,
+                         "traffic_source": "ncu dram__bytes_read+write of one 128^3 launch of the same kernel, "
+                                           "scaled to 256^3 by the byte model (profiles/)",
                          "kernel": KERNEL_NAMES[kernel_used], "bytes_per_launch": bytes_per_spmv,
                          "avg_launch_ms": avg_launch_ms},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n,
@@ -424,6 +465,7 @@ def main():
                     "single_call": {"api": "hbdia_spmv_host per step", "value": single_value,
                                     "ms_per_step": single_ms / args.e2e_steps}},
             "cpu_baseline": cpu,
+            "parity": parity,
             "gpu_launches": args.steps,
             "clocks": cs,
             "spmv_per_s": 1e3 * args.steps * world / total_ms,

@@ -18,7 +18,7 @@ from typing import List, Optional, Sequence
 import numpy as np
 
 from . import _lib
-from ._lib import (BATCH_CONCURRENT, BATCH_QUEUE, REQ_CG, REQ_SPMV, KERNEL_AUTO, KERNEL_PIPE, KERNEL_ROWWISE, KERNEL_STAGED, KERNEL_WARP, TUNE_PREFETCH, TUNE_SPMM_TILE, TUNE_TAIL,
+from ._lib import (BATCH_CONCURRENT, BATCH_QUEUE, REQ_CG, REQ_SPMV, KERNEL_AUTO, KERNEL_PIPE, KERNEL_QUAD, KERNEL_ROWWISE, KERNEL_STAGED, KERNEL_WARP, TUNE_PREFETCH, TUNE_QUAD_GROUP, TUNE_SPMM_TILE, TUNE_STAGES, TUNE_TAIL,
                    TUNE_UNROLL, HBDIACudaError,
                    HBDIADeviceTimeout, STORE_BF16_SCALED, STORE_F32, STORE_NATIVE, MatrixInfo,
                    check as _check, load as _load)
@@ -287,9 +287,10 @@ class HBDIA:
     def setWaitTimeout(self, nanoseconds: int) -> None:
         _check(_load().hbdia_matrix_set_wait_timeout(self._h, int(nanoseconds)))
 
-    def testSkipChunk(self, chunk: int) -> None:
-        """Test hook: the staged kernel never publishes `chunk` (-1: off)."""
-        _check(_load().hbdia_matrix_test_skip_chunk(self._h, int(chunk)))
+    def testSkipTile(self, tile: int) -> None:
+        """Test hook: the staged kernel never issues the copies of 32-row
+        tile `tile`, so its bounded wait runs out (-1: off)."""
+        _check(_load().hbdia_matrix_test_skip_tile(self._h, int(tile)))
 
     # ---- partial matrices: one rank's rows (include/Format/HBDIA.hpp:37-39, 77-79, 117-136)
     @classmethod

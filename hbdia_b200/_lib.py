@@ -26,8 +26,8 @@ HBDIA_ERR_NOT_CONVERTED = -6
 HBDIA_ERR_UNSUPPORTED = -7
 HBDIA_ERR_DEVICE_TIMEOUT = -8
 
-KERNEL_AUTO, KERNEL_ROWWISE, KERNEL_WARP, KERNEL_STAGED, KERNEL_PIPE = 0, 1, 2, 3, 4
-TUNE_UNROLL, TUNE_SPMM_TILE, TUNE_PREFETCH, TUNE_TAIL = 1, 2, 3, 4
+KERNEL_AUTO, KERNEL_ROWWISE, KERNEL_WARP, KERNEL_STAGED, KERNEL_PIPE, KERNEL_QUAD = 0, 1, 2, 3, 4, 5
+TUNE_UNROLL, TUNE_SPMM_TILE, TUNE_PREFETCH, TUNE_TAIL, TUNE_STAGES, TUNE_QUAD_GROUP = 1, 2, 3, 4, 5, 6
 
 HBDIA_F64, HBDIA_F32 = 0, 1
 BATCH_CONCURRENT, BATCH_QUEUE = 0, 1
@@ -155,7 +155,7 @@ _SIGS = [
     ("hbdia_matrix_autotune", ctypes.c_int, [c_vp, c_vp, c_i64, c_vp, c_i64, c_i32, c_vp, c_i32,
                                              ctypes.POINTER(TuneResult)]),
     ("hbdia_autotune_clear", ctypes.c_int, []),
-    ("hbdia_matrix_test_skip_chunk", ctypes.c_int, [c_vp, c_i32]),
+    ("hbdia_matrix_test_skip_tile", ctypes.c_int, [c_vp, c_i32]),
     ("hbdia_vector_create", ctypes.c_int, [ctypes.c_int, c_vp, c_i64, c_vpp]),
     ("hbdia_vector_destroy", None, [c_vp]),
     ("hbdia_vector_device_ptr", ctypes.c_int, [c_vp, c_vpp]),

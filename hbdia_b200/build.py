@@ -26,8 +26,8 @@ NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 CU_SOURCES = ["plan.cu", "autotune.cu", "cg.cu", "noalloc.cu", "batch.cu", "convert_gpu.cu", "halo.cu", "layout_plan.cu"]
-CPP_SOURCES = ["convert.cpp", "generate.cpp", "chunks.cpp", "capi.cpp", "hbdia_cxx.cpp", "serve.cpp", "dia.cpp", "partition.cpp"]
-HEADERS = ["hbdia_internal.hpp", "spmv_kernels.cuh", "spmv_tma.cuh", "spmm_kernels.cuh", "chunks.hpp", "args.cuh",
+CPP_SOURCES = ["convert.cpp", "generate.cpp", "capi.cpp", "hbdia_cxx.cpp", "serve.cpp", "dia.cpp", "partition.cpp"]
+HEADERS = ["hbdia_internal.hpp", "spmv_kernels.cuh", "spmv_xstage.cuh", "spmv_quad.cuh", "spmm_kernels.cuh", "args.cuh",
            "batch_kernels.cuh", "handles.hpp"]
 
 

@@ -105,9 +105,9 @@ void autotune(DevicePlan &P, const void *X, int64_t ldx, void *Y, int64_t ldy, i
         std::vector<Choice> cand;
         if (k == 1) {
             if (P.bw == 32) {
-                for (int32_t kern : {HBDIA_KERNEL_PIPE, HBDIA_KERNEL_WARP, HBDIA_KERNEL_STAGED})
+                for (int32_t kern : {HBDIA_KERNEL_PIPE, HBDIA_KERNEL_QUAD, HBDIA_KERNEL_WARP, HBDIA_KERNEL_STAGED})
                     for (int32_t u : {0, 27}) {
-                        if (kern == HBDIA_KERNEL_WARP && u) continue;
+                        if (kern != HBDIA_KERNEL_PIPE && u) continue;  // unroll is the pipelined kernel's knob
                         Choice c;
                         c.kernel = kern;
                         c.unroll = u;

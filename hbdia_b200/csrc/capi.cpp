@@ -527,7 +527,7 @@ int hbdia_matrix_device_status(const hbdia_matrix *m, int32_t *bits) {
 int hbdia_matrix_set_kernel(hbdia_matrix *m, int32_t kernel) {
     return guarded([&] {
         need(m != nullptr, HBDIA_ERR_INVALID_ARGUMENT, "null matrix");
-        need(kernel >= HBDIA_KERNEL_AUTO && kernel <= HBDIA_KERNEL_PIPE, HBDIA_ERR_INVALID_ARGUMENT,
+        need(kernel >= HBDIA_KERNEL_AUTO && kernel <= HBDIA_KERNEL_QUAD, HBDIA_ERR_INVALID_ARGUMENT,
              "unknown kernel");
         m->plan.kernel = kernel;
     });
@@ -557,6 +557,17 @@ int hbdia_matrix_set_tuning(hbdia_matrix *m, int32_t key, int32_t value) {
         if (key == HBDIA_TUNE_TAIL) {
             need(value >= -1 && value <= 1, HBDIA_ERR_INVALID_ARGUMENT, "tail must be -1, 0 or 1");
             m->plan.maskedTail = value;
+            return;
+        }
+        if (key == HBDIA_TUNE_QUAD_GROUP) {
+            need(value == 0 || value == 1 || value == 2 || value == 4 || value == 8, HBDIA_ERR_INVALID_ARGUMENT,
+                 "quad group must be 0, 1, 2, 4 or 8");
+            m->plan.quadGroup = value;
+            return;
+        }
+        if (key == HBDIA_TUNE_STAGES) {
+            need(value >= 0 && value <= 4, HBDIA_ERR_INVALID_ARGUMENT, "stage configuration must be 0-4");
+            m->plan.xsConfig = value;
             return;
         }
         if (key == HBDIA_TUNE_SPMM_TILE) {
@@ -592,10 +603,10 @@ int hbdia_matrix_set_wait_timeout(hbdia_matrix *m, uint64_t ns) {
     });
 }
 
-int hbdia_matrix_test_skip_chunk(hbdia_matrix *m, int32_t chunk) {
+int hbdia_matrix_test_skip_tile(hbdia_matrix *m, int32_t tile) {
     return guarded([&] {
-        need(m != nullptr && chunk >= -1, HBDIA_ERR_INVALID_ARGUMENT, "bad chunk");
-        m->plan.skipChunk = chunk;
+        need(m != nullptr && tile >= -1, HBDIA_ERR_INVALID_ARGUMENT, "bad tile");
+        m->plan.skipTile = tile;
     });
 }
 

@@ -24,8 +24,6 @@
 //      CSR row pointer.
 //   6. histograms (HBDIA.cpp:619-631) and numberDiagonals (distinct offsets
 //      over all blocks) with atomics.
-// The staged kernel's chunk schedule is not built (STAGED falls back to the
-// warp kernel on such a plan).
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -440,7 +438,9 @@ void convert_on_device(const Coo<T> &coo, int32_t bw, int32_t thr, int64_t maxCo
     DevicePlan Q;
     Q.kernel = P.kernel;
     Q.waitTimeoutNs = P.waitTimeoutNs;
-    Q.skipChunk = P.skipChunk;
+    Q.skipTile = P.skipTile;
+    Q.xsConfig = P.xsConfig;
+    Q.quadGroup = P.quadGroup;
     Q.unroll = P.unroll;
     free_plan(P);
     Q.dtype = dtype;

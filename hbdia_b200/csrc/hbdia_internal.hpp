@@ -7,7 +7,6 @@
 #include <string>
 #include <vector>
 
-#include "chunks.hpp"
 #include "hbdia_b200.h"
 
 namespace hbdia {
@@ -127,15 +126,12 @@ struct DevicePlan {
     void *stream = nullptr;              // cudaStream_t owned by the plan
     void *xScratch = nullptr, *yScratch = nullptr;  // hbdia_spmv_host buffers
     int64_t bytesPerSpmv = 0;            // algorithmic HBM bytes of one SpMV
-    // staged (TMA) kernel schedule, blockWidth 32 only
-    int32_t numChunks = 0;
-    int32_t *chunkRec = nullptr;         // kRecInts per chunk
-    void *windows = nullptr;             // XWindow lists
-    int64_t numWindows = 0;
-    int32_t *status = nullptr;           // device error bits of bounded waits
+    int32_t *status = nullptr;           // device error bits of bounded waits (staged kernel)
     int32_t kernel = HBDIA_KERNEL_AUTO;  // hbdia_kernel choice
     uint64_t waitTimeoutNs = 2000000000ull;
-    int32_t skipChunk = -1;              // test hook of the staged kernel
+    int32_t skipTile = -1;               // test hook of the staged kernel
+    int32_t xsConfig = 0;                // HBDIA_TUNE_STAGES: staged kernel's shape (0: default)
+    int32_t quadGroup = 0;               // HBDIA_TUNE_QUAD_GROUP: quad kernel's offsets in flight (0: default)
     int32_t unroll = 0;                  // offsets in flight per lane (0: default)
     std::map<int32_t, int32_t> spmmTile; // autotuned RHS tile per k
     int32_t spmmTileForced = 0;          // HBDIA_TUNE_SPMM_TILE (0: autotuned / default)
@@ -158,9 +154,6 @@ template <typename T>
 void convert_on_device(const Coo<T> &coo, int32_t blockWidth, int32_t threshold, int64_t maxCoo, int storage,
                        DevicePlan &P, DeviceLayoutMeta &meta);
 
-void build_chunk_schedule(int32_t n, int32_t numBlocks, int32_t numTiles, const int32_t *blkOff,
-                          const int32_t *offs, const int32_t *cooTile, int vrows, int xcap,
-                          int xElemBytes, std::vector<int32_t> &rec, std::vector<XWindow> &win);
 // kernel that launch_spmv would use for x (HBDIA_KERNEL_*)
 int32_t select_kernel(const DevicePlan &P, const void *x);
 

@@ -14,6 +14,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <type_traits>
@@ -21,7 +22,8 @@
 #include "args.cuh"
 #include "hbdia_internal.hpp"
 #include "spmv_kernels.cuh"
-#include "spmv_tma.cuh"
+#include "spmv_quad.cuh"
+#include "spmv_xstage.cuh"
 #include "spmm_kernels.cuh"
 
 namespace hbdia {
@@ -36,9 +38,6 @@ void check_cuda(int err, const char *what) {
 namespace {
 
 constexpr int kUnroll = 9;  // offsets in flight per lane in the bw == 32 kernels
-// the staged kernel's shared memory must fit one CTA per SM (227 KB on sm_100)
-static_assert(sizeof(dev::TmaSmem<double, double>) <= 232448, "staged SpMV stage ring too large");
-static_assert(sizeof(dev::TmaSmem<float, float>) <= 232448, "staged SpMV stage ring too large");
 
 size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
 
@@ -77,7 +76,9 @@ void build_plan(const HostLayout<T> &L, int storage, DevicePlan &P, const Column
     DevicePlan Q;
     Q.kernel = P.kernel;  // settings survive a rebuild
     Q.waitTimeoutNs = P.waitTimeoutNs;
-    Q.skipChunk = P.skipChunk;
+    Q.skipTile = P.skipTile;
+    Q.xsConfig = P.xsConfig;
+    Q.quadGroup = P.quadGroup;
     Q.unroll = P.unroll;
     Q.prefetchL2 = P.prefetchL2;
     Q.maskedTail = P.maskedTail;
@@ -145,17 +146,6 @@ void build_plan(const HostLayout<T> &L, int storage, DevicePlan &P, const Column
     std::vector<int32_t> tile(static_cast<size_t>(Q.numTiles) + 1);
     for (int64_t t = 0; t <= Q.numTiles; ++t) tile[t] = crp[std::min<int64_t>(t * 32, Q.n)];
 
-    // chunk schedule of the staged kernel (blockWidth 32)
-    std::vector<int32_t> rec;
-    std::vector<XWindow> win;
-    if (Q.bw == 32 && !W) {  // (the schedule's x ranges assume x holds numRows entries)
-        // x windows are prefetched into L2, not staged: no capacity limit
-        build_chunk_schedule(Q.n, Q.numBlocks, Q.numTiles, L.blockStart.data(), ko, tile.data(),
-                             dev::kVRows, 1 << 30, static_cast<int>(sizeof(T)), rec, win);
-        Q.numChunks = static_cast<int32_t>(rec.size() / kRecInts);
-        Q.numWindows = static_cast<int64_t>(win.size());
-    }
-
     // host-side value conversion for reduced storage
     const size_t vsz = storage_bytes(storage, Q.dtype);
     std::vector<float> vf, sf;
@@ -197,8 +187,6 @@ void build_plan(const HostLayout<T> &L, int storage, DevicePlan &P, const Column
     const size_t oCV = carve(Q.nCoo * sizeof(T));
     const size_t oRP = carve((static_cast<size_t>(Q.n) + 1) * sizeof(int32_t));
     const size_t oTile = carve((static_cast<size_t>(Q.numTiles) + 1) * sizeof(int32_t));
-    const size_t oRec = carve(rec.size() * sizeof(int32_t));
-    const size_t oWin = carve(win.size() * sizeof(XWindow));
     const size_t oStatus = carve(sizeof(int32_t));
     Q.bytes = off;
     check_cuda(cudaMalloc(&Q.base, Q.bytes), "cudaMalloc(matrix layout)");
@@ -213,8 +201,6 @@ void build_plan(const HostLayout<T> &L, int storage, DevicePlan &P, const Column
         Q.cooVal = base + oCV;
         Q.cooRowPtr = reinterpret_cast<int32_t *>(base + oRP);
         Q.cooTile = reinterpret_cast<int32_t *>(base + oTile);
-        Q.chunkRec = rec.empty() ? nullptr : reinterpret_cast<int32_t *>(base + oRec);
-        Q.windows = win.empty() ? nullptr : base + oWin;
         Q.status = reinterpret_cast<int32_t *>(base + oStatus);
         check_cuda(cudaMemset(Q.status, 0, sizeof(int32_t)), "cudaMemset(status)");
         auto up = [](void *dst, const void *src, size_t bytes) {
@@ -229,8 +215,6 @@ void build_plan(const HostLayout<T> &L, int storage, DevicePlan &P, const Column
         up(Q.cooVal, cv, Q.nCoo * sizeof(T));
         up(Q.cooRowPtr, crp, (static_cast<size_t>(Q.n) + 1) * sizeof(int32_t));
         up(Q.cooTile, tile.data(), (static_cast<size_t>(Q.numTiles) + 1) * sizeof(int32_t));
-        if (Q.chunkRec) up(Q.chunkRec, rec.data(), rec.size() * sizeof(int32_t));
-        if (Q.windows) up(Q.windows, win.data(), win.size() * sizeof(XWindow));
         cudaStream_t s;
         check_cuda(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "cudaStreamCreate");
         Q.stream = s;
@@ -257,23 +241,55 @@ template void build_plan<float>(const HostLayout<float> &, int, DevicePlan &, co
 
 namespace {
 
-// One CTA per SM (the stage ring fills the SM's shared memory).  The
-// dynamic shared-memory opt-in is a per-device function attribute.
-template <typename VT, typename XT, int U>
-void launch_staged(const dev::TmaArgs<VT, XT> &T, int32_t numChunks, const XT *x, XT *y, cudaStream_t s) {
-    const size_t smem = sizeof(dev::TmaSmem<VT, XT>);
-    static uint64_t configured = 0;  // bit d: attribute set on device d
-    int dev = 0, sms = 0;
-    check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
-    if (dev >= 64 || !(configured & (uint64_t(1) << dev))) {
-        check_cuda(cudaFuncSetAttribute(dev::spmv_bw32_tma<VT, XT, U>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        static_cast<int>(smem)),
+int stream_device(cudaStream_t s) {
+    int dev = 0;
+    check_cuda(cudaStreamGetDevice(s, &dev), "cudaStreamGetDevice");
+    return dev;
+}
+
+// The staged kernel with U stored values in flight per lane and stages of SB
+// bytes; as many 256-thread CTAs as fit on all SMs at once (shared memory and
+// registers decide).
+template <typename VT, typename XT, int U, int SB>
+void launch_xs_cfg(const dev::XsArgs<VT, XT> &A, const XT *x, XT *y, cudaStream_t s) {
+    auto kernel = dev::spmv_bw32_xs<VT, XT, U, SB>;
+    constexpr size_t smem = dev::xs_smem_bytes(SB);
+    static_assert(smem <= 232448, "staged SpMV stages too large for one CTA");
+    constexpr int threads = dev::kXsWarps * 32;
+    // bit d: the shared-memory opt-in is in place on device d.  Several host
+    // threads (a server's scheduler and solver threads) launch at once.
+    static std::atomic<uint64_t> configured{0};
+    const int dev = stream_device(s);
+    const uint64_t bit = uint64_t(1) << (dev < 63 ? dev : 63);
+    if (dev >= 63 || !(configured.load(std::memory_order_acquire) & bit)) {
+        check_cuda(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
                    "cudaFuncSetAttribute(staged SpMV)");
-        if (dev < 64) configured |= uint64_t(1) << dev;
+        if (dev < 63) configured.fetch_or(bit, std::memory_order_acq_rel);
     }
+    int sms = 0, perSm = 0;
     check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "cudaDeviceGetAttribute");
-    const unsigned grid = static_cast<unsigned>(std::min<int64_t>(sms, numChunks));
-    dev::spmv_bw32_tma<VT, XT, U><<<grid, dev::kTmaThreads, smem, s>>>(T, x, y);
+    check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kernel, threads, smem),
+               "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+    const int64_t ctasNeeded = (static_cast<int64_t>(A.a.numTiles) + dev::kXsWarps - 1) / dev::kXsWarps;
+    const unsigned grid = static_cast<unsigned>(
+        std::max<int64_t>(1, std::min<int64_t>(ctasNeeded, int64_t(sms) * std::max(1, perSm))));
+    kernel<<<grid, threads, smem, s>>>(A, x, y);
+}
+
+// Staged kernel shapes (HBDIA_TUNE_STAGES): values in flight per lane U
+// (32 for 4- and 2-byte values, 16 for 8-byte ones by default) and stage
+// bytes SB (x runs of up to ~2.7 KB by default: a 27-point stencil tile needs
+// 2.6 KB).
+template <typename VT, typename XT>
+void launch_xs(const dev::XsArgs<VT, XT> &A, int32_t cfg, const XT *x, XT *y, cudaStream_t s) {
+    constexpr int Ud = sizeof(VT) == 8 ? 16 : 32;
+    constexpr int Ua = sizeof(VT) == 8 ? 32 : 16;
+    switch (cfg) {
+        case 2: return launch_xs_cfg<VT, XT, Ud, 4352>(A, x, y, s);
+        case 3: return launch_xs_cfg<VT, XT, Ua, 3328>(A, x, y, s);
+        case 4: return launch_xs_cfg<VT, XT, Ud, 6400>(A, x, y, s);
+        default: return launch_xs_cfg<VT, XT, Ud, 3328>(A, x, y, s);
+    }
 }
 
 // Persistent grid: as many 256-thread CTAs as fit on all SMs at once (the
@@ -281,8 +297,8 @@ void launch_staged(const dev::TmaArgs<VT, XT> &T, int32_t numChunks, const XT *x
 template <typename VT, typename XT, typename Kernel>
 void launch_pipe(Kernel kernel, const dev::SpmvArgs<VT, XT> &a, int32_t numTiles, const XT *x, XT *y,
                  cudaStream_t s, int threads = 256) {
-    int dev = 0, sms = 0, perSm = 0;
-    check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
+    int sms = 0, perSm = 0;
+    const int dev = stream_device(s);
     check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "cudaDeviceGetAttribute");
     check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kernel, threads, 0),
                "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
@@ -291,6 +307,30 @@ void launch_pipe(Kernel kernel, const dev::SpmvArgs<VT, XT> &a, int32_t numTiles
     const unsigned grid = static_cast<unsigned>(std::max<int64_t>(1, std::min<int64_t>(ctasNeeded,
                                                                                        int64_t(sms) * std::max(1, perSm))));
     kernel<<<grid, threads, 0, s>>>(a, x, y);
+}
+
+// The quad kernel: U offsets of four blocks in flight per lane (default 4
+// for 4- and 2-byte values, 2 for 8-byte ones), L2 prefetch of the next
+// quad's values when x exceeds L2 (the pipelined kernel's rule).
+template <typename VT, typename XT>
+void launch_quad(const DevicePlan &P, const dev::SpmvArgs<VT, XT> &a, const XT *x, XT *y, cudaStream_t s) {
+    int l2 = 0;
+    check_cuda(cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, stream_device(s)), "cudaDeviceGetAttribute(L2)");
+    const bool pf = P.prefetchL2 > 0 ||
+                    (P.prefetchL2 < 0 &&
+                     static_cast<int64_t>(std::max(P.n, P.numCols)) * static_cast<int64_t>(sizeof(XT)) > l2);
+    const int32_t g = P.quadGroup ? P.quadGroup : (sizeof(VT) == 8 ? 2 : 4);
+    const int32_t quads = (P.numTiles + 3) / 4 * 4;  // tiles covered by whole quads (4 per warp)
+#define HBDIA_QUAD(U)                                                                                  \
+    return pf ? launch_pipe(dev::spmv_bw32_quad<VT, XT, U, true>, a, quads / 4, x, y, s)              \
+              : launch_pipe(dev::spmv_bw32_quad<VT, XT, U, false>, a, quads / 4, x, y, s)
+    switch (g) {
+        case 1: HBDIA_QUAD(1);
+        case 2: HBDIA_QUAD(2);
+        case 8: HBDIA_QUAD(8);
+        default: HBDIA_QUAD(4);
+    }
+#undef HBDIA_QUAD
 }
 
 template <typename VT, typename XT>
@@ -303,8 +343,8 @@ void launch_pipe_tuned(const DevicePlan &P, const dev::SpmvArgs<VT, XT> &a, cons
     // -10 % at 57 MB and below).
     bool pf = P.prefetchL2 > 0;
     if (P.prefetchL2 < 0) {
-        int dev = 0, l2 = 0;
-        check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
+        int l2 = 0;
+        const int dev = stream_device(s);
         check_cuda(cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, dev), "cudaDeviceGetAttribute(L2)");
         pf = static_cast<int64_t>(std::max(P.n, P.numCols)) * static_cast<int64_t>(sizeof(XT)) > l2;
     }
@@ -327,18 +367,16 @@ void launch_typed(const DevicePlan &P, const void *x, void *y, cudaStream_t s) {
     XT *yp = static_cast<XT *>(y);
     const int32_t kern = select_kernel(P, x);
     if (kern == HBDIA_KERNEL_STAGED) {
-        dev::TmaArgs<VT, XT> T;
-        T.a = a;
-        T.rec = P.chunkRec;
-        T.win = static_cast<const XWindow *>(P.windows);
-        T.numChunks = P.numChunks;
-        T.status = P.status;
-        T.timeoutNs = P.waitTimeoutNs;
-        T.skipChunk = P.skipChunk;
-        if (P.unroll == 27) launch_staged<VT, XT, 27>(T, P.numChunks, xp, yp, s);
-        else launch_staged<VT, XT, kUnroll>(T, P.numChunks, xp, yp, s);
+        dev::XsArgs<VT, XT> A;
+        A.a = a;
+        A.status = P.status;
+        A.timeoutNs = P.waitTimeoutNs;
+        A.skipTile = P.skipTile;
+        launch_xs<VT, XT>(A, P.xsConfig, xp, yp, s);
     } else if (kern == HBDIA_KERNEL_PIPE) {
         launch_pipe_tuned<VT, XT>(P, a, xp, yp, s);
+    } else if (kern == HBDIA_KERNEL_QUAD) {
+        launch_quad<VT, XT>(P, a, xp, yp, s);
 
     } else if (kern == HBDIA_KERNEL_WARP) {
         const int64_t warpsPerCta = 8;
@@ -355,9 +393,12 @@ void launch_typed(const DevicePlan &P, const void *x, void *y, cudaStream_t s) {
 
 int32_t select_kernel(const DevicePlan &P, const void *x) {
     const bool bw32 = P.bw == 32;
-    const bool aligned = (reinterpret_cast<uintptr_t>(x) & 15) == 0;
-    // the staged kernel does row/column arithmetic in 32 bits (n <= 2^30)
-    const bool stagedOk = bw32 && aligned && P.numChunks > 0 && P.n <= (1 << 30);
+    // the staged kernel bulk-copies x and the value slabs (16-byte aligned
+    // starts), needs a status word for its bounded waits, and does row/column
+    // arithmetic in 32 bits (n <= 2^30)
+    const bool aligned = (reinterpret_cast<uintptr_t>(x) & 15) == 0 && (reinterpret_cast<uintptr_t>(P.vals) & 15) == 0;
+    // (x holds numCols >= the column bound entries: the runs never pass its end)
+    const bool stagedOk = bw32 && aligned && P.status && P.numCols >= P.xn && P.n <= (1 << 30);
     const bool pipeOk = bw32 && P.n <= (1 << 30);  // 32-bit row/column arithmetic
     switch (P.kernel) {
         case HBDIA_KERNEL_ROWWISE: return HBDIA_KERNEL_ROWWISE;
@@ -367,9 +408,15 @@ int32_t select_kernel(const DevicePlan &P, const void *x) {
         case HBDIA_KERNEL_PIPE:
             if (pipeOk) return HBDIA_KERNEL_PIPE;
             return bw32 ? HBDIA_KERNEL_WARP : HBDIA_KERNEL_ROWWISE;
+        case HBDIA_KERNEL_QUAD:
+            if (pipeOk) return HBDIA_KERNEL_QUAD;
+            return bw32 ? HBDIA_KERNEL_WARP : HBDIA_KERNEL_ROWWISE;
         case HBDIA_KERNEL_WARP: return bw32 ? HBDIA_KERNEL_WARP : HBDIA_KERNEL_ROWWISE;
         default:  // AUTO: the fastest measured on B200 for blockWidth 32
-            if (pipeOk) return HBDIA_KERNEL_PIPE;
+            // (BF16 storage: the quad kernel, 4-12 % ahead of the pipelined
+            // one on the 27-point 256^3 and banded 8M workloads; FP64 / FP32
+            // values: the pipelined kernel)
+            if (pipeOk) return P.storage == HBDIA_STORE_BF16_SCALED ? HBDIA_KERNEL_QUAD : HBDIA_KERNEL_PIPE;
             return bw32 ? HBDIA_KERNEL_WARP : HBDIA_KERNEL_ROWWISE;
     }
 }

@@ -60,15 +60,18 @@ typedef enum hbdia_value_storage {
 } hbdia_value_storage;
 
 /* SpMV kernel choice (all give bit-identical y).  AUTO picks the kernel
- * measured fastest on B200: PIPE for blockWidth 32, else ROWWISE.  STAGED
- * needs a 16-byte aligned x (else WARP runs); PIPE and STAGED need
- * numRows <= 2^30. */
+ * measured fastest on B200: for blockWidth 32 QUAD with BF16 value storage,
+ * PIPE otherwise; ROWWISE for other block widths.  STAGED
+ * needs a 16-byte aligned x and value array (else WARP runs); PIPE and STAGED
+ * need numRows <= 2^30. */
 typedef enum hbdia_kernel {
     HBDIA_KERNEL_AUTO = 0,
     HBDIA_KERNEL_ROWWISE = 1, /* one thread per row, any blockWidth             */
     HBDIA_KERNEL_WARP = 2,    /* one warp per 32-row block, blockWidth 32       */
-    HBDIA_KERNEL_STAGED = 3,  /* persistent TMA-staged pipeline, blockWidth 32  */
-    HBDIA_KERNEL_PIPE = 4     /* persistent warp per block, pipelined across blocks, blockWidth 32 */
+    HBDIA_KERNEL_STAGED = 3,  /* persistent; each warp bulk-copies its next tiles' values and
+                                 x runs into shared memory, blockWidth 32 */
+    HBDIA_KERNEL_PIPE = 4,    /* persistent warp per block, pipelined across blocks, blockWidth 32 */
+    HBDIA_KERNEL_QUAD = 5     /* persistent warp per 4 blocks sharing one offset list, blockWidth 32 */
 } hbdia_kernel;
 
 typedef struct hbdia_matrix hbdia_matrix; /* HBDIA<T>       (include/Format/HBDIA.hpp:24-291)      */
@@ -374,12 +377,23 @@ int hbdia_matrix_selected_kernel(const hbdia_matrix *m, const void *x, int32_t *
  * -1 (default) = masked when at least half of the stored offsets lie past
  * full groups (e.g. 7-point stencils: 7 offsets per block).  Measured on
  * B200: 7-point stencil +13-20 % (FP64), +40-49 % (FP32 storage); the masked
- * form costs 80 registers in FP64 and 14-26 % where there is no tail. */
+ * form costs 80 registers in FP64 and 14-26 % where there is no tail.
+ * HBDIA_TUNE_STAGES: the staged kernel's shape: 0 (default) or 1 = all of
+ * a tile's stored values in flight per lane (16 per group for 8-byte values)
+ * and 3.3 KB stages (x runs of up to ~2.7 KB), 2 = 4.3 KB stages, 3 = the
+ * other group size (16 for 4- and 2-byte values, 32 for 8-byte ones),
+ * 4 = 6.4 KB stages.  Tiles whose x runs do not fit a stage read x from
+ * global memory.
+ * HBDIA_TUNE_QUAD_GROUP: offsets of the four blocks in flight per lane in the
+ * quad kernel (0 = default: 4 for 4- and 2-byte values, 2 for 8-byte ones;
+ * or 1, 2, 4, 8). */
 typedef enum hbdia_tuning_key {
     HBDIA_TUNE_UNROLL = 1,
     HBDIA_TUNE_SPMM_TILE = 2,
     HBDIA_TUNE_PREFETCH = 3,
-    HBDIA_TUNE_TAIL = 4
+    HBDIA_TUNE_TAIL = 4,
+    HBDIA_TUNE_STAGES = 5,
+    HBDIA_TUNE_QUAD_GROUP = 6
 } hbdia_tuning_key;
 int hbdia_matrix_set_tuning(hbdia_matrix *m, int32_t key, int32_t value);
 
@@ -404,10 +418,11 @@ int hbdia_autotune_clear(void);
 /* Time limit of every device-side wait of the staged kernel (default 2 s). */
 int hbdia_matrix_set_wait_timeout(hbdia_matrix *m, uint64_t nanoseconds);
 
-/* Test hook of the staged kernel: its producer never publishes chunk
- * `chunk`, so the waiting consumers run into their time limit and the kernel
- * reports HBDIA_ERR_DEVICE_TIMEOUT at the next synchronize.  -1 turns it off. */
-int hbdia_matrix_test_skip_chunk(hbdia_matrix *m, int32_t chunk);
+/* Test hook of the staged kernel: the warp that owns 32-row tile `tile` never
+ * issues that tile's copies, so its wait runs into the time limit and the
+ * kernel reports HBDIA_ERR_DEVICE_TIMEOUT at the next synchronize.  -1 turns
+ * it off. */
+int hbdia_matrix_test_skip_tile(hbdia_matrix *m, int32_t tile);
 
 /* ---------------------------------------------------------------- solver */
 

@@ -115,7 +115,32 @@ class Restated:
         lib.orc_spmv_f32.argtypes = [_vp, _vp, _vp]
         lib.orc_spmv_f64_values.argtypes = [_vp, _vp, _vp, _vp]
         lib.orc_coo_spmv_f64.argtypes = [_vp, _vp, _vp, ctypes.c_int64, _vp, ctypes.c_int32, _vp]
+        lib.orc_fill_uniform.argtypes = [_vp, ctypes.c_int64, ctypes.c_double, ctypes.c_double, ctypes.c_uint64]
+        lib.orc_workload_stencil27.argtypes = [ctypes.c_int32] * 3 + [ctypes.c_double] * 5 + [ctypes.c_uint64, _i64p,
+                                                                                               _vp, _vp, _vp]
+        lib.orc_workload_stencil27.restype = ctypes.c_int
         self.lib = lib
+
+    def fill_uniform(self, n, lo, hi, seed):
+        """x[i] = lo + (hi - lo) * U[0, 1), MT19937-64(seed): the bench's x."""
+        out = np.empty(n, np.float64)
+        self.lib.orc_fill_uniform(_ptr(out), n, lo, hi, seed)
+        return out
+
+    def workload_stencil27(self, nx, ny, nz, center, neighbor, frac, lo, hi, seed):
+        """The bench's 27-point stencil with extra off-pattern entries
+        (rows, cols, vals), built by the oracle's own restatement."""
+        nnz = ctypes.c_int64()
+        if self.lib.orc_workload_stencil27(nx, ny, nz, center, neighbor, frac, lo, hi, seed, ctypes.byref(nnz),
+                                           None, None, None) != 0:
+            raise ValueError("bad stencil arguments")
+        rows = np.empty(nnz.value, np.int32)
+        cols = np.empty(nnz.value, np.int32)
+        vals = np.empty(nnz.value, np.float64)
+        if self.lib.orc_workload_stencil27(nx, ny, nz, center, neighbor, frac, lo, hi, seed, ctypes.byref(nnz),
+                                           _ptr(rows), _ptr(cols), _ptr(vals)) != 0:
+            raise MemoryError("stencil workload")
+        return rows, cols, vals
 
     def convert(self, rows, cols, vals, num_rows, num_cols, bw=32, thr=1, max_coo=1_000_000_000):
         rows = np.ascontiguousarray(rows, np.int32)

@@ -336,3 +336,162 @@ void orc_coo_spmv_f64(const int32_t *rows, const int32_t *cols, const double *va
     }
     if (current >= 0 && current < numRows) y[current] = row_sum;
 }
+
+/* ------------------------------------------------------------------------
+ * Seeded benchmark workloads, restated so that bench.py's reference arm and
+ * the tests can build the bench matrix without the product library.  This
+ * follows the product's own generator (hbdia_b200/csrc/generate.cpp,
+ * generate_stencil / fill_uniform), which tests/test_oracle.py pins entry for
+ * entry: MT19937-64 (Matsumoto & Nishimura's published generator, the one
+ * std::mt19937_64 implements), a draw in [0, n) as the high 64 bits of
+ * draw * n, a draw in [0, 1) as the top 53 bits times 2^-53. */
+typedef struct {
+    uint64_t mt[312];
+    int idx;
+} orc_mt64;
+
+static void mt64_seed(orc_mt64 *g, uint64_t seed) {
+    g->mt[0] = seed;
+    for (int i = 1; i < 312; ++i)
+        g->mt[i] = 6364136223846793005ULL * (g->mt[i - 1] ^ (g->mt[i - 1] >> 62)) + (uint64_t)i;
+    g->idx = 312;
+}
+
+static uint64_t mt64_next(orc_mt64 *g) {
+    if (g->idx >= 312) {
+        for (int i = 0; i < 312; ++i) {
+            const uint64_t v = (g->mt[i] & 0xFFFFFFFF80000000ULL) | (g->mt[(i + 1) % 312] & 0x7FFFFFFFULL);
+            uint64_t va = v >> 1;
+            if (v & 1) va ^= 0xB5026F5AA96619E9ULL;
+            g->mt[i] = g->mt[(i + 156) % 312] ^ va;
+        }
+        g->idx = 0;
+    }
+    uint64_t y = g->mt[g->idx++];
+    y ^= (y >> 29) & 0x5555555555555555ULL;
+    y ^= (y << 17) & 0x71D67FFFEDA60000ULL;
+    y ^= (y << 37) & 0xFFF7EEE000000000ULL;
+    y ^= y >> 43;
+    return y;
+}
+
+static uint64_t mt64_bounded(orc_mt64 *g, uint64_t n) {
+    return (uint64_t)(((unsigned __int128)mt64_next(g) * n) >> 64);
+}
+
+static double mt64_unit(orc_mt64 *g) { return (double)(mt64_next(g) >> 11) * 0x1.0p-53; }
+
+void orc_fill_uniform(double *out, int64_t n, double lo, double hi, uint64_t seed) {
+    orc_mt64 g;
+    mt64_seed(&g, seed);
+    for (int64_t i = 0; i < n; ++i) out[i] = lo + (hi - lo) * mt64_unit(&g);
+}
+
+static int64_t iabs64(int64_t v) { return v < 0 ? -v : v; }
+
+int orc_workload_stencil27(int32_t nx, int32_t ny, int32_t nz, double center, double neighbor, double frac,
+                           double lo, double hi, uint64_t seed, int64_t *nnzOut, int32_t *rows, int32_t *cols,
+                           double *vals) {
+    if (nx <= 0 || ny <= 0 || nz <= 0 || !nnzOut) return -1;
+    const int64_t n = (int64_t)nx * ny * nz;
+    if (n > 2147483647LL) return -1;
+    const int64_t stencilNnz = (3LL * nx - 2) * (3LL * ny - 2) * (3LL * nz - 2);
+    const int64_t nExtra = (int64_t)floor(frac * (double)stencilNnz);
+    *nnzOut = stencilNnz + nExtra;
+    if (!rows) return 0;
+    /* extras: rows, columns, values in draw order, outside the stencil and
+     * without repeats */
+    int32_t *er = NULL, *ec = NULL;
+    double *ev = NULL;
+    uint64_t *set = NULL;
+    int64_t cap = 16;
+    if (nExtra > 0) {
+        er = (int32_t *)malloc((size_t)nExtra * sizeof(int32_t));
+        ec = (int32_t *)malloc((size_t)nExtra * sizeof(int32_t));
+        ev = (double *)malloc((size_t)nExtra * sizeof(double));
+        while (cap < 2 * nExtra + 16) cap <<= 1;
+        set = (uint64_t *)calloc((size_t)cap, sizeof(uint64_t));
+        if (!er || !ec || !ev || !set) {
+            free(er), free(ec), free(ev), free(set);
+            return -1;
+        }
+        orc_mt64 g;
+        mt64_seed(&g, seed);
+        for (int64_t t = 0; t < nExtra; ++t) {
+            int64_t r, c;
+            for (;;) {
+                r = (int64_t)mt64_bounded(&g, (uint64_t)n);
+                c = (int64_t)mt64_bounded(&g, (uint64_t)n);
+                const int64_t dx = iabs64(c % nx - r % nx), dy = iabs64((c / nx) % ny - (r / nx) % ny),
+                              dz = iabs64(c / ((int64_t)nx * ny) - r / ((int64_t)nx * ny));
+                if (dx <= 1 && dy <= 1 && dz <= 1) continue; /* inside the stencil */
+                const uint64_t key = (uint64_t)r * (uint64_t)n + (uint64_t)c + 1u;
+                uint64_t h = key * 0x9E3779B97F4A7C15ULL;
+                int64_t slot = (int64_t)(h >> 20) & (cap - 1);
+                int dup = 0;
+                while (set[slot]) {
+                    if (set[slot] == key) {
+                        dup = 1;
+                        break;
+                    }
+                    slot = (slot + 1) & (cap - 1);
+                }
+                if (dup) continue;
+                set[slot] = key;
+                break;
+            }
+            er[t] = (int32_t)r;
+            ec[t] = (int32_t)c;
+            ev[t] = lo + (hi - lo) * mt64_unit(&g);
+        }
+        free(set);
+    }
+    /* extras grouped by row, draw order kept */
+    int64_t *xstart = (int64_t *)calloc((size_t)n + 1, sizeof(int64_t));
+    int64_t *order = nExtra > 0 ? (int64_t *)malloc((size_t)nExtra * sizeof(int64_t)) : NULL;
+    if (!xstart || (nExtra > 0 && !order)) {
+        free(xstart), free(order), free(er), free(ec), free(ev);
+        return -1;
+    }
+    for (int64_t t = 0; t < nExtra; ++t) xstart[er[t] + 1]++;
+    for (int64_t r = 0; r < n; ++r) xstart[r + 1] += xstart[r];
+    {
+        int64_t *fill = (int64_t *)malloc((size_t)n * sizeof(int64_t));
+        if (!fill) {
+            free(xstart), free(order), free(er), free(ec), free(ev);
+            return -1;
+        }
+        memcpy(fill, xstart, (size_t)n * sizeof(int64_t));
+        for (int64_t t = 0; t < nExtra; ++t) order[fill[er[t]]++] = t;
+        free(fill);
+    }
+    /* rows in order: the stencil entries (z, y, x neighbours ascending), then
+     * the row's extras */
+    const int64_t plane = (int64_t)nx * ny;
+    int64_t p = 0;
+    for (int64_t r = 0; r < n; ++r) {
+        const int64_t x = r % nx, y = (r / nx) % ny, z = r / plane;
+        for (int dz = -1; dz <= 1; ++dz) {
+            if (z + dz < 0 || z + dz >= nz) continue;
+            for (int dy = -1; dy <= 1; ++dy) {
+                if (y + dy < 0 || y + dy >= ny) continue;
+                for (int dx = -1; dx <= 1; ++dx) {
+                    if (x + dx < 0 || x + dx >= nx) continue;
+                    rows[p] = (int32_t)r;
+                    cols[p] = (int32_t)(r + dz * plane + dy * nx + dx);
+                    vals[p] = (dx == 0 && dy == 0 && dz == 0) ? center : neighbor;
+                    ++p;
+                }
+            }
+        }
+        for (int64_t q = xstart[r]; q < xstart[r + 1]; ++q) {
+            const int64_t t = order[q];
+            rows[p] = er[t];
+            cols[p] = ec[t];
+            vals[p] = ev[t];
+            ++p;
+        }
+    }
+    free(xstart), free(order), free(er), free(ec), free(ev);
+    return 0;
+}

@@ -53,4 +53,17 @@ void orc_spmv_f64_values(const orc_layout *h, const double *values, double *y, c
 void orc_coo_spmv_f64(const int32_t *rows, const int32_t *cols, const double *vals,
                       int64_t nnz, const double *x, int32_t numRows, double *y);
 
+/* Seeded benchmark workloads (restated from this library's own generator so
+ * that the checker and the reference's CPU arm need no product code):
+ * x[i] = lo + (hi - lo) * U[0, 1) from MT19937-64(seed) */
+void orc_fill_uniform(double *out, int64_t n, double lo, double hi, uint64_t seed);
+/* 27-point stencil on nx*ny*nz (index k*nx*ny + j*nx + i; centre `center`,
+ * neighbours `neighbor`) plus floor(frac * stencil entries) extra entries at
+ * uniform (row, column) positions outside the stencil, without repeats,
+ * values U(lo, hi); row-sorted, each row's stencil entries first.  Call with
+ * rows == NULL for the count.  Returns 0, or -1 on bad arguments. */
+int orc_workload_stencil27(int32_t nx, int32_t ny, int32_t nz, double center, double neighbor, double frac,
+                           double lo, double hi, uint64_t seed, int64_t *nnzOut, int32_t *rows, int32_t *cols,
+                           double *vals);
+
 #endif

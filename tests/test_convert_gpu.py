@@ -102,7 +102,7 @@ def test_stencil_float32_and_spmv(lib, orc):
     x = np.random.default_rng(2).uniform(-1, 1, n)
     xt = torch.from_numpy(x).cuda()
     yt = torch.zeros(n, dtype=torch.float64, device="cuda")
-    for kern in (lib.KERNEL_PIPE, lib.KERNEL_WARP, lib.KERNEL_ROWWISE, lib.KERNEL_STAGED):
+    for kern in (lib.KERNEL_PIPE, lib.KERNEL_QUAD, lib.KERNEL_WARP, lib.KERNEL_ROWWISE, lib.KERNEL_STAGED):
         dev.setKernel(kern)
         lib.spmv_device(dev, xt.data_ptr(), yt.data_ptr(), 0)
         torch.cuda.synchronize()

@@ -1,6 +1,6 @@
 """Failure detection without a GPU fault: every wait inside the staged SpMV
-kernel is bounded.  A test hook makes the producer withhold one chunk, so the
-waiting consumer warps run into their (here 50 ms) limit; the kernel records
+kernel is bounded.  A test hook makes the warp that owns tile 0 withhold that
+tile's copies, so its wait runs into the (here 50 ms) limit; the kernel records
 the error, drains its copies and returns, the host reports
 HBDIA_ERR_DEVICE_TIMEOUT at the next synchronize, and the context stays
 usable for the next, correct SpMV."""
@@ -24,14 +24,14 @@ def test_staged_wait_timeout_is_reported_and_recoverable(lib, orc):
     x = np.random.default_rng(2).uniform(-1, 1, n)
     xv, yv = lib.HBDIAVector(x), lib.HBDIAVector(np.zeros(n))
     assert m.selectedKernel(xv.getDeviceDataPtr()) == lib.KERNEL_STAGED
-    m.testSkipChunk(0)
+    m.testSkipTile(0)
     t = time.time()
     lib.hbdiaSpMV(m, xv, yv, True, False)
     with pytest.raises(lib.HBDIADeviceTimeout):
         m.synchronize()
     assert time.time() - t < 10.0
     assert m.deviceStatus() == 0          # reported once, then cleared
-    m.testSkipChunk(-1)
+    m.testSkipTile(-1)
     lib.hbdiaSpMV(m, xv, yv, True, False)
     m.synchronize()
     yref = orc.convert(rows, cols, vals, n, n, 32, 2).spmv(x)

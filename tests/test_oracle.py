@@ -102,3 +102,18 @@ def test_reference_coo_kernel_vs_restated_sorted(orc, ref):
     y_ref = ref.cpu_coo(rows, cols, vals).spmv(x, n)
     y_orc = orc.coo_spmv(rows, cols, vals, x, n)
     assert bits_equal(y_ref, y_orc)
+
+
+@pytest.mark.parametrize("grid,frac,seed", [((16, 16, 16), 0.01, 1), ((20, 12, 9), 0.02, 3), ((33, 8, 5), 0.0, 0)])
+def test_workload_generator_restated(orc, grid, frac, seed):
+    """The oracle's restated bench-workload generator (used by the reference
+    arm of bench.py, which must not load the product library) builds exactly
+    the product generator's matrix and x."""
+    import hbdia_b200 as hb
+    a = orc.workload_stencil27(*grid, 26.0, -1.0, frac, 0.1, 1.0, seed)
+    b = hb.generate_stencil27(*grid, 26.0, -1.0, frac, 0.1, 1.0, seed)
+    for u, v in zip(a, b):
+        assert u.dtype == v.dtype and np.array_equal(u.view(np.uint8), v.view(np.uint8))
+    n = grid[0] * grid[1] * grid[2]
+    assert np.array_equal(orc.fill_uniform(n, -1.0, 1.0, seed).view(np.uint64),
+                          hb.fill_uniform(n, -1.0, 1.0, seed).view(np.uint64))

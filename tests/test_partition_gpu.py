@@ -107,7 +107,7 @@ def _emulated(lib, rows, cols, vals, n, P, bw, thr, x, kernel=None):
 def test_emulated_ranks_equal_oracle(lib, orc, P, bw, thr, grid):
     rows, cols, vals, n = _stencil(lib, *grid, 0.01, 2)
     x = np.random.default_rng(P).uniform(-1, 1, n)
-    kernels = [None, lib.KERNEL_WARP, lib.KERNEL_ROWWISE, lib.KERNEL_STAGED] if bw == 32 else [None]
+    kernels = [None, lib.KERNEL_QUAD, lib.KERNEL_WARP, lib.KERNEL_ROWWISE, lib.KERNEL_STAGED] if bw == 32 else [None]
     whole = orc.convert(rows, cols, vals, n, n, bw, thr).spmv(x)
     for kern in kernels:
         ys, ranks = _emulated(lib, rows, cols, vals, n, P, bw, thr, x, kern)

@@ -36,7 +36,7 @@ def banded(lib):
     return n, rows, cols, vals, x
 
 
-@pytest.mark.parametrize("kernel", [4, 3, 2, 1], ids=["pipe", "staged", "warp", "rowwise"])
+@pytest.mark.parametrize("kernel", [4, 5, 3, 2, 1], ids=["pipe", "quad", "staged", "warp", "rowwise"])
 @pytest.mark.parametrize("storage", ["f32", "bf16"])
 def test_reduced_storage(lib, orc, banded, storage, kernel):
     n, rows, cols, vals, x = banded

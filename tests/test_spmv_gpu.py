@@ -22,7 +22,7 @@ def _scaled_err(y, yref, rows, cols, vals, x):
     return np.abs(y - yref) / np.maximum(scale, np.finfo(float).tiny)
 
 
-KERNELS = {"pipe": 4, "staged": 3, "warp": 2, "rowwise": 1}
+KERNELS = {"pipe": 4, "quad": 5, "staged": 3, "warp": 2, "rowwise": 1}
 
 
 @pytest.fixture(params=list(KERNELS), ids=list(KERNELS))
@@ -161,6 +161,52 @@ def test_tuning_keeps_bits(lib, orc, unroll):
     lib.hbdiaSpMV(m, lib.HBDIAVector(x), yv, True, False)
     m.synchronize()
     assert bits_equal(yv.toHost(), orc.convert(rows, cols, vals, n, n, 32, 2).spmv(x))
+
+
+@pytest.mark.parametrize("storage", [0, 1, 2], ids=["native", "f32", "bf16"])
+def test_staged_configs_keep_bits(lib, orc, storage):
+    """Every shape of the staged kernel (warps per CTA x stages per warp) gives
+    the pipelined kernel's y bit for bit, on a stencil whose tiles carry COO
+    entries (up to more than 32 in a tile) and boundary tiles, with an odd
+    row count (the unaligned end of x is loaded by plain loads)."""
+    n = 40 * 41 * 40 + 7
+    r, c, v = lib.generate_stencil27(40, 41, 40, 26.0, -1.0, 0.02, 0.1, 1.0, 9)
+    # a dense COO corner: tile 3 gets 70 remainder entries
+    extra_r = np.repeat(np.arange(96, 101, dtype=np.int32), 14)
+    extra_c = (np.arange(70, dtype=np.int32) * 977 + 5) % n
+    rows = np.concatenate([r, extra_r])
+    cols = np.concatenate([c, extra_c])
+    vals = np.concatenate([v, np.random.default_rng(5).uniform(0.1, 1.0, 70)])
+    o = np.argsort(rows, kind="stable")
+    rows, cols, vals = rows[o], cols[o], vals[o]
+    x = np.random.default_rng(6).uniform(-1, 1, n)
+    m = lib.HBDIA(rows, cols, vals, n, n)
+    m.convertToHBDIAFormat(32, 2, upload=False)
+    m.prepareForGPU(storage)
+    xv = lib.HBDIAVector(x)
+    m.setKernel(lib.KERNEL_PIPE)
+    yp = lib.HBDIAVector(np.zeros(n))
+    lib.hbdiaSpMV(m, xv, yp, True, False)
+    m.synchronize()
+    ypipe = yp.toHost()
+    if storage == 0:
+        assert bits_equal(ypipe, orc.convert(rows, cols, vals, n, n, 32, 2).spmv(x))
+    m.setKernel(lib.KERNEL_STAGED)
+    assert m.selectedKernel(xv.getDeviceDataPtr()) == lib.KERNEL_STAGED
+    for cfg in range(5):
+        m.setTuning(lib.TUNE_STAGES, cfg)
+        yv = lib.HBDIAVector(np.full(n, np.nan))
+        for _ in range(2):
+            lib.hbdiaSpMV(m, xv, yv, True, False)
+        m.synchronize()
+        assert bits_equal(yv.toHost(), ypipe), cfg
+    m.setKernel(lib.KERNEL_QUAD)
+    for g in (0, 1, 2, 4, 8):
+        m.setTuning(lib.TUNE_QUAD_GROUP, g)
+        yv = lib.HBDIAVector(np.full(n, np.nan))
+        lib.hbdiaSpMV(m, xv, yv, True, False)
+        m.synchronize()
+        assert bits_equal(yv.toHost(), ypipe), ("quad", g)
 
 
 def test_flags_and_errors(lib):
