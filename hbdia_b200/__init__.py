@@ -247,6 +247,13 @@ class HBDIA:
         _check(_load().hbdia_matrix_stream(self._h, ctypes.byref(s)))
         return s.value or 0
 
+    def deviceArrays(self) -> dict:
+        """The device arrays of the GPU getters (include/Format/HBDIA.hpp:155-165):
+        name -> device address (0 where the reference's getter returns null)."""
+        a = _lib.DeviceArrays()
+        _check(_load().hbdia_matrix_device_arrays(self._h, ctypes.byref(a)))
+        return {name: getattr(a, name) or 0 for name, _ in a._fields_}
+
     def bytesPerSpmv(self) -> int:
         """Algorithmic HBM bytes of one SpMV over the device layout."""
         return self.info().bytesPerSpmv
@@ -422,6 +429,13 @@ class HBDIAVector:
 
     getDeviceLocalPtr = getDeviceDataPtr
 
+    def getDeviceCOOResultsPtr(self) -> int:
+        """include/Format/HBDIAVector.hpp:53: a zeroed buffer of the vector's
+        length, kept for callers that clear it; the fused SpMV never uses it."""
+        p = ctypes.c_void_p()
+        _check(_load().hbdia_vector_coo_results_ptr(self._h, ctypes.byref(p)))
+        return p.value or 0
+
     def getLocalSize(self) -> int:
         return self._n
 
@@ -595,12 +609,15 @@ def generate_stencil27_spd(nx: int, ny: int, nz: int, shift: float = 1e-3, seed:
     return _two_call(_load().hbdia_generate_stencil27_spd, nx, ny, nz, float(shift), float(extra_fraction), seed)
 
 
-def cg_solve(matrix: HBDIA, b_ptr: int, x_ptr: int, tol: float = 1e-10, inner_storage: int = STORE_F32,
-             inner_tol: float = 1e-6, max_outer: int = 50, max_inner: int = 5000, check_every: int = 10,
-             stream: Optional[int] = None) -> "_lib.CgResult":
-    """Mixed-precision CG (FP64 refinement around reduced-storage inner CG) on
-    device buffers b, x (x: initial guess in, solution out)."""
-    o = _lib.CgOptions(tol, inner_tol, max_outer, max_inner, inner_storage, check_every)
+def cg_solve(matrix: HBDIA, b_ptr: int, x_ptr: int, tol: float = 1e-10, iter_storage: int = STORE_F32,
+             update_factor: float = 0.1, max_updates: int = 100, max_iterations: int = 20000,
+             check_every: int = 10, l2_persist: bool = True, stream: Optional[int] = None) -> "_lib.CgResult":
+    """CG on device buffers b, x (x: initial guess in, solution out): the
+    iterations' SpMVs use the ``iter_storage`` values (STORE_F32: mixed
+    precision, STORE_NATIVE: plain FP64 CG), with reliable updates of the
+    FP64 residual and convergence judged on it (hbdia_cg_solve)."""
+    o = _lib.CgOptions(tol, update_factor, max_updates, max_iterations, iter_storage, check_every,
+                       1 if l2_persist else 0)
     r = _lib.CgResult()
     _check(_load().hbdia_cg_solve(matrix.handle, ctypes.c_void_p(b_ptr), ctypes.c_void_p(x_ptr), ctypes.byref(o),
                                   _stream_arg(stream), ctypes.byref(r)))
@@ -692,7 +709,7 @@ class Server:
     served with continuous batching (each matrix's pending requests become one
     SpMM whenever the matrix is free), CG requests on a pool of solver threads.  ``options`` overrides
     fields of hbdia_server_default_options (memoryBudget, batching, maxRhs,
-    spmvStorage, cgInnerStorage, cgWorkers, cgTol, cgInnerTol, maxInFlight, ...)."""
+    spmvStorage, cgIterStorage, cgWorkers, cgTol, cgUpdateFactor, cgL2Persist, maxInFlight, ...)."""
 
     def __init__(self, **options):
         o = _lib.ServerOptions()

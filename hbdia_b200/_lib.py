@@ -52,12 +52,12 @@ class TuneResult(ctypes.Structure):
 
 
 class CgOptions(ctypes.Structure):
-    _fields_ = [("tol", c_dbl), ("innerTol", c_dbl), ("maxOuter", c_i32), ("maxInner", c_i32),
-                ("innerStorage", c_i32), ("checkEvery", c_i32)]
+    _fields_ = [("tol", c_dbl), ("updateFactor", c_dbl), ("maxUpdates", c_i32), ("maxIterations", c_i32),
+                ("iterStorage", c_i32), ("checkEvery", c_i32), ("l2Persist", c_i32)]
 
 
 class CgResult(ctypes.Structure):
-    _fields_ = [("outerIterations", c_i32), ("innerIterations", c_i32), ("converged", c_i32),
+    _fields_ = [("updates", c_i32), ("iterations", c_i32), ("converged", c_i32),
                 ("relResidual", c_dbl), ("seconds", c_dbl)]
 
 
@@ -68,14 +68,15 @@ class BatchConfig(ctypes.Structure):
 
 class ServerOptions(ctypes.Structure):
     _fields_ = [("memoryBudget", c_i64), ("batching", c_i32), ("maxRhs", c_i32), ("spmvStorage", c_i32),
-                ("cgInnerStorage", c_i32), ("cgWorkers", c_i32), ("cgMaxOuter", c_i32), ("cgMaxInner", c_i32),
-                ("cgCheckEvery", c_i32), ("cgTol", c_dbl), ("cgInnerTol", c_dbl), ("maxInFlight", c_i32)]
+                ("cgIterStorage", c_i32), ("cgWorkers", c_i32), ("cgMaxUpdates", c_i32), ("cgMaxIterations", c_i32),
+                ("cgCheckEvery", c_i32), ("cgTol", c_dbl), ("cgUpdateFactor", c_dbl), ("cgL2Persist", c_i32),
+                ("maxInFlight", c_i32)]
 
 
 class RequestInfo(ctypes.Structure):
     _fields_ = [("status", c_i32), ("kind", c_i32), ("matrix", c_i32), ("batchRhs", c_i32),
                 ("submitted", c_dbl), ("started", c_dbl), ("finished", c_dbl),
-                ("cgOuter", c_i32), ("cgInner", c_i32), ("cgRelResidual", c_dbl)]
+                ("cgUpdates", c_i32), ("cgIterations", c_i32), ("cgRelResidual", c_dbl)]
 
 
 class ServerStats(ctypes.Structure):
@@ -100,6 +101,12 @@ class LayoutDesc(ctypes.Structure):
                 ("blockWidth", c_i32), ("numBlocks", c_i32), ("totalOffsets", c_i64), ("numCoo", c_i64),
                 ("values", c_vp), ("scales", c_vp), ("offsets", c_vp), ("blockStart", c_vp), ("cooRow", c_vp),
                 ("cooCol", c_vp), ("cooVal", c_vp), ("cooRowPtr", c_vp)]
+
+
+class DeviceArrays(ctypes.Structure):
+    _fields_ = [("hbdiaData", c_vp), ("flattenedOffsets", c_vp), ("blockStartIndices", c_vp),
+                ("blockSizes", c_vp), ("flattenedVectorOffsets", c_vp), ("cpuRowIndices", c_vp),
+                ("cpuColIndices", c_vp), ("cpuValues", c_vp), ("cpuRowPtr", c_vp)]
 
 
 class HBDIACudaError(RuntimeError):
@@ -146,6 +153,7 @@ _SIGS = [
     ("hbdia_matrix_export_coo", ctypes.c_int, [c_vp, c_vp, c_vp, c_vp]),
     ("hbdia_matrix_export_nnz_per_row", ctypes.c_int, [c_vp, c_vp]),
     ("hbdia_matrix_stream", ctypes.c_int, [c_vp, c_vpp]),
+    ("hbdia_matrix_device_arrays", ctypes.c_int, [c_vp, ctypes.POINTER(DeviceArrays)]),
     ("hbdia_matrix_synchronize", ctypes.c_int, [c_vp]),
     ("hbdia_matrix_device_status", ctypes.c_int, [c_vp, c_i32p]),
     ("hbdia_matrix_set_kernel", ctypes.c_int, [c_vp, c_i32]),
@@ -159,6 +167,7 @@ _SIGS = [
     ("hbdia_vector_create", ctypes.c_int, [ctypes.c_int, c_vp, c_i64, c_vpp]),
     ("hbdia_vector_destroy", None, [c_vp]),
     ("hbdia_vector_device_ptr", ctypes.c_int, [c_vp, c_vpp]),
+    ("hbdia_vector_coo_results_ptr", ctypes.c_int, [c_vp, c_vpp]),
     ("hbdia_vector_size", ctypes.c_int, [c_vp, c_i64p]),
     ("hbdia_vector_upload", ctypes.c_int, [c_vp, c_vp]),
     ("hbdia_vector_download", ctypes.c_int, [c_vp, c_vp]),

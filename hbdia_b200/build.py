@@ -31,6 +31,10 @@ HEADERS = ["hbdia_internal.hpp", "spmv_kernels.cuh", "spmv_xstage.cuh", "spmv_qu
            "batch_kernels.cuh", "handles.hpp"]
 
 
+# the C++ drop-in headers, in the reference's include/ shape
+CXX_HEADERS = ["Format/HBDIA.hpp", "Format/HBDIAVector.hpp", "Operations/HBDIASpMV.hpp", "types.hpp"]
+
+
 def _cxx() -> str:
     return os.environ.get("CXX") or shutil.which("g++") or "g++"
 
@@ -74,8 +78,7 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> str:
             continue
         o = os.path.join(BUILD, src + ".o")
         objs.append(o)
-        if _stale(o, [s] + hdrs + [os.path.join(ROOT, "include", "hbdia", h)
-                                   for h in ("HBDIA.hpp", "HBDIAVector.hpp", "HBDIASpMV.hpp", "types.hpp")]):
+        if _stale(o, [s] + hdrs + [os.path.join(ROOT, "include", "hbdia", h) for h in CXX_HEADERS]):
             _run([_cxx(), "-std=c++17", "-O3", "-fPIC", "-fopenmp", "-Wall", *inc,
                   "-I", os.path.join(CUDA_HOME, "include"), "-c", s, "-o", o], verbose)
     if _stale(LIB, objs):
@@ -95,9 +98,12 @@ CPP_TEST_BIN = os.path.join(BUILD, "test_dropin")
 def build_cpp_tests(verbose: bool = False) -> str:
     """The C++ drop-in test program (tests/cpp/test_dropin.cpp), linked
     against the in-tree library."""
-    if os.path.exists(CPP_TEST_SRC) and _stale(CPP_TEST_BIN, [CPP_TEST_SRC, LIB]):
+    deps = [CPP_TEST_SRC, LIB] + [os.path.join(ROOT, "include", "hbdia", h) for h in CXX_HEADERS]
+    if os.path.exists(CPP_TEST_SRC) and _stale(CPP_TEST_BIN, deps):
         _run([_cxx(), "-std=c++17", "-O2", "-ffp-contract=off", "-I", os.path.join(ROOT, "include"),
-              CPP_TEST_SRC, "-o", CPP_TEST_BIN, LIB, "-Wl,-rpath,$ORIGIN/..", "-l:libstdc++.so.6"], verbose)
+              "-I", os.path.join(CUDA_HOME, "include"), CPP_TEST_SRC, "-o", CPP_TEST_BIN, LIB,
+              "-Wl,-rpath,$ORIGIN/..", "-L", os.path.join(CUDA_HOME, "lib64"),
+              "-Wl,-rpath," + os.path.join(CUDA_HOME, "lib64"), "-lcudart", "-l:libstdc++.so.6"], verbose)
     return CPP_TEST_BIN
 
 

@@ -118,8 +118,14 @@ void free_host_pipeline(hbdia_matrix *m) {
     }
 }
 
+void free_block_sizes(hbdia_matrix *m) {
+    if (m->blockSizesDev) cudaFree(m->blockSizesDev);
+    m->blockSizesDev = nullptr;
+}
+
 void reset_hbdia(hbdia_matrix *m) {
     free_host_pipeline(m);
+    free_block_sizes(m);
     hbdia::free_plan(m->plan);
     hbdia::free_plan(m->innerPlan);
     hbdia::cg_free(m->cg);
@@ -141,6 +147,7 @@ void prepare(hbdia_matrix *m, int32_t storage) {
         w.rowBase = m->dtype == HBDIA_F32 ? m->c32.rowBase : m->c64.rowBase;
         W = &w;
     }
+    free_block_sizes(m);
     if (m->dtype == HBDIA_F32) hbdia::build_plan(m->L32, storage, m->plan, W);
     else hbdia::build_plan(m->L64, storage, m->plan, W);
 }
@@ -478,6 +485,41 @@ int hbdia_matrix_export_nnz_per_row(const hbdia_matrix *m, int32_t *nnzPerRow) {
     });
 }
 
+int hbdia_matrix_device_arrays(hbdia_matrix *m, hbdia_device_arrays *a) {
+    return guarded([&] {
+        need(m && a, HBDIA_ERR_INVALID_ARGUMENT, "null argument");
+        const hbdia::DevicePlan &P = m->plan;
+        need(P.base != nullptr, HBDIA_ERR_NOT_CONVERTED, "matrix has no device layout");
+        if (!m->blockSizesDev && P.numBlocks > 0) {
+            // blockSizes[b] = blockStart[b + 1] - blockStart[b] (src/Format/HBDIA.cpp:741)
+            std::vector<int32_t> start(static_cast<size_t>(P.numBlocks) + 1), sizes(P.numBlocks);
+            hbdia::check_cuda(cudaMemcpy(start.data(), P.blkOff, start.size() * sizeof(int32_t),
+                                         cudaMemcpyDeviceToHost), "cudaMemcpy(block starts)");
+            for (int32_t b = 0; b < P.numBlocks; ++b) sizes[b] = start[b + 1] - start[b];
+            int32_t *d = nullptr;
+            hbdia::check_cuda(cudaMalloc(&d, sizes.size() * sizeof(int32_t)), "cudaMalloc(block sizes)");
+            const cudaError_t e = cudaMemcpy(d, sizes.data(), sizes.size() * sizeof(int32_t), cudaMemcpyHostToDevice);
+            if (e != cudaSuccess) {
+                cudaFree(d);
+                hbdia::check_cuda(e, "cudaMemcpy(block sizes)");
+            }
+            m->blockSizesDev = d;
+        }
+        std::memset(a, 0, sizeof(*a));
+        a->hbdiaData = P.storage == HBDIA_STORE_NATIVE ? P.vals : nullptr;
+        if (m->part.partial) a->flattenedVectorOffsets = P.offs;
+        else a->flattenedOffsets = P.offs;
+        a->blockStartIndices = P.blkOff;
+        a->blockSizes = m->blockSizesDev;
+        if (P.nCoo > 0) {
+            a->cpuRowIndices = P.cooRow;
+            a->cpuColIndices = P.cooCol;
+            a->cpuValues = P.cooVal;
+            a->cpuRowPtr = P.cooRowPtr;
+        }
+    });
+}
+
 int hbdia_matrix_stream(const hbdia_matrix *m, void **stream) {
     return guarded([&] {
         need(m && stream, HBDIA_ERR_INVALID_ARGUMENT, "null argument");
@@ -633,6 +675,7 @@ int hbdia_vector_create(hbdia_dtype dtype, const void *host, int64_t n, hbdia_ve
 void hbdia_vector_destroy(hbdia_vector *v) {
     if (!v) return;
     if (v->d) cudaFree(v->d);
+    if (v->cooResult) cudaFree(v->cooResult);
     delete v;
 }
 
@@ -640,6 +683,24 @@ int hbdia_vector_device_ptr(const hbdia_vector *v, void **p) {
     return guarded([&] {
         need(v && p, HBDIA_ERR_INVALID_ARGUMENT, "null argument");
         *p = v->d;
+    });
+}
+
+int hbdia_vector_coo_results_ptr(hbdia_vector *v, void **p) {
+    return guarded([&] {
+        need(v && p, HBDIA_ERR_INVALID_ARGUMENT, "null argument");
+        if (!v->cooResult) {
+            const size_t bytes = static_cast<size_t>(v->n) * esize(v->dtype);
+            void *d = nullptr;
+            hbdia::check_cuda(cudaMalloc(&d, bytes ? bytes : 256), "cudaMalloc(COO result buffer)");
+            const cudaError_t e = cudaMemset(d, 0, bytes ? bytes : 256);
+            if (e != cudaSuccess) {
+                cudaFree(d);
+                hbdia::check_cuda(e, "cudaMemset(COO result buffer)");
+            }
+            v->cooResult = d;
+        }
+        *p = v->cooResult;
     });
 }
 
@@ -813,24 +874,36 @@ int hbdia_cg_solve(hbdia_matrix *m, const double *b, double *x, const hbdia_cg_o
         need(m->hasHBDIA, HBDIA_ERR_NOT_CONVERTED, "matrix is not in HBDIA format");
         need(num_rows(m) == num_cols(m), HBDIA_ERR_INVALID_ARGUMENT, "CG needs a square matrix");
         need(!m->part.partial, HBDIA_ERR_UNSUPPORTED, "CG runs on whole matrices, not on one rank's rows");
-        need(opt->tol > 0 && opt->innerTol > 0 && opt->maxOuter >= 0 && opt->maxInner > 0 && opt->checkEvery > 0,
+        need(opt->tol > 0 && opt->updateFactor > 0 && opt->updateFactor < 1 && opt->maxUpdates >= 0 &&
+                 opt->maxIterations > 0 && opt->checkEvery > 0,
              HBDIA_ERR_INVALID_ARGUMENT, "bad CG options");
         ensure_device(m);
-        const hbdia::DevicePlan *inner = &m->plan;
-        if (opt->innerStorage != HBDIA_STORE_NATIVE) {
-            if (!m->innerPlan.base || m->innerPlan.storage != opt->innerStorage) {
-                need(m->hostLayout, HBDIA_ERR_NOT_CONVERTED, "no host layout to build the inner operator");
-                hbdia::build_plan(m->L64, opt->innerStorage, m->innerPlan);
+        const hbdia::DevicePlan *it = &m->plan;
+        if (opt->iterStorage != HBDIA_STORE_NATIVE) {
+            if (!m->innerPlan.base || m->innerPlan.storage != opt->iterStorage) {
+                need(m->hostLayout, HBDIA_ERR_NOT_CONVERTED, "no host layout to build the iteration operator");
+                hbdia::build_plan(m->L64, opt->iterStorage, m->innerPlan);
                 m->innerPlan.kernel = m->plan.kernel;
                 m->innerPlan.unroll = m->plan.unroll;
             }
-            inner = &m->innerPlan;
+            it = &m->innerPlan;
         }
         m->cg = hbdia::cg_work(m->cg, num_rows(m));
+        hbdia::CgParams prm;
+        prm.tol = opt->tol;
+        prm.updateFactor = opt->updateFactor;
+        prm.maxUpdates = opt->maxUpdates;
+        prm.maxIterations = opt->maxIterations;
+        prm.checkEvery = opt->checkEvery;
+        prm.l2Persist = opt->l2Persist != 0;
+        hbdia::CgStats st;
+        hbdia::cg_solve(m->plan, *it, m->cg, b, x, prm, stream, &st);
         hbdia_cg_result r;
         std::memset(&r, 0, sizeof(r));
-        hbdia::cg_solve(m->plan, *inner, m->cg, b, x, opt->tol, opt->maxOuter, opt->maxInner, opt->innerTol,
-                        opt->checkEvery, stream, &r.outerIterations, &r.innerIterations, &r.relResidual, &r.seconds);
+        r.updates = st.updates;
+        r.iterations = st.iterations;
+        r.relResidual = st.relResidual;
+        r.seconds = st.seconds;
         r.converged = r.relResidual <= opt->tol;
         throw_if_timeout(read_status(m, true));
         if (out) *out = r;

@@ -10,6 +10,7 @@ struct hbdia_vector {
     int32_t dtype = HBDIA_F64;
     int64_t n = 0;
     void *d = nullptr;
+    void *cooResult = nullptr;  // getDeviceCOOResultsPtr's buffer (first request)
 };
 
 struct hbdia_matrix {
@@ -22,6 +23,7 @@ struct hbdia_matrix {
     hbdia::HostLayout<double> L64;
     hbdia::HostLayout<float> L32;
     hbdia::DevicePlan plan;
+    int32_t *blockSizesDev = nullptr;   // getBlockSizesDevice (first request; freed with the plan)
     hbdia::DeviceLayoutMeta devMeta;    // layout facts when the GPU converter built the plan
     bool hasDIA = false;                // DIA format (host data)
     std::vector<int32_t> diaOffsets;

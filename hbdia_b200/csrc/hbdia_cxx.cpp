@@ -7,9 +7,9 @@
 #include <type_traits>
 #include <utility>
 
-#include "hbdia/HBDIA.hpp"
-#include "hbdia/HBDIASpMV.hpp"
-#include "hbdia/HBDIAVector.hpp"
+#include "hbdia/Format/HBDIA.hpp"
+#include "hbdia/Format/HBDIAVector.hpp"
+#include "hbdia/Operations/HBDIASpMV.hpp"
 
 namespace {
 
@@ -79,7 +79,7 @@ HBDIA<T> &HBDIA<T>::operator=(HBDIA &&o) noexcept {
         h_ = o.h_;
         executionMode_ = o.executionMode_;
         o.h_ = nullptr;
-        layoutCached_ = cooCached_ = false;
+        layoutCached_ = cooCached_ = diaCached_ = false;
     }
     return *this;
 }
@@ -88,7 +88,7 @@ template <typename T>
 bool HBDIA<T>::loadMTX(const std::string &f) {
     int32_t ok = 0;
     raise(hbdia_matrix_load_mtx(h_, f.c_str(), 0, 0, &ok));
-    layoutCached_ = cooCached_ = false;
+    layoutCached_ = cooCached_ = diaCached_ = false;
     return ok != 0;
 }
 
@@ -97,14 +97,14 @@ bool HBDIA<T>::loadMTX(const std::string &f, int numRows, int numCols) {
     if (numRows <= 0 || numCols <= 0) return false;  // src/Format/HBDIA.cpp:267-271
     int32_t ok = 0;
     raise(hbdia_matrix_load_mtx(h_, f.c_str(), numRows, numCols, &ok));
-    layoutCached_ = cooCached_ = false;
+    layoutCached_ = cooCached_ = diaCached_ = false;
     return ok != 0;
 }
 
 template <typename T>
 void HBDIA<T>::create3DStencil27Point(int nx, int ny, int nz, double noise, int iteration) {
     raise(hbdia_matrix_stencil27(h_, nx, ny, nz, noise, iteration));
-    layoutCached_ = cooCached_ = false;
+    layoutCached_ = cooCached_ = diaCached_ = false;
 }
 
 template <typename T>
@@ -120,6 +120,78 @@ template <typename T>
 void HBDIA<T>::prepareForGPU() {
     raise(hbdia_matrix_prepare_gpu(h_, HBDIA_STORE_NATIVE));
 }
+
+template <typename T>
+void HBDIA<T>::removeCOODuplicates() {
+    raise(hbdia_matrix_remove_duplicates(h_));
+    cooCached_ = false;
+}
+
+template <typename T>
+void HBDIA<T>::convertToDIAFormat(bool cooUnique) {
+    raise(hbdia_matrix_convert_dia(h_, cooUnique ? 1 : 0));
+    cooCached_ = diaCached_ = false;  // without cooUnique the COO loses its duplicates
+}
+
+template <typename T>
+bool HBDIA<T>::isDIAFormat() const {
+    int32_t has = 0, nd = 0, len = 0;
+    raise(hbdia_matrix_dia_info(h_, &has, &nd, &len));
+    return has != 0;
+}
+
+template <typename T>
+void HBDIA<T>::refreshDiaCache() const {
+    if (diaCached_) return;
+    int32_t has = 0, nd = 0, len = 0;
+    raise(hbdia_matrix_dia_info(h_, &has, &nd, &len));
+    diaOffsets_.assign(static_cast<size_t>(has ? nd : 0), 0);
+    diagonals_.clear();
+    if (has && nd > 0) {
+        std::vector<T> flat(static_cast<size_t>(nd) * static_cast<size_t>(len));
+        raise(hbdia_matrix_export_dia(h_, diaOffsets_.data(), flat.data()));
+        diagonals_.resize(static_cast<size_t>(nd));
+        for (int32_t d = 0; d < nd; ++d)
+            diagonals_[d].assign(flat.begin() + static_cast<size_t>(d) * len,
+                                 flat.begin() + static_cast<size_t>(d + 1) * len);
+    }
+    diaCached_ = true;
+}
+
+template <typename T>
+const std::vector<std::vector<T>> &HBDIA<T>::getDiagonals() const { refreshDiaCache(); return diagonals_; }
+template <typename T>
+const std::vector<int> &HBDIA<T>::getOffsets() const { refreshDiaCache(); return diaOffsets_; }
+
+template <typename T>
+hbdia_device_arrays HBDIA<T>::deviceArrays() const {
+    hbdia_device_arrays a{};
+    const hbdia_matrix_info i = info_of<T>(h_);
+    if (!i.hasHBDIA) return a;  // nothing on the device yet: the reference's getters return null too
+    const int status = hbdia_matrix_device_arrays(h_, &a);
+    if (status == HBDIA_ERR_NOT_CONVERTED) return hbdia_device_arrays{};  // converted on the host only
+    raise(status);
+    return a;
+}
+
+template <typename T>
+const T *HBDIA<T>::getHBDIADataDevice() const { return static_cast<const T *>(deviceArrays().hbdiaData); }
+template <typename T>
+const int *HBDIA<T>::getFlattenedOffsetsDevice() const { return deviceArrays().flattenedOffsets; }
+template <typename T>
+const int *HBDIA<T>::getBlockStartIndicesDevice() const { return deviceArrays().blockStartIndices; }
+template <typename T>
+const int *HBDIA<T>::getBlockSizesDevice() const { return deviceArrays().blockSizes; }
+template <typename T>
+const int *HBDIA<T>::getFlattenedVectorOffsetsDevice() const { return deviceArrays().flattenedVectorOffsets; }
+template <typename T>
+const int *HBDIA<T>::getCpuRowIndicesDevice() const { return deviceArrays().cpuRowIndices; }
+template <typename T>
+const int *HBDIA<T>::getCpuColIndicesDevice() const { return deviceArrays().cpuColIndices; }
+template <typename T>
+const T *HBDIA<T>::getCpuValuesDevice() const { return static_cast<const T *>(deviceArrays().cpuValues); }
+template <typename T>
+const int *HBDIA<T>::getCpuRowPtrDevice() const { return deviceArrays().cpuRowPtr; }
 
 template <typename T>
 bool HBDIA<T>::isCOOFormat() const { return info_of<T>(h_).hasCOO != 0; }
@@ -226,6 +298,9 @@ HBDIAVector<T>::HBDIAVector(const std::vector<T> &localData) : localVector_(loca
 }
 
 template <typename T>
+HBDIAVector<T>::HBDIAVector(const std::vector<T> &localData, bool, bool, bool, bool) : HBDIAVector(localData) {}
+
+template <typename T>
 HBDIAVector<T>::~HBDIAVector() {
     hbdia_vector_destroy(h_);
 }
@@ -250,6 +325,13 @@ template <typename T>
 T *HBDIAVector<T>::getDeviceDataPtr() const {
     void *p = nullptr;
     raise(hbdia_vector_device_ptr(h_, &p));
+    return static_cast<T *>(p);
+}
+
+template <typename T>
+T *HBDIAVector<T>::getDeviceCOOResultsPtr() const {
+    void *p = nullptr;
+    raise(hbdia_vector_coo_results_ptr(h_, &p));
     return static_cast<T *>(p);
 }
 

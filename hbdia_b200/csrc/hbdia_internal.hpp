@@ -187,13 +187,27 @@ void autotune(DevicePlan &P, const void *X, int64_t ldx, void *Y, int64_t ldy, i
               int32_t *kernel, int32_t *unroll, int32_t *tile, int32_t *fromCache, float *ms);
 void autotune_clear_cache();
 
-// CG with mixed-precision refinement (cg.cu)
+// CG with reliable updates (cg.cu): iterations on Ait (reduced or FP64
+// storage), FP64 residual recomputations with A64.
 struct CgWork;
 CgWork *cg_work(CgWork *w, int64_t n);
 void cg_free(CgWork *w);
-void cg_solve(const DevicePlan &A64, const DevicePlan &Ainner, CgWork *w, const double *b, double *x, double tol,
-              int maxOuter, int maxInner, double innerTol, int checkEvery, void *stream, int32_t *outerIt,
-              int32_t *innerIt, double *relRes, double *seconds);
+int64_t cg_work_bytes(int64_t n, int sms);  // device bytes of a workspace for n rows
+struct CgParams {
+    double tol = 1e-10;          // target ||b - A x|| / ||b||
+    double updateFactor = 0.1;   // reliable update when the iterated residual falls below this
+                                 // times the largest one since the last update
+    int32_t maxUpdates = 100;    // FP64 residual recomputations
+    int32_t maxIterations = 20000;
+    int32_t checkEvery = 10;     // iterations per CUDA-graph replay / host check
+    bool l2Persist = true;       // keep r, p, q persisting in L2 during the solve
+};
+struct CgStats {
+    int32_t updates = 0, iterations = 0;
+    double relResidual = 0.0, seconds = 0.0;
+};
+void cg_solve(const DevicePlan &A64, const DevicePlan &Ait, CgWork *w, const double *b, double *x,
+              const CgParams &prm, void *stream, CgStats *stats);
 // Many matrices in one persistent launch (batch.cu)
 struct Batch;
 Batch *batch_create(const std::vector<const DevicePlan *> &plans);

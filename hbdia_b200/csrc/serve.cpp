@@ -75,7 +75,7 @@ struct ServedMatrix {
     std::deque<SpmvBatch> running;         // issued, in stream order (scheduler thread)
     std::deque<Request *> pending;         // SpMV requests not yet issued (server lock)
     const DevicePlan &spmvPlan(int32_t storage) const { return storage == HBDIA_STORE_NATIVE ? p64 : pLow; }
-    const DevicePlan &cgInner(int32_t storage) const { return storage == HBDIA_STORE_NATIVE ? p64 : pLow; }
+    const DevicePlan &cgIter(int32_t storage) const { return storage == HBDIA_STORE_NATIVE ? p64 : pLow; }
 };
 
 struct Request {
@@ -328,9 +328,18 @@ void cg_worker(Server *S) {
                 check_cuda(cudaMemcpyAsync(bx, r->x, nb, cudaMemcpyHostToDevice, st), "cudaMemcpyAsync(CG b)");
             check_cuda(cudaMemsetAsync(x, 0, nb, st), "cudaMemsetAsync(CG x)");
             const hbdia_server_options &o = S->opt;
-            double secs = 0.0;
-            cg_solve(M.p64, M.cgInner(o.cgInnerStorage), w, b, x, o.cgTol, o.cgMaxOuter, o.cgMaxInner, o.cgInnerTol,
-                     o.cgCheckEvery, st, &r->info.cgOuter, &r->info.cgInner, &r->info.cgRelResidual, &secs);
+            CgParams prm;
+            prm.tol = o.cgTol;
+            prm.updateFactor = o.cgUpdateFactor;
+            prm.maxUpdates = o.cgMaxUpdates;
+            prm.maxIterations = o.cgMaxIterations;
+            prm.checkEvery = o.cgCheckEvery;
+            prm.l2Persist = o.cgL2Persist != 0;
+            CgStats cs;
+            cg_solve(M.p64, M.cgIter(o.cgIterStorage), w, b, x, prm, st, &cs);
+            r->info.cgUpdates = cs.updates;
+            r->info.cgIterations = cs.iterations;
+            r->info.cgRelResidual = cs.relResidual;
             if (!r->device)
                 check_cuda(cudaMemcpyAsync(r->y, x, nb, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync(CG y)");
             check_cuda(cudaStreamSynchronize(st), "cudaStreamSynchronize(CG)");
@@ -367,27 +376,29 @@ void server_default_options(hbdia_server_options *o) {
     o->batching = 1;
     o->maxRhs = 16;
     o->spmvStorage = HBDIA_STORE_F32;
-    o->cgInnerStorage = HBDIA_STORE_F32;
+    o->cgIterStorage = HBDIA_STORE_F32;
     o->cgWorkers = 4;
     o->cgTol = 1e-10;
-    o->cgInnerTol = 1e-6;
-    o->cgMaxOuter = 50;
-    o->cgMaxInner = 5000;
+    o->cgUpdateFactor = 0.1;
+    o->cgMaxUpdates = 100;
+    o->cgMaxIterations = 20000;
     o->cgCheckEvery = 10;
+    o->cgL2Persist = 1;
     o->maxInFlight = 1;
 }
 
 Server *server_create(const hbdia_server_options &o) {
     if (o.memoryBudget <= 0 || o.maxRhs < 1 || o.maxRhs > 64 || o.cgWorkers < 1 || o.cgWorkers > 64 ||
-        o.cgTol <= 0 || o.cgInnerTol <= 0 || o.cgMaxOuter < 1 || o.cgMaxInner < 1 || o.cgCheckEvery < 1 ||
+        o.cgTol <= 0 || o.cgUpdateFactor <= 0 || o.cgUpdateFactor >= 1 || o.cgMaxUpdates < 1 ||
+        o.cgMaxIterations < 1 || o.cgCheckEvery < 1 ||
         o.maxInFlight < 1 || o.maxInFlight > 8)
         throw Error(HBDIA_ERR_INVALID_ARGUMENT, "bad server options");
-    for (int32_t st : {o.spmvStorage, o.cgInnerStorage})
+    for (int32_t st : {o.spmvStorage, o.cgIterStorage})
         if (st != HBDIA_STORE_NATIVE && st != HBDIA_STORE_F32 && st != HBDIA_STORE_BF16_SCALED)
             throw Error(HBDIA_ERR_INVALID_ARGUMENT, "unknown value storage");
-    if (o.spmvStorage != HBDIA_STORE_NATIVE && o.cgInnerStorage != HBDIA_STORE_NATIVE &&
-        o.spmvStorage != o.cgInnerStorage)
-        throw Error(HBDIA_ERR_UNSUPPORTED, "SpMV and CG inner storage must match when both are reduced");
+    if (o.spmvStorage != HBDIA_STORE_NATIVE && o.cgIterStorage != HBDIA_STORE_NATIVE &&
+        o.spmvStorage != o.cgIterStorage)
+        throw Error(HBDIA_ERR_UNSUPPORTED, "SpMV and CG iteration storage must match when both are reduced");
     auto S = std::make_unique<Server>();
     S->opt = o;
     check_cuda(cudaGetDevice(&S->device), "cudaGetDevice");
@@ -423,17 +434,17 @@ int32_t server_add_matrix(Server *S, const hbdia_matrix *m) {
     auto M = std::make_unique<ServedMatrix>();
     M->n = L.numRows;
     M->rowsX = std::max(L.numRows, L.numCols);
-    const int32_t low = S->opt.spmvStorage != HBDIA_STORE_NATIVE ? S->opt.spmvStorage : S->opt.cgInnerStorage;
+    const int32_t low = S->opt.spmvStorage != HBDIA_STORE_NATIVE ? S->opt.spmvStorage : S->opt.cgIterStorage;
     try {
         build_plan(L, HBDIA_STORE_NATIVE, M->p64);
         if (low != HBDIA_STORE_NATIVE) build_plan(L, low, M->pLow);
         const int64_t staging =
             static_cast<int64_t>(S->opt.maxRhs) * (static_cast<int64_t>(M->rowsX) + M->n) * 8;
-        // CG workspaces grow to the largest system: 5 vectors of the workspace + b, x per worker
+        // CG workspaces grow to the largest system: 3 vectors of the workspace + b, x per worker
         int64_t cgGrow = 0;
         {
             std::lock_guard<std::mutex> lk(S->mu);
-            if (M->n > S->maxN) cgGrow = static_cast<int64_t>(S->opt.cgWorkers) * 7 * 8 * (M->n - S->maxN);
+            if (M->n > S->maxN) cgGrow = static_cast<int64_t>(S->opt.cgWorkers) * 5 * 8 * (M->n - S->maxN);
         }
         M->bytes = static_cast<int64_t>(M->p64.bytes + M->pLow.bytes) + staging;
         {

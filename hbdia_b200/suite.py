@@ -192,21 +192,24 @@ def cg(args):
     bt = torch.from_numpy(b).cuda()
     m = hb.HBDIA(rows, cols, vals, n, n)
     m.convertToHBDIAFormat(32, 2)
-    for name, st, itol in (("mixed fp32-storage inner + fp64 refinement", hb.STORE_F32, 1e-6),
-                           ("plain fp64 CG", hb.STORE_NATIVE, 1e-11)):
+    for name, st, persist in (("mixed: fp32-storage iterations, fp64 reliable updates, L2-resident vectors",
+                                hb.STORE_F32, True),
+                               ("mixed without the L2 window", hb.STORE_F32, False),
+                               ("fp64 iterations, L2-resident vectors", hb.STORE_NATIVE, True),
+                               ("plain fp64 CG", hb.STORE_NATIVE, False)):
         xt = torch.zeros(n, dtype=torch.float64, device="cuda")
-        hb.cg_solve(m, bt.data_ptr(), xt.data_ptr(), tol=1e-10, inner_storage=st, inner_tol=itol)  # warm
+        hb.cg_solve(m, bt.data_ptr(), xt.data_ptr(), tol=1e-10, iter_storage=st, l2_persist=persist)  # warm
         xt.zero_()
         torch.cuda.synchronize()
-        r = hb.cg_solve(m, bt.data_ptr(), xt.data_ptr(), tol=1e-10, inner_storage=st, inner_tol=itol)
+        r = hb.cg_solve(m, bt.data_ptr(), xt.data_ptr(), tol=1e-10, iter_storage=st, l2_persist=persist)
         x = xt.cpu().numpy()
         ax = np.zeros(n)
         np.add.at(ax, rows, vals * x[cols])
         host_res = float(np.linalg.norm(b - ax) / np.linalg.norm(b))
         print(json.dumps({"suite": "cg", "workload": f"SPD symmetrised 27-point stencil {g}^3, b ~ U(-1,1)",
-                          "method": name, "outer_iterations": r.outerIterations,
-                          "inner_spmvs": r.innerIterations, "seconds": r.seconds,
-                          "ms_per_inner_iteration": 1e3 * r.seconds / max(1, r.innerIterations),
+                          "method": name, "fp64_residual_updates": r.updates,
+                          "iterations": r.iterations, "seconds": r.seconds,
+                          "ms_per_iteration": 1e3 * r.seconds / max(1, r.iterations),
                           "rel_residual": r.relResidual, "rel_residual_host_check": host_res,
                           "converged": bool(r.converged)}), flush=True)
 
@@ -393,8 +396,8 @@ def serve(args):
         ybuf = [[pinned(n, np.zeros) for _ in range(8)] for n in ns]
     servers = {
         "batched": hb.Server(),
-        "plain": hb.Server(batching=0, spmvStorage=hb.STORE_NATIVE, cgInnerStorage=hb.STORE_NATIVE,
-                           cgInnerTol=1e-11, cgWorkers=1),
+        "plain": hb.Server(batching=0, spmvStorage=hb.STORE_NATIVE, cgIterStorage=hb.STORE_NATIVE,
+                           cgL2Persist=0, cgWorkers=1),
     }
     if args.serial_too:
         servers["batched, 2 batches in flight"] = hb.Server(maxInFlight=2)

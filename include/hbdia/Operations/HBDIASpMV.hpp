@@ -13,8 +13,10 @@
 #ifndef HBDIA_B200_HBDIASPMV_HPP
 #define HBDIA_B200_HBDIASPMV_HPP
 
-#include "HBDIA.hpp"
-#include "HBDIAVector.hpp"
+#include <cuda_runtime.h>
+
+#include "../Format/HBDIA.hpp"
+#include "../Format/HBDIAVector.hpp"
 
 template <typename T>
 bool hbdiaSpMV(HBDIA<T> &matrix, const HBDIAVector<T> &inputVector, HBDIAVector<T> &outputVector,

@@ -1,7 +1,7 @@
 /*
  * hbdia_b200 -- C ABI of the B200-native HBDIA SpMV library (libhbdia_b200.so).
  *
- * This is the drop-in boundary under the C++ API of include/hbdia/HBDIA.hpp,
+ * This is the drop-in boundary under the C++ API of include/hbdia/Format/HBDIA.hpp,
  * HBDIAVector.hpp and HBDIASpMV.hpp (HBDIA<T>, HBDIAVector<T>, hbdiaSpMV), which mirror the reference's
  * classes.  Every entry point names the reference interface it replaces
  * (paths relative to the reference project root).  The signatures use plain
@@ -219,6 +219,38 @@ int hbdia_matrix_export_nnz_per_row(const hbdia_matrix *m, int32_t *nnzPerRow);
  * SpMVs run on (created by prepare_gpu). */
 int hbdia_matrix_stream(const hbdia_matrix *m, void **stream);
 
+/* The device arrays prepareForGPU leaves (src/Format/HBDIA.cpp:720-816),
+ * returned by the GPU getters of include/Format/HBDIA.hpp:155-165
+ * (getHBDIADataDevice, getFlattenedOffsetsDevice,
+ * getBlockStartIndicesDevice, getBlockSizesDevice,
+ * getFlattenedVectorOffsetsDevice, getCpuRowIndicesDevice,
+ * getCpuColIndicesDevice, getCpuValuesDevice, getCpuRowPtrDevice).  They are
+ * the arrays the fused SpMV reads, owned by the matrix and valid until it is
+ * destroyed or prepared again:
+ *  - hbdiaData: [block][offsetIdx][lane] values of T, blockWidth per offset;
+ *    NULL when the values are stored in a reduced format (prepare_gpu with
+ *    HBDIA_STORE_F32 / HBDIA_STORE_BF16_SCALED);
+ *  - flattenedOffsets, blockStartIndices (numBlocks + 1, offset units) and
+ *    blockSizes (numBlocks; built on the first request);
+ *  - flattenedVectorOffsets: NULL for a whole matrix, as in the reference; for
+ *    a partial matrix the offsets into its x window (column - windowLo - local
+ *    row), which is what the fused kernel reads, with flattenedOffsets NULL;
+ *  - the COO remainder cpuRowIndices / cpuColIndices / cpuValues (numCoo) in
+ *    row order (the reference's list order for its row-sorted input) and
+ *    cpuRowPtr (numRows + 1).  NULL when the matrix has no COO remainder. */
+typedef struct hbdia_device_arrays {
+    const void *hbdiaData;
+    const int32_t *flattenedOffsets;
+    const int32_t *blockStartIndices;
+    const int32_t *blockSizes;
+    const int32_t *flattenedVectorOffsets;
+    const int32_t *cpuRowIndices;
+    const int32_t *cpuColIndices;
+    const void *cpuValues;
+    const int32_t *cpuRowPtr;
+} hbdia_device_arrays;
+int hbdia_matrix_device_arrays(hbdia_matrix *m, hbdia_device_arrays *arrays);
+
 /* ---------------------------------------------------------------- vectors */
 
 /* HBDIAVector(localData) (src/Format/HBDIAVector.cpp:17-23): device buffer
@@ -228,6 +260,13 @@ int hbdia_vector_create(hbdia_dtype dtype, const void *hostData, int64_t n, hbdi
 void hbdia_vector_destroy(hbdia_vector *v);
 /* getDeviceDataPtr / getDeviceLocalPtr (include/Format/HBDIAVector.hpp:48-50) */
 int hbdia_vector_device_ptr(const hbdia_vector *v, void **devicePtr);
+/* getDeviceCOOResultsPtr (include/Format/HBDIAVector.hpp:53): the
+ * reference's separate buffer for the COO remainder's partial result, which
+ * its callers clear before each SpMV (benchmarking/benchHBDIA.cpp:33).  The
+ * fused SpMV never reads or writes it; it exists (n zeroed elements,
+ * allocated on the first request, owned by the vector) so such callers run
+ * unchanged. */
+int hbdia_vector_coo_results_ptr(hbdia_vector *v, void **devicePtr);
 int hbdia_vector_size(const hbdia_vector *v, int64_t *n);
 /* blocking host<->device copies of the whole vector */
 int hbdia_vector_upload(hbdia_vector *v, const void *hostData);
@@ -426,26 +465,33 @@ int hbdia_matrix_test_skip_tile(hbdia_matrix *m, int32_t tile);
 
 /* ---------------------------------------------------------------- solver */
 
-/* Conjugate gradients for a symmetric positive definite double matrix, with
- * mixed-precision iterative refinement: the residual r = b - A x, the dot
- * products, norms and the solution update are FP64; each refinement step
- * solves A d = r with CG whose SpMVs use the `innerStorage` copy of the values
- * (HBDIA_STORE_F32: mixed precision; HBDIA_STORE_NATIVE: plain FP64 CG).  No
+/* Conjugate gradients for a symmetric positive definite double matrix.  No
  * counterpart in the reference (its SpMV has no solver); it runs on the same
- * SpMV kernels.  x holds the initial guess on entry and the solution on
- * return (device buffers of numRows doubles).  Synchronous. */
+ * SpMV kernels.  The iterations' SpMVs use the `iterStorage` copy of the
+ * values (HBDIA_STORE_F32: mixed precision; HBDIA_STORE_NATIVE: plain FP64
+ * CG); x, the residual r, the search direction, the dot products, norms and
+ * the solution update are FP64.  Reliable updates: whenever the iterated
+ * residual has fallen below updateFactor times the largest one since the last
+ * update, and before convergence is declared, r is recomputed as b - A x with
+ * the FP64 values while the search direction is kept, so the iterations do
+ * not restart.  Convergence is judged on that FP64 residual.  With l2Persist
+ * the solver's vectors are kept persisting in L2 during the solve (this sets
+ * the process's persisting-L2 limit of the device to its maximum on first
+ * use).  x holds the initial guess on entry and the solution on return
+ * (device buffers of numRows doubles).  Synchronous. */
 typedef struct hbdia_cg_options {
-    double tol;           /* target ||b - A x|| / ||b|| (FP64), e.g. 1e-10       */
-    double innerTol;      /* inner CG stops at ||r_in|| <= innerTol ||r||        */
-    int32_t maxOuter;     /* refinement steps                                    */
-    int32_t maxInner;     /* inner iterations per step                           */
-    int32_t innerStorage; /* hbdia_value_storage of the inner operator           */
-    int32_t checkEvery;   /* inner iterations per CUDA-graph replay / host check */
+    double tol;            /* target ||b - A x|| / ||b|| (FP64), e.g. 1e-10              */
+    double updateFactor;   /* reliable-update trigger, 0 < f < 1 (e.g. 0.1)              */
+    int32_t maxUpdates;    /* FP64 residual recomputations                               */
+    int32_t maxIterations; /* iterations in all                                          */
+    int32_t iterStorage;   /* hbdia_value_storage of the iterations' operator            */
+    int32_t checkEvery;    /* iterations per CUDA-graph replay / host check              */
+    int32_t l2Persist;     /* keep the solver's vectors persisting in L2 (0 / 1)         */
 } hbdia_cg_options;
 
 typedef struct hbdia_cg_result {
-    int32_t outerIterations;
-    int32_t innerIterations;   /* inner SpMVs */
+    int32_t updates;           /* FP64 residual recomputations (reliable updates) */
+    int32_t iterations;        /* SpMVs with the iteration operator */
     int32_t converged;
     double relResidual;        /* final ||b - A x|| / ||b|| in FP64 */
     double seconds;
@@ -531,8 +577,9 @@ int hbdia_batch_stream(const hbdia_batch *b, void **stream);
  *    requests arriving while their matrix is busy join its next batch.
  *    batching = 0 serves one request per launch in arrival order.
  *  - CG requests (solve A y = x, A symmetric positive definite) run on
- *    cgWorkers worker threads: mixed-precision CG (hbdia_cg_solve) with
- *    cgInnerStorage inner iterations, refined to cgTol.
+ *    cgWorkers worker threads: CG with reliable updates (hbdia_cg_solve)
+ *    iterating on the cgIterStorage values, converged to cgTol on the FP64
+ *    residual.
  * A request's result does not depend on the requests it is served with.
  * Admission: hbdia_server_add_matrix returns HBDIA_ERR_NO_MEMORY when the
  * matrix's plans, staging blocks and CG workspace growth would take the
@@ -546,13 +593,14 @@ typedef struct hbdia_server_options {
     int32_t batching;       /* continuous batching of SpMVs (default 1)                     */
     int32_t maxRhs;         /* SpMV requests of one matrix per batch, 1-64 (default 16)    */
     int32_t spmvStorage;    /* hbdia_value_storage of SpMVs (default HBDIA_STORE_F32)       */
-    int32_t cgInnerStorage; /* storage of the CG inner iterations (default HBDIA_STORE_F32) */
+    int32_t cgIterStorage;  /* storage of the CG iterations' SpMVs (default HBDIA_STORE_F32) */
     int32_t cgWorkers;      /* concurrent CG solves, 1-64 (default 4)                       */
-    int32_t cgMaxOuter;     /* refinement steps (default 50)                                */
-    int32_t cgMaxInner;     /* inner iterations per step (default 5000)                     */
-    int32_t cgCheckEvery;   /* inner iterations per graph replay (default 10)               */
+    int32_t cgMaxUpdates;   /* FP64 residual recomputations per solve (default 100)         */
+    int32_t cgMaxIterations;/* iterations per solve (default 20000)                         */
+    int32_t cgCheckEvery;   /* iterations per graph replay (default 10)                     */
     double cgTol;           /* target ||b - A y|| / ||b|| (default 1e-10)                   */
-    double cgInnerTol;      /* inner relative tolerance (default 1e-6)                      */
+    double cgUpdateFactor;  /* reliable-update trigger (default 0.1)                        */
+    int32_t cgL2Persist;    /* CG vectors persisting in L2 during a solve (default 1)       */
     int32_t maxInFlight;    /* SpMV batches of one matrix issued and not yet completed,     */
                             /* 1-8 (default 1: the next batch forms while one runs)         */
 } hbdia_server_options;
@@ -562,7 +610,7 @@ typedef struct hbdia_request_info {
     int32_t kind, matrix;
     int32_t batchRhs;       /* SpMV: requests in its batch                               */
     double submitted, started, finished; /* seconds since the server was created         */
-    int32_t cgOuter, cgInner;
+    int32_t cgUpdates, cgIterations;
     double cgRelResidual;
 } hbdia_request_info;
 

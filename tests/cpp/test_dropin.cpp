@@ -1,18 +1,22 @@
 // C++ drop-in check: the reference's single-GPU usage
 // (simple_hbdia_example.cpp:15-33) and the shape of its cuSPARSE comparison
 // test (tests/run_HBDIA_cusparse_comparison.cpp:128-250), written against
-// include/hbdia/*.hpp.  The expected y is computed here from the layout
-// getters with the reference's arithmetic (ascending-offset FMA chain for the
-// blocked-DIA part, sequential multiply-then-add for the COO remainder), so
-// the comparison is exact.  Exit status 0 only if every check passes.
+// include/hbdia/, plus the GPU getters, the DIA format, duplicate removal,
+// the unified-memory vector constructor, the COO result buffer and
+// CHECK_CUDA.  The expected y is computed here from the layout getters with
+// the reference's arithmetic (ascending-offset FMA chain for the blocked-DIA
+// part, sequential multiply-then-add for the COO remainder), so the
+// comparison is exact.  Exit status 0 only if every check passes.
 #include <cmath>
 #include <cstdio>
 #include <stdexcept>
+#include <string>
+#include <type_traits>
 #include <vector>
 
-#include "hbdia/HBDIA.hpp"
-#include "hbdia/HBDIASpMV.hpp"
-#include "hbdia/HBDIAVector.hpp"
+#include "hbdia/Format/HBDIA.hpp"
+#include "hbdia/Format/HBDIAVector.hpp"
+#include "hbdia/Operations/HBDIASpMV.hpp"
 
 static int failures = 0;
 #define CHECK(cond, what)                                   \
@@ -119,6 +123,77 @@ int main() {
             oor = true;
         }
         CHECK(oor, "out-of-range index throws std::out_of_range");
+    }
+    {  // GPU getters (include/Format/HBDIA.hpp:155-165) hold the host layout's contents
+        HBDIA<double> m;
+        m.create3DStencil27Point(16, 16, 16, 0.02, 2);
+        m.convertToHBDIAFormat(32, 2);
+        const auto &opb = m.getOffsetsPerBlock();
+        std::vector<int> flat, start, sizes;
+        for (const auto &b : opb) {
+            start.push_back(static_cast<int>(flat.size()));
+            sizes.push_back(static_cast<int>(b.size()));
+            flat.insert(flat.end(), b.begin(), b.end());
+        }
+        start.push_back(static_cast<int>(flat.size()));
+        auto down = [](const auto *d, size_t count) {
+            using E = std::remove_cv_t<std::remove_pointer_t<decltype(d)>>;
+            std::vector<E> h(count);
+            if (d && count) CHECK_CUDA(cudaMemcpy(h.data(), d, count * sizeof(E), cudaMemcpyDeviceToHost));
+            return h;
+        };
+        const auto &data = m.getHBDIAData();
+        CHECK(m.getHBDIADataDevice() && down(m.getHBDIADataDevice(), data.size()) == data,
+              "getHBDIADataDevice holds getHBDIAData");
+        CHECK(down(m.getFlattenedOffsetsDevice(), flat.size()) == flat, "getFlattenedOffsetsDevice");
+        CHECK(down(m.getBlockStartIndicesDevice(), start.size()) == start, "getBlockStartIndicesDevice");
+        CHECK(down(m.getBlockSizesDevice(), sizes.size()) == sizes, "getBlockSizesDevice");
+        CHECK(m.getFlattenedVectorOffsetsDevice() == nullptr, "no vector offsets for a whole matrix");
+        const auto &cr = m.getCpuRowIndices();
+        CHECK(!cr.empty() && down(m.getCpuRowIndicesDevice(), cr.size()) == cr, "getCpuRowIndicesDevice");
+        CHECK(down(m.getCpuColIndicesDevice(), cr.size()) == m.getCpuColIndices(), "getCpuColIndicesDevice");
+        CHECK(down(m.getCpuValuesDevice(), cr.size()) == m.getCpuValues(), "getCpuValuesDevice");
+        CHECK(down(m.getCpuRowPtrDevice(), m.getCpuRowPtr().size()) == m.getCpuRowPtr(), "getCpuRowPtrDevice");
+    }
+    {  // DIA format and duplicate removal (src/Format/HBDIA.cpp:372-505)
+        std::vector<int> r = {2, 0, 1, 0, 2, 1}, c = {0, 1, 1, 1, 2, 0};
+        std::vector<double> v = {5, 1, 2, 3, 4, 6};
+        HBDIA<double> d(r, c, v, 3, 3);
+        CHECK(!d.isDIAFormat() && !d.getHasDIA(), "not DIA before convertToDIAFormat");
+        d.convertToDIAFormat();
+        CHECK(d.isDIAFormat(), "isDIAFormat after convertToDIAFormat");
+        CHECK(d.getNumNonZeros() == 5, "duplicate (0,1) merged by convertToDIAFormat");
+        CHECK((d.getOffsets() == std::vector<int>{-2, -1, 0, 1}), "DIA offsets ascending");
+        const auto &dg = d.getDiagonals();
+        CHECK(dg.size() == 4 && dg[3][0] == 4.0 && dg[2][1] == 2.0 && dg[2][2] == 4.0 && dg[1][1] == 6.0,
+              "DIA diagonals hold the merged values");
+        HBDIA<double> u(r, c, v, 3, 3);
+        u.removeCOODuplicates();
+        CHECK((u.getRowIndices() == std::vector<int>{0, 1, 1, 2, 2}) &&
+                  (u.getColIndices() == std::vector<int>{1, 0, 1, 0, 2}) && u.getValues()[0] == 4.0,
+              "removeCOODuplicates sums duplicates and sorts by (row, col)");
+    }
+    {  // the unified-memory constructor and the COO result buffer
+        std::vector<double> xv(100, 2.0);
+        HBDIAVector<double> a(xv, true, true, false, false);
+        std::vector<double> back;
+        a.copyToHost(back);
+        CHECK(back == xv, "unified-memory ctor holds the data");
+        double *coo = a.getDeviceCOOResultsPtr();
+        CHECK(coo != nullptr && coo == a.getDeviceCOOResultsPtr(), "getDeviceCOOResultsPtr is one buffer");
+        std::vector<double> z(100, 1.0);
+        CHECK_CUDA(cudaMemcpy(z.data(), coo, 100 * sizeof(double), cudaMemcpyDeviceToHost));
+        CHECK(z == std::vector<double>(100, 0.0), "COO result buffer starts zeroed");
+    }
+    {  // CHECK_CUDA throws where the reference's exits
+        bool threw = false;
+        try {
+            CHECK_CUDA(cudaSetDevice(1 << 20));
+        } catch (const std::runtime_error &e) {
+            threw = std::string(e.what()).find("CUDA error at") != std::string::npos;
+        }
+        cudaGetLastError();
+        CHECK(threw, "CHECK_CUDA throws std::runtime_error");
     }
     std::printf(failures ? "FAILED (%d)\n" : "ALL PASSED\n", failures);
     return failures ? 1 : 0;

@@ -1,7 +1,9 @@
-"""Mixed-precision CG: FP64 refinement around FP32-storage inner CG reaches
-the FP64 residual target; the final residual is recomputed independently on
-the host from the COO triplets.  Plain FP64 CG (inner storage FP64) is the
-comparison point; runs are bit-reproducible."""
+"""CG with reliable updates: iterations on FP32-stored values (FP64 x, r,
+dots and updates; FP64 residual recomputations) reach the FP64 residual
+target; the final residual is recomputed independently on the host from the
+COO triplets.  Plain FP64 CG (iteration storage FP64) is the comparison point:
+the mixed form needs about as many iterations.  Runs are bit-reproducible,
+with or without the L2 residency window."""
 import numpy as np
 import pytest
 
@@ -36,17 +38,37 @@ def test_cg_reaches_fp64_tolerance(lib, spd, inner):
     bt = torch.from_numpy(b).cuda()
     xt = torch.zeros(n, dtype=torch.float64, device="cuda")
     st = lib.STORE_F32 if inner == "f32" else lib.STORE_NATIVE
-    r = lib.cg_solve(m, bt.data_ptr(), xt.data_ptr(), tol=1e-10, inner_storage=st, inner_tol=1e-6 if inner == "f32" else 1e-11)
+    r = lib.cg_solve(m, bt.data_ptr(), xt.data_ptr(), tol=1e-10, iter_storage=st)
     assert r.converged == 1 and r.relResidual <= 1e-10
     assert _host_residual(rows, cols, vals, xt.cpu().numpy(), b) <= 2e-10
-    if inner == "f32":
-        assert r.outerIterations >= 2  # FP32-stored values need refinement
-    # bit-reproducible
-    x2 = torch.zeros(n, dtype=torch.float64, device="cuda")
-    r2 = lib.cg_solve(m, bt.data_ptr(), x2.data_ptr(), tol=1e-10, inner_storage=st,
-                      inner_tol=1e-6 if inner == "f32" else 1e-11)
-    assert r2.innerIterations == r.innerIterations
-    assert bits_equal(x2.cpu().numpy(), xt.cpu().numpy())
+    assert r.updates >= 1  # convergence is only declared on a recomputed FP64 residual
+    # bit-reproducible, and the L2 window changes no arithmetic
+    for persist in (True, False):
+        x2 = torch.zeros(n, dtype=torch.float64, device="cuda")
+        r2 = lib.cg_solve(m, bt.data_ptr(), x2.data_ptr(), tol=1e-10, iter_storage=st, l2_persist=persist)
+        assert r2.iterations == r.iterations and r2.updates == r.updates
+        assert bits_equal(x2.cpu().numpy(), xt.cpu().numpy())
+
+
+def test_cg_64cube_mixed_close_to_plain_iterations(lib):
+    """The SPD 27-point stencil on 64^3: the FP32-storage solve converges to
+    1e-10 (host-checked) within 15 % more iterations than plain FP64 CG."""
+    import torch
+    g = 64
+    n = g ** 3
+    rows, cols, vals = lib.generate_stencil27_spd(g, g, g, 1e-3, 7)
+    b = lib.fill_uniform(n, -1.0, 1.0, 11)
+    m = lib.HBDIA(rows, cols, vals, n, n)
+    m.convertToHBDIAFormat(32, 2)
+    bt = torch.from_numpy(b).cuda()
+    res = {}
+    for name, st in (("f64", lib.STORE_NATIVE), ("f32", lib.STORE_F32)):
+        xt = torch.zeros(n, dtype=torch.float64, device="cuda")
+        r = lib.cg_solve(m, bt.data_ptr(), xt.data_ptr(), tol=1e-10, iter_storage=st)
+        assert r.converged == 1
+        assert _host_residual(rows, cols, vals, xt.cpu().numpy(), b) <= 2e-10
+        res[name] = r.iterations
+    assert res["f32"] <= 1.15 * res["f64"] + 10, res
 
 
 def test_cg_rejects_bad_input(lib, spd):
