@@ -18,6 +18,13 @@ roofline    the fused kernel's achieved algorithmic GB/s over the measured HBM
             copy bandwidth (MEASURED_PEAKS.json)
 cpu_baseline the reference's own OpenMP COO SpMV (cpu_coo_spmv_kernel) on the
             same matrix, all host threads, bounded sample
+parity      the timed SpMV's y against the reference's cpu_coo_spmv_kernel
+            (1e-12 scaled) and the oracle's restated HBDIA SpMV (bit for bit)
+served      the serving comparison on 32 resident SPD stencils (edge U[32,160]):
+            80 % SpMV / 20 % CG requests, capacity of the served form (FP32
+            storage, continuous batching, CG with FP64 reliable updates) and of
+            the plain FP64 one-request-per-launch form, then 10,000 Poisson
+            requests at 0.7 x each one's capacity with p50 / p99 latency
 
 Multi-GPU (torchrun): replicas only -- every rank holds its own copy of the
 matrix and runs its own SpMVs; there is no data-path collective.
@@ -328,6 +335,8 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-parity", action="store_true", help="skip the full-size parity check against the oracles")
+    ap.add_argument("--no-serve", action="store_true", help="skip the served comparison (config 5)")
+    ap.add_argument("--serve-requests", type=int, default=10000, help="Poisson requests per server (config 5)")
     ap.add_argument("--unroll", type=int, default=0, choices=[0, 9, 27],
                     help="offsets in flight per lane in the staged kernel (0: default)")
     ap.add_argument("--kernel", default=None, choices=["pipe", "quad", "staged", "warp", "rowwise"],
@@ -446,6 +455,14 @@ def main():
         if not args.no_parity:
             parity = parity_report(rows, cols, vals, n, x, yt.cpu().numpy(), y_ref)
 
+    served = None
+    if rank == 0 and world == 1 and not args.no_serve:
+        from hbdia_b200 import suite
+        del m  # the headline matrix's device layout is not needed any more
+        torch.cuda.empty_cache()
+        served = suite.served_comparison(requests=args.serve_requests,
+                                         capacity_requests=min(3000, args.serve_requests), log=log)
+
     if rank == 0:
         cs = clk.summary()
         out = {
@@ -466,6 +483,7 @@ def main():
                                     "ms_per_step": single_ms / args.e2e_steps}},
             "cpu_baseline": cpu,
             "parity": parity,
+            "served": served,
             "gpu_launches": args.steps,
             "clocks": cs,
             "spmv_per_s": 1e3 * args.steps * world / total_ms,

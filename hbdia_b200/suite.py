@@ -343,6 +343,107 @@ def _serve_run(hb, srv, ids, mats_n, kinds, mids, xbuf, ybuf, rate, seed):
     return last - first, np.array(lat), np.array(widths), lag[0]
 
 
+def _latency_summary(hb, kinds, lat, widths):
+    is_cg = kinds == hb.REQ_CG
+    pct = lambda a, q: 1e3 * float(np.percentile(a, q)) if len(a) else None  # noqa: E731
+    return {"p50_ms": pct(lat, 50), "p99_ms": pct(lat, 99),
+            "spmv_p50_ms": pct(lat[~is_cg], 50), "spmv_p99_ms": pct(lat[~is_cg], 99),
+            "cg_p50_ms": pct(lat[is_cg], 50), "cg_p99_ms": pct(lat[is_cg], 99),
+            "mean_spmv_batch": float(widths.mean()) if len(widths) else None}
+
+
+def serve_workload(hb, matrices=32, edge_min=32, edge_max=160, seed=5):
+    """Config 5's matrices: SPD 27-point stencils of edge U[edge_min,
+    edge_max] (numpy default_rng(seed)), each with 0.5 % symmetric
+    off-pattern entries (seed 50 + i), converted on the host (blockWidth 32,
+    threshold 2)."""
+    edges = np.random.default_rng(seed).integers(edge_min, edge_max + 1, matrices)
+    mats, ns = [], []
+    for i, e in enumerate(edges.tolist()):
+        r, c, v = hb.generate_stencil27_spd(e, e, e, 1e-3, 50 + i, extra_fraction=0.005)
+        n = e ** 3
+        m = hb.HBDIA(r, c, v, n, n)
+        del r, c, v
+        m.convertToHBDIAFormat(32, 2, upload=False)
+        mats.append(m)
+        ns.append(n)
+    return mats, ns, edges
+
+
+def served_comparison(requests=10000, capacity_requests=3000, load=0.7, cg_fraction=0.2, matrices=32,
+                      edge_min=32, edge_max=160, log=None):
+    """Config 5 measured as one comparison, for the benchmark line.
+
+    Workload: serve_workload's 32 resident matrices (150 GB admission cap);
+    requests 80 % SpMV / 20 % CG (CG to ||b - A y|| / ||b|| <= 1e-10 on the
+    FP64 residual), matrix uniform (default_rng(6)), x / b and y in device
+    memory.  Two servers:
+      * served: continuous batching of SpMVs into SpMMs, FP32-stored values
+        (FP64 accumulation), CG iterating on the FP32 values with FP64
+        reliable updates and L2-resident vectors, 4 concurrent solvers;
+      * plain: FP64 values, one request per launch, FP64 CG, one solver.
+    Each server's capacity is its closed-loop rate (capacity_requests queued,
+    then released); then each takes `requests` Poisson arrivals at `load` x
+    its own capacity, and reports the completed rate and p50 / p99 latency
+    (completion - submission).  The SpMV-only capacity of both (same
+    matrices, no CG) is reported beside it."""
+    import time
+    import torch
+    import hbdia_b200 as hb
+    t_start = time.time()
+    mats, ns, edges = serve_workload(hb, matrices, edge_min, edge_max)
+    rng = np.random.default_rng(6)
+    mids = rng.integers(0, len(mats), requests)
+    kinds = np.where(rng.random(requests) < cg_fraction, hb.REQ_CG, hb.REQ_SPMV)
+    xbuf = [[torch.from_numpy(rng.uniform(-1, 1, n)).cuda() for _ in range(2)] for n in ns]
+    ybuf = [[torch.zeros(n, dtype=torch.float64, device="cuda") for _ in range(40)] for n in ns]
+    servers = {
+        "served": hb.Server(),
+        "plain": hb.Server(batching=0, spmvStorage=hb.STORE_NATIVE, cgIterStorage=hb.STORE_NATIVE,
+                           cgL2Persist=0, cgWorkers=1),
+    }
+    ids = {k: [s.add_matrix(m) for m in mats] for k, s in servers.items()}
+    del mats
+    if log:
+        log(f"[serve] {len(ns)} matrices, {sum(ns)} rows resident in {time.time() - t_start:.1f}s")
+    out = {"workload": f"{len(ns)} SPD 27-point stencils, edge U[{edge_min},{edge_max}] seed 5 "
+                       f"(min {int(edges.min())}, max {int(edges.max())}), 0.5% symmetric extras, {int(sum(ns))} rows; "
+                       f"{requests} Poisson requests, {cg_fraction:.0%} CG to 1e-10, device vectors",
+           "servers": {"served": "continuous batching, FP32-stored values with FP64 accumulation, CG on the "
+                                 "FP32 values with FP64 reliable updates and L2-resident vectors, 4 solvers",
+                       "plain": "FP64 values, one request per launch, FP64 CG, 1 solver"}}
+    spmv_only = np.full(capacity_requests, hb.REQ_SPMV)
+    for name, srv in servers.items():
+        w_k = np.array([hb.REQ_SPMV] * len(ns) + [hb.REQ_CG] * min(4, len(ns)))
+        w_m = np.concatenate([np.arange(len(ns)), np.arange(min(4, len(ns)))])
+        _serve_run(hb, srv, ids[name], ns, w_k, w_m, xbuf, ybuf, None, 0)  # warm-up
+        wall, _, _, _ = _serve_run(hb, srv, ids[name], ns, kinds[:capacity_requests], mids[:capacity_requests],
+                                   xbuf, ybuf, None, 0)
+        cap = capacity_requests / wall
+        wall_s, _, wid_s, _ = _serve_run(hb, srv, ids[name], ns, spmv_only, mids[:capacity_requests], xbuf, ybuf,
+                                         None, 0)
+        rate = load * cap
+        wall, lat, widths, lag = _serve_run(hb, srv, ids[name], ns, kinds, mids, xbuf, ybuf, rate, 7)
+        thr = requests / wall
+        out[name] = dict(capacity_req_s=cap, offered_req_s=rate, throughput_req_s=thr,
+                         saturated=bool(thr < 0.97 * rate), **_latency_summary(hb, kinds, lat, widths),
+                         spmv_only_capacity_req_s=capacity_requests / wall_s,
+                         spmv_only_mean_batch=float(wid_s.mean()), max_submit_lag_ms=1e3 * lag,
+                         device_bytes=int(srv.stats().deviceBytes))
+        if log:
+            log(f"[serve] {name}: capacity {cap:.1f} req/s, {thr:.1f} req/s at {rate:.1f} offered, "
+                f"p50 {out[name]['p50_ms']:.2f} ms p99 {out[name]['p99_ms']:.2f} ms")
+    for s in servers.values():
+        s.close()
+    out["capacity_ratio"] = out["served"]["capacity_req_s"] / out["plain"]["capacity_req_s"]
+    out["spmv_only_capacity_ratio"] = (out["served"]["spmv_only_capacity_req_s"] /
+                                       out["plain"]["spmv_only_capacity_req_s"])
+    out["load"] = load
+    out["memory_budget_bytes"] = 150 * 10 ** 9
+    out["seconds"] = time.time() - t_start
+    return out
+
+
 def serve(args):
     """Config 5: resident matrices, Poisson arrivals, continuous batching.
 
