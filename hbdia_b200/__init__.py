@@ -566,6 +566,14 @@ def spmv_host(matrix: HBDIA, x: np.ndarray, y: np.ndarray) -> None:
     _check(_load().hbdia_spmv_host(matrix.handle, ctypes.c_void_p(x.ctypes.data), ctypes.c_void_p(y.ctypes.data)))
 
 
+def allocation_count() -> tuple:
+    """(device, page-locked host) allocations the library has made since it
+    was loaded (hbdia_allocation_count)."""
+    d, h = ctypes.c_int64(), ctypes.c_int64()
+    _check(_load().hbdia_allocation_count(ctypes.byref(d), ctypes.byref(h)))
+    return d.value, h.value
+
+
 def spmv_host_noalloc(matrix: HBDIA, x: np.ndarray, y: np.ndarray) -> None:
     """spmv_host through the library's fixed per-device array (no device
     allocation; max(numRows, numCols) <= 2^21; calls must not overlap)."""

@@ -154,6 +154,7 @@ _SIGS = [
     ("hbdia_matrix_export_nnz_per_row", ctypes.c_int, [c_vp, c_vp]),
     ("hbdia_matrix_stream", ctypes.c_int, [c_vp, c_vpp]),
     ("hbdia_matrix_device_arrays", ctypes.c_int, [c_vp, ctypes.POINTER(DeviceArrays)]),
+    ("hbdia_allocation_count", ctypes.c_int, [c_i64p, c_i64p]),
     ("hbdia_matrix_synchronize", ctypes.c_int, [c_vp]),
     ("hbdia_matrix_device_status", ctypes.c_int, [c_vp, c_i32p]),
     ("hbdia_matrix_set_kernel", ctypes.c_int, [c_vp, c_i32]),

@@ -385,7 +385,7 @@ Batch *batch_create(const std::vector<const DevicePlan *> &plans) {
         for (size_t i = 0; i < plans.size(); ++i) b->order[i] = static_cast<int32_t>(i);
         std::stable_sort(b->order.begin(), b->order.end(),
                          [&](int32_t a, int32_t c) { return plans[a]->numTiles > plans[c]->numTiles; });
-        check_cuda(cudaMalloc(reinterpret_cast<void **>(&b->counters), sizeof(int32_t) * segs.size()),
+        check_cuda(dev_alloc(reinterpret_cast<void **>(&b->counters), sizeof(int32_t) * segs.size()),
                    "cudaMalloc(batch counters)");
         int dev = 0;
         check_cuda(cudaGetDevice(&dev), "cudaGetDevice");

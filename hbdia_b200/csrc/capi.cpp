@@ -485,6 +485,13 @@ int hbdia_matrix_export_nnz_per_row(const hbdia_matrix *m, int32_t *nnzPerRow) {
     });
 }
 
+int hbdia_allocation_count(int64_t *device, int64_t *pinnedHost) {
+    return guarded([&] {
+        need(device && pinnedHost, HBDIA_ERR_INVALID_ARGUMENT, "null argument");
+        hbdia::allocation_counts(device, pinnedHost);
+    });
+}
+
 int hbdia_matrix_device_arrays(hbdia_matrix *m, hbdia_device_arrays *a) {
     return guarded([&] {
         need(m && a, HBDIA_ERR_INVALID_ARGUMENT, "null argument");
@@ -497,7 +504,7 @@ int hbdia_matrix_device_arrays(hbdia_matrix *m, hbdia_device_arrays *a) {
                                          cudaMemcpyDeviceToHost), "cudaMemcpy(block starts)");
             for (int32_t b = 0; b < P.numBlocks; ++b) sizes[b] = start[b + 1] - start[b];
             int32_t *d = nullptr;
-            hbdia::check_cuda(cudaMalloc(&d, sizes.size() * sizeof(int32_t)), "cudaMalloc(block sizes)");
+            hbdia::check_cuda(hbdia::dev_alloc(&d, sizes.size() * sizeof(int32_t)), "cudaMalloc(block sizes)");
             const cudaError_t e = cudaMemcpy(d, sizes.data(), sizes.size() * sizeof(int32_t), cudaMemcpyHostToDevice);
             if (e != cudaSuccess) {
                 cudaFree(d);
@@ -661,7 +668,7 @@ int hbdia_vector_create(hbdia_dtype dtype, const void *host, int64_t n, hbdia_ve
         v->dtype = dtype;
         v->n = n;
         const size_t bytes = static_cast<size_t>(n) * esize(dtype);
-        hbdia::check_cuda(cudaMalloc(&v->d, bytes ? bytes : 256), "cudaMalloc(vector)");
+        hbdia::check_cuda(hbdia::dev_alloc(&v->d, bytes ? bytes : 256), "cudaMalloc(vector)");
         int err = host && bytes ? cudaMemcpy(v->d, host, bytes, cudaMemcpyHostToDevice)
                                 : cudaMemset(v->d, 0, bytes ? bytes : 256);
         if (err != cudaSuccess) {
@@ -692,7 +699,7 @@ int hbdia_vector_coo_results_ptr(hbdia_vector *v, void **p) {
         if (!v->cooResult) {
             const size_t bytes = static_cast<size_t>(v->n) * esize(v->dtype);
             void *d = nullptr;
-            hbdia::check_cuda(cudaMalloc(&d, bytes ? bytes : 256), "cudaMalloc(COO result buffer)");
+            hbdia::check_cuda(hbdia::dev_alloc(&d, bytes ? bytes : 256), "cudaMalloc(COO result buffer)");
             const cudaError_t e = cudaMemset(d, 0, bytes ? bytes : 256);
             if (e != cudaSuccess) {
                 cudaFree(d);
@@ -798,8 +805,8 @@ int hbdia_spmv_host(hbdia_matrix *m, const void *xh, void *yh) {
         const size_t es = esize(m->dtype);
         const size_t xb = static_cast<size_t>(std::max(P.n, P.numCols)) * es;
         const size_t yb = static_cast<size_t>(P.n) * es;
-        if (!P.xScratch) hbdia::check_cuda(cudaMalloc(&P.xScratch, xb), "cudaMalloc(x scratch)");
-        if (!P.yScratch) hbdia::check_cuda(cudaMalloc(&P.yScratch, yb), "cudaMalloc(y scratch)");
+        if (!P.xScratch) hbdia::check_cuda(hbdia::dev_alloc(&P.xScratch, xb), "cudaMalloc(x scratch)");
+        if (!P.yScratch) hbdia::check_cuda(hbdia::dev_alloc(&P.yScratch, yb), "cudaMalloc(y scratch)");
         cudaStream_t s = static_cast<cudaStream_t>(P.stream);
         hbdia::check_cuda(cudaMemcpyAsync(P.xScratch, xh, xb, cudaMemcpyHostToDevice, s), "cudaMemcpyAsync(x)");
         hbdia::launch_spmv(P, P.xScratch, P.yScratch, s);
@@ -830,8 +837,8 @@ int hbdia_spmv_host_many(hbdia_matrix *m, const void *const *xh, void *const *yh
                 hbdia::check_cuda(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "cudaStreamCreate(pipeline)");
                 m->pipeStream[d] = s;
             }
-            if (!m->pipeX[d]) hbdia::check_cuda(cudaMalloc(&m->pipeX[d], xb), "cudaMalloc(pipeline x)");
-            if (!m->pipeY[d]) hbdia::check_cuda(cudaMalloc(&m->pipeY[d], yb), "cudaMalloc(pipeline y)");
+            if (!m->pipeX[d]) hbdia::check_cuda(hbdia::dev_alloc(&m->pipeX[d], xb), "cudaMalloc(pipeline x)");
+            if (!m->pipeY[d]) hbdia::check_cuda(hbdia::dev_alloc(&m->pipeY[d], yb), "cudaMalloc(pipeline y)");
         }
         // step j on stage j % depth: its copy in, SpMV and copy out are ordered
         // on that stage's stream (so the stage's buffers are free again when

@@ -209,8 +209,8 @@ CgWork *cg_work(CgWork *w, int64_t n) {
     if (w->nparts < 1) w->nparts = 1;
     const size_t words = 3 * static_cast<size_t>(n) + 3 * static_cast<size_t>(w->nparts) + 8;
     try {
-        check_cuda(cudaMalloc(&w->buf, words * sizeof(double)), "cudaMalloc(CG workspace)");
-        check_cuda(cudaMallocHost(&w->host, (static_cast<size_t>(w->nparts) + 1) * sizeof(double)),
+        check_cuda(dev_alloc(&w->buf, words * sizeof(double)), "cudaMalloc(CG workspace)");
+        check_cuda(pinned_alloc(&w->host, (static_cast<size_t>(w->nparts) + 1) * sizeof(double)),
                    "cudaMallocHost(CG partials)");
     } catch (...) {
         cg_free(w);

@@ -53,7 +53,7 @@ struct Scratch {
     template <typename T>
     T *get(size_t count) {
         void *p = nullptr;
-        check_cuda(cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T)), "cudaMalloc(converter scratch)");
+        check_cuda(dev_alloc(&p, std::max<size_t>(count, 1) * sizeof(T)), "cudaMalloc(converter scratch)");
         ptrs.push_back(p);
         return static_cast<T *>(p);
     }
@@ -472,7 +472,7 @@ void convert_on_device(const Coo<T> &coo, int32_t bw, int32_t thr, int64_t maxCo
     const size_t oTile = carve((static_cast<size_t>(Q.numTiles) + 1) * sizeof(int32_t));
     const size_t oStatus = carve(sizeof(int32_t));
     Q.bytes = off;
-    check_cuda(cudaMalloc(&Q.base, Q.bytes), "cudaMalloc(matrix layout)");
+    check_cuda(dev_alloc(&Q.base, Q.bytes), "cudaMalloc(matrix layout)");
     try {
         char *base = static_cast<char *>(Q.base);
         Q.vals = base + oVals;

@@ -73,7 +73,7 @@ Halo *halo_create(int32_t elemBytes, const int64_t *srcOff, const int64_t *dstOf
     h->numSegments = numSegments;
     h->total = total;
     if (total > 0) {
-        const int err = cudaMalloc(&h->table, t.size() * sizeof(int64_t));
+        const int err = dev_alloc(&h->table, t.size() * sizeof(int64_t));
         if (err != cudaSuccess) {
             delete h;
             throw Error(HBDIA_ERR_NO_MEMORY, "cudaMalloc(halo table)");

@@ -234,6 +234,20 @@ void server_stats(Server *S, hbdia_server_stats *out);
 
 // throws Error(HBDIA_ERR_CUDA) with the CUDA error string
 void check_cuda(int err, const char *what);
+// Every device allocation (cudaMalloc) and page-locked host allocation
+// (cudaMallocHost) of the library goes through these, which count the
+// successful ones (hbdia_allocation_count).  They return the cudaError_t.
+int dev_alloc_bytes(void **p, size_t bytes);
+int pinned_alloc_bytes(void **p, size_t bytes);
+template <typename T>
+int dev_alloc(T **p, size_t bytes) {
+    return dev_alloc_bytes(reinterpret_cast<void **>(p), bytes);
+}
+template <typename T>
+int pinned_alloc(T **p, size_t bytes) {
+    return pinned_alloc_bytes(reinterpret_cast<void **>(p), bytes);
+}
+void allocation_counts(int64_t *device, int64_t *pinned);
 // Sets the message hbdia_last_error() reports on this thread; returns status.
 int record_error(int status, const std::string &msg);
 

@@ -119,7 +119,7 @@ void borrow_plan(const hbdia_layout_desc &d, DevicePlan &P) {
     const size_t oStatus = up256((static_cast<size_t>(Q.numTiles) + 1) * sizeof(int32_t));
     const size_t oFlags = oStatus + 256;
     Q.bytes = oFlags + 256;
-    check_cuda(cudaMalloc(&Q.base, Q.bytes), "cudaMalloc(plan)");
+    check_cuda(dev_alloc(&Q.base, Q.bytes), "cudaMalloc(plan)");
     try {
         char *base = static_cast<char *>(Q.base);
         Q.cooTile = reinterpret_cast<int32_t *>(base + oTile);

@@ -10,9 +10,8 @@
 //  - a latency-bound service loop that must not pay for an allocation (and
 //    the device-wide synchronisation an allocation may imply) inside a
 //    request.
-// This entry point needs only memory that exists once the library's module
-// is loaded, so after its set-up it issues copies and one SpMV launch and
-// nothing else.
+// This entry point needs only the array below, so after its set-up it issues
+// copies and one SpMV launch and nothing else.
 //
 // Limits and sharing:
 //  - max(numRows, numCols) <= kMaxElems (2^21, a 128^3 grid); larger
@@ -23,9 +22,12 @@
 //  - Nothing in the array has to start at zero: each call first copies all of
 //    x in, and the SpMV writes every one of the numRows elements of y before
 //    they are copied out.
-//  - The first call on a device does the set-up (looks up the array's device
-//    address with the device current); make that first call before any
-//    stream capture on that device.
+//  - The first call on a device does the set-up: it looks up the array's
+//    device address with the device current.  Under CUDA's lazy module
+//    loading (the default) that lookup is also what loads this file's module
+//    and so commits the array's 32 MiB on the device, so the first call can
+//    fail for lack of device memory; make it at start-up, before other
+//    allocators claim the device, and before any stream capture on it.
 #include <cuda_runtime.h>
 
 #include <algorithm>

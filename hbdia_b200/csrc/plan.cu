@@ -35,6 +35,25 @@ void check_cuda(int err, const char *what) {
     }
 }
 
+std::atomic<int64_t> g_deviceAllocs{0}, g_pinnedAllocs{0};
+
+int dev_alloc_bytes(void **p, size_t bytes) {
+    const cudaError_t e = cudaMalloc(p, bytes);
+    if (e == cudaSuccess) g_deviceAllocs.fetch_add(1, std::memory_order_relaxed);
+    return e;
+}
+
+int pinned_alloc_bytes(void **p, size_t bytes) {
+    const cudaError_t e = cudaMallocHost(p, bytes);
+    if (e == cudaSuccess) g_pinnedAllocs.fetch_add(1, std::memory_order_relaxed);
+    return e;
+}
+
+void allocation_counts(int64_t *device, int64_t *pinned) {
+    *device = g_deviceAllocs.load();
+    *pinned = g_pinnedAllocs.load();
+}
+
 namespace {
 
 constexpr int kUnroll = 9;  // offsets in flight per lane in the bw == 32 kernels
@@ -189,7 +208,7 @@ void build_plan(const HostLayout<T> &L, int storage, DevicePlan &P, const Column
     const size_t oTile = carve((static_cast<size_t>(Q.numTiles) + 1) * sizeof(int32_t));
     const size_t oStatus = carve(sizeof(int32_t));
     Q.bytes = off;
-    check_cuda(cudaMalloc(&Q.base, Q.bytes), "cudaMalloc(matrix layout)");
+    check_cuda(dev_alloc(&Q.base, Q.bytes), "cudaMalloc(matrix layout)");
     char *base = static_cast<char *>(Q.base);
     try {
         Q.vals = base + oVals;

@@ -316,7 +316,7 @@ void cg_worker(Server *S) {
             if (!r->device && M.n > cap) {
                 if (bx) cudaFree(bx);
                 bx = nullptr;
-                check_cuda(cudaMalloc(&bx, 2 * sizeof(double) * static_cast<size_t>(M.n)), "cudaMalloc(CG b, x)");
+                check_cuda(dev_alloc(&bx, 2 * sizeof(double) * static_cast<size_t>(M.n)), "cudaMalloc(CG b, x)");
                 cap = M.n;
             }
             w = cg_work(w, M.n);
@@ -455,9 +455,9 @@ int32_t server_add_matrix(Server *S, const hbdia_matrix *m) {
                                 " device bytes and the server holds " + std::to_string(S->used) + " of its " +
                                 std::to_string(S->opt.memoryBudget) + "-byte budget");
         }
-        check_cuda(cudaMalloc(&M->X, sizeof(double) * static_cast<size_t>(S->opt.maxRhs) * M->rowsX),
+        check_cuda(dev_alloc(&M->X, sizeof(double) * static_cast<size_t>(S->opt.maxRhs) * M->rowsX),
                    "cudaMalloc(server staging x)");
-        check_cuda(cudaMalloc(&M->Y, sizeof(double) * static_cast<size_t>(S->opt.maxRhs) * M->n),
+        check_cuda(dev_alloc(&M->Y, sizeof(double) * static_cast<size_t>(S->opt.maxRhs) * M->n),
                    "cudaMalloc(server staging y)");
         check_cuda(cudaStreamCreateWithFlags(&M->stream, cudaStreamNonBlocking), "cudaStreamCreate(server)");
         for (int32_t i = 0; i < S->opt.maxInFlight; ++i) {

@@ -90,6 +90,11 @@ int hbdia_set_device(int32_t device);
 int hbdia_get_device(int32_t *device);
 /* Status name, e.g. "HBDIA_ERR_RUNTIME". */
 const char *hbdia_status_string(int status);
+/* Allocations the library has made since it was loaded: device memory
+ * (cudaMalloc) and page-locked host memory (cudaMallocHost), successful calls
+ * only.  No counterpart in the reference.  Read it around a call to check
+ * that the call allocated nothing. */
+int hbdia_allocation_count(int64_t *device, int64_t *pinnedHost);
 
 /* ---------------------------------------------------------------- matrices */
 
@@ -382,8 +387,12 @@ void hbdia_plan_destroy(hbdia_plan *p);
  *    (hbdia_matrix_prepare_gpu; HBDIA_ERR_NOT_CONVERTED otherwise);
  *  - every call shares that array: calls that overlap in time race and give
  *    undefined y, so callers serialise them;
- *  - the first call on a device does the set-up (a symbol-address lookup);
- *    make it before any stream capture on that device.
+ *  - the first call on a device does the set-up (a symbol-address lookup).
+ *    With CUDA's lazy module loading (the default) that lookup loads the
+ *    array's module and commits its 32 MiB on the device, so the first call
+ *    can fail with HBDIA_ERR_CUDA when the device is full: make it at
+ *    start-up, before other allocators take the device, and before any
+ *    stream capture on that device.  Later calls commit nothing.
  * Same kernels and results as hbdia_spmv_host; synchronous. */
 int hbdia_spmv_host_noalloc(hbdia_matrix *m, const void *xHost, void *yHost);
 
