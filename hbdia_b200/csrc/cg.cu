@@ -306,7 +306,17 @@ void cg_solve(const DevicePlan &A64, const DevicePlan &Ait, CgWork *w, const dou
         while (rnorm > target && std::isfinite(rnorm) && iters < prm.maxIterations) {
             if (!exec) {
                 check_cuda(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
-                for (int k = 0; k < prm.checkEvery; ++k) iteration(s);
+                try {
+                    for (int k = 0; k < prm.checkEvery; ++k) iteration(s);
+                } catch (...) {
+                    // end the failed capture: a stream left capturing would
+                    // refuse this thread's later allocations and launches
+                    cudaGraph_t g = nullptr;
+                    cudaStreamEndCapture(s, &g);
+                    if (g) cudaGraphDestroy(g);
+                    cudaGetLastError();
+                    throw;
+                }
                 check_cuda(cudaStreamEndCapture(s, &graph), "cudaStreamEndCapture");
                 check_cuda(cudaGraphInstantiate(&exec, graph, 0), "cudaGraphInstantiate");
             }

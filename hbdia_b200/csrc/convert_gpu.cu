@@ -534,6 +534,7 @@ void convert_on_device(const Coo<T> &coo, int32_t bw, int32_t thr, int64_t maxCo
         cudaStream_t s;
         check_cuda(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "cudaStreamCreate");
         Q.stream = s;
+        check_cuda(cudaGetDevice(&Q.device), "cudaGetDevice");
     } catch (...) {
         free_plan(Q);
         throw;

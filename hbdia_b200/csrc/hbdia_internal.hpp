@@ -124,6 +124,7 @@ struct DevicePlan {
     void *cooVal = nullptr;              // T
     int32_t *cooRowPtr = nullptr, *cooTile = nullptr;
     void *stream = nullptr;              // cudaStream_t owned by the plan
+    int32_t device = -1;                 // the device the layout lives on (current when it was built)
     void *xScratch = nullptr, *yScratch = nullptr;  // hbdia_spmv_host buffers
     int64_t bytesPerSpmv = 0;            // algorithmic HBM bytes of one SpMV
     int32_t *status = nullptr;           // device error bits of bounded waits (staged kernel)

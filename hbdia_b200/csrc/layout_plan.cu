@@ -145,6 +145,7 @@ void borrow_plan(const hbdia_layout_desc &d, DevicePlan &P) {
         cudaStream_t s;
         check_cuda(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "cudaStreamCreate");
         Q.stream = s;
+        check_cuda(cudaGetDevice(&Q.device), "cudaGetDevice");
         check_cuda(cudaDeviceSynchronize(), "plan set-up");
     } catch (...) {
         free_plan(Q);

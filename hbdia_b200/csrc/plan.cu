@@ -237,6 +237,7 @@ void build_plan(const HostLayout<T> &L, int storage, DevicePlan &P, const Column
         cudaStream_t s;
         check_cuda(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "cudaStreamCreate");
         Q.stream = s;
+        check_cuda(cudaGetDevice(&Q.device), "cudaGetDevice");
     } catch (...) {
         free_plan(Q);
         throw;
@@ -260,9 +261,12 @@ template void build_plan<float>(const HostLayout<float> &, int, DevicePlan &, co
 
 namespace {
 
-int stream_device(cudaStream_t s) {
+// The device a plan's kernels run on: the one its layout lives on (a stream
+// query would fail while the stream is being captured into a graph).
+int plan_device(const DevicePlan &P) {
+    if (P.device >= 0) return P.device;
     int dev = 0;
-    check_cuda(cudaStreamGetDevice(s, &dev), "cudaStreamGetDevice");
+    check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
     return dev;
 }
 
@@ -270,7 +274,7 @@ int stream_device(cudaStream_t s) {
 // bytes; as many 256-thread CTAs as fit on all SMs at once (shared memory and
 // registers decide).
 template <typename VT, typename XT, int U, int SB>
-void launch_xs_cfg(const dev::XsArgs<VT, XT> &A, const XT *x, XT *y, cudaStream_t s) {
+void launch_xs_cfg(const dev::XsArgs<VT, XT> &A, const XT *x, XT *y, cudaStream_t s, int device) {
     auto kernel = dev::spmv_bw32_xs<VT, XT, U, SB>;
     constexpr size_t smem = dev::xs_smem_bytes(SB);
     static_assert(smem <= 232448, "staged SpMV stages too large for one CTA");
@@ -278,15 +282,14 @@ void launch_xs_cfg(const dev::XsArgs<VT, XT> &A, const XT *x, XT *y, cudaStream_
     // bit d: the shared-memory opt-in is in place on device d.  Several host
     // threads (a server's scheduler and solver threads) launch at once.
     static std::atomic<uint64_t> configured{0};
-    const int dev = stream_device(s);
-    const uint64_t bit = uint64_t(1) << (dev < 63 ? dev : 63);
-    if (dev >= 63 || !(configured.load(std::memory_order_acquire) & bit)) {
+    const uint64_t bit = uint64_t(1) << (device < 63 ? device : 63);
+    if (device >= 63 || !(configured.load(std::memory_order_acquire) & bit)) {
         check_cuda(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
                    "cudaFuncSetAttribute(staged SpMV)");
-        if (dev < 63) configured.fetch_or(bit, std::memory_order_acq_rel);
+        if (device < 63) configured.fetch_or(bit, std::memory_order_acq_rel);
     }
     int sms = 0, perSm = 0;
-    check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "cudaDeviceGetAttribute");
+    check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "cudaDeviceGetAttribute");
     check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kernel, threads, smem),
                "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
     const int64_t ctasNeeded = (static_cast<int64_t>(A.a.numTiles) + dev::kXsWarps - 1) / dev::kXsWarps;
@@ -300,14 +303,14 @@ void launch_xs_cfg(const dev::XsArgs<VT, XT> &A, const XT *x, XT *y, cudaStream_
 // bytes SB (x runs of up to ~2.7 KB by default: a 27-point stencil tile needs
 // 2.6 KB).
 template <typename VT, typename XT>
-void launch_xs(const dev::XsArgs<VT, XT> &A, int32_t cfg, const XT *x, XT *y, cudaStream_t s) {
+void launch_xs(const dev::XsArgs<VT, XT> &A, int32_t cfg, const XT *x, XT *y, cudaStream_t s, int device) {
     constexpr int Ud = sizeof(VT) == 8 ? 16 : 32;
     constexpr int Ua = sizeof(VT) == 8 ? 32 : 16;
     switch (cfg) {
-        case 2: return launch_xs_cfg<VT, XT, Ud, 4352>(A, x, y, s);
-        case 3: return launch_xs_cfg<VT, XT, Ua, 3328>(A, x, y, s);
-        case 4: return launch_xs_cfg<VT, XT, Ud, 6400>(A, x, y, s);
-        default: return launch_xs_cfg<VT, XT, Ud, 3328>(A, x, y, s);
+        case 2: return launch_xs_cfg<VT, XT, Ud, 4352>(A, x, y, s, device);
+        case 3: return launch_xs_cfg<VT, XT, Ua, 3328>(A, x, y, s, device);
+        case 4: return launch_xs_cfg<VT, XT, Ud, 6400>(A, x, y, s, device);
+        default: return launch_xs_cfg<VT, XT, Ud, 3328>(A, x, y, s, device);
     }
 }
 
@@ -315,10 +318,9 @@ void launch_xs(const dev::XsArgs<VT, XT> &A, int32_t cfg, const XT *x, XT *y, cu
 // warps then walk the tiles grid-stride).
 template <typename VT, typename XT, typename Kernel>
 void launch_pipe(Kernel kernel, const dev::SpmvArgs<VT, XT> &a, int32_t numTiles, const XT *x, XT *y,
-                 cudaStream_t s, int threads = 256) {
+                 cudaStream_t s, int device, int threads = 256) {
     int sms = 0, perSm = 0;
-    const int dev = stream_device(s);
-    check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "cudaDeviceGetAttribute");
+    check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "cudaDeviceGetAttribute");
     check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kernel, threads, 0),
                "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
     const int64_t warpsPerCta = threads / 32;
@@ -334,15 +336,16 @@ void launch_pipe(Kernel kernel, const dev::SpmvArgs<VT, XT> &a, int32_t numTiles
 template <typename VT, typename XT>
 void launch_quad(const DevicePlan &P, const dev::SpmvArgs<VT, XT> &a, const XT *x, XT *y, cudaStream_t s) {
     int l2 = 0;
-    check_cuda(cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, stream_device(s)), "cudaDeviceGetAttribute(L2)");
+    const int device = plan_device(P);
+    check_cuda(cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, device), "cudaDeviceGetAttribute(L2)");
     const bool pf = P.prefetchL2 > 0 ||
                     (P.prefetchL2 < 0 &&
                      static_cast<int64_t>(std::max(P.n, P.numCols)) * static_cast<int64_t>(sizeof(XT)) > l2);
     const int32_t g = P.quadGroup ? P.quadGroup : (sizeof(VT) == 8 ? 2 : 4);
     const int32_t quads = (P.numTiles + 3) / 4 * 4;  // tiles covered by whole quads (4 per warp)
 #define HBDIA_QUAD(U)                                                                                  \
-    return pf ? launch_pipe(dev::spmv_bw32_quad<VT, XT, U, true>, a, quads / 4, x, y, s)              \
-              : launch_pipe(dev::spmv_bw32_quad<VT, XT, U, false>, a, quads / 4, x, y, s)
+    return pf ? launch_pipe(dev::spmv_bw32_quad<VT, XT, U, true>, a, quads / 4, x, y, s, device)              \
+              : launch_pipe(dev::spmv_bw32_quad<VT, XT, U, false>, a, quads / 4, x, y, s, device)
     switch (g) {
         case 1: HBDIA_QUAD(1);
         case 2: HBDIA_QUAD(2);
@@ -360,23 +363,23 @@ void launch_pipe_tuned(const DevicePlan &P, const dev::SpmvArgs<VT, XT> &a, cons
     // and +8 % FP32 storage with a 134 MB x); with x resident in L2 the
     // prefetched value rows evict x lines that would have been reused (-2 to
     // -10 % at 57 MB and below).
+    const int device = plan_device(P);
     bool pf = P.prefetchL2 > 0;
     if (P.prefetchL2 < 0) {
         int l2 = 0;
-        const int dev = stream_device(s);
-        check_cuda(cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, dev), "cudaDeviceGetAttribute(L2)");
+        check_cuda(cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, device), "cudaDeviceGetAttribute(L2)");
         pf = static_cast<int64_t>(std::max(P.n, P.numCols)) * static_cast<int64_t>(sizeof(XT)) > l2;
     }
     if (P.unroll != 27 && (P.maskedTail > 0 || (P.maskedTail < 0 && P.tailHeavy))) {
-        if (pf) return launch_pipe(dev::spmv_bw32_pipe<VT, XT, kUnroll, true, true>, a, P.numTiles, x, y, s);
-        return launch_pipe(dev::spmv_bw32_pipe<VT, XT, kUnroll, false, true>, a, P.numTiles, x, y, s);
+        if (pf) return launch_pipe(dev::spmv_bw32_pipe<VT, XT, kUnroll, true, true>, a, P.numTiles, x, y, s, device);
+        return launch_pipe(dev::spmv_bw32_pipe<VT, XT, kUnroll, false, true>, a, P.numTiles, x, y, s, device);
     }
     if (pf) {
-        if (P.unroll == 27) return launch_pipe(dev::spmv_bw32_pipe<VT, XT, 27, true>, a, P.numTiles, x, y, s);
-        return launch_pipe(dev::spmv_bw32_pipe<VT, XT, kUnroll, true>, a, P.numTiles, x, y, s);
+        if (P.unroll == 27) return launch_pipe(dev::spmv_bw32_pipe<VT, XT, 27, true>, a, P.numTiles, x, y, s, device);
+        return launch_pipe(dev::spmv_bw32_pipe<VT, XT, kUnroll, true>, a, P.numTiles, x, y, s, device);
     }
-    if (P.unroll == 27) return launch_pipe(dev::spmv_bw32_pipe<VT, XT, 27>, a, P.numTiles, x, y, s);
-    return launch_pipe(dev::spmv_bw32_pipe<VT, XT, kUnroll>, a, P.numTiles, x, y, s);
+    if (P.unroll == 27) return launch_pipe(dev::spmv_bw32_pipe<VT, XT, 27>, a, P.numTiles, x, y, s, device);
+    return launch_pipe(dev::spmv_bw32_pipe<VT, XT, kUnroll>, a, P.numTiles, x, y, s, device);
 }
 
 template <typename VT, typename XT>
@@ -391,7 +394,7 @@ void launch_typed(const DevicePlan &P, const void *x, void *y, cudaStream_t s) {
         A.status = P.status;
         A.timeoutNs = P.waitTimeoutNs;
         A.skipTile = P.skipTile;
-        launch_xs<VT, XT>(A, P.xsConfig, xp, yp, s);
+        launch_xs<VT, XT>(A, P.xsConfig, xp, yp, s, plan_device(P));
     } else if (kern == HBDIA_KERNEL_PIPE) {
         launch_pipe_tuned<VT, XT>(P, a, xp, yp, s);
     } else if (kern == HBDIA_KERNEL_QUAD) {
