@@ -615,7 +615,7 @@ int hbdia_matrix_set_tuning(hbdia_matrix *m, int32_t key, int32_t value) {
             return;
         }
         if (key == HBDIA_TUNE_STAGES) {
-            need(value >= 0 && value <= 4, HBDIA_ERR_INVALID_ARGUMENT, "stage configuration must be 0-4");
+            need(value >= 0 && value <= 5, HBDIA_ERR_INVALID_ARGUMENT, "stage configuration must be 0-5");
             m->plan.xsConfig = value;
             return;
         }

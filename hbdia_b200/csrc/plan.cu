@@ -270,15 +270,15 @@ int plan_device(const DevicePlan &P) {
     return dev;
 }
 
-// The staged kernel with U stored values in flight per lane and stages of SB
-// bytes; as many 256-thread CTAs as fit on all SMs at once (shared memory and
-// registers decide).
-template <typename VT, typename XT, int U, int SB>
+// The staged kernel with NW warps per CTA and D stages per warp; as many
+// CTAs as fit on all SMs at once (shared memory decides: one per SM).
+template <typename VT, typename XT, int NW, int D>
 void launch_xs_cfg(const dev::XsArgs<VT, XT> &A, const XT *x, XT *y, cudaStream_t s, int device) {
-    auto kernel = dev::spmv_bw32_xs<VT, XT, U, SB>;
-    constexpr size_t smem = dev::xs_smem_bytes(SB);
+    constexpr int SB = dev::xs_stage_bytes<VT>();
+    auto kernel = dev::spmv_bw32_xs<VT, XT, NW, D, SB>;
+    constexpr size_t smem = dev::xs_smem_bytes(NW, D, SB);
     static_assert(smem <= 232448, "staged SpMV stages too large for one CTA");
-    constexpr int threads = dev::kXsWarps * 32;
+    constexpr int threads = NW * 32;
     // bit d: the shared-memory opt-in is in place on device d.  Several host
     // threads (a server's scheduler and solver threads) launch at once.
     static std::atomic<uint64_t> configured{0};
@@ -292,26 +292,36 @@ void launch_xs_cfg(const dev::XsArgs<VT, XT> &A, const XT *x, XT *y, cudaStream_
     check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "cudaDeviceGetAttribute");
     check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kernel, threads, smem),
                "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
-    const int64_t ctasNeeded = (static_cast<int64_t>(A.a.numTiles) + dev::kXsWarps - 1) / dev::kXsWarps;
+    const int64_t ctasNeeded = (static_cast<int64_t>(A.a.numTiles) + NW - 1) / NW;
     const unsigned grid = static_cast<unsigned>(
         std::max<int64_t>(1, std::min<int64_t>(ctasNeeded, int64_t(sms) * std::max(1, perSm))));
     kernel<<<grid, threads, smem, s>>>(A, x, y);
 }
 
-// Staged kernel shapes (HBDIA_TUNE_STAGES): values in flight per lane U
-// (32 for 4- and 2-byte values, 16 for 8-byte ones by default) and stage
-// bytes SB (x runs of up to ~2.7 KB by default: a 27-point stencil tile needs
-// 2.6 KB).
+// Staged kernel shapes (HBDIA_TUNE_STAGES), warps per CTA x stages per warp:
+// 1 = 8 x 2, 2 = 4 x 4, 3 = 8 x 3 (4- and 2-byte values), 4 = 12 x 2 (4- and
+// 2-byte values), 5 = 8 x 4 (2-byte values); 0 = the default: 8 x 2 for
+// 8-byte values, 8 x 3 for 4-byte, 8 x 4 for 2-byte (about 192 KB per CTA).
 template <typename VT, typename XT>
 void launch_xs(const dev::XsArgs<VT, XT> &A, int32_t cfg, const XT *x, XT *y, cudaStream_t s, int device) {
-    constexpr int Ud = sizeof(VT) == 8 ? 16 : 32;
-    constexpr int Ua = sizeof(VT) == 8 ? 32 : 16;
+    constexpr int V = sizeof(VT);
     switch (cfg) {
-        case 2: return launch_xs_cfg<VT, XT, Ud, 4352>(A, x, y, s, device);
-        case 3: return launch_xs_cfg<VT, XT, Ua, 3328>(A, x, y, s, device);
-        case 4: return launch_xs_cfg<VT, XT, Ud, 6400>(A, x, y, s, device);
-        default: return launch_xs_cfg<VT, XT, Ud, 3328>(A, x, y, s, device);
+        case 1: return launch_xs_cfg<VT, XT, 8, 2>(A, x, y, s, device);
+        case 2: return launch_xs_cfg<VT, XT, 4, 4>(A, x, y, s, device);
+        case 3:
+            if constexpr (V <= 4) return launch_xs_cfg<VT, XT, 8, 3>(A, x, y, s, device);
+            break;
+        case 4:
+            if constexpr (V <= 4) return launch_xs_cfg<VT, XT, 12, 2>(A, x, y, s, device);
+            break;
+        case 5:
+            if constexpr (V <= 2) return launch_xs_cfg<VT, XT, 8, 4>(A, x, y, s, device);
+            break;
+        default: break;
     }
+    if constexpr (V == 8) return launch_xs_cfg<VT, XT, 8, 2>(A, x, y, s, device);
+    else if constexpr (V == 4) return launch_xs_cfg<VT, XT, 8, 3>(A, x, y, s, device);
+    else return launch_xs_cfg<VT, XT, 8, 4>(A, x, y, s, device);
 }
 
 // Persistent grid: as many 256-thread CTAs as fit on all SMs at once (the

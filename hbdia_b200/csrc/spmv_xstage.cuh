@@ -1,35 +1,32 @@
-// Staged HBDIA SpMV for blockWidth 32 on sm_100a: the x window of every row
-// tile is staged in shared memory by bulk copies, one tile ahead.
+// Staged HBDIA SpMV for blockWidth 32 on sm_100a: each warp bulk-copies the
+// value rows and the merged x runs of its next tiles into its own
+// shared-memory stages, so its compute reads only shared memory.
 //
-// The HBDIA kernel's x reads (src/Operations/HBDIASpMV.cu:42-71) are one
-// gather per stored value: for a 32-row tile and offset o, lanes read
-// x[row0 + o + lane].  Neighbouring diagonals (o, o+1, o+2 of a stencil) read
-// nearly the same 32 elements, so a tile's x reads collapse into a few runs:
-// the union of [row0 + o, row0 + o + 32) over the tile's offsets, merged where
-// windows overlap or touch (9 runs of 34 elements for a 27-point stencil
-// instead of 27 gathers of 32).  The kernel copies those runs once into
-// shared memory and reads x from there.
+// A 32-row tile's work in the reference's kernel (src/Operations/HBDIASpMV.cu:42-71)
+// is one value load and one x gather per stored offset.  Loaded into
+// registers, those are a few dependent round trips per tile whatever the
+// value width, so 4- and 2-byte value storage gains little over 8-byte (the
+// kernels that load into registers are latency-bound there).  Here a tile's
+// value rows (contiguous in the layout: [k0, k1) x 32 values) arrive by ONE
+// bulk copy, and its x reads -- the union of [row0 + o, row0 + o + 32) over
+// its offsets, merged where windows overlap or touch (9 runs of 34 elements
+// for a 27-point stencil instead of 27 gathers of 32) -- by one bulk copy per
+// run, all issued D - 1 tiles ahead into a ring of D stages per warp and
+// completing on the stage's mbarrier.  Bytes in flight then cost no
+// registers (D - 1 tiles per warp, 8-12 warps per SM).
 //
 // Persistent: warp g of W walks tiles g, g + W, ... (neighbouring warps on
 // neighbouring tiles).  Per tile i the warp
-//   * issues the bulk copies of tile i+1's x runs (one cp.async.bulk per run,
-//     issued by the run's first lane; an unaligned end of x by plain loads)
-//     and the cp.async gathers of x for tile i+1's COO entries into the other
-//     of its two stages, all completing on that stage's mbarrier, and asks L2
-//     for tile i+1's value rows (cp.async.bulk.prefetch.L2);
-//   * loads tile i's stored values into registers, all of the tile's offsets
-//     (up to U) in flight at once, and meanwhile the offsets, COO entries and
-//     block pointers of tiles i+2 and i+3;
-//   * waits for tile i's stage (issued one tile earlier) and runs the FMA
-//     chain with x from shared memory, then the COO remainder.
-// So a tile costs one round trip (its value loads, from L2 after the
-// prefetch) instead of one per group of offsets and x gathers, and the x
-// reads leave the L1/LSU path.  A stage is small (the x runs, 32 COO entries),
-// which keeps 24-32 warps per SM.
-//
+//   * issues the copies of tile i + D - 1 (value rows, x runs, the cp.async
+//     gathers of x for the tile's first 32 COO entries) and records in the
+//     stage head where each offset's x lies;
+//   * loads the offsets / COO entries / scale of tile i + D and the block
+//     pointers of tile i + D + 1 (registers, consumed next iteration);
+//   * waits for tile i's stage and runs the FMA chain from shared memory,
+//     then the COO remainder.
 // Tiles with more than 32 offsets or a window larger than a stage run from
-// global memory (same arithmetic); COO entries past the first 32 of a tile are
-// read from global memory too.
+// global memory (same arithmetic); COO entries past the first 32 of a tile
+// are read from global memory too.
 //
 // Arithmetic is the reference's, in the reference's order (spmv_kernels.cuh):
 // per row, offsets ascending, stored zeros and columns outside [0, xn)
@@ -39,7 +36,8 @@
 //
 // Every wait is bounded by a time limit; on expiry the kernel records an error
 // bit in *status, waits (again bounded) for the copies it has in flight and
-// returns.  No multicast anywhere: each CTA copies into its own shared memory.
+// returns.  No multicast anywhere: each warp copies into its own CTA's shared
+// memory.
 #pragma once
 
 #include "spmv_kernels.cuh"
@@ -126,15 +124,21 @@ __device__ __forceinline__ void fence_proxy_async_smem() {
 }
 
 // ---------------------------------------------------------------- layout
-constexpr int kXsCoo = 32;       // COO entries a stage holds
-constexpr int kXsWarps = 8;      // warps per CTA
+constexpr int kXsCoo = 32;  // COO entries a stage holds
+constexpr int kXsHead = 1024;  // bytes of a stage's head (below)
 
+// A stage's head: what the warp computed about the tile when it issued its
+// copies, read back when it computes the tile.
 template <typename XT>
 struct XsStageHead {
+    int32_t xoff[32];      // offset k: stage element of x[row0 + off_k] (lane 0's row)
+    int32_t off[32];       // offset k (column checks of tiles at the matrix edge)
     int32_t crow[kXsCoo];  // local row of each staged COO entry
+    int32_t meta[8];       // K, k0, c0, c1, flags, scale bits
     XT cval[kXsCoo];
     XT cx[kXsCoo];         // x[col] of the staged COO entries
 };
+enum : int32_t { kXsStaged = 1, kXsInterior = 2 };
 
 template <typename VT, typename XT>
 struct XsArgs {
@@ -144,10 +148,17 @@ struct XsArgs {
     int32_t skipTile;    // test hook: this tile's copies are never issued (-1: off)
 };
 
-// Bytes of dynamic shared memory of one CTA: two stages of SB bytes per warp
-// plus their mbarriers.
-__host__ __device__ constexpr size_t xs_smem_bytes(int stageBytes) {
-    return static_cast<size_t>(kXsWarps) * 2 * stageBytes + static_cast<size_t>(kXsWarps) * 2 * sizeof(uint64_t);
+// Bytes of one stage: head, the value rows of up to 32 offsets, 3 KB of x runs
+// (a 27-point stencil tile needs 9 runs of 34-36 elements, 2.6-2.7 KB in FP64).
+template <typename VT>
+__host__ __device__ constexpr int xs_stage_bytes() {
+    return kXsHead + 32 * 32 * static_cast<int>(sizeof(VT)) + 3072;
+}
+
+// Bytes of dynamic shared memory of one CTA: NW warps x D stages of SB bytes
+// plus one mbarrier per stage.
+__host__ __device__ constexpr size_t xs_smem_bytes(int NW, int D, int SB) {
+    return static_cast<size_t>(NW) * D * SB + static_cast<size_t>(NW) * D * sizeof(uint64_t);
 }
 
 // The DIA part of one tile from global memory (tiles that are not staged):
@@ -180,38 +191,32 @@ __device__ __forceinline__ XT tile_dia_global(const SpmvArgs<VT, XT> &a, const X
     return sum;
 }
 
-// Where a tile's x reads live in its stage.
-struct XsPlace {
-    int32_t xpos;   // this lane's offset: stage element index of x[row0 + off]
-    bool staged;    // K <= 32 and the runs fit the stage (warp-uniform)
-    bool interior;  // every column of the tile inside [0, xn) (warp-uniform)
-};
-
-// U: stored values in flight per lane (one group per U offsets);
-// SB: bytes of one stage (head + x runs).
-template <typename VT, typename XT, int U, int SB>
-__global__ void __launch_bounds__(kXsWarps * 32)
+// NW warps per CTA, D stages of SB bytes per warp: head, the values of up to
+// 32 offsets, then the x runs.
+template <typename VT, typename XT, int NW, int D, int SB>
+__global__ void __launch_bounds__(NW * 32, 1)
 spmv_bw32_xs(const XsArgs<VT, XT> A, const XT *__restrict__ x, XT *__restrict__ y) {
-    static_assert(SB % 128 == 0 && SB > static_cast<int>(sizeof(XsStageHead<XT>)), "bad stage size");
-    static_assert(U >= 8 && U <= 32, "bad group size");
+    constexpr int kVal = 32 * 32 * static_cast<int>(sizeof(VT));  // value rows of 32 offsets
+    static_assert(sizeof(XsStageHead<XT>) <= kXsHead, "stage head too large");
+    static_assert(SB % 128 == 0 && SB > kXsHead + kVal, "bad stage size");
+    static_assert(D >= 2, "need at least two stages");
     constexpr int al = 16 / static_cast<int>(sizeof(XT));  // x elements per 16 bytes
-    constexpr int kHead = (static_cast<int>(sizeof(XsStageHead<XT>)) + 127) & ~127;
-    constexpr int kWinElems = (SB - kHead) / static_cast<int>(sizeof(XT));
+    constexpr int kWinElems = (SB - kXsHead - kVal) / static_cast<int>(sizeof(XT));
     extern __shared__ __align__(128) unsigned char smraw[];
     const int w = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
     const SpmvArgs<VT, XT> &a = A.a;
-    unsigned char *mine = smraw + static_cast<size_t>(w) * 2 * SB;
-    uint64_t *bars = reinterpret_cast<uint64_t *>(smraw + static_cast<size_t>(kXsWarps) * 2 * SB) + w * 2;
+    unsigned char *mine = smraw + static_cast<size_t>(w) * D * SB;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smraw + static_cast<size_t>(NW) * D * SB) + w * D;
 
-    const int32_t W = static_cast<int32_t>(gridDim.x) * kXsWarps;
-    const int32_t gw = static_cast<int32_t>(blockIdx.x) * kXsWarps + w;
+    const int32_t W = static_cast<int32_t>(gridDim.x) * NW;
+    const int32_t gw = static_cast<int32_t>(blockIdx.x) * NW + w;
     if (gw >= a.numTiles) return;  // warp-uniform; this warp's barriers stay unused
     const int32_t nT = (a.numTiles - gw + W - 1) / W;  // tiles of this warp
     if (lane == 0) {
         // lane 0's arrive.expect_tx + 32 cp.async arrivals per phase
-        mbar_init(&bars[0], 1 + 32);
-        mbar_init(&bars[1], 1 + 32);
+#pragma unroll
+        for (int d = 0; d < D; ++d) mbar_init(&bars[d], 1 + 32);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncwarp();
@@ -219,18 +224,43 @@ spmv_bw32_xs(const XsArgs<VT, XT> A, const XT *__restrict__ x, XT *__restrict__ 
     const int32_t xnAl = a.xn & ~(al - 1);
     auto tileOf = [&](int32_t j) { return gw + j * W; };
 
-    // Stage tile j (meta m, this lane's offset `off`, COO entry (cr, cc, cv))
-    // into stage j & 1.
-    auto issue = [&](int32_t j, const TileMeta &m, int32_t off, int32_t cr, int32_t cc, XT cv) -> XsPlace {
+    struct Front {  // what issuing a tile needs, loaded one iteration ahead
+        TileMeta m;
+        int32_t off;  // lane k: offset k of the tile (k < min(K, 32))
+        int32_t cr, cc;
+        XT cv;
+        float s;
+    };
+    auto loadFront = [&](const TileMeta &m, int32_t t) {
+        Front f;
+        f.m = m;
+        f.off = lane < m.k1 - m.k0 ? __ldg(a.offs + m.k0 + lane) : 0;
+        f.cr = 0;
+        f.cc = 0;
+        f.cv = XT(0);
+        const int32_t ce = m.c0 + lane;
+        if (ce < min(m.c1, m.c0 + kXsCoo)) {
+            f.cr = __ldg(a.cooRow + ce) - t * 32;
+            f.cc = __ldg(a.cooCol + ce);
+            f.cv = __ldg(a.cooVal + ce);
+        }
+        f.s = (a.scale && t < a.numBlocks) ? __ldg(a.scale + t) : 1.0f;
+        return f;
+    };
+
+    // Stage tile j: its head, its COO x values (cp.async), its value rows and
+    // its merged x runs (bulk copies), all completing on stage j % D's barrier.
+    auto issue = [&](int32_t j, const Front &f) {
         const int32_t t = tileOf(j);
-        unsigned char *B = mine + (j & 1) * SB;
-        uint64_t *bar = &bars[j & 1];
+        unsigned char *B = mine + (j % D) * SB;
+        uint64_t *bar = &bars[j % D];
         XsStageHead<XT> &H = *reinterpret_cast<XsStageHead<XT> *>(B);
-        XT *win = reinterpret_cast<XT *>(B + kHead);
+        VT *vals = reinterpret_cast<VT *>(B + kXsHead);
+        XT *win = reinterpret_cast<XT *>(B + kXsHead + kVal);
         const int32_t row0 = t * 32;
-        const int32_t K = m.k1 - m.k0;
+        const int32_t K = f.m.k1 - f.m.k0;
         const bool act = lane < K;
-        off = act ? off : 0;
+        const int32_t off = act ? f.off : 0;
         // runs of merged windows [off, off + 32)
         const int32_t prev = __shfl_up_sync(kFull, off, 1);
         const bool isStart = act && (lane == 0 || off > prev + 32);
@@ -259,150 +289,117 @@ spmv_bw32_xs(const XsArgs<VT, XT> A, const XT *__restrict__ x, XT *__restrict__ 
         }
         const int32_t P = incl - len;
         const int32_t xElems = __shfl_sync(kFull, incl, 31);
-        XsPlace pl;
-        pl.staged = K <= 32 && xElems <= kWinElems;
+        const bool staged = K <= 32 && xElems <= kWinElems;
         const int myStart = act ? 31 - __clz(starts & le) : 0;
         const int32_t Pk = __shfl_sync(kFull, P, myStart);
         const int32_t alok = __shfl_sync(kFull, alo, myStart);
-        pl.xpos = Pk + (row0 + off - alok);
         const int32_t offFirst = __shfl_sync(kFull, off, 0);
         const int32_t offLast = __shfl_sync(kFull, off, K > 0 && K <= 32 ? K - 1 : 0);
-        pl.interior = K > 0 && int64_t(row0) + offFirst >= 0 && int64_t(row0) + 31 + offLast < int64_t(a.xn);
-        const int32_t ncoo = min(m.c1 - m.c0, kXsCoo);
+        const bool interior = K > 0 && int64_t(row0) + offFirst >= 0 && int64_t(row0) + 31 + offLast < int64_t(a.xn);
+        if (act) {
+            H.xoff[lane] = Pk + (row0 + off - alok);
+            H.off[lane] = off;
+        }
+        if (lane == 0) {
+            H.meta[0] = K;
+            H.meta[1] = f.m.k0;
+            H.meta[2] = f.m.c0;
+            H.meta[3] = f.m.c1;
+            H.meta[4] = (staged ? kXsStaged : 0) | (interior ? kXsInterior : 0);
+            H.meta[5] = __float_as_int(f.s);
+        }
+        const int32_t ncoo = min(f.m.c1 - f.m.c0, kXsCoo);
         if (lane < ncoo) {
-            H.crow[lane] = cr;
-            H.cval[lane] = cv;
-            cp_async<sizeof(XT)>(&H.cx[lane], x + cc);
+            H.crow[lane] = f.cr;
+            H.cval[lane] = f.cv;
+            cp_async<sizeof(XT)>(&H.cx[lane], x + f.cc);
         }
         // an unaligned end of x (at most al - 1 elements): plain loads
-        if (pl.staged && isStart && hi > bhi) {
+        if (staged && isStart && hi > bhi) {
             for (int32_t e = max(bhi, alo); e < hi; ++e) win[P + (e - alo)] = __ldg(x + e);
         }
         const bool skip = t == A.skipTile;
         if (!skip) cp_async_arrive_noinc(bar);
-        int32_t tot = pl.staged && isStart ? (bhi - alo) * static_cast<int32_t>(sizeof(XT)) : 0;
+        const int32_t valBytes = staged ? K * 32 * static_cast<int32_t>(sizeof(VT)) : 0;
+        int32_t tot = staged && isStart ? (bhi - alo) * static_cast<int32_t>(sizeof(XT)) : 0;
 #pragma unroll
         for (int d = 16; d > 0; d >>= 1) tot += __shfl_xor_sync(kFull, tot, d);
+        tot += valBytes;
         if (lane == 0 && !skip) mbar_arrive_expect_tx(bar, static_cast<uint32_t>(tot));
         __syncwarp();
-        if (pl.staged && !skip && isStart && bhi > alo)
-            bulk_g2s(win + P, x + alo, static_cast<uint32_t>(bhi - alo) * sizeof(XT), bar);
-        return pl;
-    };
-    auto loadOffs = [&](const TileMeta &m) { return lane < m.k1 - m.k0 ? __ldg(a.offs + m.k0 + lane) : 0; };
-    struct CooE {
-        int32_t r, c;
-        XT v;
-    };
-    auto loadCoo = [&](const TileMeta &m, int32_t t) {
-        CooE e{0, 0, XT(0)};
-        const int32_t ce = m.c0 + lane;
-        if (ce < min(m.c1, m.c0 + kXsCoo)) {
-            e.r = __ldg(a.cooRow + ce) - t * 32;
-            e.c = __ldg(a.cooCol + ce);
-            e.v = __ldg(a.cooVal + ce);
+        if (!skip && staged) {
+            if (isStart && bhi > alo)
+                bulk_g2s(win + P, x + alo, static_cast<uint32_t>(bhi - alo) * sizeof(XT), bar);
+            // the tile's value rows: contiguous, 64-byte aligned
+            if (lane == 0 && valBytes > 0)
+                bulk_g2s(vals, a.vals + static_cast<int64_t>(f.m.k0) * 32, static_cast<uint32_t>(valBytes), bar);
         }
-        return e;
     };
-    auto loadScale = [&](int32_t t) { return (a.scale && t < a.numBlocks) ? __ldg(a.scale + t) : 1.0f; };
-    const TileMeta zero{0, 0, 0, 0};
 
-    // tile 0: staged now; tile 1: frontier registers; tile 2: meta
-    TileMeta mC = load_meta(a, tileOf(0));
-    float sC = loadScale(tileOf(0));
-    XsPlace pC;
-    int32_t offC;
-    {
-        offC = loadOffs(mC);
-        const CooE e = loadCoo(mC, tileOf(0));
-        pC = issue(0, mC, offC, e.r, e.c, e.v);
+    // prologue: tiles 0 .. D-2 staged, tile D-1's front in registers
+    TileMeta mNext = load_meta(a, tileOf(0));
+    for (int32_t j = 0; j < D - 1; ++j) {
+        if (j < nT) {
+            const Front f = loadFront(mNext, tileOf(j));
+            mNext = j + 1 < nT ? load_meta(a, tileOf(j + 1)) : TileMeta{0, 0, 0, 0};
+            issue(j, f);
+        }
     }
-    TileMeta mN = nT > 1 ? load_meta(a, tileOf(1)) : zero;
-    int32_t offN = loadOffs(mN);
-    CooE eN = nT > 1 ? loadCoo(mN, tileOf(1)) : CooE{0, 0, XT(0)};
-    float sN = nT > 1 ? loadScale(tileOf(1)) : 1.0f;
-    TileMeta mNN = nT > 2 ? load_meta(a, tileOf(2)) : zero;
+    Front F = D - 1 < nT ? loadFront(mNext, tileOf(D - 1)) : Front{};
+    mNext = D < nT ? load_meta(a, tileOf(D)) : TileMeta{0, 0, 0, 0};
 
     for (int32_t i = 0; i < nT; ++i) {
         const int32_t t = tileOf(i);
-        // stage tile i+1; ask L2 for its value rows
-        XsPlace pN{0, false, false};
-        if (i + 1 < nT) {
-            pN = issue(i + 1, mN, offN, eN.r, eN.c, eN.v);
-            if (lane == 0 && mN.k1 > mN.k0) {  // values of [k0, k1) are contiguous, 64-byte aligned
-                const int64_t bytes = static_cast<int64_t>(mN.k1 - mN.k0) * 32 * static_cast<int64_t>(sizeof(VT));
-                prefetch_l2_bulk(a.vals + static_cast<int64_t>(mN.k0) * 32,
-                                 static_cast<uint32_t>(bytes < 32768 ? bytes : 32768));
-            }
+        // stage tile i + D - 1, then fetch the front of the tile after it
+        if (i + D - 1 < nT) issue(i + D - 1, F);
+        if (i + D < nT) {
+            F = loadFront(mNext, tileOf(i + D));
+            mNext = i + D + 1 < nT ? load_meta(a, tileOf(i + D + 1)) : TileMeta{0, 0, 0, 0};
         }
-        // tile i's values: the first group of up to U offsets in flight
-        const int32_t K = mC.k1 - mC.k0;
-        const int32_t row0 = t * 32;
-        const int32_t row = row0 + lane;
-        const VT *vp = a.vals + static_cast<int64_t>(mC.k0) * 32 + lane;
-        VT v[U];
-        if (pC.staged) {
-#pragma unroll
-            for (int u = 0; u < U; ++u) v[u] = u < K ? ld_stream(vp + u * 32) : VT(0);
-        }
-        // frontier: offsets / COO entries / scale of tile i+2, meta of tile i+3
-        const TileMeta m2 = mNN;
-        const int32_t off2 = i + 2 < nT ? loadOffs(m2) : 0;
-        const CooE e2 = i + 2 < nT ? loadCoo(m2, tileOf(i + 2)) : CooE{0, 0, XT(0)};
-        const float s2 = i + 2 < nT ? loadScale(tileOf(i + 2)) : 1.0f;
-        mNN = i + 3 < nT ? load_meta(a, tileOf(i + 3)) : zero;
-
-        unsigned char *B = mine + (i & 1) * SB;
-        if (!mbar_wait(&bars[i & 1], static_cast<uint32_t>(i >> 1) & 1u, A.timeoutNs)) {
+        unsigned char *B = mine + (i % D) * SB;
+        if (!mbar_wait(&bars[i % D], static_cast<uint32_t>(i / D) & 1u, A.timeoutNs)) {
             // give up: record it, let the copies in flight land, return
             if (lane == 0) atomicOr(A.status, kErrConsumerWait);
             cp_async_wait_all();
             bool drained = true;
-            for (int32_t j = i; j < min(nT, i + 2) && drained; ++j) {
+            for (int32_t j = i; j < min(nT, i + D) && drained; ++j) {
                 if (tileOf(j) == A.skipTile) continue;
-                drained = mbar_wait(&bars[j & 1], static_cast<uint32_t>(j >> 1) & 1u, A.timeoutNs);
+                drained = mbar_wait(&bars[j % D], static_cast<uint32_t>(j / D) & 1u, A.timeoutNs);
             }
             if (!drained && lane == 0) atomicOr(A.status, kErrDrain);
             __syncwarp();
             return;
         }
         const XsStageHead<XT> &H = *reinterpret_cast<const XsStageHead<XT> *>(B);
-        const XT *win = reinterpret_cast<const XT *>(B + kHead) + lane;
+        const VT *vals = reinterpret_cast<const VT *>(B + kXsHead) + lane;
+        const XT *win = reinterpret_cast<const XT *>(B + kXsHead + kVal) + lane;
+        const int32_t K = H.meta[0], flags = H.meta[4];
+        const int32_t c0 = H.meta[2], c1 = H.meta[3];
+        const float s = __int_as_float(H.meta[5]);
+        const int32_t row0 = t * 32;
+        const int32_t row = row0 + lane;
         XT sum = XT(0);
-        if (pC.staged) {
-            // groups of U offsets (K <= 32): the first group's loads were
-            // issued before the wait, later groups' loads go here
-            for (int32_t g = 0; g < K; g += U) {
-                if (g > 0) {
-#pragma unroll
-                    for (int u = 0; u < U; ++u) v[u] = g + u < K ? ld_stream(vp + (g + u) * 32) : VT(0);
+        if (flags & kXsStaged) {
+            if (flags & kXsInterior) {
+#pragma unroll 9
+                for (int32_t k = 0; k < K; ++k) {
+                    const XT vv = widen<XT>(vals[k * 32], s);
+                    const XT xv = win[H.xoff[k]];
+                    if (vv != XT(0)) sum = fma_rn(vv, xv, sum);
                 }
-                if (pC.interior) {
-#pragma unroll
-                    for (int u = 0; u < U; ++u) {
-                        if (g + u < K) {
-                            const XT xv = win[__shfl_sync(kFull, pC.xpos, g + u)];
-                            const XT vv = widen<XT>(v[u], sC);
-                            if (vv != XT(0)) sum = fma_rn(vv, xv, sum);
-                        }
-                    }
-                } else {
-#pragma unroll
-                    for (int u = 0; u < U; ++u) {
-                        if (g + u < K) {
-                            const int32_t col = row + __shfl_sync(kFull, offC, g + u);
-                            const int32_t p = __shfl_sync(kFull, pC.xpos, g + u);
-                            const XT vv = widen<XT>(v[u], sC);
-                            if (static_cast<uint32_t>(col) < xn && vv != XT(0)) sum = fma_rn(vv, win[p], sum);
-                        }
-                    }
+            } else {
+#pragma unroll 4
+                for (int32_t k = 0; k < K; ++k) {
+                    const int32_t col = row + H.off[k];
+                    const XT vv = widen<XT>(vals[k * 32], s);
+                    if (static_cast<uint32_t>(col) < xn && vv != XT(0)) sum = fma_rn(vv, win[H.xoff[k]], sum);
                 }
             }
         } else if (K > 0) {
-            sum = tile_dia_global<VT, XT>(a, x, mC.k0, K, row, sC);
+            sum = tile_dia_global<VT, XT>(a, x, H.meta[1], K, row, s);
         }
         if (a.hasCoo) {
-            const int32_t nc = min(mC.c1 - mC.c0, kXsCoo);
+            const int32_t nc = min(c1 - c0, kXsCoo);
             int lr = -1;
             XT p = XT(0);
             if (lane < nc) {
@@ -415,23 +412,14 @@ spmv_bw32_xs(const XsArgs<VT, XT> A, const XT *__restrict__ x, XT *__restrict__ 
                 const XT pt = __shfl_sync(kFull, p, q);
                 if (rt == lane) c = add_rn(c, pt);
             }
-            if (mC.c1 - mC.c0 > kXsCoo)  // rare: continue in list order from global memory
-                c = tile_coo<XT>(a.cooRow, a.cooCol, a.cooVal, mC.c0 + kXsCoo, mC.c1, row0, lane, x, c);
+            if (c1 - c0 > kXsCoo)  // rare: continue in list order from global memory
+                c = tile_coo<XT>(a.cooRow, a.cooCol, a.cooVal, c0 + kXsCoo, c1, row0, lane, x, c);
             sum = add_rn(sum, c);
         }
         if (row < a.n) __stcs(y + row, sum);
-        // this stage is refilled next iteration: reads before the async writes
+        // this stage is refilled D - 1 iterations from now: reads before the async writes
         fence_proxy_async_smem();
         __syncwarp();
-        // rotate the frontier
-        mC = mN;
-        sC = sN;
-        offC = offN;
-        pC = pN;
-        mN = m2;
-        offN = off2;
-        eN = e2;
-        sN = s2;
     }
 }
 

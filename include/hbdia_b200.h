@@ -426,12 +426,11 @@ int hbdia_matrix_selected_kernel(const hbdia_matrix *m, const void *x, int32_t *
  * full groups (e.g. 7-point stencils: 7 offsets per block).  Measured on
  * B200: 7-point stencil +13-20 % (FP64), +40-49 % (FP32 storage); the masked
  * form costs 80 registers in FP64 and 14-26 % where there is no tail.
- * HBDIA_TUNE_STAGES: the staged kernel's shape: 0 (default) or 1 = all of
- * a tile's stored values in flight per lane (16 per group for 8-byte values)
- * and 3.3 KB stages (x runs of up to ~2.7 KB), 2 = 4.3 KB stages, 3 = the
- * other group size (16 for 4- and 2-byte values, 32 for 8-byte ones),
- * 4 = 6.4 KB stages.  Tiles whose x runs do not fit a stage read x from
- * global memory.
+ * HBDIA_TUNE_STAGES: the staged kernel's shape, warps per CTA x stages per
+ * warp: 1 = 8 x 2, 2 = 4 x 4, 3 = 8 x 3, 4 = 12 x 2, 5 = 8 x 4; 0 (default)
+ * = 8 x 2 for 8-byte values, 8 x 3 for 4-byte, 8 x 4 for 2-byte.  Shapes
+ * that do not fit shared memory for the value type run the default.  Tiles
+ * with more than 32 offsets or x runs beyond 3 KB read global memory.
  * HBDIA_TUNE_QUAD_GROUP: offsets of the four blocks in flight per lane in the
  * quad kernel (0 = default: 4 for 4- and 2-byte values, 2 for 8-byte ones;
  * or 1, 2, 4, 8). */

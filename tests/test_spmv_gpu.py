@@ -193,7 +193,7 @@ def test_staged_configs_keep_bits(lib, orc, storage):
         assert bits_equal(ypipe, orc.convert(rows, cols, vals, n, n, 32, 2).spmv(x))
     m.setKernel(lib.KERNEL_STAGED)
     assert m.selectedKernel(xv.getDeviceDataPtr()) == lib.KERNEL_STAGED
-    for cfg in range(5):
+    for cfg in range(6):
         m.setTuning(lib.TUNE_STAGES, cfg)
         yv = lib.HBDIAVector(np.full(n, np.nan))
         for _ in range(2):
