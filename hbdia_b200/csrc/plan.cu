@@ -299,29 +299,33 @@ void launch_xs_cfg(const dev::XsArgs<VT, XT> &A, const XT *x, XT *y, cudaStream_
 }
 
 // Staged kernel shapes (HBDIA_TUNE_STAGES), warps per CTA x stages per warp:
-// 1 = 8 x 2, 2 = 4 x 4, 3 = 8 x 3 (4- and 2-byte values), 4 = 12 x 2 (4- and
-// 2-byte values), 5 = 8 x 4 (2-byte values); 0 = the default: 8 x 2 for
-// 8-byte values, 8 x 3 for 4-byte, 8 x 4 for 2-byte (about 192 KB per CTA).
+// 1 = 8 x 2, 2 = 12 x 2, 3 = 16 x 2, 4 = 12 x 3, 5 = 16 x 4; 0 = the default:
+// 12 x 2 for 8-byte values, 16 x 2 for 4-byte, 16 x 3 for 2-byte.  A shape
+// whose stages do not fit one CTA's shared memory runs the default.
+template <typename VT, typename XT, int NW, int D>
+constexpr bool xs_fits() {
+    return dev::xs_smem_bytes(NW, D, dev::xs_stage_bytes<VT>()) <= 232448;
+}
+
 template <typename VT, typename XT>
 void launch_xs(const dev::XsArgs<VT, XT> &A, int32_t cfg, const XT *x, XT *y, cudaStream_t s, int device) {
-    constexpr int V = sizeof(VT);
     switch (cfg) {
         case 1: return launch_xs_cfg<VT, XT, 8, 2>(A, x, y, s, device);
-        case 2: return launch_xs_cfg<VT, XT, 4, 4>(A, x, y, s, device);
+        case 2: return launch_xs_cfg<VT, XT, 12, 2>(A, x, y, s, device);
         case 3:
-            if constexpr (V <= 4) return launch_xs_cfg<VT, XT, 8, 3>(A, x, y, s, device);
+            if constexpr (xs_fits<VT, XT, 16, 2>()) return launch_xs_cfg<VT, XT, 16, 2>(A, x, y, s, device);
             break;
         case 4:
-            if constexpr (V <= 4) return launch_xs_cfg<VT, XT, 12, 2>(A, x, y, s, device);
+            if constexpr (xs_fits<VT, XT, 12, 3>()) return launch_xs_cfg<VT, XT, 12, 3>(A, x, y, s, device);
             break;
         case 5:
-            if constexpr (V <= 2) return launch_xs_cfg<VT, XT, 8, 4>(A, x, y, s, device);
+            if constexpr (xs_fits<VT, XT, 16, 4>()) return launch_xs_cfg<VT, XT, 16, 4>(A, x, y, s, device);
             break;
         default: break;
     }
-    if constexpr (V == 8) return launch_xs_cfg<VT, XT, 8, 2>(A, x, y, s, device);
-    else if constexpr (V == 4) return launch_xs_cfg<VT, XT, 8, 3>(A, x, y, s, device);
-    else return launch_xs_cfg<VT, XT, 8, 4>(A, x, y, s, device);
+    if constexpr (sizeof(VT) == 8) return launch_xs_cfg<VT, XT, 12, 2>(A, x, y, s, device);
+    else if constexpr (sizeof(VT) == 4) return launch_xs_cfg<VT, XT, 16, 2>(A, x, y, s, device);
+    else return launch_xs_cfg<VT, XT, 16, 3>(A, x, y, s, device);
 }
 
 // Persistent grid: as many 256-thread CTAs as fit on all SMs at once (the

@@ -1,32 +1,36 @@
 // Staged HBDIA SpMV for blockWidth 32 on sm_100a: each warp bulk-copies the
-// value rows and the merged x runs of its next tiles into its own
-// shared-memory stages, so its compute reads only shared memory.
+// value rows of its next tiles into its own shared-memory stages and gathers
+// a tile's x values all at once.
 //
 // A 32-row tile's work in the reference's kernel (src/Operations/HBDIASpMV.cu:42-71)
-// is one value load and one x gather per stored offset.  Loaded into
-// registers, those are a few dependent round trips per tile whatever the
-// value width, so 4- and 2-byte value storage gains little over 8-byte (the
-// kernels that load into registers are latency-bound there).  Here a tile's
-// value rows (contiguous in the layout: [k0, k1) x 32 values) arrive by ONE
-// bulk copy, and its x reads -- the union of [row0 + o, row0 + o + 32) over
-// its offsets, merged where windows overlap or touch (9 runs of 34 elements
-// for a 27-point stencil instead of 27 gathers of 32) -- by one bulk copy per
-// run, all issued D - 1 tiles ahead into a ring of D stages per warp and
-// completing on the stage's mbarrier.  Bytes in flight then cost no
-// registers (D - 1 tiles per warp, 8-12 warps per SM).
+// is one value load and one x gather per stored offset.  With values and x
+// loaded into registers in groups (the pipelined kernel), a tile costs a few
+// dependent round trips whatever the value width, so 4- and 2-byte value
+// storage gains little over 8-byte: that kernel is latency-bound there.  Here
+// a tile's value rows -- contiguous in the layout: [k0, k1) x 32 values --
+// arrive by ONE bulk copy issued D - 1 tiles ahead into a ring of D stages per
+// warp, completing on the stage's mbarrier, so the value stream is in flight
+// without holding registers; the tile's x gathers (one per offset, up to 32)
+// are then issued together, one round trip, and the FMA chain reads the
+// values from shared memory.
+//
+// (A variant that also staged the tile's merged x runs -- about 9 bulk copies
+// of ~272 bytes per 27-point tile -- measured 0.57 / 0.33 of the byte
+// roofline in FP64 / FP32 at 256^3: the many small copies and the run
+// bookkeeping made every tile slow, and its time fell only with more warps.)
 //
 // Persistent: warp g of W walks tiles g, g + W, ... (neighbouring warps on
-// neighbouring tiles).  Per tile i the warp
-//   * issues the copies of tile i + D - 1 (value rows, x runs, the cp.async
-//     gathers of x for the tile's first 32 COO entries) and records in the
-//     stage head where each offset's x lies;
+// neighbouring tiles, so x lines are shared through L1/L2).  Per tile i the
+// warp
+//   * issues the value copy of tile i + D - 1 and the cp.async gathers of x for
+//     that tile's first 32 COO entries, and records the tile's offsets and
+//     block pointers in the stage head;
 //   * loads the offsets / COO entries / scale of tile i + D and the block
 //     pointers of tile i + D + 1 (registers, consumed next iteration);
-//   * waits for tile i's stage and runs the FMA chain from shared memory,
+//   * gathers tile i's x values, waits for its stage and runs the FMA chain,
 //     then the COO remainder.
-// Tiles with more than 32 offsets or a window larger than a stage run from
-// global memory (same arithmetic); COO entries past the first 32 of a tile
-// are read from global memory too.
+// Tiles with more than 32 offsets run from global memory (same arithmetic);
+// COO entries past the first 32 of a tile are read from global memory too.
 //
 // Arithmetic is the reference's, in the reference's order (spmv_kernels.cuh):
 // per row, offsets ascending, stored zeros and columns outside [0, xn)
@@ -124,21 +128,19 @@ __device__ __forceinline__ void fence_proxy_async_smem() {
 }
 
 // ---------------------------------------------------------------- layout
-constexpr int kXsCoo = 32;  // COO entries a stage holds
-constexpr int kXsHead = 1024;  // bytes of a stage's head (below)
+constexpr int kXsCoo = 32;    // COO entries a stage holds
+constexpr int kXsHead = 896;  // bytes of a stage's head (below)
 
-// A stage's head: what the warp computed about the tile when it issued its
-// copies, read back when it computes the tile.
+// A stage's head: what the warp knew about the tile when it issued its copy,
+// read back when it computes the tile.
 template <typename XT>
 struct XsStageHead {
-    int32_t xoff[32];      // offset k: stage element of x[row0 + off_k] (lane 0's row)
-    int32_t off[32];       // offset k (column checks of tiles at the matrix edge)
+    int32_t off[32];       // offset k of the tile (k < min(K, 32))
     int32_t crow[kXsCoo];  // local row of each staged COO entry
-    int32_t meta[8];       // K, k0, c0, c1, flags, scale bits
+    int32_t meta[8];       // K, k0, c0, c1, scale bits
     XT cval[kXsCoo];
     XT cx[kXsCoo];         // x[col] of the staged COO entries
 };
-enum : int32_t { kXsStaged = 1, kXsInterior = 2 };
 
 template <typename VT, typename XT>
 struct XsArgs {
@@ -148,11 +150,10 @@ struct XsArgs {
     int32_t skipTile;    // test hook: this tile's copies are never issued (-1: off)
 };
 
-// Bytes of one stage: head, the value rows of up to 32 offsets, 3 KB of x runs
-// (a 27-point stencil tile needs 9 runs of 34-36 elements, 2.6-2.7 KB in FP64).
+// Bytes of one stage: head and the value rows of up to 32 offsets.
 template <typename VT>
 __host__ __device__ constexpr int xs_stage_bytes() {
-    return kXsHead + 32 * 32 * static_cast<int>(sizeof(VT)) + 3072;
+    return kXsHead + 32 * 32 * static_cast<int>(sizeof(VT));
 }
 
 // Bytes of dynamic shared memory of one CTA: NW warps x D stages of SB bytes
@@ -161,8 +162,9 @@ __host__ __device__ constexpr size_t xs_smem_bytes(int NW, int D, int SB) {
     return static_cast<size_t>(NW) * D * SB + static_cast<size_t>(NW) * D * sizeof(uint64_t);
 }
 
-// The DIA part of one tile from global memory (tiles that are not staged):
-// offsets in masked groups of 8 (loads in flight together), ascending order.
+// The DIA part of one tile from global memory (tiles with more than 32
+// offsets): offsets in masked groups of 8 (loads in flight together),
+// ascending order.
 template <typename VT, typename XT>
 __device__ __forceinline__ XT tile_dia_global(const SpmvArgs<VT, XT> &a, const XT *__restrict__ x, int32_t k0,
                                               int32_t K, int32_t row, float s) {
@@ -191,17 +193,14 @@ __device__ __forceinline__ XT tile_dia_global(const SpmvArgs<VT, XT> &a, const X
     return sum;
 }
 
-// NW warps per CTA, D stages of SB bytes per warp: head, the values of up to
-// 32 offsets, then the x runs.
+// NW warps per CTA, D stages of SB bytes per warp (head, then the value rows).
 template <typename VT, typename XT, int NW, int D, int SB>
 __global__ void __launch_bounds__(NW * 32, 1)
 spmv_bw32_xs(const XsArgs<VT, XT> A, const XT *__restrict__ x, XT *__restrict__ y) {
     constexpr int kVal = 32 * 32 * static_cast<int>(sizeof(VT));  // value rows of 32 offsets
     static_assert(sizeof(XsStageHead<XT>) <= kXsHead, "stage head too large");
-    static_assert(SB % 128 == 0 && SB > kXsHead + kVal, "bad stage size");
+    static_assert(SB % 128 == 0 && SB >= kXsHead + kVal, "bad stage size");
     static_assert(D >= 2, "need at least two stages");
-    constexpr int al = 16 / static_cast<int>(sizeof(XT));  // x elements per 16 bytes
-    constexpr int kWinElems = (SB - kXsHead - kVal) / static_cast<int>(sizeof(XT));
     extern __shared__ __align__(128) unsigned char smraw[];
     const int w = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
@@ -221,7 +220,6 @@ spmv_bw32_xs(const XsArgs<VT, XT> A, const XT *__restrict__ x, XT *__restrict__ 
     }
     __syncwarp();
     const uint32_t xn = static_cast<uint32_t>(a.xn);
-    const int32_t xnAl = a.xn & ~(al - 1);
     auto tileOf = [&](int32_t j) { return gw + j * W; };
 
     struct Front {  // what issuing a tile needs, loaded one iteration ahead
@@ -248,65 +246,21 @@ spmv_bw32_xs(const XsArgs<VT, XT> A, const XT *__restrict__ x, XT *__restrict__ 
         return f;
     };
 
-    // Stage tile j: its head, its COO x values (cp.async), its value rows and
-    // its merged x runs (bulk copies), all completing on stage j % D's barrier.
+    // Stage tile j: its head, its COO x values (cp.async) and its value rows
+    // (one bulk copy), completing on stage j % D's barrier.
     auto issue = [&](int32_t j, const Front &f) {
         const int32_t t = tileOf(j);
         unsigned char *B = mine + (j % D) * SB;
         uint64_t *bar = &bars[j % D];
         XsStageHead<XT> &H = *reinterpret_cast<XsStageHead<XT> *>(B);
-        VT *vals = reinterpret_cast<VT *>(B + kXsHead);
-        XT *win = reinterpret_cast<XT *>(B + kXsHead + kVal);
-        const int32_t row0 = t * 32;
         const int32_t K = f.m.k1 - f.m.k0;
-        const bool act = lane < K;
-        const int32_t off = act ? f.off : 0;
-        // runs of merged windows [off, off + 32)
-        const int32_t prev = __shfl_up_sync(kFull, off, 1);
-        const bool isStart = act && (lane == 0 || off > prev + 32);
-        const unsigned starts = __ballot_sync(kFull, isStart);
-        const unsigned le = lane == 31 ? 0xffffffffu : ((2u << lane) - 1u);
-        const unsigned after = starts & ~le;
-        const int endLane = after ? __ffs(after) - 2 : min(K, 32) - 1;
-        const int32_t endOff = __shfl_sync(kFull, off, endLane < 0 ? 0 : endLane);
-        int32_t alo = 0, len = 0, bhi = 0, hi = 0;
-        if (isStart) {
-            const int64_t lo64 = max(int64_t(0), int64_t(row0) + off);
-            const int64_t hi64 = min(int64_t(a.xn), int64_t(row0) + endOff + 32);
-            if (hi64 > lo64) {
-                hi = static_cast<int32_t>(hi64);
-                alo = static_cast<int32_t>(lo64) & ~(al - 1);
-                len = (hi - alo + al - 1) & ~(al - 1);
-                bhi = min((hi + al - 1) & ~(al - 1), xnAl);
-                if (bhi < alo) bhi = alo;
-            }
-        }
-        int32_t incl = len;  // inclusive scan of run lengths (start lanes only)
-#pragma unroll
-        for (int d = 1; d < 32; d <<= 1) {
-            const int32_t u = __shfl_up_sync(kFull, incl, d);
-            if (lane >= d) incl += u;
-        }
-        const int32_t P = incl - len;
-        const int32_t xElems = __shfl_sync(kFull, incl, 31);
-        const bool staged = K <= 32 && xElems <= kWinElems;
-        const int myStart = act ? 31 - __clz(starts & le) : 0;
-        const int32_t Pk = __shfl_sync(kFull, P, myStart);
-        const int32_t alok = __shfl_sync(kFull, alo, myStart);
-        const int32_t offFirst = __shfl_sync(kFull, off, 0);
-        const int32_t offLast = __shfl_sync(kFull, off, K > 0 && K <= 32 ? K - 1 : 0);
-        const bool interior = K > 0 && int64_t(row0) + offFirst >= 0 && int64_t(row0) + 31 + offLast < int64_t(a.xn);
-        if (act) {
-            H.xoff[lane] = Pk + (row0 + off - alok);
-            H.off[lane] = off;
-        }
+        if (lane < K) H.off[lane] = f.off;
         if (lane == 0) {
             H.meta[0] = K;
             H.meta[1] = f.m.k0;
             H.meta[2] = f.m.c0;
             H.meta[3] = f.m.c1;
-            H.meta[4] = (staged ? kXsStaged : 0) | (interior ? kXsInterior : 0);
-            H.meta[5] = __float_as_int(f.s);
+            H.meta[4] = __float_as_int(f.s);
         }
         const int32_t ncoo = min(f.m.c1 - f.m.c0, kXsCoo);
         if (lane < ncoo) {
@@ -314,25 +268,14 @@ spmv_bw32_xs(const XsArgs<VT, XT> A, const XT *__restrict__ x, XT *__restrict__ 
             H.cval[lane] = f.cv;
             cp_async<sizeof(XT)>(&H.cx[lane], x + f.cc);
         }
-        // an unaligned end of x (at most al - 1 elements): plain loads
-        if (staged && isStart && hi > bhi) {
-            for (int32_t e = max(bhi, alo); e < hi; ++e) win[P + (e - alo)] = __ldg(x + e);
-        }
         const bool skip = t == A.skipTile;
         if (!skip) cp_async_arrive_noinc(bar);
-        const int32_t valBytes = staged ? K * 32 * static_cast<int32_t>(sizeof(VT)) : 0;
-        int32_t tot = staged && isStart ? (bhi - alo) * static_cast<int32_t>(sizeof(XT)) : 0;
-#pragma unroll
-        for (int d = 16; d > 0; d >>= 1) tot += __shfl_xor_sync(kFull, tot, d);
-        tot += valBytes;
-        if (lane == 0 && !skip) mbar_arrive_expect_tx(bar, static_cast<uint32_t>(tot));
         __syncwarp();
-        if (!skip && staged) {
-            if (isStart && bhi > alo)
-                bulk_g2s(win + P, x + alo, static_cast<uint32_t>(bhi - alo) * sizeof(XT), bar);
+        if (lane == 0 && !skip) {
             // the tile's value rows: contiguous, 64-byte aligned
-            if (lane == 0 && valBytes > 0)
-                bulk_g2s(vals, a.vals + static_cast<int64_t>(f.m.k0) * 32, static_cast<uint32_t>(valBytes), bar);
+            const uint32_t valBytes = K > 0 && K <= 32 ? static_cast<uint32_t>(K) * 32u * sizeof(VT) : 0u;
+            mbar_arrive_expect_tx(bar, valBytes);
+            if (valBytes) bulk_g2s(B + kXsHead, a.vals + static_cast<int64_t>(f.m.k0) * 32, valBytes, bar);
         }
     };
 
@@ -357,6 +300,26 @@ spmv_bw32_xs(const XsArgs<VT, XT> A, const XT *__restrict__ x, XT *__restrict__ 
             mNext = i + D + 1 < nT ? load_meta(a, tileOf(i + D + 1)) : TileMeta{0, 0, 0, 0};
         }
         unsigned char *B = mine + (i % D) * SB;
+        const XsStageHead<XT> &H = *reinterpret_cast<const XsStageHead<XT> *>(B);
+        // the head was written by this warp when the tile was issued
+        const int32_t K = H.meta[0];
+        const int32_t row0 = t * 32;
+        const int32_t row = row0 + lane;
+        // this tile's x gathers, all in flight before the wait (K <= 32)
+        XT xv[32];
+        uint32_t okMask = 0;
+        const int32_t myoff = lane < K ? H.off[lane] : 0;
+        if (K <= 32) {
+#pragma unroll
+            for (int k = 0; k < 32; ++k) {
+                if (k < K) {  // warp-uniform
+                    const int32_t col = row + __shfl_sync(kFull, myoff, k);
+                    const bool ok = static_cast<uint32_t>(col) < xn;
+                    okMask |= ok ? (1u << k) : 0u;
+                    xv[k] = ok ? __ldg(x + col) : XT(0);
+                }
+            }
+        }
         if (!mbar_wait(&bars[i % D], static_cast<uint32_t>(i / D) & 1u, A.timeoutNs)) {
             // give up: record it, let the copies in flight land, return
             if (lane == 0) atomicOr(A.status, kErrConsumerWait);
@@ -370,32 +333,19 @@ spmv_bw32_xs(const XsArgs<VT, XT> A, const XT *__restrict__ x, XT *__restrict__ 
             __syncwarp();
             return;
         }
-        const XsStageHead<XT> &H = *reinterpret_cast<const XsStageHead<XT> *>(B);
-        const VT *vals = reinterpret_cast<const VT *>(B + kXsHead) + lane;
-        const XT *win = reinterpret_cast<const XT *>(B + kXsHead + kVal) + lane;
-        const int32_t K = H.meta[0], flags = H.meta[4];
         const int32_t c0 = H.meta[2], c1 = H.meta[3];
-        const float s = __int_as_float(H.meta[5]);
-        const int32_t row0 = t * 32;
-        const int32_t row = row0 + lane;
+        const float s = __int_as_float(H.meta[4]);
+        const VT *vals = reinterpret_cast<const VT *>(B + kXsHead) + lane;
         XT sum = XT(0);
-        if (flags & kXsStaged) {
-            if (flags & kXsInterior) {
-#pragma unroll 9
-                for (int32_t k = 0; k < K; ++k) {
+        if (K <= 32) {
+#pragma unroll
+            for (int k = 0; k < 32; ++k) {
+                if (k < K) {  // warp-uniform
                     const XT vv = widen<XT>(vals[k * 32], s);
-                    const XT xv = win[H.xoff[k]];
-                    if (vv != XT(0)) sum = fma_rn(vv, xv, sum);
-                }
-            } else {
-#pragma unroll 4
-                for (int32_t k = 0; k < K; ++k) {
-                    const int32_t col = row + H.off[k];
-                    const XT vv = widen<XT>(vals[k * 32], s);
-                    if (static_cast<uint32_t>(col) < xn && vv != XT(0)) sum = fma_rn(vv, win[H.xoff[k]], sum);
+                    if (((okMask >> k) & 1u) && vv != XT(0)) sum = fma_rn(vv, xv[k], sum);
                 }
             }
-        } else if (K > 0) {
+        } else {
             sum = tile_dia_global<VT, XT>(a, x, H.meta[1], K, row, s);
         }
         if (a.hasCoo) {

@@ -427,10 +427,10 @@ int hbdia_matrix_selected_kernel(const hbdia_matrix *m, const void *x, int32_t *
  * B200: 7-point stencil +13-20 % (FP64), +40-49 % (FP32 storage); the masked
  * form costs 80 registers in FP64 and 14-26 % where there is no tail.
  * HBDIA_TUNE_STAGES: the staged kernel's shape, warps per CTA x stages per
- * warp: 1 = 8 x 2, 2 = 4 x 4, 3 = 8 x 3, 4 = 12 x 2, 5 = 8 x 4; 0 (default)
- * = 8 x 2 for 8-byte values, 8 x 3 for 4-byte, 8 x 4 for 2-byte.  Shapes
- * that do not fit shared memory for the value type run the default.  Tiles
- * with more than 32 offsets or x runs beyond 3 KB read global memory.
+ * warp: 1 = 8 x 2, 2 = 12 x 2, 3 = 16 x 2, 4 = 12 x 3, 5 = 16 x 4; 0
+ * (default) = 12 x 2 for 8-byte values, 16 x 2 for 4-byte, 16 x 3 for
+ * 2-byte.  A shape whose stages do not fit shared memory for the value type
+ * runs the default.  Tiles with more than 32 offsets read global memory.
  * HBDIA_TUNE_QUAD_GROUP: offsets of the four blocks in flight per lane in the
  * quad kernel (0 = default: 4 for 4- and 2-byte values, 2 for 8-byte ones;
  * or 1, 2, 4, 8). */
