@@ -305,11 +305,20 @@ spmv_bw32_xs(const XsArgs<VT, XT> A, const XT *__restrict__ x, XT *__restrict__ 
         const int32_t K = H.meta[0];
         const int32_t row0 = t * 32;
         const int32_t row = row0 + lane;
-        // this tile's x gathers, all in flight before the wait (K <= 32)
+        // interior tile (every column of every offset inside [0, xn), at most
+        // 32 offsets): no column checks, x read at x + row + offset
+        const bool interior = K > 0 && K <= 32 && int64_t(row0) + H.off[0] >= 0 &&
+                              int64_t(row0) + 31 + H.off[K - 1] < int64_t(a.xn);
+        // this tile's x gathers, all in flight before the wait
         XT xv[32];
         uint32_t okMask = 0;
-        const int32_t myoff = lane < K ? H.off[lane] : 0;
-        if (K <= 32) {
+        if (interior) {
+            const XT *xr = x + row;
+#pragma unroll
+            for (int k = 0; k < 32; ++k)
+                if (k < K) xv[k] = __ldg(xr + H.off[k]);  // warp-uniform bound; broadcast read of the offset
+        } else if (K <= 32) {
+            const int32_t myoff = lane < K ? H.off[lane] : 0;
 #pragma unroll
             for (int k = 0; k < 32; ++k) {
                 if (k < K) {  // warp-uniform
@@ -337,7 +346,15 @@ spmv_bw32_xs(const XsArgs<VT, XT> A, const XT *__restrict__ x, XT *__restrict__ 
         const float s = __int_as_float(H.meta[4]);
         const VT *vals = reinterpret_cast<const VT *>(B + kXsHead) + lane;
         XT sum = XT(0);
-        if (K <= 32) {
+        if (interior) {
+#pragma unroll
+            for (int k = 0; k < 32; ++k) {
+                if (k < K) {  // warp-uniform
+                    const XT vv = widen<XT>(vals[k * 32], s);
+                    if (vv != XT(0)) sum = fma_rn(vv, xv[k], sum);
+                }
+            }
+        } else if (K <= 32) {
 #pragma unroll
             for (int k = 0; k < 32; ++k) {
                 if (k < K) {  // warp-uniform
