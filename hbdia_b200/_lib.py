@@ -70,7 +70,7 @@ class ServerOptions(ctypes.Structure):
     _fields_ = [("memoryBudget", c_i64), ("batching", c_i32), ("maxRhs", c_i32), ("spmvStorage", c_i32),
                 ("cgIterStorage", c_i32), ("cgWorkers", c_i32), ("cgMaxUpdates", c_i32), ("cgMaxIterations", c_i32),
                 ("cgCheckEvery", c_i32), ("cgTol", c_dbl), ("cgUpdateFactor", c_dbl), ("cgL2Persist", c_i32),
-                ("maxInFlight", c_i32)]
+                ("maxInFlight", c_i32), ("cgMaxGroup", c_i32)]
 
 
 class RequestInfo(ctypes.Structure):
@@ -81,7 +81,7 @@ class RequestInfo(ctypes.Structure):
 
 class ServerStats(ctypes.Structure):
     _fields_ = [("completed", c_i64), ("spmvRequests", c_i64), ("cgRequests", c_i64), ("spmvSteps", c_i64),
-                ("spmvLaunches", c_i64), ("deviceBytes", c_i64), ("matrices", c_i32)]
+                ("spmvLaunches", c_i64), ("deviceBytes", c_i64), ("matrices", c_i32), ("cgGroups", c_i64)]
 
 
 class StorageCosts(ctypes.Structure):

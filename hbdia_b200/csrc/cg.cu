@@ -28,7 +28,16 @@
 // graph of `checkEvery` iterations that is replayed, so the host
 // synchronises once per `checkEvery` iterations.
 //
-// L2 residency (option): the solver's vectors r, p, q live in one range that
+// Lockstep groups: several solves on the same matrix (each with its own b, x
+// and workspace) advance together, their iterations' SpMVs forming ONE
+// vector-list SpMM (each stored value read once for all of them; column j
+// equals the SpMV of p_j bit for bit) and their vector kernels one launch
+// each (blockIdx.y = solve, the same per-solve partition as a lone solve).
+// Each solve keeps its own reliable-update and convergence schedule and
+// leaves the group when done, so its result equals what it gives alone, bit
+// for bit; a lone solve is a group of one.
+//
+// L2 residency (option, lone solves): the solver's vectors r, p, q live in one range that
 // is marked persisting in L2 (a stream access-policy window) while the solve
 // runs, so the value stream of the SpMV does not evict them; each iteration
 // then draws mostly the matrix values from HBM.
@@ -40,6 +49,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <vector>
 
 #include "hbdia_internal.hpp"
 
@@ -112,13 +122,35 @@ __global__ void __launch_bounds__(kThreads) cg_start(const double *__restrict__ 
         p[i] = r[i];
 }
 
-// alpha = r.r / p.q;  x += alpha p;  r -= alpha q;  partial sums of new r.r
-__global__ void __launch_bounds__(kThreads) cg_update(double *__restrict__ x, double *__restrict__ r,
-                                                      const double *__restrict__ p, const double *__restrict__ q,
-                                                      int64_t n, const double *__restrict__ pqPart, int nparts,
-                                                      const double *__restrict__ scal, double *__restrict__ rrPart) {
-    const double pq = sum_partials(pqPart, nparts);
-    const double alpha = pq != 0.0 ? scal[0] / pq : 0.0;
+// The iteration's vector kernels for a group: solve j = blockIdx.y uses its
+// own vectors, partial sums and scalars, with blockIdx.x / gridDim.x exactly
+// as a lone solve's launch has them.
+constexpr int kCgGroupMax = 16;
+struct GroupVecs {
+    double *x[kCgGroupMax], *r[kCgGroupMax], *p[kCgGroupMax], *q[kCgGroupMax];
+    double *pqPart[kCgGroupMax], *rrPart[kCgGroupMax], *scal[kCgGroupMax];
+};
+
+__global__ void __launch_bounds__(kThreads) g_dot_pq(const __grid_constant__ GroupVecs V, int64_t n) {
+    const int j = blockIdx.y;
+    const double *__restrict__ a = V.p[j];
+    const double *__restrict__ b = V.q[j];
+    double v = 0.0;
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * kThreads + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * kThreads)
+        v = fma(a[i], b[i], v);
+    const double s = block_sum(v);
+    if (threadIdx.x == 0) V.pqPart[j][blockIdx.x] = s;
+}
+
+__global__ void __launch_bounds__(kThreads) g_update(const __grid_constant__ GroupVecs V, int64_t n, int nparts) {
+    const int j = blockIdx.y;
+    double *__restrict__ x = V.x[j];
+    double *__restrict__ r = V.r[j];
+    const double *__restrict__ p = V.p[j];
+    const double *__restrict__ q = V.q[j];
+    const double pq = sum_partials(V.pqPart[j], nparts);
+    const double alpha = pq != 0.0 ? V.scal[j][0] / pq : 0.0;
     double v = 0.0;
     for (int64_t i = static_cast<int64_t>(blockIdx.x) * kThreads + threadIdx.x; i < n;
          i += static_cast<int64_t>(gridDim.x) * kThreads) {
@@ -128,26 +160,26 @@ __global__ void __launch_bounds__(kThreads) cg_update(double *__restrict__ x, do
         v = fma(ri, ri, v);
     }
     const double s = block_sum(v);
-    if (threadIdx.x == 0) rrPart[blockIdx.x] = s;
+    if (threadIdx.x == 0) V.rrPart[j][blockIdx.x] = s;
 }
 
-// beta = r.r_new / r.r;  p = r + beta p.  Every block reads r.r from scalIn;
-// block 0 writes r.r_new to the separate slot scalOut, which copy_scalar moves
-// into scalIn before the next iteration, so no block sees a half-updated value.
-__global__ void __launch_bounds__(kThreads) cg_direction(const double *__restrict__ r, double *__restrict__ p,
-                                                         int64_t n, const double *__restrict__ rrPart, int nparts,
-                                                         const double *__restrict__ scalIn,
-                                                         double *__restrict__ scalOut) {
-    const double rrNew = sum_partials(rrPart, nparts);
-    const double rrOld = scalIn[0];
+__global__ void __launch_bounds__(kThreads) g_direction(const __grid_constant__ GroupVecs V, int64_t n, int nparts) {
+    const int j = blockIdx.y;
+    const double *__restrict__ r = V.r[j];
+    double *__restrict__ p = V.p[j];
+    const double rrNew = sum_partials(V.rrPart[j], nparts);
+    const double rrOld = V.scal[j][0];
     const double beta = rrOld != 0.0 ? rrNew / rrOld : 0.0;
-    if (blockIdx.x == 0 && threadIdx.x == 0) scalOut[0] = rrNew;
+    if (blockIdx.x == 0 && threadIdx.x == 0) V.scal[j][1] = rrNew;
     for (int64_t i = static_cast<int64_t>(blockIdx.x) * kThreads + threadIdx.x; i < n;
          i += static_cast<int64_t>(gridDim.x) * kThreads)
         p[i] = fma(beta, p[i], r[i]);
 }
 
-__global__ void copy_scalar(const double *__restrict__ src, double *__restrict__ dst) { dst[0] = src[0]; }
+__global__ void g_copy_scalar(const __grid_constant__ GroupVecs V, int k) {
+    const int j = threadIdx.x;
+    if (j < k) V.scal[j][0] = V.scal[j][1];
+}
 
 // The partials land in page-locked memory: a copy into pageable memory is
 // synchronous inside the driver, and with several solvers on their own
@@ -232,21 +264,44 @@ int64_t cg_work_bytes(int64_t n, int sms) {
     return 8 * (3 * n + 3 * parts + 8);
 }
 
-void cg_solve(const DevicePlan &A64, const DevicePlan &Ait, CgWork *w, const double *b, double *x,
-              const CgParams &prm, void *stream, CgStats *st) {
+void cg_solve_group(const DevicePlan &A64, const DevicePlan &Ait, CgCall *calls, int k, const CgParams &prm,
+                    void *stream) {
+    if (k < 1 || k > kCgGroupMax) throw Error(HBDIA_ERR_INVALID_ARGUMENT, "CG group of 1 to 16 solves");
     const auto t0 = std::chrono::steady_clock::now();
     cudaStream_t s = static_cast<cudaStream_t>(stream ? stream : A64.stream);
     const int64_t n = A64.n;
-    if (n > w->n) throw Error(HBDIA_ERR_INVALID_ARGUMENT, "CG workspace smaller than the system");
+    for (int j = 0; j < k; ++j)
+        if (!calls[j].w || n > calls[j].w->n) throw Error(HBDIA_ERR_INVALID_ARGUMENT, "CG workspace smaller than the system");
     // reduction partitions from n alone (what a workspace sized to n has), so
     // the result does not depend on the workspace's size
-    const int G = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(w->nparts, (n + kThreads - 1) / kThreads)));
+    int G = 1;
+    {
+        int dev = 0, sms = 0;
+        check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
+        check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "cudaDeviceGetAttribute");
+        G = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(int64_t(sms) * 4, (n + kThreads - 1) / kThreads)));
+    }
+    for (int j = 0; j < k; ++j)  // a workspace for at least n rows holds at least G partial sums
+        if (calls[j].w->nparts < G) throw Error(HBDIA_ERR_INVALID_ARGUMENT, "CG workspace smaller than the system");
+    struct State {
+        double bnorm = 0, target = 0, rnorm = 0, maxIterated = 0;
+        int iters = 0, updates = 0;
+        bool fresh = true, done = false;
+    };
+    std::vector<State> S(static_cast<size_t>(k));
     cudaGraphExec_t exec = nullptr;
     cudaGraph_t graph = nullptr;
+    std::vector<int> graphSet;  // the active solves the captured graph iterates
     bool window = false;
-    auto cleanup = [&] {
+    auto dropGraph = [&] {
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
+        exec = nullptr;
+        graph = nullptr;
+        graphSet.clear();
+    };
+    auto cleanup = [&] {
+        dropGraph();
         if (window) {  // the stream goes back to normal caching
             cudaStreamAttrValue a;
             std::memset(&a, 0, sizeof(a));
@@ -255,10 +310,19 @@ void cg_solve(const DevicePlan &A64, const DevicePlan &Ait, CgWork *w, const dou
             cudaGetLastError();
         }
     };
-    int updates = 0, iters = 0;
-    double rel = 0.0;
+    // FP64 residual of solve j: r = b - A x, its norm on the host and r.r in
+    // its scal[0]; with `start` also p = r
+    auto true_residual = [&](int j, int start) {
+        CgWork *w = calls[j].w;
+        launch_spmv(A64, calls[j].x, w->q, s);
+        residual<<<G, kThreads, 0, s>>>(calls[j].b, w->q, w->r, n, w->nPart);
+        cg_start<<<G, kThreads, 0, s>>>(w->r, w->p, n, w->nPart, G, w->scal, start);
+        check_cuda(cudaGetLastError(), "CG residual");
+        return std::sqrt(host_sum(w->nPart, G, s, w->host));
+    };
+    auto alive = [&](const State &st) { return st.rnorm > st.target && std::isfinite(st.rnorm) && st.iters < prm.maxIterations; };
     try {
-        if (prm.l2Persist) {
+        if (prm.l2Persist && k == 1) {
             int dev = 0;
             check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
             const size_t persist = persisting_l2_bytes(dev);
@@ -269,7 +333,7 @@ void cg_solve(const DevicePlan &A64, const DevicePlan &Ait, CgWork *w, const dou
             if (persist > 0 && maxWindow > 0) {
                 cudaStreamAttrValue a;
                 std::memset(&a, 0, sizeof(a));
-                a.accessPolicyWindow.base_ptr = w->r;
+                a.accessPolicyWindow.base_ptr = calls[0].w->r;
                 a.accessPolicyWindow.num_bytes = std::min(bytes, static_cast<size_t>(maxWindow));
                 a.accessPolicyWindow.hitRatio =
                     static_cast<float>(std::min(1.0, double(persist) / double(a.accessPolicyWindow.num_bytes)));
@@ -279,35 +343,51 @@ void cg_solve(const DevicePlan &A64, const DevicePlan &Ait, CgWork *w, const dou
                 cudaGetLastError();
             }
         }
-        // ||b||
-        dot_partial<<<G, kThreads, 0, s>>>(b, b, n, w->nPart);
-        const double bnorm = std::sqrt(host_sum(w->nPart, G, s, w->host));
-        const double target = prm.tol * (bnorm > 0 ? bnorm : 1.0);
-        // FP64 residual r = b - A x, its norm on the host and r.r in scal[0]
-        auto true_residual = [&](int start) {
-            launch_spmv(A64, x, w->q, s);
-            residual<<<G, kThreads, 0, s>>>(b, w->q, w->r, n, w->nPart);
-            cg_start<<<G, kThreads, 0, s>>>(w->r, w->p, n, w->nPart, G, w->scal, start);
-            check_cuda(cudaGetLastError(), "CG residual");
-            return std::sqrt(host_sum(w->nPart, G, s, w->host));
-        };
-        double rnorm = true_residual(1);
-        rel = bnorm > 0 ? rnorm / bnorm : rnorm;
-        double maxIterated = rnorm;  // largest iterated residual since the last update
-        // one iteration = 5 launches; scal[0] holds r.r, scal[1] the next value
-        auto iteration = [&](cudaStream_t stq) {
-            launch_spmv(Ait, w->p, w->q, stq);
-            dot_partial<<<G, kThreads, 0, stq>>>(w->p, w->q, n, w->pqPart);
-            cg_update<<<G, kThreads, 0, stq>>>(x, w->r, w->p, w->q, n, w->pqPart, G, w->scal, w->rrPart);
-            cg_direction<<<G, kThreads, 0, stq>>>(w->r, w->p, n, w->rrPart, G, w->scal, w->scal + 1);
-            copy_scalar<<<1, 1, 0, stq>>>(w->scal + 1, w->scal);
-        };
-        bool fresh = true;  // rnorm is the FP64 residual of the current x
-        while (rnorm > target && std::isfinite(rnorm) && iters < prm.maxIterations) {
-            if (!exec) {
+        for (int j = 0; j < k; ++j) {
+            CgWork *w = calls[j].w;
+            dot_partial<<<G, kThreads, 0, s>>>(calls[j].b, calls[j].b, n, w->nPart);
+            S[j].bnorm = std::sqrt(host_sum(w->nPart, G, s, w->host));
+            S[j].target = prm.tol * (S[j].bnorm > 0 ? S[j].bnorm : 1.0);
+            S[j].rnorm = true_residual(j, 1);
+            S[j].maxIterated = S[j].rnorm;
+            S[j].done = !alive(S[j]);
+        }
+        for (;;) {
+            std::vector<int> act;
+            for (int j = 0; j < k; ++j)
+                if (!S[j].done) act.push_back(j);
+            if (act.empty()) break;
+            if (act != graphSet) {
+                // one iteration = the SpMM of the active solves + 4 launches
+                dropGraph();
+                GroupVecs V;
+                std::memset(&V, 0, sizeof(V));
+                std::vector<const void *> ps;
+                std::vector<void *> qs;
+                for (size_t a = 0; a < act.size(); ++a) {
+                    CgWork *w = calls[act[a]].w;
+                    V.x[a] = calls[act[a]].x;
+                    V.r[a] = w->r;
+                    V.p[a] = w->p;
+                    V.q[a] = w->q;
+                    V.pqPart[a] = w->pqPart;
+                    V.rrPart[a] = w->rrPart;
+                    V.scal[a] = w->scal;
+                    ps.push_back(w->p);
+                    qs.push_back(w->q);
+                }
+                const int ka = static_cast<int>(act.size());
+                const dim3 grid(static_cast<unsigned>(G), static_cast<unsigned>(ka));
                 check_cuda(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
                 try {
-                    for (int k = 0; k < prm.checkEvery; ++k) iteration(s);
+                    for (int it = 0; it < prm.checkEvery; ++it) {
+                        if (ka == 1) launch_spmv(Ait, ps[0], qs[0], s);
+                        else launch_spmv_list(Ait, ps.data(), qs.data(), ka, s);
+                        g_dot_pq<<<grid, kThreads, 0, s>>>(V, n);
+                        g_update<<<grid, kThreads, 0, s>>>(V, n, G);
+                        g_direction<<<grid, kThreads, 0, s>>>(V, n, G);
+                        g_copy_scalar<<<1, 32, 0, s>>>(V, ka);
+                    }
                 } catch (...) {
                     // end the failed capture: a stream left capturing would
                     // refuse this thread's later allocations and launches
@@ -319,39 +399,66 @@ void cg_solve(const DevicePlan &A64, const DevicePlan &Ait, CgWork *w, const dou
                 }
                 check_cuda(cudaStreamEndCapture(s, &graph), "cudaStreamEndCapture");
                 check_cuda(cudaGraphInstantiate(&exec, graph, 0), "cudaGraphInstantiate");
+                graphSet = act;
             }
             check_cuda(cudaGraphLaunch(exec, s), "cudaGraphLaunch");
-            iters += prm.checkEvery;
-            fresh = false;
-            double *rrHost = w->host + w->nparts;
-            check_cuda(cudaMemcpyAsync(rrHost, w->scal, sizeof(double), cudaMemcpyDeviceToHost, s), "copy r.r");
+            for (int j : act) {
+                S[j].iters += prm.checkEvery;
+                S[j].fresh = false;
+                CgWork *w = calls[j].w;
+                check_cuda(cudaMemcpyAsync(w->host + w->nparts, w->scal, sizeof(double), cudaMemcpyDeviceToHost, s),
+                           "copy r.r");
+            }
             check_cuda(cudaStreamSynchronize(s), "cudaStreamSynchronize");
-            const double iterated = std::sqrt(*rrHost);
-            if (!std::isfinite(iterated)) break;
-            maxIterated = std::max(maxIterated, iterated);
-            const bool converging = iterated <= target;
-            const bool drifted = iterated < prm.updateFactor * maxIterated;
-            if (!(converging || drifted || iters >= prm.maxIterations)) continue;
-            // reliable update: the FP64 residual replaces the iterated one
-            // (p, the search direction, is kept)
-            if (updates >= prm.maxUpdates) break;
-            ++updates;
-            rnorm = true_residual(0);
-            fresh = true;
-            maxIterated = rnorm;
+            for (int j : act) {
+                State &st = S[j];
+                CgWork *w = calls[j].w;
+                const double iterated = std::sqrt(w->host[w->nparts]);
+                if (!std::isfinite(iterated)) {
+                    st.done = true;
+                    continue;
+                }
+                st.maxIterated = std::max(st.maxIterated, iterated);
+                const bool converging = iterated <= st.target;
+                const bool drifted = iterated < prm.updateFactor * st.maxIterated;
+                if (!(converging || drifted || st.iters >= prm.maxIterations)) continue;
+                // reliable update: the FP64 residual replaces the iterated one
+                // (p, the search direction, is kept)
+                if (st.updates >= prm.maxUpdates) {
+                    st.done = true;
+                    continue;
+                }
+                ++st.updates;
+                st.rnorm = true_residual(j, 0);
+                st.fresh = true;
+                st.maxIterated = st.rnorm;
+                if (!alive(st)) st.done = true;
+            }
         }
-        if (!fresh) rnorm = true_residual(0);  // the reported residual is always b - A x in FP64
-        rel = bnorm > 0 ? rnorm / bnorm : rnorm;
+        // the reported residual is always b - A x in FP64
+        for (int j = 0; j < k; ++j)
+            if (!S[j].fresh) S[j].rnorm = true_residual(j, 0);
     } catch (...) {
         cleanup();
         throw;
     }
     cleanup();
     check_cuda(cudaStreamSynchronize(s), "cudaStreamSynchronize");
-    st->updates = updates;
-    st->iterations = iters;
-    st->relResidual = rel;
-    st->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    for (int j = 0; j < k; ++j) {
+        CgStats *st = calls[j].stats;
+        if (!st) continue;
+        st->updates = S[j].updates;
+        st->iterations = S[j].iters;
+        st->relResidual = S[j].bnorm > 0 ? S[j].rnorm / S[j].bnorm : S[j].rnorm;
+        st->seconds = secs;
+    }
+}
+
+void cg_solve(const DevicePlan &A64, const DevicePlan &Ait, CgWork *w, const double *b, double *x,
+              const CgParams &prm, void *stream, CgStats *st) {
+    CgCall c{b, x, w, st};
+    cg_solve_group(A64, Ait, &c, 1, prm, stream);
 }
 
 }  // namespace hbdia

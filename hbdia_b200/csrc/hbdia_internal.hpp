@@ -209,6 +209,16 @@ struct CgStats {
 };
 void cg_solve(const DevicePlan &A64, const DevicePlan &Ait, CgWork *w, const double *b, double *x,
               const CgParams &prm, void *stream, CgStats *stats);
+// Up to 16 solves on one matrix in lockstep (one SpMM per iteration), each
+// with its own workspace; every result equals its lone cg_solve bit for bit.
+struct CgCall {
+    const double *b;
+    double *x;
+    CgWork *w;
+    CgStats *stats;
+};
+void cg_solve_group(const DevicePlan &A64, const DevicePlan &Ait, CgCall *calls, int k, const CgParams &prm,
+                    void *stream);
 // Many matrices in one persistent launch (batch.cu)
 struct Batch;
 Batch *batch_create(const std::vector<const DevicePlan *> &plans);

@@ -291,42 +291,72 @@ void scheduler(Server *S) {
     }
 }
 
+// A CG worker takes the oldest CG request and the other pending CG requests
+// on the same matrix (up to cgMaxGroup) and solves them as one lockstep
+// group: one SpMM per iteration over all of them, each with its own
+// workspace, schedule and result (bit-identical to solving it alone).
 void cg_worker(Server *S) {
     cudaSetDevice(S->device);
     cudaStream_t st = nullptr;
-    CgWork *w = nullptr;
-    double *bx = nullptr;  // b and x, maxN each
-    int32_t cap = 0;
+    std::vector<CgWork *> ws;   // one workspace per group slot
+    std::vector<double *> bx;   // per slot: b and x of host requests, cap each
+    std::vector<int32_t> caps;
     const bool ok = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) == cudaSuccess;
+    const size_t maxGroup = static_cast<size_t>(S->opt.cgMaxGroup);
     for (;;) {
-        Request *r = nullptr;
+        std::vector<Request *> grp;
         {
             std::unique_lock<std::mutex> lk(S->mu);
             S->cvCg.wait(lk, [&] { return S->stop || (!S->paused && !S->cgQ.empty()); });
             if (S->cgQ.empty()) break;
-            r = S->cgQ.front();
+            grp.push_back(S->cgQ.front());
             S->cgQ.pop_front();
+            for (auto it = S->cgQ.begin(); it != S->cgQ.end() && grp.size() < maxGroup;) {
+                if ((*it)->m == grp[0]->m) {
+                    grp.push_back(*it);
+                    it = S->cgQ.erase(it);
+                } else {
+                    ++it;
+                }
+            }
+            S->stats.cgGroups += 1;
         }
-        r->info.started = now_since(S->t0);
-        r->info.batchRhs = 1;
-        int status = HBDIA_OK;
+        const double started = now_since(S->t0);
+        const int32_t k = static_cast<int32_t>(grp.size());
+        std::vector<int> status(grp.size(), HBDIA_OK);
+        for (Request *r : grp) {
+            r->info.started = started;
+            r->info.batchRhs = k;
+        }
         try {
             if (!ok) throw Error(HBDIA_ERR_CUDA, "CG worker stream");
-            const ServedMatrix &M = *r->m;
-            if (!r->device && M.n > cap) {
-                if (bx) cudaFree(bx);
-                bx = nullptr;
-                check_cuda(dev_alloc(&bx, 2 * sizeof(double) * static_cast<size_t>(M.n)), "cudaMalloc(CG b, x)");
-                cap = M.n;
-            }
-            w = cg_work(w, M.n);
-            // device requests solve in place: b = request x, solution into request y
-            const double *b = r->device ? r->x : bx;
-            double *x = r->device ? r->y : bx + cap;
+            const ServedMatrix &M = *grp[0]->m;
             const size_t nb = sizeof(double) * static_cast<size_t>(M.n);
-            if (!r->device)
-                check_cuda(cudaMemcpyAsync(bx, r->x, nb, cudaMemcpyHostToDevice, st), "cudaMemcpyAsync(CG b)");
-            check_cuda(cudaMemsetAsync(x, 0, nb, st), "cudaMemsetAsync(CG x)");
+            if (ws.size() < grp.size()) {
+                ws.resize(grp.size(), nullptr);
+                bx.resize(grp.size(), nullptr);
+                caps.resize(grp.size(), 0);
+            }
+            std::vector<CgCall> calls(grp.size());
+            std::vector<CgStats> stats(grp.size());
+            for (size_t i = 0; i < grp.size(); ++i) {
+                Request *r = grp[i];
+                ws[i] = cg_work(ws[i], M.n);
+                if (!r->device && M.n > caps[i]) {
+                    if (bx[i]) cudaFree(bx[i]);
+                    bx[i] = nullptr;
+                    caps[i] = 0;
+                    check_cuda(dev_alloc(&bx[i], 2 * nb), "cudaMalloc(CG b, x)");
+                    caps[i] = M.n;
+                }
+                // device requests solve in place: b = request x, solution into request y
+                const double *b = r->device ? r->x : bx[i];
+                double *x = r->device ? r->y : bx[i] + caps[i];
+                if (!r->device)
+                    check_cuda(cudaMemcpyAsync(bx[i], r->x, nb, cudaMemcpyHostToDevice, st), "cudaMemcpyAsync(CG b)");
+                check_cuda(cudaMemsetAsync(x, 0, nb, st), "cudaMemsetAsync(CG x)");
+                calls[i] = CgCall{b, x, ws[i], &stats[i]};
+            }
             const hbdia_server_options &o = S->opt;
             CgParams prm;
             prm.tol = o.cgTol;
@@ -335,24 +365,31 @@ void cg_worker(Server *S) {
             prm.maxIterations = o.cgMaxIterations;
             prm.checkEvery = o.cgCheckEvery;
             prm.l2Persist = o.cgL2Persist != 0;
-            CgStats cs;
-            cg_solve(M.p64, M.cgIter(o.cgIterStorage), w, b, x, prm, st, &cs);
-            r->info.cgUpdates = cs.updates;
-            r->info.cgIterations = cs.iterations;
-            r->info.cgRelResidual = cs.relResidual;
-            if (!r->device)
-                check_cuda(cudaMemcpyAsync(r->y, x, nb, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync(CG y)");
+            cg_solve_group(M.p64, M.cgIter(o.cgIterStorage), calls.data(), k, prm, st);
+            for (size_t i = 0; i < grp.size(); ++i) {
+                Request *r = grp[i];
+                if (!r->device)
+                    check_cuda(cudaMemcpyAsync(r->y, calls[i].x, nb, cudaMemcpyDeviceToHost, st),
+                               "cudaMemcpyAsync(CG y)");
+                r->info.cgUpdates = stats[i].updates;
+                r->info.cgIterations = stats[i].iterations;
+                r->info.cgRelResidual = stats[i].relResidual;
+                if (stats[i].relResidual > o.cgTol) status[i] = HBDIA_ERR_RUNTIME;  // not converged
+            }
             check_cuda(cudaStreamSynchronize(st), "cudaStreamSynchronize(CG)");
-            if (r->info.cgRelResidual > o.cgTol) status = HBDIA_ERR_RUNTIME;  // not converged
         } catch (const Error &e) {
-            status = e.status;
+            cudaStreamSynchronize(st);  // nothing issued may still touch the request buffers
+            std::fill(status.begin(), status.end(), e.status);
         } catch (const std::exception &) {
-            status = HBDIA_ERR_RUNTIME;
+            cudaStreamSynchronize(st);
+            std::fill(status.begin(), status.end(), static_cast<int>(HBDIA_ERR_RUNTIME));
         }
-        complete(S, {r}, status, now_since(S->t0));
+        const double finished = now_since(S->t0);
+        for (size_t i = 0; i < grp.size(); ++i) complete(S, {grp[i]}, status[i], finished);
     }
-    cg_free(w);
-    if (bx) cudaFree(bx);
+    for (CgWork *w : ws) cg_free(w);
+    for (double *p : bx)
+        if (p) cudaFree(p);
     if (st) cudaStreamDestroy(st);
 }
 
@@ -384,13 +421,14 @@ void server_default_options(hbdia_server_options *o) {
     o->cgMaxIterations = 20000;
     o->cgCheckEvery = 10;
     o->cgL2Persist = 1;
+    o->cgMaxGroup = 8;
     o->maxInFlight = 1;
 }
 
 Server *server_create(const hbdia_server_options &o) {
     if (o.memoryBudget <= 0 || o.maxRhs < 1 || o.maxRhs > 64 || o.cgWorkers < 1 || o.cgWorkers > 64 ||
         o.cgTol <= 0 || o.cgUpdateFactor <= 0 || o.cgUpdateFactor >= 1 || o.cgMaxUpdates < 1 ||
-        o.cgMaxIterations < 1 || o.cgCheckEvery < 1 ||
+        o.cgMaxIterations < 1 || o.cgCheckEvery < 1 || o.cgMaxGroup < 1 || o.cgMaxGroup > 16 ||
         o.maxInFlight < 1 || o.maxInFlight > 8)
         throw Error(HBDIA_ERR_INVALID_ARGUMENT, "bad server options");
     for (int32_t st : {o.spmvStorage, o.cgIterStorage})
@@ -440,11 +478,13 @@ int32_t server_add_matrix(Server *S, const hbdia_matrix *m) {
         if (low != HBDIA_STORE_NATIVE) build_plan(L, low, M->pLow);
         const int64_t staging =
             static_cast<int64_t>(S->opt.maxRhs) * (static_cast<int64_t>(M->rowsX) + M->n) * 8;
-        // CG workspaces grow to the largest system: 3 vectors of the workspace + b, x per worker
+        // CG workspaces grow to the largest system: 3 vectors of the workspace + b, x per
+        // group slot of every worker
         int64_t cgGrow = 0;
         {
             std::lock_guard<std::mutex> lk(S->mu);
-            if (M->n > S->maxN) cgGrow = static_cast<int64_t>(S->opt.cgWorkers) * 5 * 8 * (M->n - S->maxN);
+            if (M->n > S->maxN)
+                cgGrow = static_cast<int64_t>(S->opt.cgWorkers) * S->opt.cgMaxGroup * 5 * 8 * (M->n - S->maxN);
         }
         M->bytes = static_cast<int64_t>(M->p64.bytes + M->pLow.bytes) + staging;
         {

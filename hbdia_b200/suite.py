@@ -400,7 +400,7 @@ def served_comparison(requests=10000, capacity_requests=3000, load=0.7, cg_fract
     servers = {
         "served": hb.Server(),
         "plain": hb.Server(batching=0, spmvStorage=hb.STORE_NATIVE, cgIterStorage=hb.STORE_NATIVE,
-                           cgL2Persist=0, cgWorkers=1),
+                           cgL2Persist=0, cgWorkers=1, cgMaxGroup=1),
     }
     ids = {k: [s.add_matrix(m) for m in mats] for k, s in servers.items()}
     del mats
@@ -409,9 +409,10 @@ def served_comparison(requests=10000, capacity_requests=3000, load=0.7, cg_fract
     out = {"workload": f"{len(ns)} SPD 27-point stencils, edge U[{edge_min},{edge_max}] seed 5 "
                        f"(min {int(edges.min())}, max {int(edges.max())}), 0.5% symmetric extras, {int(sum(ns))} rows; "
                        f"{requests} Poisson requests, {cg_fraction:.0%} CG to 1e-10, device vectors",
-           "servers": {"served": "continuous batching, FP32-stored values with FP64 accumulation, CG on the "
-                                 "FP32 values with FP64 reliable updates and L2-resident vectors, 4 solvers",
-                       "plain": "FP64 values, one request per launch, FP64 CG, 1 solver"}}
+           "servers": {"served": "continuous batching: SpMV requests of a matrix as one SpMM, CG requests of a "
+                                 "matrix as one lockstep group (one SpMM per iteration); FP32-stored values with "
+                                 "FP64 accumulation, CG on the FP32 values with FP64 reliable updates; 4 solvers",
+                       "plain": "FP64 values, one request per launch, FP64 CG, one solve at a time"}}
     spmv_only = np.full(capacity_requests, hb.REQ_SPMV)
     for name, srv in servers.items():
         w_k = np.array([hb.REQ_SPMV] * len(ns) + [hb.REQ_CG] * min(4, len(ns)))
@@ -422,13 +423,16 @@ def served_comparison(requests=10000, capacity_requests=3000, load=0.7, cg_fract
         cap = capacity_requests / wall
         wall_s, _, wid_s, _ = _serve_run(hb, srv, ids[name], ns, spmv_only, mids[:capacity_requests], xbuf, ybuf,
                                          None, 0)
+        g0 = srv.stats()
         rate = load * cap
         wall, lat, widths, lag = _serve_run(hb, srv, ids[name], ns, kinds, mids, xbuf, ybuf, rate, 7)
+        g1 = srv.stats()
         thr = requests / wall
         out[name] = dict(capacity_req_s=cap, offered_req_s=rate, throughput_req_s=thr,
                          saturated=bool(thr < 0.97 * rate), **_latency_summary(hb, kinds, lat, widths),
                          spmv_only_capacity_req_s=capacity_requests / wall_s,
                          spmv_only_mean_batch=float(wid_s.mean()), max_submit_lag_ms=1e3 * lag,
+                         mean_cg_group=(g1.cgRequests - g0.cgRequests) / max(1, g1.cgGroups - g0.cgGroups),
                          device_bytes=int(srv.stats().deviceBytes))
         if log:
             log(f"[serve] {name}: capacity {cap:.1f} req/s, {thr:.1f} req/s at {rate:.1f} offered, "
@@ -498,7 +502,7 @@ def serve(args):
     servers = {
         "batched": hb.Server(),
         "plain": hb.Server(batching=0, spmvStorage=hb.STORE_NATIVE, cgIterStorage=hb.STORE_NATIVE,
-                           cgL2Persist=0, cgWorkers=1),
+                           cgL2Persist=0, cgWorkers=1, cgMaxGroup=1),
     }
     if args.serial_too:
         servers["batched, 2 batches in flight"] = hb.Server(maxInFlight=2)

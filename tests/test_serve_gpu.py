@@ -104,6 +104,48 @@ def test_same_alone_and_in_mix(lib, mats, batching):
     srv.close()
 
 
+def test_cg_group_equals_lone_solves(lib, mats):
+    """CG requests queued together on one matrix are solved as one lockstep
+    group (one SpMM per iteration); each result equals its lone cg_solve bit
+    for bit, whatever the group's other members -- including a zero right-hand
+    side (done before the first iteration) and a smooth one that converges at
+    its own iteration count."""
+    import torch
+    m, rcv, n = mats[2]
+    rows, cols, vals = rcv
+    rng = np.random.default_rng(21)
+    bs = [rng.uniform(-1, 1, n), np.zeros(n), np.cos(np.arange(n) * 0.001), rng.uniform(-1, 1, n) * 1e3,
+          rng.uniform(0, 1, n)]
+    srv = lib.Server(cgWorkers=1)
+    mid = srv.add_matrix(m)
+    srv.pause(True)
+    keep, pending = [], []
+    for b0 in bs:
+        tb, b = _pinned(n)
+        b[:] = b0
+        tc, c = _pinned(n)
+        keep += [tb, tc]
+        pending.append((b0, c, srv.submit(mid, lib.REQ_CG, b, c)))
+    srv.pause(False)
+    infos = [srv.wait(t) for _, _, t in pending]
+    st = srv.stats()
+    srv.close()
+    assert all(i.status == 0 for i in infos)
+    assert max(i.batchRhs for i in infos) == len(bs)  # all five went as one group
+    assert st.cgGroups == 1
+    ref = lib.HBDIA(rows, cols, vals, n, n)
+    ref.convertToHBDIAFormat(32, 2)
+    iters = set()
+    for (b0, c, _), info in zip(pending, infos):
+        bt = torch.from_numpy(b0).cuda()
+        xt = torch.zeros(n, dtype=torch.float64, device="cuda")
+        r = lib.cg_solve(ref, bt.data_ptr(), xt.data_ptr(), tol=1e-10, iter_storage=lib.STORE_F32)
+        assert r.iterations == info.cgIterations and r.updates == info.cgUpdates
+        assert bits_equal(xt.cpu().numpy(), c)
+        iters.add(info.cgIterations)
+    assert len(iters) > 1  # the members left the group at different iterations
+
+
 def test_spmv_matches_entry_points_and_fp64(lib, mats):
     import torch
     m, rcv, n = mats[1]
