@@ -619,13 +619,12 @@ def generate_stencil27_spd(nx: int, ny: int, nz: int, shift: float = 1e-3, seed:
 
 def cg_solve(matrix: HBDIA, b_ptr: int, x_ptr: int, tol: float = 1e-10, iter_storage: int = STORE_F32,
              update_factor: float = 0.1, max_updates: int = 100, max_iterations: int = 20000,
-             check_every: int = 10, l2_persist: bool = True, stream: Optional[int] = None) -> "_lib.CgResult":
+             check_every: int = 10, stream: Optional[int] = None) -> "_lib.CgResult":
     """CG on device buffers b, x (x: initial guess in, solution out): the
     iterations' SpMVs use the ``iter_storage`` values (STORE_F32: mixed
     precision, STORE_NATIVE: plain FP64 CG), with reliable updates of the
     FP64 residual and convergence judged on it (hbdia_cg_solve)."""
-    o = _lib.CgOptions(tol, update_factor, max_updates, max_iterations, iter_storage, check_every,
-                       1 if l2_persist else 0)
+    o = _lib.CgOptions(tol, update_factor, max_updates, max_iterations, iter_storage, check_every)
     r = _lib.CgResult()
     _check(_load().hbdia_cg_solve(matrix.handle, ctypes.c_void_p(b_ptr), ctypes.c_void_p(x_ptr), ctypes.byref(o),
                                   _stream_arg(stream), ctypes.byref(r)))
@@ -717,7 +716,7 @@ class Server:
     served with continuous batching (each matrix's pending requests become one
     SpMM whenever the matrix is free), CG requests on a pool of solver threads.  ``options`` overrides
     fields of hbdia_server_default_options (memoryBudget, batching, maxRhs,
-    spmvStorage, cgIterStorage, cgWorkers, cgTol, cgUpdateFactor, cgL2Persist, maxInFlight, ...)."""
+    spmvStorage, cgIterStorage, cgWorkers, cgTol, cgUpdateFactor, cgMaxGroup, maxInFlight, ...)."""
 
     def __init__(self, **options):
         o = _lib.ServerOptions()

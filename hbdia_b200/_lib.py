@@ -53,7 +53,7 @@ class TuneResult(ctypes.Structure):
 
 class CgOptions(ctypes.Structure):
     _fields_ = [("tol", c_dbl), ("updateFactor", c_dbl), ("maxUpdates", c_i32), ("maxIterations", c_i32),
-                ("iterStorage", c_i32), ("checkEvery", c_i32), ("l2Persist", c_i32)]
+                ("iterStorage", c_i32), ("checkEvery", c_i32)]
 
 
 class CgResult(ctypes.Structure):
@@ -69,7 +69,7 @@ class BatchConfig(ctypes.Structure):
 class ServerOptions(ctypes.Structure):
     _fields_ = [("memoryBudget", c_i64), ("batching", c_i32), ("maxRhs", c_i32), ("spmvStorage", c_i32),
                 ("cgIterStorage", c_i32), ("cgWorkers", c_i32), ("cgMaxUpdates", c_i32), ("cgMaxIterations", c_i32),
-                ("cgCheckEvery", c_i32), ("cgTol", c_dbl), ("cgUpdateFactor", c_dbl), ("cgL2Persist", c_i32),
+                ("cgCheckEvery", c_i32), ("cgTol", c_dbl), ("cgUpdateFactor", c_dbl),
                 ("maxInFlight", c_i32), ("cgMaxGroup", c_i32)]
 
 

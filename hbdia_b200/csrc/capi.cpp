@@ -902,7 +902,6 @@ int hbdia_cg_solve(hbdia_matrix *m, const double *b, double *x, const hbdia_cg_o
         prm.maxUpdates = opt->maxUpdates;
         prm.maxIterations = opt->maxIterations;
         prm.checkEvery = opt->checkEvery;
-        prm.l2Persist = opt->l2Persist != 0;
         hbdia::CgStats st;
         hbdia::cg_solve(m->plan, *it, m->cg, b, x, prm, stream, &st);
         hbdia_cg_result r;

@@ -37,15 +37,9 @@
 // leaves the group when done, so its result equals what it gives alone, bit
 // for bit; a lone solve is a group of one.
 //
-// L2 residency (option, lone solves): the solver's vectors r, p, q live in one range that
-// is marked persisting in L2 (a stream access-policy window) while the solve
-// runs, so the value stream of the SpMV does not evict them; each iteration
-// then draws mostly the matrix values from HBM.
-
 #include <cuda_runtime.h>
 
 #include <algorithm>
-#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -193,31 +187,12 @@ double host_sum(const double *dpart, int nparts, cudaStream_t s, double *pinned)
     return t;
 }
 
-// Bytes of L2 this process may keep persisting (set once per device, to the
-// device's maximum; a per-context limit that ends with the process).
-size_t persisting_l2_bytes(int dev) {
-    static std::atomic<int64_t> cached[64];
-    static std::atomic<uint64_t> done{0};
-    if (dev < 0 || dev >= 64) return 0;
-    if (done.load() & (1ull << dev)) return static_cast<size_t>(cached[dev].load());
-    int maxPersist = 0;
-    size_t granted = 0;
-    if (cudaDeviceGetAttribute(&maxPersist, cudaDevAttrMaxPersistingL2CacheSize, dev) == cudaSuccess &&
-        maxPersist > 0 && cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, maxPersist) == cudaSuccess &&
-        cudaDeviceGetLimit(&granted, cudaLimitPersistingL2CacheSize) != cudaSuccess)
-        granted = 0;
-    cudaGetLastError();
-    cached[dev].store(static_cast<int64_t>(granted));
-    done.fetch_or(1ull << dev);
-    return granted;
-}
-
 }  // namespace
 
 struct CgWork {
     int64_t n = 0;
     int nparts = 0;
-    double *buf = nullptr;  // r, p, q (n each, contiguous: the L2 window) + 3 partial arrays + scalars
+    double *buf = nullptr;  // r, p, q (n each) + 3 partial arrays + scalars
     double *r, *p, *q, *pqPart, *rrPart, *nPart, *scal;
     double *host = nullptr;  // page-locked: nparts partial sums, then r.r
 };
@@ -292,7 +267,6 @@ void cg_solve_group(const DevicePlan &A64, const DevicePlan &Ait, CgCall *calls,
     cudaGraphExec_t exec = nullptr;
     cudaGraph_t graph = nullptr;
     std::vector<int> graphSet;  // the active solves the captured graph iterates
-    bool window = false;
     auto dropGraph = [&] {
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
@@ -300,16 +274,7 @@ void cg_solve_group(const DevicePlan &A64, const DevicePlan &Ait, CgCall *calls,
         graph = nullptr;
         graphSet.clear();
     };
-    auto cleanup = [&] {
-        dropGraph();
-        if (window) {  // the stream goes back to normal caching
-            cudaStreamAttrValue a;
-            std::memset(&a, 0, sizeof(a));
-            a.accessPolicyWindow.num_bytes = 0;
-            cudaStreamSetAttribute(s, cudaStreamAttributeAccessPolicyWindow, &a);
-            cudaGetLastError();
-        }
-    };
+    auto cleanup = [&] { dropGraph(); };
     // FP64 residual of solve j: r = b - A x, its norm on the host and r.r in
     // its scal[0]; with `start` also p = r
     auto true_residual = [&](int j, int start) {
@@ -322,27 +287,6 @@ void cg_solve_group(const DevicePlan &A64, const DevicePlan &Ait, CgCall *calls,
     };
     auto alive = [&](const State &st) { return st.rnorm > st.target && std::isfinite(st.rnorm) && st.iters < prm.maxIterations; };
     try {
-        if (prm.l2Persist && k == 1) {
-            int dev = 0;
-            check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
-            const size_t persist = persisting_l2_bytes(dev);
-            const size_t bytes = 3 * sizeof(double) * static_cast<size_t>(n);
-            int maxWindow = 0;
-            cudaDeviceGetAttribute(&maxWindow, cudaDevAttrMaxAccessPolicyWindowSize, dev);
-            cudaGetLastError();
-            if (persist > 0 && maxWindow > 0) {
-                cudaStreamAttrValue a;
-                std::memset(&a, 0, sizeof(a));
-                a.accessPolicyWindow.base_ptr = calls[0].w->r;
-                a.accessPolicyWindow.num_bytes = std::min(bytes, static_cast<size_t>(maxWindow));
-                a.accessPolicyWindow.hitRatio =
-                    static_cast<float>(std::min(1.0, double(persist) / double(a.accessPolicyWindow.num_bytes)));
-                a.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
-                a.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
-                window = cudaStreamSetAttribute(s, cudaStreamAttributeAccessPolicyWindow, &a) == cudaSuccess;
-                cudaGetLastError();
-            }
-        }
         for (int j = 0; j < k; ++j) {
             CgWork *w = calls[j].w;
             dot_partial<<<G, kThreads, 0, s>>>(calls[j].b, calls[j].b, n, w->nPart);

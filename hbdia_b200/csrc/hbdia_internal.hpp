@@ -201,7 +201,6 @@ struct CgParams {
     int32_t maxUpdates = 100;    // FP64 residual recomputations
     int32_t maxIterations = 20000;
     int32_t checkEvery = 10;     // iterations per CUDA-graph replay / host check
-    bool l2Persist = true;       // keep r, p, q persisting in L2 during the solve
 };
 struct CgStats {
     int32_t updates = 0, iterations = 0;

@@ -364,7 +364,6 @@ void cg_worker(Server *S) {
             prm.maxUpdates = o.cgMaxUpdates;
             prm.maxIterations = o.cgMaxIterations;
             prm.checkEvery = o.cgCheckEvery;
-            prm.l2Persist = o.cgL2Persist != 0;
             cg_solve_group(M.p64, M.cgIter(o.cgIterStorage), calls.data(), k, prm, st);
             for (size_t i = 0; i < grp.size(); ++i) {
                 Request *r = grp[i];
@@ -420,7 +419,6 @@ void server_default_options(hbdia_server_options *o) {
     o->cgMaxUpdates = 100;
     o->cgMaxIterations = 20000;
     o->cgCheckEvery = 10;
-    o->cgL2Persist = 1;
     o->cgMaxGroup = 8;
     o->maxInFlight = 1;
 }

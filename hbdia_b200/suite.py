@@ -192,16 +192,13 @@ def cg(args):
     bt = torch.from_numpy(b).cuda()
     m = hb.HBDIA(rows, cols, vals, n, n)
     m.convertToHBDIAFormat(32, 2)
-    for name, st, persist in (("mixed: fp32-storage iterations, fp64 reliable updates, L2-resident vectors",
-                                hb.STORE_F32, True),
-                               ("mixed without the L2 window", hb.STORE_F32, False),
-                               ("fp64 iterations, L2-resident vectors", hb.STORE_NATIVE, True),
-                               ("plain fp64 CG", hb.STORE_NATIVE, False)):
+    for name, st in (("mixed: fp32-storage iterations, fp64 reliable updates", hb.STORE_F32),
+                     ("plain fp64 CG", hb.STORE_NATIVE)):
         xt = torch.zeros(n, dtype=torch.float64, device="cuda")
-        hb.cg_solve(m, bt.data_ptr(), xt.data_ptr(), tol=1e-10, iter_storage=st, l2_persist=persist)  # warm
+        hb.cg_solve(m, bt.data_ptr(), xt.data_ptr(), tol=1e-10, iter_storage=st)  # warm
         xt.zero_()
         torch.cuda.synchronize()
-        r = hb.cg_solve(m, bt.data_ptr(), xt.data_ptr(), tol=1e-10, iter_storage=st, l2_persist=persist)
+        r = hb.cg_solve(m, bt.data_ptr(), xt.data_ptr(), tol=1e-10, iter_storage=st)
         x = xt.cpu().numpy()
         ax = np.zeros(n)
         np.add.at(ax, rows, vals * x[cols])
@@ -380,7 +377,8 @@ def served_comparison(requests=10000, capacity_requests=3000, load=0.7, cg_fract
     memory.  Two servers:
       * served: continuous batching of SpMVs into SpMMs, FP32-stored values
         (FP64 accumulation), CG iterating on the FP32 values with FP64
-        reliable updates and L2-resident vectors, 4 concurrent solvers;
+        reliable updates, pending CG requests on one matrix solved as one
+        lockstep group (one SpMM per iteration), 4 concurrent solvers;
       * plain: FP64 values, one request per launch, FP64 CG, one solver.
     Each server's capacity is its closed-loop rate (capacity_requests queued,
     then released); then each takes `requests` Poisson arrivals at `load` x
@@ -400,7 +398,7 @@ def served_comparison(requests=10000, capacity_requests=3000, load=0.7, cg_fract
     servers = {
         "served": hb.Server(),
         "plain": hb.Server(batching=0, spmvStorage=hb.STORE_NATIVE, cgIterStorage=hb.STORE_NATIVE,
-                           cgL2Persist=0, cgWorkers=1, cgMaxGroup=1),
+                           cgWorkers=1, cgMaxGroup=1),
     }
     ids = {k: [s.add_matrix(m) for m in mats] for k, s in servers.items()}
     del mats
@@ -418,8 +416,10 @@ def served_comparison(requests=10000, capacity_requests=3000, load=0.7, cg_fract
         w_k = np.array([hb.REQ_SPMV] * len(ns) + [hb.REQ_CG] * min(4, len(ns)))
         w_m = np.concatenate([np.arange(len(ns)), np.arange(min(4, len(ns)))])
         _serve_run(hb, srv, ids[name], ns, w_k, w_m, xbuf, ybuf, None, 0)  # warm-up
+        c0 = srv.stats()
         wall, _, _, _ = _serve_run(hb, srv, ids[name], ns, kinds[:capacity_requests], mids[:capacity_requests],
                                    xbuf, ybuf, None, 0)
+        c1 = srv.stats()
         cap = capacity_requests / wall
         wall_s, _, wid_s, _ = _serve_run(hb, srv, ids[name], ns, spmv_only, mids[:capacity_requests], xbuf, ybuf,
                                          None, 0)
@@ -433,6 +433,7 @@ def served_comparison(requests=10000, capacity_requests=3000, load=0.7, cg_fract
                          spmv_only_capacity_req_s=capacity_requests / wall_s,
                          spmv_only_mean_batch=float(wid_s.mean()), max_submit_lag_ms=1e3 * lag,
                          mean_cg_group=(g1.cgRequests - g0.cgRequests) / max(1, g1.cgGroups - g0.cgGroups),
+                         capacity_mean_cg_group=(c1.cgRequests - c0.cgRequests) / max(1, c1.cgGroups - c0.cgGroups),
                          device_bytes=int(srv.stats().deviceBytes))
         if log:
             log(f"[serve] {name}: capacity {cap:.1f} req/s, {thr:.1f} req/s at {rate:.1f} offered, "
@@ -502,7 +503,7 @@ def serve(args):
     servers = {
         "batched": hb.Server(),
         "plain": hb.Server(batching=0, spmvStorage=hb.STORE_NATIVE, cgIterStorage=hb.STORE_NATIVE,
-                           cgL2Persist=0, cgWorkers=1, cgMaxGroup=1),
+                           cgWorkers=1, cgMaxGroup=1),
     }
     if args.serial_too:
         servers["batched, 2 batches in flight"] = hb.Server(maxInFlight=2)

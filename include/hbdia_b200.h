@@ -482,10 +482,8 @@ int hbdia_matrix_test_skip_tile(hbdia_matrix *m, int32_t tile);
  * residual has fallen below updateFactor times the largest one since the last
  * update, and before convergence is declared, r is recomputed as b - A x with
  * the FP64 values while the search direction is kept, so the iterations do
- * not restart.  Convergence is judged on that FP64 residual.  With l2Persist
- * the solver's vectors are kept persisting in L2 during the solve (this sets
- * the process's persisting-L2 limit of the device to its maximum on first
- * use).  x holds the initial guess on entry and the solution on return
+ * not restart.  Convergence is judged on that FP64 residual.  x holds the
+ * initial guess on entry and the solution on return
  * (device buffers of numRows doubles).  Synchronous. */
 typedef struct hbdia_cg_options {
     double tol;            /* target ||b - A x|| / ||b|| (FP64), e.g. 1e-10              */
@@ -494,7 +492,6 @@ typedef struct hbdia_cg_options {
     int32_t maxIterations; /* iterations in all                                          */
     int32_t iterStorage;   /* hbdia_value_storage of the iterations' operator            */
     int32_t checkEvery;    /* iterations per CUDA-graph replay / host check              */
-    int32_t l2Persist;     /* keep the solver's vectors persisting in L2 (0 / 1)         */
 } hbdia_cg_options;
 
 typedef struct hbdia_cg_result {
@@ -612,7 +609,6 @@ typedef struct hbdia_server_options {
     int32_t cgCheckEvery;   /* iterations per graph replay (default 10)                     */
     double cgTol;           /* target ||b - A y|| / ||b|| (default 1e-10)                   */
     double cgUpdateFactor;  /* reliable-update trigger (default 0.1)                        */
-    int32_t cgL2Persist;    /* CG vectors persisting in L2 during a solve (default 1)       */
     int32_t maxInFlight;    /* SpMV batches of one matrix issued and not yet completed,     */
                             /* 1-8 (default 1: the next batch forms while one runs)         */
     int32_t cgMaxGroup;     /* pending CG requests on one matrix solved as one lockstep     */

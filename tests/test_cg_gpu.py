@@ -2,8 +2,7 @@
 dots and updates; FP64 residual recomputations) reach the FP64 residual
 target; the final residual is recomputed independently on the host from the
 COO triplets.  Plain FP64 CG (iteration storage FP64) is the comparison point:
-the mixed form needs about as many iterations.  Runs are bit-reproducible,
-with or without the L2 residency window."""
+the mixed form needs about as many iterations.  Runs are bit-reproducible."""
 import numpy as np
 import pytest
 
@@ -42,12 +41,11 @@ def test_cg_reaches_fp64_tolerance(lib, spd, inner):
     assert r.converged == 1 and r.relResidual <= 1e-10
     assert _host_residual(rows, cols, vals, xt.cpu().numpy(), b) <= 2e-10
     assert r.updates >= 1  # convergence is only declared on a recomputed FP64 residual
-    # bit-reproducible, and the L2 window changes no arithmetic
-    for persist in (True, False):
-        x2 = torch.zeros(n, dtype=torch.float64, device="cuda")
-        r2 = lib.cg_solve(m, bt.data_ptr(), x2.data_ptr(), tol=1e-10, iter_storage=st, l2_persist=persist)
-        assert r2.iterations == r.iterations and r2.updates == r.updates
-        assert bits_equal(x2.cpu().numpy(), xt.cpu().numpy())
+    # bit-reproducible
+    x2 = torch.zeros(n, dtype=torch.float64, device="cuda")
+    r2 = lib.cg_solve(m, bt.data_ptr(), x2.data_ptr(), tol=1e-10, iter_storage=st)
+    assert r2.iterations == r.iterations and r2.updates == r.updates
+    assert bits_equal(x2.cpu().numpy(), xt.cpu().numpy())
 
 
 def test_cg_64cube_mixed_close_to_plain_iterations(lib):

@@ -199,14 +199,19 @@ def test_admission_budget(lib, mats):
         lib.Server(memoryBudget=1 << 16).add_matrix(m0)  # the 1000-row matrix needs about 1 MB
     big = lib.Server()
     big.add_matrix(m0)
-    need = big.stats().deviceBytes
+    need1 = big.stats().deviceBytes  # plans, staging and the CG workspaces' share
+    big.add_matrix(m0)
+    need2 = big.stats().deviceBytes  # a second copy adds no CG workspace growth
     big.close()
-    srv = lib.Server(memoryBudget=int(need * 2.2))  # two copies fit (the CG workspace share counts once), not three
+    per = need2 - need1
+    assert 0 < per < need1
+    budget = need2 + per // 2  # two copies fit, not three
+    srv = lib.Server(memoryBudget=budget)
     srv.add_matrix(m0)
     srv.add_matrix(m0)
     with pytest.raises(MemoryError):
         srv.add_matrix(m0)
-    assert srv.stats().deviceBytes <= int(need * 2.2)
+    assert srv.stats().deviceBytes <= budget
     srv.close()
 
 
