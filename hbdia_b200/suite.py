@@ -8,6 +8,8 @@
     python -m hbdia_b200.suite serve       # 32 resident matrices, Poisson arrivals: batched server vs plain FP64
     python -m hbdia_b200.suite convert --grid 256   # host vs GPU converter, COO -> device layout
     python -m hbdia_b200.suite partition   # 256^3 cut into 2/4/8 row partitions: per-rank SpMV and halo
+    python -m hbdia_b200.suite spmv --grid 128 --storage 1 --kernel pipe   # one kernel on the
+                                           # headline workload's shape (what the profiles capture)
 
 Each measurement prints one JSON line.  Times are CUDA-event device times on
 a dedicated stream after warm-up; inputs exceed L2 unless stated.  Accuracy
@@ -634,9 +636,38 @@ def convert(args):
         del m
 
 
+def spmv(args):
+    """The headline workload's shape at --grid (27-point stencil, centre 26,
+    neighbours -1, 1 % extras U(0.1, 1) seed 1, blockWidth 32, threshold 2,
+    x ~ U(-1, 1) seed 1) with --storage value storage and --kernel: --reps
+    SpMVs after 3 warm-up ones, each timed with CUDA events.  The profiles
+    capture its launches."""
+    import torch
+    import hbdia_b200 as hb
+    g = args.grid
+    n = g ** 3
+    rows, cols, vals = hb.generate_stencil27(g, g, g, 26.0, -1.0, 0.01, 0.1, 1.0, 1)
+    m = hb.HBDIA(rows, cols, vals, n, n)
+    m.convertToHBDIAFormat(32, 2, upload=False)
+    m.prepareForGPU(args.storage)
+    kern = {"auto": hb.KERNEL_AUTO, "pipe": hb.KERNEL_PIPE, "quad": hb.KERNEL_QUAD, "staged": hb.KERNEL_STAGED,
+            "warp": hb.KERNEL_WARP, "rowwise": hb.KERNEL_ROWWISE}[args.kernel]
+    m.setKernel(kern)
+    x = torch.from_numpy(hb.fill_uniform(n, -1.0, 1.0, 1)).cuda()
+    y = torch.zeros(n, dtype=torch.float64, device="cuda")
+    stream = torch.cuda.Stream()
+    ms = _time(lambda: hb.spmv_device(m, x.data_ptr(), y.data_ptr(), stream.cuda_stream), stream, reps=args.reps)
+    m.synchronize()
+    b = m.bytesPerSpmv()
+    print(json.dumps({"suite": "spmv", "workload": f"27-point stencil {g}^3 + 1% extras", "storage": args.storage,
+                      "kernel": args.kernel, "selected": m.selectedKernel(x.data_ptr()), "ms": ms, "bytes": b,
+                      "gbs": b / (ms / 1e3) / 1e9, "frac_of_peak": b / (ms / 1e3) / 1e9 / _peak()}), flush=True)
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("what", choices=["precision", "spmm", "cg", "batched", "serve", "convert", "small", "partition"])
+    ap.add_argument("what", choices=["precision", "spmm", "cg", "batched", "serve", "convert", "small", "partition",
+                                     "spmv"])
     ap.add_argument("--requests", type=int, default=10000)
     ap.add_argument("--matrices", type=int, default=32)
     ap.add_argument("--edge-min", type=int, default=32)
@@ -649,11 +680,13 @@ def main(argv=None):
     ap.add_argument("--n", type=int, default=8 * 1024 * 1024)
     ap.add_argument("--grid", type=int, default=128)
     ap.add_argument("--device", action="store_true", help="serve: request vectors in device memory")
+    ap.add_argument("--kernel", default="auto", choices=["auto", "pipe", "quad", "staged", "warp", "rowwise"])
+    ap.add_argument("--reps", type=int, default=20)
     args = ap.parse_args(argv)
     import torch
     torch.cuda.set_device(0)
     {"precision": precision, "spmm": spmm, "cg": cg, "batched": batched, "serve": serve,
-     "convert": convert, "small": small, "partition": partition}[args.what](args)
+     "convert": convert, "small": small, "partition": partition, "spmv": spmv}[args.what](args)
     return 0
 
 
