@@ -478,8 +478,7 @@ template <typename VT, typename XT, int KT, bool CM>
 void launch_spmm_kt(const DevicePlan &P, const dev::SpmvArgs<VT, XT> &a, const XT *X, int64_t ldx, XT *Y,
                     int64_t ldy, int32_t k, cudaStream_t s) {
     if (P.bw == 32) {
-        constexpr int W = dev::kSpmmWarps;
-        const unsigned grid = static_cast<unsigned>((static_cast<int64_t>(P.numTiles) + W - 1) / W);
+        const unsigned grid = static_cast<unsigned>((static_cast<int64_t>(P.numTiles) + 7) / 8);
         // The full passes in one launch, a partial last pass (k not a multiple
         // of KT) in a second one on the remaining columns; 32-bit gather
         // indices when every pass's block has fewer than 2^31 elements.
@@ -489,11 +488,11 @@ void launch_spmm_kt(const DevicePlan &P, const dev::SpmvArgs<VT, XT> &a, const X
         const XT *Xr = CM ? X + static_cast<int64_t>(kfull) * ldx : X + kfull;
         XT *Yr = CM ? Y + static_cast<int64_t>(kfull) * ldy : Y + kfull;
         if (i32) {
-            if (kfull) dev::spmm_bw32<VT, XT, KT, CM, int32_t, true><<<grid, W * 32, 0, s>>>(a, X, ldx, Y, ldy, kfull);
-            if (krest) dev::spmm_bw32<VT, XT, KT, CM, int32_t, false><<<grid, W * 32, 0, s>>>(a, Xr, ldx, Yr, ldy, krest);
+            if (kfull) dev::spmm_bw32<VT, XT, KT, CM, int32_t, true><<<grid, 256, 0, s>>>(a, X, ldx, Y, ldy, kfull);
+            if (krest) dev::spmm_bw32<VT, XT, KT, CM, int32_t, false><<<grid, 256, 0, s>>>(a, Xr, ldx, Yr, ldy, krest);
         } else {
-            if (kfull) dev::spmm_bw32<VT, XT, KT, CM, int64_t, true><<<grid, W * 32, 0, s>>>(a, X, ldx, Y, ldy, kfull);
-            if (krest) dev::spmm_bw32<VT, XT, KT, CM, int64_t, false><<<grid, W * 32, 0, s>>>(a, Xr, ldx, Yr, ldy, krest);
+            if (kfull) dev::spmm_bw32<VT, XT, KT, CM, int64_t, true><<<grid, 256, 0, s>>>(a, X, ldx, Y, ldy, kfull);
+            if (krest) dev::spmm_bw32<VT, XT, KT, CM, int64_t, false><<<grid, 256, 0, s>>>(a, Xr, ldx, Yr, ldy, krest);
         }
     } else {
         const unsigned grid = static_cast<unsigned>((static_cast<int64_t>(P.n) + 255) / 256);
@@ -558,8 +557,7 @@ template <typename VT, typename XT, int KT>
 void launch_list_kt(const DevicePlan &P, const dev::SpmvArgs<VT, XT> &a, const void *const *x, void *const *y,
                     int32_t k, cudaStream_t s) {
     // full passes in one launch, a partial last pass in a second
-    constexpr int W = dev::kSpmmWarps;
-    const unsigned grid = static_cast<unsigned>((static_cast<int64_t>(P.numTiles) + W - 1) / W);
+    const unsigned grid = static_cast<unsigned>((static_cast<int64_t>(P.numTiles) + 7) / 8);
     const int32_t kfull = k - k % KT, krest = k % KT;
     auto fill = [&](int32_t j0, int32_t cnt) {
         dev::VecList<XT> L{};
@@ -569,8 +567,8 @@ void launch_list_kt(const DevicePlan &P, const dev::SpmvArgs<VT, XT> &a, const v
         }
         return L;
     };
-    if (kfull) dev::spmm_bw32_list<VT, XT, KT, true><<<grid, W * 32, 0, s>>>(a, fill(0, kfull), kfull);
-    if (krest) dev::spmm_bw32_list<VT, XT, KT, false><<<grid, W * 32, 0, s>>>(a, fill(kfull, krest), krest);
+    if (kfull) dev::spmm_bw32_list<VT, XT, KT, true><<<grid, 256, 0, s>>>(a, fill(0, kfull), kfull);
+    if (krest) dev::spmm_bw32_list<VT, XT, KT, false><<<grid, 256, 0, s>>>(a, fill(kfull, krest), krest);
 }
 
 template <typename VT, typename XT>

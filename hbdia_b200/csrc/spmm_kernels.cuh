@@ -8,11 +8,8 @@
 // entries, one final add), so it equals hbdia_spmv(A, X[:, j]) bit for bit.
 //
 // Each stored value is fetched from HBM once and used for every right-hand
-// side: the RHS are processed in passes of KT columns inside the warp that
-// owns the row block, and the standalone SpMM kernels first copy the block's
-// value rows (up to 32 offsets x 32 values) into the warp's own shared-memory
-// slice with cp.async -- no registers held while they are in flight -- so
-// every pass reads them from there instead of going back to L1 / L2 / HBM.
+// side: the RHS are processed in tiles of KT columns inside the warp that owns
+// the row block, and the block's values (a few KB) stay in L1 between tiles.
 #pragma once
 
 #include "spmv_kernels.cuh"
@@ -93,7 +90,7 @@ __device__ __forceinline__ void spmm_group(const SpmvArgs<VT, XT> &a, const XS &
     for (int u = 0; u < U; ++u) {
         const int64_t col = row + __shfl_sync(kFull, myoff, j + u);
         ok[u] = static_cast<uint64_t>(col) < static_cast<uint64_t>(a.xn);
-        v[u] = vp[(j + u) * 32];  // global memory or the warp's shared-memory copy
+        v[u] = __ldg(vp + (j + u) * 32);
         xs.load(ok[u] ? static_cast<IT>(col) : IT(0), kc, xv[u]);
     }
 #pragma unroll
@@ -109,46 +106,20 @@ __device__ __forceinline__ void spmm_group(const SpmvArgs<VT, XT> &a, const XS &
 // The offsets of one row block for one pass, in groups of U = 16 / KT (at
 // least 1), so about 16 x gathers per lane are in flight (32 measured slower
 // on B200 at every tile width).
-// sv: the block's value rows staged in shared memory (k1 - k0 <= 32), or
-// nullptr (read from global memory).
 template <typename VT, typename XT, int KT, typename IT, bool FULL, typename XS>
 __device__ __forceinline__ void spmm_pass(const SpmvArgs<VT, XT> &a, const XS &xs, int32_t k0, int32_t k1,
-                                          int64_t row, int lane, int kc, float s, const VT *sv, XT (&acc)[KT]) {
+                                          int64_t row, int lane, int kc, float s, XT (&acc)[KT]) {
     constexpr int U = KT >= 16 ? 1 : 16 / KT;
     for (int32_t kb = k0; kb < k1; kb += 32) {
         const int cnt = min(32, k1 - kb);
         const int32_t myoff = lane < cnt ? __ldg(a.offs + kb + lane) : 0;
-        const VT *vp = sv ? sv + static_cast<int64_t>(kb - k0) * 32 + lane : a.vals + static_cast<int64_t>(kb) * 32 + lane;
+        const VT *vp = a.vals + static_cast<int64_t>(kb) * 32 + lane;
         int j = 0;
         for (; j + U <= cnt; j += U)
             spmm_group<VT, XT, KT, U, IT, FULL>(a, xs, vp, myoff, j, row, kc, s, acc);
         for (; j < cnt; ++j)  // warp-uniform tail
             spmm_group<VT, XT, KT, 1, IT, FULL>(a, xs, vp, myoff, j, row, kc, s, acc);
     }
-}
-
-// Copies the value rows of offsets [k0, k1) of a block (k1 - k0 <= 32) into
-// the warp's shared-memory slice with cp.async (4- or 8-byte granules; every
-// row is 32 values, 64-byte aligned), then waits for them.
-template <typename VT>
-__device__ __forceinline__ const VT *stage_block_values(const VT *__restrict__ vals, int32_t k0, int32_t K,
-                                                        VT *slice, int lane) {
-    constexpr int G = sizeof(VT) >= 8 ? 8 : 4;                 // bytes per granule
-    constexpr int perRow = 32 * static_cast<int>(sizeof(VT)) / G;  // granules per value row (32, 32 or 16)
-    const char *src = reinterpret_cast<const char *>(vals + static_cast<int64_t>(k0) * 32);
-    char *dst = reinterpret_cast<char *>(slice);
-    const uint32_t d0 = static_cast<uint32_t>(__cvta_generic_to_shared(dst));
-    if (lane < perRow) {
-        for (int32_t k = 0; k < K; ++k) {
-            const int64_t o = static_cast<int64_t>(k) * 32 * static_cast<int64_t>(sizeof(VT)) + lane * G;
-            asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(d0 + static_cast<uint32_t>(o)),
-                         "l"(src + o), "n"(G)
-                         : "memory");
-        }
-    }
-    asm volatile("cp.async.wait_all;" ::: "memory");
-    __syncwarp();
-    return slice;
 }
 
 // The COO remainder of one 32-row tile for one pass of the vector-list form,
@@ -196,7 +167,7 @@ __device__ __forceinline__ void spmm_coo(const int32_t *cooRow, const int32_t *c
 template <typename VT, typename XT, int KT, bool CM, typename IT, bool FULL>
 __device__ __forceinline__ void bw32_spmm_tile_t(const SpmvArgs<VT, XT> &a, const XT *__restrict__ X, int64_t ldx,
                                                  XT *__restrict__ Y, int64_t ldy, int32_t k, int32_t tile,
-                                                 int lane, VT *slice = nullptr) {
+                                                 int lane) {
     const int64_t row0 = static_cast<int64_t>(tile) * 32;
     const int64_t row = row0 + lane;
     int32_t k0 = 0, k1 = 0;
@@ -208,9 +179,6 @@ __device__ __forceinline__ void bw32_spmm_tile_t(const SpmvArgs<VT, XT> &a, cons
     const int32_t c1 = a.hasCoo ? __ldg(a.cooTile + tile + 1) : 0;
     const float s = (a.scale && tile < a.numBlocks) ? __ldg(a.scale + tile) : 1.0f;
     const bool xAligned = !CM && (reinterpret_cast<uintptr_t>(X) & 15) == 0 && (ldx & 1) == 0;
-    // more than one pass: the block's values once into shared memory
-    const VT *sv = slice && k > KT && k1 > k0 && k1 - k0 <= 32 ? stage_block_values(a.vals, k0, k1 - k0, slice, lane)
-                                                               : nullptr;
     for (int32_t r0 = 0; r0 < k; r0 += KT) {
         const int kc = min(KT, k - r0);
         const XBlock<XT, KT, CM, IT, FULL> xs{CM ? X + static_cast<int64_t>(r0) * ldx : X + r0,
@@ -218,7 +186,7 @@ __device__ __forceinline__ void bw32_spmm_tile_t(const SpmvArgs<VT, XT> &a, cons
         XT acc[KT];
 #pragma unroll
         for (int q = 0; q < KT; ++q) acc[q] = XT(0);
-        spmm_pass<VT, XT, KT, IT, FULL>(a, xs, k0, k1, row, lane, kc, s, sv, acc);
+        spmm_pass<VT, XT, KT, IT, FULL>(a, xs, k0, k1, row, lane, kc, s, acc);
         if (a.hasCoo) {
             // per column: the row's COO entries in list order, then one add;
             // each batch of 32 entries is loaded once for all columns
@@ -274,7 +242,7 @@ struct VecList {
 // offsets: each vector has fewer than 2^31 elements).
 template <typename VT, typename XT, int KT, bool FULL>
 __device__ __forceinline__ void bw32_spmm_list_tile(const SpmvArgs<VT, XT> &a, const VecList<XT> &L, int32_t k,
-                                                    int32_t tile, int lane, VT *slice) {
+                                                    int32_t tile, int lane) {
     const int64_t row0 = static_cast<int64_t>(tile) * 32;
     const int64_t row = row0 + lane;
     int32_t k0 = 0, k1 = 0;
@@ -285,8 +253,6 @@ __device__ __forceinline__ void bw32_spmm_list_tile(const SpmvArgs<VT, XT> &a, c
     const int32_t c0 = a.hasCoo ? __ldg(a.cooTile + tile) : 0;
     const int32_t c1 = a.hasCoo ? __ldg(a.cooTile + tile + 1) : 0;
     const float s = (a.scale && tile < a.numBlocks) ? __ldg(a.scale + tile) : 1.0f;
-    // more than one pass: the block's values once into shared memory
-    const VT *sv = k > KT && k1 > k0 && k1 - k0 <= 32 ? stage_block_values(a.vals, k0, k1 - k0, slice, lane) : nullptr;
     for (int32_t r0 = 0; r0 < k; r0 += KT) {
         const int kc = min(KT, k - r0);
         XList<XT, KT, FULL> xs;
@@ -295,7 +261,7 @@ __device__ __forceinline__ void bw32_spmm_list_tile(const SpmvArgs<VT, XT> &a, c
         XT acc[KT];
 #pragma unroll
         for (int q = 0; q < KT; ++q) acc[q] = XT(0);
-        spmm_pass<VT, XT, KT, int32_t, FULL>(a, xs, k0, k1, row, lane, kc, s, sv, acc);
+        spmm_pass<VT, XT, KT, int32_t, FULL>(a, xs, k0, k1, row, lane, kc, s, acc);
         if (a.hasCoo)
             spmm_coo<XT, KT>(a.cooRow, a.cooCol, a.cooVal, c0, c1, row0, lane, kc,
                              [&](int64_t cc, int q) { return __ldg(xs.p[q] + cc); }, acc);
@@ -315,29 +281,23 @@ __device__ __forceinline__ void bw32_spmm_tile(const SpmvArgs<VT, XT> &a, const 
     bw32_spmm_tile_t<VT, XT, KT, CM, int64_t, false>(a, X, ldx, Y, ldy, k, tile, lane);
 }
 
-// Standalone SpMM kernels: kSpmmWarps warps per CTA, one 32-row block per
-// warp, each warp with a shared-memory slice for its block's value rows.
-constexpr int kSpmmWarps = 4;
-
 template <typename VT, typename XT, int KT, bool CM, typename IT, bool FULL>
-__global__ void __launch_bounds__(kSpmmWarps * 32)
+__global__ void __launch_bounds__(256)
 spmm_bw32(const SpmvArgs<VT, XT> a, const XT *__restrict__ X, int64_t ldx, XT *__restrict__ Y, int64_t ldy,
           int32_t k) {
-    __shared__ __align__(16) VT slices[kSpmmWarps][32 * 32];
     const int lane = threadIdx.x & 31;
     const int32_t tile = static_cast<int32_t>((static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5);
     if (tile >= a.numTiles) return;  // warp-uniform
-    bw32_spmm_tile_t<VT, XT, KT, CM, IT, FULL>(a, X, ldx, Y, ldy, k, tile, lane, slices[threadIdx.x >> 5]);
+    bw32_spmm_tile_t<VT, XT, KT, CM, IT, FULL>(a, X, ldx, Y, ldy, k, tile, lane);
 }
 
 template <typename VT, typename XT, int KT, bool FULL>
-__global__ void __launch_bounds__(kSpmmWarps * 32)
+__global__ void __launch_bounds__(256)
 spmm_bw32_list(const SpmvArgs<VT, XT> a, const __grid_constant__ VecList<XT> L, int32_t k) {
-    __shared__ __align__(16) VT slices[kSpmmWarps][32 * 32];
     const int lane = threadIdx.x & 31;
     const int32_t tile = static_cast<int32_t>((static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5);
     if (tile >= a.numTiles) return;  // warp-uniform
-    bw32_spmm_list_tile<VT, XT, KT, FULL>(a, L, k, tile, lane, slices[threadIdx.x >> 5]);
+    bw32_spmm_list_tile<VT, XT, KT, FULL>(a, L, k, tile, lane);
 }
 
 // Any block width: one thread per row (the reference's mapping).

@@ -370,7 +370,7 @@ def serve_workload(hb, matrices=32, edge_min=32, edge_max=160, seed=5):
 
 
 def served_comparison(requests=10000, capacity_requests=3000, load=0.7, cg_fraction=0.2, matrices=32,
-                      edge_min=32, edge_max=160, log=None):
+                      edge_min=32, edge_max=160, log=None, served_options=None):
     """Config 5 measured as one comparison, for the benchmark line.
 
     Workload: serve_workload's 32 resident matrices (150 GB admission cap);
@@ -398,7 +398,7 @@ def served_comparison(requests=10000, capacity_requests=3000, load=0.7, cg_fract
     xbuf = [[torch.from_numpy(rng.uniform(-1, 1, n)).cuda() for _ in range(2)] for n in ns]
     ybuf = [[torch.zeros(n, dtype=torch.float64, device="cuda") for _ in range(40)] for n in ns]
     servers = {
-        "served": hb.Server(),
+        "served": hb.Server(**(served_options or {})),
         "plain": hb.Server(batching=0, spmvStorage=hb.STORE_NATIVE, cgIterStorage=hb.STORE_NATIVE,
                            cgWorkers=1, cgMaxGroup=1),
     }
