@@ -419,7 +419,7 @@ void server_default_options(hbdia_server_options *o) {
     o->cgMaxUpdates = 100;
     o->cgMaxIterations = 20000;
     o->cgCheckEvery = 10;
-    o->cgMaxGroup = 8;
+    o->cgMaxGroup = 1;
     o->maxInFlight = 1;
 }
 

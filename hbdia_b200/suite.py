@@ -379,8 +379,8 @@ def served_comparison(requests=10000, capacity_requests=3000, load=0.7, cg_fract
     memory.  Two servers:
       * served: continuous batching of SpMVs into SpMMs, FP32-stored values
         (FP64 accumulation), CG iterating on the FP32 values with FP64
-        reliable updates, pending CG requests on one matrix solved as one
-        lockstep group (one SpMM per iteration), 4 concurrent solvers;
+        reliable updates, 4 concurrent solves (served_options override the
+        server's defaults, e.g. cgMaxGroup for lockstep CG groups);
       * plain: FP64 values, one request per launch, FP64 CG, one solver.
     Each server's capacity is its closed-loop rate (capacity_requests queued,
     then released); then each takes `requests` Poisson arrivals at `load` x
@@ -409,9 +409,9 @@ def served_comparison(requests=10000, capacity_requests=3000, load=0.7, cg_fract
     out = {"workload": f"{len(ns)} SPD 27-point stencils, edge U[{edge_min},{edge_max}] seed 5 "
                        f"(min {int(edges.min())}, max {int(edges.max())}), 0.5% symmetric extras, {int(sum(ns))} rows; "
                        f"{requests} Poisson requests, {cg_fraction:.0%} CG to 1e-10, device vectors",
-           "servers": {"served": "continuous batching: SpMV requests of a matrix as one SpMM, CG requests of a "
-                                 "matrix as one lockstep group (one SpMM per iteration); FP32-stored values with "
-                                 "FP64 accumulation, CG on the FP32 values with FP64 reliable updates; 4 solvers",
+           "servers": {"served": "continuous batching of the SpMV requests of a matrix into one SpMM; FP32-stored "
+                                 "values with FP64 accumulation; CG on the FP32 values with FP64 reliable "
+                                 "updates, 4 concurrent solves",
                        "plain": "FP64 values, one request per launch, FP64 CG, one solve at a time"}}
     spmv_only = np.full(capacity_requests, hb.REQ_SPMV)
     for name, srv in servers.items():

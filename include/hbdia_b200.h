@@ -584,11 +584,11 @@ int hbdia_batch_stream(const hbdia_batch *b, void **stream);
  *  - CG requests (solve A y = x, A symmetric positive definite) run on
  *    cgWorkers worker threads: CG with reliable updates (hbdia_cg_solve)
  *    iterating on the cgIterStorage values, converged to cgTol on the FP64
- *    residual.  A worker takes the oldest CG request together with the other
- *    pending CG requests on the same matrix (up to cgMaxGroup) and solves them
- *    in lockstep: one SpMM per iteration reads each stored value once for
- *    all of them, and each solve keeps its own schedule, so its result is the
- *    one it gives alone, bit for bit.
+ *    residual.  With cgMaxGroup > 1 a worker takes the oldest CG request
+ *    together with the other pending CG requests on the same matrix (up to
+ *    cgMaxGroup) and solves them in lockstep: one SpMM per iteration reads
+ *    each stored value once for all of them, and each solve keeps its own
+ *    schedule, so its result is the one it gives alone, bit for bit.
  * A request's result does not depend on the requests it is served with.
  * Admission: hbdia_server_add_matrix returns HBDIA_ERR_NO_MEMORY when the
  * matrix's plans, staging blocks and CG workspace growth would take the
@@ -612,7 +612,7 @@ typedef struct hbdia_server_options {
     int32_t maxInFlight;    /* SpMV batches of one matrix issued and not yet completed,     */
                             /* 1-8 (default 1: the next batch forms while one runs)         */
     int32_t cgMaxGroup;     /* pending CG requests on one matrix solved as one lockstep     */
-                            /* group, 1-16 (default 8; 1: one solve at a time)              */
+                            /* group, 1-16 (default 1: every solve on its own)              */
 } hbdia_server_options;
 
 typedef struct hbdia_request_info {

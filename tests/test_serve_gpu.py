@@ -116,7 +116,7 @@ def test_cg_group_equals_lone_solves(lib, mats):
     rng = np.random.default_rng(21)
     bs = [rng.uniform(-1, 1, n), np.zeros(n), np.cos(np.arange(n) * 0.001), rng.uniform(-1, 1, n) * 1e3,
           rng.uniform(0, 1, n)]
-    srv = lib.Server(cgWorkers=1)
+    srv = lib.Server(cgWorkers=1, cgMaxGroup=8)
     mid = srv.add_matrix(m)
     srv.pause(True)
     keep, pending = [], []
