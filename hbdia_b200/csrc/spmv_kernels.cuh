@@ -272,11 +272,44 @@ spmv_bw32_pipe(const SpmvArgs<VT, XT> a, const XT *__restrict__ x, XT *__restric
         const float s = a.scale && t < a.numBlocks ? __ldg(a.scale + t) : 1.0f;
         int32_t myoff = offNext;
         bool gathered = false;
+        // interior tile (at most 32 offsets, every column of every offset in
+        // [0, n)): full groups skip the column checks, x read at x + row +
+        // offset.  For 4- and 2-byte values only, where the instruction stream
+        // co-limits the kernel; the 8-byte instance is bandwidth-bound and the
+        // extra path would cost it registers (80 instead of 64: fewer warps).
+        const int32_t K = m.k1 - m.k0;
+        const bool interior = sizeof(VT) < 8 && K > 0 && K <= 32 && row0 + __shfl_sync(kFull, myoff, 0) >= 0 &&
+                              static_cast<int64_t>(row0) + 31 + __shfl_sync(kFull, myoff, K > 0 && K <= 32 ? K - 1 : 0) <
+                                  static_cast<int64_t>(a.xn);
+        const XT *xr = x + row;
+        (void)xr;
         for (int32_t kb = m.k0; kb < m.k1; kb += 32) {
             const int cnt = min(32, m.k1 - kb);
             if (kb != m.k0) myoff = lane < cnt ? __ldg(a.offs + kb + lane) : 0;
             const VT *vp = a.vals + static_cast<int64_t>(kb) * 32 + lane;
             int j = 0;
+            if constexpr (sizeof(VT) < 8) {
+                if (interior) {
+                    for (; j + U <= cnt; j += U) {
+                        VT v[U];
+                        XT xv[U];
+#pragma unroll
+                        for (int u = 0; u < U; ++u) {
+                            v[u] = ld_stream(vp + (j + u) * 32);
+                            xv[u] = __ldg(xr + __shfl_sync(kFull, myoff, j + u));
+                        }
+                        if (!gathered) {  // COO columns have arrived by now
+                            if (hasC) cx = __ldg(x + ccol);
+                            gathered = true;
+                        }
+#pragma unroll
+                        for (int u = 0; u < U; ++u) {
+                            const XT vv = widen<XT>(v[u], s);
+                            if (vv != XT(0)) sum = fma_rn(vv, xv[u], sum);
+                        }
+                    }
+                }
+            }
             for (; j + U <= cnt; j += U) {
                 VT v[U];
                 XT xv[U];
