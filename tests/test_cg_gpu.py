@@ -81,3 +81,28 @@ def test_cg_rejects_bad_input(lib, spd):
     t = torch.zeros(n, dtype=torch.float64, device="cuda")
     with pytest.raises(NotImplementedError):
         lib.cg_solve(m32, t.data_ptr(), t.data_ptr())
+
+
+def test_cg_config3b_128cube(lib):
+    """The CG configuration at its own size: the SPD 27-point stencil on 128^3,
+    b ~ U(-1, 1), FP32-stored iterations with FP64 reliable updates to a
+    relative residual of 1e-10, checked on the host from the COO triplets;
+    no more than 10 % more iterations than plain FP64 CG."""
+    import torch
+    g = 128
+    n = g ** 3
+    rows, cols, vals = lib.generate_stencil27_spd(g, g, g, 1e-3, 7)
+    b = lib.fill_uniform(n, -1.0, 1.0, 11)
+    m = lib.HBDIA(rows, cols, vals, n, n)
+    m.convertToHBDIAFormat(32, 2)
+    bt = torch.from_numpy(b).cuda()
+    its = {}
+    for name, st in (("f32", lib.STORE_F32), ("f64", lib.STORE_NATIVE)):
+        xt = torch.zeros(n, dtype=torch.float64, device="cuda")
+        r = lib.cg_solve(m, bt.data_ptr(), xt.data_ptr(), tol=1e-10, iter_storage=st)
+        assert r.converged == 1 and r.relResidual <= 1e-10
+        x = xt.cpu().numpy()
+        ax = np.bincount(rows, weights=vals * x[cols], minlength=n)
+        assert np.linalg.norm(b - ax) / np.linalg.norm(b) <= 2e-10
+        its[name] = r.iterations
+    assert its["f32"] <= 1.10 * its["f64"], its

@@ -9,7 +9,8 @@ arithmetic stay FP64.  Each result is checked two ways:
     FP32 storage <= 2^-24 (one rounding of each value), BF16 <= 2^-8.
 The workload is the banded matrix of the precision configuration (offsets
 0, +-1, +-2, +-64, +-4096; off-diagonals U(0.5, 1.5) dropped with p = 0.3;
-centre = row |sum| + 1; 0.2% scattered entries), at n = 2^18 here.
+centre = row |sum| + 1; 0.2% scattered entries), at n = 2^18 for every kernel
+and at the configuration's own n = 8M (2^23) for the default kernel.
 """
 import numpy as np
 import pytest
@@ -73,3 +74,30 @@ def test_storage_bytes_model(lib, banded):
     slots, blocks = sizes[lib.STORE_NATIVE][1], sizes[lib.STORE_NATIVE][2]
     assert sizes[lib.STORE_NATIVE][0] - sizes[lib.STORE_F32][0] == 4 * slots
     assert sizes[lib.STORE_NATIVE][0] - sizes[lib.STORE_BF16_SCALED][0] == 6 * slots - 4 * blocks
+
+
+def test_config3a_full_size(lib, orc):
+    """The precision configuration at its own size, n = 8M: the default
+    kernel with FP32 and BF16-scaled storage, bit-exact for the stored values
+    and within one rounding of them against the FP64 SpMV."""
+    n = 1 << 23
+    rows, cols, vals = lib.generate_banded(n, OFFSETS, 0.5, 1.5, 0.3, 0.002, 2)
+    x = lib.fill_uniform(n, -1.0, 1.0, 2)
+    om = orc.convert(rows, cols, vals, n, n, 32, 2)
+    L = om.layout()
+    y64 = om.spmv(x)
+    scale = np.maximum(np.bincount(rows, weights=np.abs(vals * x[cols]), minlength=n), np.finfo(float).tiny)
+    for storage, st, bound in (("f32", lib.STORE_F32, 2.0 ** -24), ("bf16", lib.STORE_BF16_SCALED, 2.0 ** -8)):
+        m = lib.HBDIA(rows, cols, vals, n, n)
+        m.convertToHBDIAFormat(32, 2, upload=False)
+        m.prepareForGPU(st)
+        yv = lib.HBDIAVector(np.zeros(n))
+        lib.hbdiaSpMV(m, lib.HBDIAVector(x), yv, True, False)
+        m.synchronize()
+        y = yv.toHost()
+        stored = (L.data.astype(np.float32).astype(np.float64) if storage == "f32"
+                  else oracle.bf16_block_scaled(L.data, L.block_start, 32))
+        assert bits_equal(y, om.spmv_with_values(stored, x)), storage
+        err = float(np.max(np.abs(y - y64) / scale))
+        assert err <= bound, (storage, err)
+        del m
