@@ -20,12 +20,13 @@ import numpy as np
 from . import _lib
 from ._lib import (BATCH_CONCURRENT, BATCH_QUEUE, REQ_CG, REQ_SPMV, KERNEL_AUTO, KERNEL_PIPE, KERNEL_QUAD, KERNEL_ROWWISE, KERNEL_STAGED, KERNEL_WARP, TUNE_PREFETCH, TUNE_QUAD_GROUP, TUNE_SPMM_TILE, TUNE_STAGES, TUNE_TAIL,
                    TUNE_UNROLL, HBDIACudaError,
-                   HBDIADeviceTimeout, STORE_BF16_SCALED, STORE_F32, STORE_NATIVE, MatrixInfo,
+                   HBDIADeviceTimeout, STORE_BF16_SCALED, STORE_F32, STORE_NATIVE, STORE_F32_QUAD, STORE_BF16_QUAD, MatrixInfo,
                    check as _check, load as _load)
 
 __all__ = ["ExecutionMode", "HBDIA", "HBDIAVector", "hbdiaSpMV", "spmv_device", "spmm_device",
            "spmv_host", "generate_stencil27", "generate_stencil7", "generate_banded", "fill_uniform",
-           "HBDIACudaError", "set_device", "STORE_NATIVE", "STORE_F32", "STORE_BF16_SCALED", "library_path"]
+           "HBDIACudaError", "set_device", "STORE_NATIVE", "STORE_F32", "STORE_BF16_SCALED", "STORE_F32_QUAD",
+           "STORE_BF16_QUAD", "library_path"]
 
 DEFAULT_BLOCK_WIDTH = 32      # include/types.hpp:14
 DEFAULT_THRESHOLD = 1         # include/types.hpp:15

@@ -32,7 +32,7 @@ TUNE_UNROLL, TUNE_SPMM_TILE, TUNE_PREFETCH, TUNE_TAIL, TUNE_STAGES, TUNE_QUAD_GR
 HBDIA_F64, HBDIA_F32 = 0, 1
 BATCH_CONCURRENT, BATCH_QUEUE = 0, 1
 REQ_SPMV, REQ_CG = 0, 1
-STORE_NATIVE, STORE_F32, STORE_BF16_SCALED = 0, 1, 2
+STORE_NATIVE, STORE_F32, STORE_BF16_SCALED, STORE_F32_QUAD, STORE_BF16_QUAD = 0, 1, 2, 3, 4
 
 
 class MatrixInfo(ctypes.Structure):

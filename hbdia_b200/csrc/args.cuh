@@ -24,6 +24,7 @@ inline dev::SpmvArgs<VT, XT> make_args(const DevicePlan &P) {
     a.numBlocks = P.numBlocks;
     a.numTiles = P.numTiles;
     a.hasCoo = P.nCoo > 0;
+    a.quadLayout = P.quadLayout ? 1 : 0;
     return a;
 }
 

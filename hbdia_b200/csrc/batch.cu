@@ -360,6 +360,9 @@ Batch *batch_create(const std::vector<const DevicePlan *> &plans) {
         if (!P.base) throw Error(HBDIA_ERR_NOT_CONVERTED, "matrix " + std::to_string(i) + " has no device layout");
         if (P.bw != 32)
             throw Error(HBDIA_ERR_UNSUPPORTED, "batches need blockWidth 32 (matrix " + std::to_string(i) + ")");
+        if (P.quadLayout)
+            throw Error(HBDIA_ERR_UNSUPPORTED, "quad-interleaved value storage supports SpMV only (matrix " +
+                                                   std::to_string(i) + ")");
         if (P.dtype != P0.dtype || P.storage != P0.storage)
             throw Error(HBDIA_ERR_INVALID_ARGUMENT, "all matrices of a batch need the same value type and storage");
         if (segs.empty() || segs.back().count == dev::kBatchSeg ||

@@ -118,6 +118,12 @@ void free_host_pipeline(hbdia_matrix *m) {
     }
 }
 
+// The public storage code of a plan (hbdia_value_storage).
+int32_t plan_storage_code(const hbdia::DevicePlan &P) {
+    if (!P.quadLayout) return P.storage;
+    return P.storage == HBDIA_STORE_F32 ? HBDIA_STORE_F32_QUAD : HBDIA_STORE_BF16_QUAD;
+}
+
 void free_block_sizes(hbdia_matrix *m) {
     if (m->blockSizesDev) cudaFree(m->blockSizesDev);
     m->blockSizesDev = nullptr;
@@ -392,7 +398,7 @@ int hbdia_matrix_get_info(const hbdia_matrix *m, hbdia_matrix_info *info) {
         I.blockWidth = m->blockWidth;
         I.threshold = m->threshold;
         I.maxCooEntries = m->maxCoo;
-        I.storage = m->plan.storage;
+        I.storage = plan_storage_code(m->plan);
         I.deviceBytes = static_cast<int64_t>(m->plan.bytes);
         I.bytesPerSpmv = m->plan.bytesPerSpmv;
         if (m->hostLayout) {
@@ -887,7 +893,7 @@ int hbdia_cg_solve(hbdia_matrix *m, const double *b, double *x, const hbdia_cg_o
         ensure_device(m);
         const hbdia::DevicePlan *it = &m->plan;
         if (opt->iterStorage != HBDIA_STORE_NATIVE) {
-            if (!m->innerPlan.base || m->innerPlan.storage != opt->iterStorage) {
+            if (!m->innerPlan.base || plan_storage_code(m->innerPlan) != opt->iterStorage) {
                 need(m->hostLayout, HBDIA_ERR_NOT_CONVERTED, "no host layout to build the iteration operator");
                 hbdia::build_plan(m->L64, opt->iterStorage, m->innerPlan);
                 m->innerPlan.kernel = m->plan.kernel;

@@ -325,8 +325,11 @@ void cg_solve_group(const DevicePlan &A64, const DevicePlan &Ait, CgCall *calls,
                 check_cuda(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
                 try {
                     for (int it = 0; it < prm.checkEvery; ++it) {
-                        if (ka == 1) launch_spmv(Ait, ps[0], qs[0], s);
-                        else launch_spmv_list(Ait, ps.data(), qs.data(), ka, s);
+                        if (ka == 1 || Ait.quadLayout) {  // (quad-interleaved values: SpMV only)
+                            for (int a = 0; a < ka; ++a) launch_spmv(Ait, ps[a], qs[a], s);
+                        } else {
+                            launch_spmv_list(Ait, ps.data(), qs.data(), ka, s);
+                        }
                         g_dot_pq<<<grid, kThreads, 0, s>>>(V, n);
                         g_update<<<grid, kThreads, 0, s>>>(V, n, G);
                         g_direction<<<grid, kThreads, 0, s>>>(V, n, G);

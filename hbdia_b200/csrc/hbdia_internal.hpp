@@ -111,7 +111,9 @@ namespace hbdia {
 // one device allocation, each 256-byte aligned.
 struct DevicePlan {
     int32_t dtype = HBDIA_F64;          // T of x, y and the COO values
-    int32_t storage = HBDIA_STORE_NATIVE;
+    int32_t storage = HBDIA_STORE_NATIVE;  // value type: NATIVE, F32 or BF16_SCALED
+    bool quadLayout = false;             // F32 / BF16 values of uniform quads interleaved
+                                         // (HBDIA_STORE_F32_QUAD / _BF16_QUAD: QUAD kernel only)
     int32_t n = 0, numCols = 0, bw = 0, numBlocks = 0, numTiles = 0;
     int32_t xn = 0;  // DIA column bound: n, or a partial matrix's x-window length
     int64_t totalOffsets = 0, slots = 0, nCoo = 0;

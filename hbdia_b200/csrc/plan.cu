@@ -106,8 +106,15 @@ void build_plan(const HostLayout<T> &L, int storage, DevicePlan &P, const Column
     Q.dtype = std::is_same<T, float>::value ? HBDIA_F32 : HBDIA_F64;
     if (storage != HBDIA_STORE_NATIVE && Q.dtype != HBDIA_F64)
         throw Error(HBDIA_ERR_UNSUPPORTED, "reduced value storage needs a double matrix");
-    if (storage < HBDIA_STORE_NATIVE || storage > HBDIA_STORE_BF16_SCALED)
+    if (storage < HBDIA_STORE_NATIVE || storage > HBDIA_STORE_BF16_QUAD)
         throw Error(HBDIA_ERR_INVALID_ARGUMENT, "unknown value storage");
+    // the quad-interleaved storages hold F32 / BF16 values for the quad kernel
+    Q.quadLayout = storage == HBDIA_STORE_F32_QUAD || storage == HBDIA_STORE_BF16_QUAD;
+    if (Q.quadLayout) {
+        if (L.blockWidth != 32 || L.numRows > (1 << 30))
+            throw Error(HBDIA_ERR_UNSUPPORTED, "quad-interleaved storage needs blockWidth 32 and numRows <= 2^30");
+        storage = storage == HBDIA_STORE_F32_QUAD ? HBDIA_STORE_F32 : HBDIA_STORE_BF16_SCALED;
+    }
     Q.storage = storage;
     Q.n = L.numRows;
     Q.numCols = W ? W->len : L.numCols;
@@ -188,6 +195,31 @@ void build_plan(const HostLayout<T> &L, int storage, DevicePlan &P, const Column
                 vb[i] = __float2bfloat16_rn(static_cast<float>(static_cast<double>(L.data[i]) / s));
         }
         valSrc = vb.data();
+    }
+    if (Q.quadLayout) {
+        // uniform quads (the quad kernel's run-time test: four blocks, one list
+        // of 1-32 offsets) go [offset][lane][block]
+        const int32_t *bs = L.blockStart.data();
+        auto interleave = [&](auto &v) {
+            using E = typename std::remove_reference<decltype(v)>::type::value_type;
+            std::vector<E> tmp;
+            for (int64_t b0 = 0; b0 + 4 <= Q.numBlocks; b0 += 4) {
+                const int32_t K = bs[b0 + 1] - bs[b0];
+                if (K < 1 || K > 32) continue;
+                bool uni = bs[b0 + 2] - bs[b0 + 1] == K && bs[b0 + 3] - bs[b0 + 2] == K && bs[b0 + 4] - bs[b0 + 3] == K;
+                for (int32_t q = 1; uni && q < 4; ++q)
+                    for (int32_t k = 0; uni && k < K; ++k) uni = L.offsets[bs[b0 + q] + k] == L.offsets[bs[b0] + k];
+                if (!uni) continue;
+                const int64_t base = static_cast<int64_t>(bs[b0]) * 32;
+                tmp.assign(v.begin() + base, v.begin() + base + 4 * 32 * K);
+                for (int32_t q = 0; q < 4; ++q)
+                    for (int32_t k = 0; k < K; ++k)
+                        for (int32_t l = 0; l < 32; ++l)
+                            v[base + (static_cast<int64_t>(k) * 32 + l) * 4 + q] = tmp[(static_cast<int64_t>(q) * K + k) * 32 + l];
+            }
+        };
+        if (storage == HBDIA_STORE_F32) interleave(vf);
+        else interleave(vb);
     }
 
     // one allocation
@@ -428,6 +460,7 @@ void launch_typed(const DevicePlan &P, const void *x, void *y, cudaStream_t s) {
 }  // namespace
 
 int32_t select_kernel(const DevicePlan &P, const void *x) {
+    if (P.quadLayout) return HBDIA_KERNEL_QUAD;  // the only kernel that reads that layout
     const bool bw32 = P.bw == 32;
     // the staged kernel bulk-copies x and the value slabs (16-byte aligned
     // starts), needs a status word for its bounded waits, and does row/column
@@ -538,6 +571,7 @@ int32_t default_spmm_tile(int32_t k, bool colMajor) {
 void launch_spmm_tile(const DevicePlan &P, const void *X, int64_t ldx, void *Y, int64_t ldy, int32_t k,
                       int32_t tile, void *stream, bool colMajor) {
     if (!P.base) throw Error(HBDIA_ERR_NOT_CONVERTED, "matrix has no device layout");
+    if (P.quadLayout) throw Error(HBDIA_ERR_UNSUPPORTED, "quad-interleaved value storage supports SpMV only");
     if (!X || !Y) throw Error(HBDIA_ERR_INVALID_ARGUMENT, "null matrix pointer");
     if (k <= 0) throw Error(HBDIA_ERR_INVALID_ARGUMENT, "need k > 0");
     if (!colMajor && (ldx < k || ldy < k)) throw Error(HBDIA_ERR_INVALID_ARGUMENT, "need ldx, ldy >= k");
@@ -589,6 +623,7 @@ void launch_list_typed(const DevicePlan &P, const void *const *x, void *const *y
 
 void launch_spmv_list(const DevicePlan &P, const void *const *x, void *const *y, int32_t k, void *stream) {
     if (!P.base) throw Error(HBDIA_ERR_NOT_CONVERTED, "matrix has no device layout");
+    if (P.quadLayout) throw Error(HBDIA_ERR_UNSUPPORTED, "quad-interleaved value storage supports SpMV only");
     if (k < 0 || (k > 0 && (!x || !y))) throw Error(HBDIA_ERR_INVALID_ARGUMENT, "bad vector list");
     for (int32_t j = 0; j < k; ++j)
         if (!x[j] || !y[j]) throw Error(HBDIA_ERR_INVALID_ARGUMENT, "null vector in the list");

@@ -65,7 +65,8 @@ struct SpmvBatch {
 
 struct ServedMatrix {
     DevicePlan p64;   // FP64 values: CG outer residual; SpMVs when spmvStorage is NATIVE
-    DevicePlan pLow;  // reduced storage (when one is asked for)
+    DevicePlan pLow;  // reduced storage of the SpMVs (when one is asked for)
+    DevicePlan pCg;   // the CG iterations' storage when it differs from pLow's
     int32_t n = 0, rowsX = 0;
     double *X = nullptr, *Y = nullptr;  // column-major staging blocks, maxRhs columns
     int64_t bytes = 0;
@@ -75,7 +76,9 @@ struct ServedMatrix {
     std::deque<SpmvBatch> running;         // issued, in stream order (scheduler thread)
     std::deque<Request *> pending;         // SpMV requests not yet issued (server lock)
     const DevicePlan &spmvPlan(int32_t storage) const { return storage == HBDIA_STORE_NATIVE ? p64 : pLow; }
-    const DevicePlan &cgIter(int32_t storage) const { return storage == HBDIA_STORE_NATIVE ? p64 : pLow; }
+    const DevicePlan &cgIter(int32_t storage) const {
+        return storage == HBDIA_STORE_NATIVE ? p64 : pCg.base ? pCg : pLow;
+    }
 };
 
 struct Request {
@@ -395,6 +398,7 @@ void cg_worker(Server *S) {
 void free_matrix(ServedMatrix &M) {
     free_plan(M.p64);
     free_plan(M.pLow);
+    free_plan(M.pCg);
     if (M.X) cudaFree(M.X);
     if (M.Y) cudaFree(M.Y);
     if (M.stream) cudaStreamDestroy(M.stream);
@@ -429,12 +433,11 @@ Server *server_create(const hbdia_server_options &o) {
         o.cgMaxIterations < 1 || o.cgCheckEvery < 1 || o.cgMaxGroup < 1 || o.cgMaxGroup > 16 ||
         o.maxInFlight < 1 || o.maxInFlight > 8)
         throw Error(HBDIA_ERR_INVALID_ARGUMENT, "bad server options");
-    for (int32_t st : {o.spmvStorage, o.cgIterStorage})
-        if (st != HBDIA_STORE_NATIVE && st != HBDIA_STORE_F32 && st != HBDIA_STORE_BF16_SCALED)
-            throw Error(HBDIA_ERR_INVALID_ARGUMENT, "unknown value storage");
-    if (o.spmvStorage != HBDIA_STORE_NATIVE && o.cgIterStorage != HBDIA_STORE_NATIVE &&
-        o.spmvStorage != o.cgIterStorage)
-        throw Error(HBDIA_ERR_UNSUPPORTED, "SpMV and CG iteration storage must match when both are reduced");
+    if (o.spmvStorage != HBDIA_STORE_NATIVE && o.spmvStorage != HBDIA_STORE_F32 &&
+        o.spmvStorage != HBDIA_STORE_BF16_SCALED)  // SpMV batches are SpMMs: no quad-interleaved storage
+        throw Error(HBDIA_ERR_INVALID_ARGUMENT, "unknown or unsupported SpMV value storage");
+    if (o.cgIterStorage < HBDIA_STORE_NATIVE || o.cgIterStorage > HBDIA_STORE_BF16_QUAD)
+        throw Error(HBDIA_ERR_INVALID_ARGUMENT, "unknown CG iteration value storage");
     auto S = std::make_unique<Server>();
     S->opt = o;
     check_cuda(cudaGetDevice(&S->device), "cudaGetDevice");
@@ -470,10 +473,11 @@ int32_t server_add_matrix(Server *S, const hbdia_matrix *m) {
     auto M = std::make_unique<ServedMatrix>();
     M->n = L.numRows;
     M->rowsX = std::max(L.numRows, L.numCols);
-    const int32_t low = S->opt.spmvStorage != HBDIA_STORE_NATIVE ? S->opt.spmvStorage : S->opt.cgIterStorage;
+    const int32_t sp = S->opt.spmvStorage, cgs = S->opt.cgIterStorage;
     try {
         build_plan(L, HBDIA_STORE_NATIVE, M->p64);
-        if (low != HBDIA_STORE_NATIVE) build_plan(L, low, M->pLow);
+        if (sp != HBDIA_STORE_NATIVE) build_plan(L, sp, M->pLow);
+        if (cgs != HBDIA_STORE_NATIVE && cgs != sp) build_plan(L, cgs, M->pCg);
         const int64_t staging =
             static_cast<int64_t>(S->opt.maxRhs) * (static_cast<int64_t>(M->rowsX) + M->n) * 8;
         // CG workspaces grow to the largest system: 3 vectors of the workspace + b, x per
@@ -484,7 +488,7 @@ int32_t server_add_matrix(Server *S, const hbdia_matrix *m) {
             if (M->n > S->maxN)
                 cgGrow = static_cast<int64_t>(S->opt.cgWorkers) * S->opt.cgMaxGroup * 5 * 8 * (M->n - S->maxN);
         }
-        M->bytes = static_cast<int64_t>(M->p64.bytes + M->pLow.bytes) + staging;
+        M->bytes = static_cast<int64_t>(M->p64.bytes + M->pLow.bytes + M->pCg.bytes) + staging;
         {
             std::lock_guard<std::mutex> lk(S->mu);
             if (S->used + M->bytes + cgGrow > S->opt.memoryBudget)

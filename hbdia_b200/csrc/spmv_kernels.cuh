@@ -46,6 +46,7 @@ struct SpmvArgs {
     int32_t numBlocks;       // DIA blocks
     int32_t numTiles;        // ceil(n / 32)
     int32_t hasCoo;          // COO remainder non-empty
+    int32_t quadLayout;      // 4- / 2-byte values of uniform quads interleaved (spmv_quad.cuh)
 };
 
 __device__ __forceinline__ double fma_rn(double a, double b, double c) { return __fma_rn(a, b, c); }

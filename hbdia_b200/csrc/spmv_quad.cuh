@@ -24,6 +24,15 @@
 // next chunk.  The quad's 128 DIA sums wait in a per-warp shared buffer, each
 // head adds its row's COO sum there once, and the owning lanes write y.
 //
+// Quad-interleaved value storage (HBDIA_STORE_F32_QUAD / _BF16_QUAD): the
+// values of a uniform quad -- four blocks with one offset list of at most 32
+// offsets -- are stored [offset][lane][block] instead of [block][offset][lane]
+// (same region, same size), so a lane's four values of one offset are ONE
+// 16-byte (FP32) or 8-byte (BF16) load, a warp's request 512 / 256 bytes --
+// what an FP64 value row gives the other kernels.  Non-uniform quads keep the
+// per-block order.  The layout is built by build_plan with the same
+// uniformity test this kernel makes at run time.
+//
 // Arithmetic is the reference's, in the reference's order: per row, offsets
 // ascending, stored zeros and columns outside [0, xn) skipped, fma; COO
 // products summed from zero in list order with separately rounded multiply
@@ -106,6 +115,63 @@ __device__ __forceinline__ void quad_dia(const XT *__restrict__ x, const VT *__r
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
                 const XT vv = widen<XT>(v[q][u], sc[q]);
+                if (ok[q][u] && vv != XT(0)) sum[q] = fma_rn(vv, xv[q][u], sum[q]);
+            }
+        }
+    }
+}
+
+// The lane's values of the four blocks for offset element i = k * 32 + lane
+// of a quad-interleaved region: one vector load.
+__device__ __forceinline__ void ld_quad(const float *base, int32_t i, float (&v)[4]) {
+    const float4 f = __ldcs(reinterpret_cast<const float4 *>(base) + i);
+    v[0] = f.x;
+    v[1] = f.y;
+    v[2] = f.z;
+    v[3] = f.w;
+}
+__device__ __forceinline__ void ld_quad(const __nv_bfloat16 *base, int32_t i, __nv_bfloat16 (&v)[4]) {
+    const uint2 r = __ldcs(reinterpret_cast<const uint2 *>(base) + i);
+    v[0] = __ushort_as_bfloat16(static_cast<unsigned short>(r.x & 0xffffu));
+    v[1] = __ushort_as_bfloat16(static_cast<unsigned short>(r.x >> 16));
+    v[2] = __ushort_as_bfloat16(static_cast<unsigned short>(r.y & 0xffffu));
+    v[3] = __ushort_as_bfloat16(static_cast<unsigned short>(r.y >> 16));
+}
+
+// quad_dia over a quad-interleaved region (vq: the quad's first value); same
+// arithmetic and order.
+template <typename VT, typename XT, int U, bool CHECK>
+__device__ __forceinline__ void quad_dia_v(const XT *__restrict__ x, const VT *__restrict__ vq, int32_t K,
+                                           int32_t myoff, int32_t row, uint32_t xn, const float (&sc)[4],
+                                           XT (&sum)[4]) {
+    const int lane = row & 31;
+    for (int32_t g = 0; g < K; g += U) {
+        VT v[U][4];
+        XT xv[4][U];
+        bool ok[4][U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const bool in = g + u < K;  // warp-uniform
+            const int32_t off = __shfl_sync(kFull, myoff, (g + u) & 31);
+            if (in) {
+                ld_quad(vq, (g + u) * 32 + lane, v[u]);
+            } else {
+#pragma unroll
+                for (int q = 0; q < 4; ++q) v[u][q] = VT(0);
+            }
+            const int32_t col = row + off;
+            const XT *xp = x + col;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                ok[q][u] = in && (!CHECK || static_cast<uint32_t>(col + 32 * q) < xn);
+                xv[q][u] = ok[q][u] ? __ldg(xp + 32 * q) : XT(0);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const XT vv = widen<XT>(v[u][q], sc[q]);
                 if (ok[q][u] && vv != XT(0)) sum[q] = fma_rn(vv, xv[q][u], sum[q]);
             }
         }
@@ -232,8 +298,19 @@ spmv_bw32_quad(const SpmvArgs<VT, XT> a, const XT *__restrict__ x, XT *__restric
                 const VT *v1 = a.vals + static_cast<int64_t>(kq[1]) * 32 + lane;
                 const VT *v2 = a.vals + static_cast<int64_t>(kq[2]) * 32 + lane;
                 const VT *v3 = a.vals + static_cast<int64_t>(kq[3]) * 32 + lane;
-                if (interior) quad_dia<VT, XT, U, false>(x, v0, v1, v2, v3, K, cur.myoff, row, xn, sc, sum);
-                else quad_dia<VT, XT, U, true>(x, v0, v1, v2, v3, K, cur.myoff, row, xn, sc, sum);
+                bool done = false;
+                if constexpr (sizeof(VT) < 8) {
+                    if (a.quadLayout) {  // interleaved region of the quad
+                        const VT *vq = a.vals + static_cast<int64_t>(kq[0]) * 32;
+                        if (interior) quad_dia_v<VT, XT, U, false>(x, vq, K, cur.myoff, row, xn, sc, sum);
+                        else quad_dia_v<VT, XT, U, true>(x, vq, K, cur.myoff, row, xn, sc, sum);
+                        done = true;
+                    }
+                }
+                if (!done) {
+                    if (interior) quad_dia<VT, XT, U, false>(x, v0, v1, v2, v3, K, cur.myoff, row, xn, sc, sum);
+                    else quad_dia<VT, XT, U, true>(x, v0, v1, v2, v3, K, cur.myoff, row, xn, sc, sum);
+                }
             }
         } else {
 #pragma unroll

@@ -195,6 +195,7 @@ def cg(args):
     m = hb.HBDIA(rows, cols, vals, n, n)
     m.convertToHBDIAFormat(32, 2)
     for name, st in (("mixed: fp32-storage iterations, fp64 reliable updates", hb.STORE_F32),
+                     ("mixed: fp32 quad-interleaved iterations, fp64 reliable updates", hb.STORE_F32_QUAD),
                      ("plain fp64 CG", hb.STORE_NATIVE)):
         xt = torch.zeros(n, dtype=torch.float64, device="cuda")
         hb.cg_solve(m, bt.data_ptr(), xt.data_ptr(), tol=1e-10, iter_storage=st)  # warm

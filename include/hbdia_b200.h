@@ -52,11 +52,20 @@ typedef enum hbdia_exec_mode { HBDIA_CPU_COO = 0, HBDIA_GPU_COO = 1 } hbdia_exec
 
 /* Device storage of the blocked-DIA values.  NATIVE stores T.  F32 and
  * BF16_SCALED store float / bfloat16 (with one float scale per block) for a
- * double matrix; the SpMV then still accumulates in double. */
+ * double matrix; the SpMV then still accumulates in double.  F32_QUAD and
+ * BF16_QUAD store the same values with those of every uniform quad (four
+ * consecutive blocks with one list of at most 32 offsets) interleaved
+ * [offset][lane][block], so that the quad kernel reads a lane's four values of
+ * an offset with one 16- / 8-byte load; they need blockWidth 32, run the SpMV
+ * through the quad kernel only (whatever kernel is set) and give the same y
+ * as F32 / BF16_SCALED bit for bit; SpMM, vector lists and batches refuse
+ * them (HBDIA_ERR_UNSUPPORTED). */
 typedef enum hbdia_value_storage {
     HBDIA_STORE_NATIVE = 0,
     HBDIA_STORE_F32 = 1,
-    HBDIA_STORE_BF16_SCALED = 2
+    HBDIA_STORE_BF16_SCALED = 2,
+    HBDIA_STORE_F32_QUAD = 3,
+    HBDIA_STORE_BF16_QUAD = 4
 } hbdia_value_storage;
 
 /* SpMV kernel choice (all give bit-identical y).  AUTO picks the kernel
@@ -601,8 +610,10 @@ typedef struct hbdia_server_options {
     int64_t memoryBudget;   /* device bytes the server may hold (default 150e9)             */
     int32_t batching;       /* continuous batching of SpMVs (default 1)                     */
     int32_t maxRhs;         /* SpMV requests of one matrix per batch, 1-64 (default 16)    */
-    int32_t spmvStorage;    /* hbdia_value_storage of SpMVs (default HBDIA_STORE_F32)       */
-    int32_t cgIterStorage;  /* storage of the CG iterations' SpMVs (default HBDIA_STORE_F32) */
+    int32_t spmvStorage;    /* hbdia_value_storage of SpMVs (default HBDIA_STORE_F32;       */
+                            /* not the quad-interleaved ones: batches are SpMMs)            */
+    int32_t cgIterStorage;  /* storage of the CG iterations' SpMVs (default HBDIA_STORE_F32; */
+                            /* a different one is kept as a second reduced copy)            */
     int32_t cgWorkers;      /* concurrent CG solves, 1-64 (default 4)                       */
     int32_t cgMaxUpdates;   /* FP64 residual recomputations per solve (default 100)         */
     int32_t cgMaxIterations;/* iterations per solve (default 20000)                         */
