@@ -618,13 +618,14 @@ def generate_stencil27_spd(nx: int, ny: int, nz: int, shift: float = 1e-3, seed:
     return _two_call(_load().hbdia_generate_stencil27_spd, nx, ny, nz, float(shift), float(extra_fraction), seed)
 
 
-def cg_solve(matrix: HBDIA, b_ptr: int, x_ptr: int, tol: float = 1e-10, iter_storage: int = STORE_F32,
+def cg_solve(matrix: HBDIA, b_ptr: int, x_ptr: int, tol: float = 1e-10, iter_storage: int = STORE_F32_QUAD,
              update_factor: float = 0.1, max_updates: int = 100, max_iterations: int = 20000,
              check_every: int = 10, stream: Optional[int] = None) -> "_lib.CgResult":
     """CG on device buffers b, x (x: initial guess in, solution out): the
-    iterations' SpMVs use the ``iter_storage`` values (STORE_F32: mixed
-    precision, STORE_NATIVE: plain FP64 CG), with reliable updates of the
-    FP64 residual and convergence judged on it (hbdia_cg_solve)."""
+    iterations' SpMVs use the ``iter_storage`` values (STORE_F32_QUAD, the
+    default, or STORE_F32: mixed precision, both giving the same iterates;
+    STORE_NATIVE: plain FP64 CG), with reliable updates of the FP64 residual
+    and convergence judged on it (hbdia_cg_solve)."""
     o = _lib.CgOptions(tol, update_factor, max_updates, max_iterations, iter_storage, check_every)
     r = _lib.CgResult()
     _check(_load().hbdia_cg_solve(matrix.handle, ctypes.c_void_p(b_ptr), ctypes.c_void_p(x_ptr), ctypes.byref(o),

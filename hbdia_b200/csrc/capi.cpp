@@ -893,9 +893,10 @@ int hbdia_cg_solve(hbdia_matrix *m, const double *b, double *x, const hbdia_cg_o
         ensure_device(m);
         const hbdia::DevicePlan *it = &m->plan;
         if (opt->iterStorage != HBDIA_STORE_NATIVE) {
-            if (!m->innerPlan.base || plan_storage_code(m->innerPlan) != opt->iterStorage) {
+            const int32_t st = m->hostLayout ? hbdia::iteration_storage(m->L64, opt->iterStorage) : opt->iterStorage;
+            if (!m->innerPlan.base || plan_storage_code(m->innerPlan) != st) {
                 need(m->hostLayout, HBDIA_ERR_NOT_CONVERTED, "no host layout to build the iteration operator");
-                hbdia::build_plan(m->L64, opt->iterStorage, m->innerPlan);
+                hbdia::build_plan(m->L64, st, m->innerPlan);
                 m->innerPlan.kernel = m->plan.kernel;
                 m->innerPlan.unroll = m->plan.unroll;
             }

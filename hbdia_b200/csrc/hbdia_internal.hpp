@@ -168,6 +168,10 @@ struct ColumnWindow {
 
 template <typename T>
 void build_plan(const HostLayout<T> &L, int storage, DevicePlan &P, const ColumnWindow *W = nullptr);
+// The storage an iteration operator (CG) is built with: a quad-interleaved
+// storage the layout cannot take (blockWidth other than 32, more than 2^30
+// rows) becomes its per-block counterpart, which gives the same y.
+int32_t iteration_storage(const HostLayout<double> &L, int32_t storage);
 // A plan over a caller-owned device layout (layout_plan.cu).
 void borrow_plan(const hbdia_layout_desc &d, DevicePlan &P);
 void free_plan(DevicePlan &P);

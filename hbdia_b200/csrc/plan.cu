@@ -387,7 +387,9 @@ void launch_quad(const DevicePlan &P, const dev::SpmvArgs<VT, XT> &a, const XT *
     const bool pf = P.prefetchL2 > 0 ||
                     (P.prefetchL2 < 0 &&
                      static_cast<int64_t>(std::max(P.n, P.numCols)) * static_cast<int64_t>(sizeof(XT)) > l2);
-    const int32_t g = P.quadGroup ? P.quadGroup : (sizeof(VT) == 8 ? 2 : 4);
+    // default: 4 offsets in flight, the fastest or within run-to-run noise of
+    // it for every value storage on B200 (27-point 128^3 / 256^3, banded 8M)
+    const int32_t g = P.quadGroup ? P.quadGroup : 4;
     const int32_t quads = (P.numTiles + 3) / 4 * 4;  // tiles covered by whole quads (4 per warp)
 #define HBDIA_QUAD(U)                                                                                  \
     return pf ? launch_pipe(dev::spmv_bw32_quad<VT, XT, U, true>, a, quads / 4, x, y, s, device)              \
@@ -459,6 +461,13 @@ void launch_typed(const DevicePlan &P, const void *x, void *y, cudaStream_t s) {
 
 }  // namespace
 
+int32_t iteration_storage(const HostLayout<double> &L, int32_t storage) {
+    const bool quad = storage == HBDIA_STORE_F32_QUAD || storage == HBDIA_STORE_BF16_QUAD;
+    if (quad && (L.blockWidth != 32 || L.numRows > (1 << 30)))
+        return storage == HBDIA_STORE_F32_QUAD ? HBDIA_STORE_F32 : HBDIA_STORE_BF16_SCALED;
+    return storage;
+}
+
 int32_t select_kernel(const DevicePlan &P, const void *x) {
     if (P.quadLayout) return HBDIA_KERNEL_QUAD;  // the only kernel that reads that layout
     const bool bw32 = P.bw == 32;
@@ -482,10 +491,10 @@ int32_t select_kernel(const DevicePlan &P, const void *x) {
             return bw32 ? HBDIA_KERNEL_WARP : HBDIA_KERNEL_ROWWISE;
         case HBDIA_KERNEL_WARP: return bw32 ? HBDIA_KERNEL_WARP : HBDIA_KERNEL_ROWWISE;
         default:  // AUTO: the fastest measured on B200 for blockWidth 32
-            // (BF16 storage: the quad kernel, 4-12 % ahead of the pipelined
-            // one on the 27-point 256^3 and banded 8M workloads; FP64 / FP32
-            // values: the pipelined kernel)
-            if (pipeOk) return P.storage == HBDIA_STORE_BF16_SCALED ? HBDIA_KERNEL_QUAD : HBDIA_KERNEL_PIPE;
+            // (4- and 2-byte values: the quad kernel, 2-10 % ahead of the
+            // pipelined one on the 27-point 128^3 and 256^3 workloads; FP64
+            // values: the pipelined kernel, which the quad one trails there)
+            if (pipeOk) return P.storage == HBDIA_STORE_NATIVE ? HBDIA_KERNEL_PIPE : HBDIA_KERNEL_QUAD;
             return bw32 ? HBDIA_KERNEL_WARP : HBDIA_KERNEL_ROWWISE;
     }
 }

@@ -416,7 +416,7 @@ void server_default_options(hbdia_server_options *o) {
     o->batching = 1;
     o->maxRhs = 16;
     o->spmvStorage = HBDIA_STORE_F32;
-    o->cgIterStorage = HBDIA_STORE_F32;
+    o->cgIterStorage = HBDIA_STORE_F32_QUAD;  // the fastest CG iterations measured on B200
     o->cgWorkers = 4;
     o->cgTol = 1e-10;
     o->cgUpdateFactor = 0.1;
@@ -473,7 +473,7 @@ int32_t server_add_matrix(Server *S, const hbdia_matrix *m) {
     auto M = std::make_unique<ServedMatrix>();
     M->n = L.numRows;
     M->rowsX = std::max(L.numRows, L.numCols);
-    const int32_t sp = S->opt.spmvStorage, cgs = S->opt.cgIterStorage;
+    const int32_t sp = S->opt.spmvStorage, cgs = iteration_storage(L, S->opt.cgIterStorage);
     try {
         build_plan(L, HBDIA_STORE_NATIVE, M->p64);
         if (sp != HBDIA_STORE_NATIVE) build_plan(L, sp, M->pLow);

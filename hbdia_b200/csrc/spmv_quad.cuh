@@ -48,8 +48,31 @@ namespace dev {
 
 constexpr int kQuadWarps = 8;  // warps per CTA
 
-// DIA sum of one 32-row block straight from its offset range [k0, k1): groups
-// of 8 offsets with all loads in flight, ascending order.
+// DIA sum of one 32-row block straight from its offset range [k0, k1): full
+// groups of 8 offsets with all loads in flight, then one at a time; ascending
+// order.
+template <typename VT, typename XT, int U>
+__device__ __forceinline__ XT block_group(const XT *__restrict__ x, const VT *__restrict__ vp, int32_t myoff, int j,
+                                          int32_t row, uint32_t n, float s, XT sum) {
+    VT v[U];
+    XT xv[U];
+    bool ok[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        const int32_t col = row + __shfl_sync(kFull, myoff, (j + u) & 31);
+        ok[u] = static_cast<uint32_t>(col) < n;
+        v[u] = ld_stream(vp + (j + u) * 32);
+        xv[u] = XT(0);
+        if (ok[u]) xv[u] = __ldg(x + col);
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        const XT vv = widen<XT>(v[u], s);
+        if (ok[u] && vv != XT(0)) sum = fma_rn(vv, xv[u], sum);
+    }
+    return sum;
+}
+
 template <typename VT, typename XT>
 __device__ __forceinline__ XT block_dia(const SpmvArgs<VT, XT> &a, const XT *__restrict__ x, int32_t k0, int32_t k1,
                                         int32_t row, int lane, float s) {
@@ -59,124 +82,96 @@ __device__ __forceinline__ XT block_dia(const SpmvArgs<VT, XT> &a, const XT *__r
         const int cnt = min(32, k1 - kb);
         const int32_t myoff = lane < cnt ? __ldg(a.offs + kb + lane) : 0;
         const VT *vp = a.vals + static_cast<int64_t>(kb) * 32 + lane;
-        for (int j = 0; j < cnt; j += 8) {
-            VT v[8];
-            XT xv[8];
-            bool ok[8];
-#pragma unroll
-            for (int u = 0; u < 8; ++u) {
-                const bool in = j + u < cnt;  // warp-uniform
-                const int32_t col = row + __shfl_sync(kFull, myoff, (j + u) & 31);
-                ok[u] = in && static_cast<uint32_t>(col) < n;
-                v[u] = in ? ld_stream(vp + (j + u) * 32) : VT(0);
-                xv[u] = ok[u] ? __ldg(x + col) : XT(0);
-            }
-#pragma unroll
-            for (int u = 0; u < 8; ++u) {
-                const XT vv = widen<XT>(v[u], s);
-                if (ok[u] && vv != XT(0)) sum = fma_rn(vv, xv[u], sum);
-            }
-        }
+        int j = 0;
+        for (; j + 8 <= cnt; j += 8) sum = block_group<VT, XT, 8>(x, vp, myoff, j, row, n, s, sum);
+        for (; j < cnt; ++j) sum = block_group<VT, XT, 1>(x, vp, myoff, j, row, n, s, sum);
     }
     return sum;
 }
 
-// The four blocks of a uniform quad: offsets (lane k holds offset k, K <= 32)
-// shared, values at vb[q] + k * 32 (+ lane).  CHECK: some column may fall
-// outside [0, xn).
-template <typename VT, typename XT, int U, bool CHECK>
-__device__ __forceinline__ void quad_dia(const XT *__restrict__ x, const VT *__restrict__ v0,
-                                         const VT *__restrict__ v1, const VT *__restrict__ v2,
-                                         const VT *__restrict__ v3, int32_t K, int32_t myoff, int32_t row,
-                                         uint32_t xn, const float (&sc)[4], XT (&sum)[4]) {
-    for (int32_t g = 0; g < K; g += U) {
-        VT v[4][U];
-        XT xv[4][U];
-        bool ok[4][U];
+// U offsets g .. g+U-1 (all < K) of the four blocks of a uniform quad: the
+// 4U values and 4U x gathers issued before any product is formed.  Values at
+// val(k, q) (element k * 32 of block q for this lane); offsets: lane k holds
+// offset k.  CHECK: some column may fall outside [0, xn).
+template <typename VT, typename XT, int U, bool CHECK, typename Val>
+__device__ __forceinline__ void quad_group(const XT *__restrict__ x, Val val, int32_t g, int32_t myoff, int32_t row,
+                                           uint32_t xn, const float (&sc)[4], XT (&sum)[4]) {
+    VT v[U][4];
+    XT xv[U][4];
+    bool ok[U][4];
 #pragma unroll
-        for (int u = 0; u < U; ++u) {
-            const bool in = g + u < K;  // warp-uniform
-            const int32_t off = __shfl_sync(kFull, myoff, (g + u) & 31);
-            const int32_t k = (g + u) * 32;
-            v[0][u] = in ? ld_stream(v0 + k) : VT(0);
-            v[1][u] = in ? ld_stream(v1 + k) : VT(0);
-            v[2][u] = in ? ld_stream(v2 + k) : VT(0);
-            v[3][u] = in ? ld_stream(v3 + k) : VT(0);
-            const int32_t col = row + off;
-            const XT *xp = x + col;
+    for (int u = 0; u < U; ++u) {
+        const int32_t off = __shfl_sync(kFull, myoff, (g + u) & 31);
+        val(g + u, v[u]);
+        const int32_t col = row + off;
+        const XT *xp = x + col;
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                ok[q][u] = in && (!CHECK || static_cast<uint32_t>(col + 32 * q) < xn);
-                xv[q][u] = ok[q][u] ? __ldg(xp + 32 * q) : XT(0);
-            }
+        for (int q = 0; q < 4; ++q) {
+            ok[u][q] = !CHECK || static_cast<uint32_t>(col + 32 * q) < xn;
+            xv[u][q] = XT(0);
+            if (ok[u][q]) xv[u][q] = __ldg(xp + 32 * q);
         }
+    }
 #pragma unroll
-        for (int u = 0; u < U; ++u) {
+    for (int u = 0; u < U; ++u) {
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const XT vv = widen<XT>(v[q][u], sc[q]);
-                if (ok[q][u] && vv != XT(0)) sum[q] = fma_rn(vv, xv[q][u], sum[q]);
-            }
+        for (int q = 0; q < 4; ++q) {
+            const XT vv = widen<XT>(v[u][q], sc[q]);
+            if (ok[u][q] && vv != XT(0)) sum[q] = fma_rn(vv, xv[u][q], sum[q]);
         }
     }
 }
 
-// The lane's values of the four blocks for offset element i = k * 32 + lane
-// of a quad-interleaved region: one vector load.
-__device__ __forceinline__ void ld_quad(const float *base, int32_t i, float (&v)[4]) {
-    const float4 f = __ldcs(reinterpret_cast<const float4 *>(base) + i);
-    v[0] = f.x;
-    v[1] = f.y;
-    v[2] = f.z;
-    v[3] = f.w;
-}
-__device__ __forceinline__ void ld_quad(const __nv_bfloat16 *base, int32_t i, __nv_bfloat16 (&v)[4]) {
-    const uint2 r = __ldcs(reinterpret_cast<const uint2 *>(base) + i);
-    v[0] = __ushort_as_bfloat16(static_cast<unsigned short>(r.x & 0xffffu));
-    v[1] = __ushort_as_bfloat16(static_cast<unsigned short>(r.x >> 16));
-    v[2] = __ushort_as_bfloat16(static_cast<unsigned short>(r.y & 0xffffu));
-    v[3] = __ushort_as_bfloat16(static_cast<unsigned short>(r.y >> 16));
+// The K offsets of a uniform quad in ascending order: full groups of U, then
+// one at a time (no per-offset range test inside a group).
+template <typename VT, typename XT, int U, bool CHECK, typename Val>
+__device__ __forceinline__ void quad_offsets(const XT *__restrict__ x, Val val, int32_t K, int32_t myoff,
+                                             int32_t row, uint32_t xn, const float (&sc)[4], XT (&sum)[4]) {
+    int32_t g = 0;
+    for (; g + U <= K; g += U) quad_group<VT, XT, U, CHECK>(x, val, g, myoff, row, xn, sc, sum);
+    for (; g < K; ++g) quad_group<VT, XT, 1, CHECK>(x, val, g, myoff, row, xn, sc, sum);
 }
 
-// quad_dia over a quad-interleaved region (vq: the quad's first value); same
-// arithmetic and order.
-template <typename VT, typename XT, int U, bool CHECK>
-__device__ __forceinline__ void quad_dia_v(const XT *__restrict__ x, const VT *__restrict__ vq, int32_t K,
-                                           int32_t myoff, int32_t row, uint32_t xn, const float (&sc)[4],
-                                           XT (&sum)[4]) {
-    const int lane = row & 31;
-    for (int32_t g = 0; g < K; g += U) {
-        VT v[U][4];
-        XT xv[4][U];
-        bool ok[4][U];
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-            const bool in = g + u < K;  // warp-uniform
-            const int32_t off = __shfl_sync(kFull, myoff, (g + u) & 31);
-            if (in) {
-                ld_quad(vq, (g + u) * 32 + lane, v[u]);
-            } else {
-#pragma unroll
-                for (int q = 0; q < 4; ++q) v[u][q] = VT(0);
-            }
-            const int32_t col = row + off;
-            const XT *xp = x + col;
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                ok[q][u] = in && (!CHECK || static_cast<uint32_t>(col + 32 * q) < xn);
-                xv[q][u] = ok[q][u] ? __ldg(xp + 32 * q) : XT(0);
-            }
-        }
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const XT vv = widen<XT>(v[u][q], sc[q]);
-                if (ok[q][u] && vv != XT(0)) sum[q] = fma_rn(vv, xv[q][u], sum[q]);
-            }
-        }
+// Values of the four blocks in their own regions (vb[q] + k * 32 + lane).
+template <typename VT>
+struct QuadVals {
+    const VT *v0, *v1, *v2, *v3;
+    __device__ __forceinline__ void operator()(int32_t k, VT (&v)[4]) const {
+        v[0] = ld_stream(v0 + k * 32);
+        v[1] = ld_stream(v1 + k * 32);
+        v[2] = ld_stream(v2 + k * 32);
+        v[3] = ld_stream(v3 + k * 32);
     }
-}
+};
+
+// The lane's values of the four blocks for offset k of a quad-interleaved
+// region (vq: the quad's first value): one vector load.
+template <typename VT>
+struct QuadValsInterleaved;
+template <>
+struct QuadValsInterleaved<float> {
+    const float *vq;
+    int lane;
+    __device__ __forceinline__ void operator()(int32_t k, float (&v)[4]) const {
+        const float4 f = __ldcs(reinterpret_cast<const float4 *>(vq) + (k * 32 + lane));
+        v[0] = f.x;
+        v[1] = f.y;
+        v[2] = f.z;
+        v[3] = f.w;
+    }
+};
+template <>
+struct QuadValsInterleaved<__nv_bfloat16> {
+    const __nv_bfloat16 *vq;
+    int lane;
+    __device__ __forceinline__ void operator()(int32_t k, __nv_bfloat16 (&v)[4]) const {
+        const uint2 r = __ldcs(reinterpret_cast<const uint2 *>(vq) + (k * 32 + lane));
+        v[0] = __ushort_as_bfloat16(static_cast<unsigned short>(r.x & 0xffffu));
+        v[1] = __ushort_as_bfloat16(static_cast<unsigned short>(r.x >> 16));
+        v[2] = __ushort_as_bfloat16(static_cast<unsigned short>(r.y & 0xffffu));
+        v[3] = __ushort_as_bfloat16(static_cast<unsigned short>(r.y >> 16));
+    }
+};
 
 // What the warp needs of a quad before its DIA part: the block pointers and
 // COO tile starts of its four tiles (lanes 0..4), whether the four blocks
@@ -294,22 +289,22 @@ spmv_bw32_quad(const SpmvArgs<VT, XT> a, const XT *__restrict__ x, XT *__restric
                 const int32_t offFirst = __shfl_sync(kFull, cur.myoff, 0);
                 const int32_t offLast = __shfl_sync(kFull, cur.myoff, K - 1);
                 const bool interior = int64_t(row0) + offFirst >= 0 && int64_t(row0) + 127 + offLast < int64_t(a.xn);
-                const VT *v0 = a.vals + static_cast<int64_t>(kq[0]) * 32 + lane;
-                const VT *v1 = a.vals + static_cast<int64_t>(kq[1]) * 32 + lane;
-                const VT *v2 = a.vals + static_cast<int64_t>(kq[2]) * 32 + lane;
-                const VT *v3 = a.vals + static_cast<int64_t>(kq[3]) * 32 + lane;
                 bool done = false;
                 if constexpr (sizeof(VT) < 8) {
                     if (a.quadLayout) {  // interleaved region of the quad
-                        const VT *vq = a.vals + static_cast<int64_t>(kq[0]) * 32;
-                        if (interior) quad_dia_v<VT, XT, U, false>(x, vq, K, cur.myoff, row, xn, sc, sum);
-                        else quad_dia_v<VT, XT, U, true>(x, vq, K, cur.myoff, row, xn, sc, sum);
+                        const QuadValsInterleaved<VT> vals{a.vals + static_cast<int64_t>(kq[0]) * 32, lane};
+                        if (interior) quad_offsets<VT, XT, U, false>(x, vals, K, cur.myoff, row, xn, sc, sum);
+                        else quad_offsets<VT, XT, U, true>(x, vals, K, cur.myoff, row, xn, sc, sum);
                         done = true;
                     }
                 }
                 if (!done) {
-                    if (interior) quad_dia<VT, XT, U, false>(x, v0, v1, v2, v3, K, cur.myoff, row, xn, sc, sum);
-                    else quad_dia<VT, XT, U, true>(x, v0, v1, v2, v3, K, cur.myoff, row, xn, sc, sum);
+                    const QuadVals<VT> vals{a.vals + static_cast<int64_t>(kq[0]) * 32 + lane,
+                                            a.vals + static_cast<int64_t>(kq[1]) * 32 + lane,
+                                            a.vals + static_cast<int64_t>(kq[2]) * 32 + lane,
+                                            a.vals + static_cast<int64_t>(kq[3]) * 32 + lane};
+                    if (interior) quad_offsets<VT, XT, U, false>(x, vals, K, cur.myoff, row, xn, sc, sum);
+                    else quad_offsets<VT, XT, U, true>(x, vals, K, cur.myoff, row, xn, sc, sum);
                 }
             }
         } else {

@@ -69,7 +69,8 @@ def precision(args):
     stream = torch.cuda.Stream()
     yref = None
     base_rate = None
-    for name, st in (("fp64", hb.STORE_NATIVE), ("fp32", hb.STORE_F32), ("bf16_scaled", hb.STORE_BF16_SCALED)):
+    for name, st in (("fp64", hb.STORE_NATIVE), ("fp32", hb.STORE_F32), ("bf16_scaled", hb.STORE_BF16_SCALED),
+                     ("fp32_quad_interleaved", hb.STORE_F32_QUAD), ("bf16_scaled_quad_interleaved", hb.STORE_BF16_QUAD)):
         m = hb.HBDIA(rows, cols, vals, n, n)
         m.convertToHBDIAFormat(32, 2, upload=False)
         m.prepareForGPU(st)

@@ -69,8 +69,8 @@ typedef enum hbdia_value_storage {
 } hbdia_value_storage;
 
 /* SpMV kernel choice (all give bit-identical y).  AUTO picks the kernel
- * measured fastest on B200: for blockWidth 32 QUAD with BF16 value storage,
- * PIPE otherwise; ROWWISE for other block widths.  STAGED
+ * measured fastest on B200: for blockWidth 32 QUAD with 4- and 2-byte value
+ * storage, PIPE with 8-byte values; ROWWISE for other block widths.  STAGED
  * needs a 16-byte aligned x and value array (else WARP runs); PIPE and STAGED
  * need numRows <= 2^30. */
 typedef enum hbdia_kernel {
@@ -441,8 +441,7 @@ int hbdia_matrix_selected_kernel(const hbdia_matrix *m, const void *x, int32_t *
  * 2-byte.  A shape whose stages do not fit shared memory for the value type
  * runs the default.  Tiles with more than 32 offsets read global memory.
  * HBDIA_TUNE_QUAD_GROUP: offsets of the four blocks in flight per lane in the
- * quad kernel (0 = default: 4 for 4- and 2-byte values, 2 for 8-byte ones;
- * or 1, 2, 4, 8). */
+ * quad kernel (0 = default: 4; or 1, 2, 4, 8). */
 typedef enum hbdia_tuning_key {
     HBDIA_TUNE_UNROLL = 1,
     HBDIA_TUNE_SPMM_TILE = 2,
@@ -612,8 +611,9 @@ typedef struct hbdia_server_options {
     int32_t maxRhs;         /* SpMV requests of one matrix per batch, 1-64 (default 16)    */
     int32_t spmvStorage;    /* hbdia_value_storage of SpMVs (default HBDIA_STORE_F32;       */
                             /* not the quad-interleaved ones: batches are SpMMs)            */
-    int32_t cgIterStorage;  /* storage of the CG iterations' SpMVs (default HBDIA_STORE_F32; */
-                            /* a different one is kept as a second reduced copy)            */
+    int32_t cgIterStorage;  /* storage of the CG iterations' SpMVs (default                 */
+                            /* HBDIA_STORE_F32_QUAD; one other than spmvStorage is kept as  */
+                            /* a second reduced copy)                                       */
     int32_t cgWorkers;      /* concurrent CG solves, 1-64 (default 4)                       */
     int32_t cgMaxUpdates;   /* FP64 residual recomputations per solve (default 100)         */
     int32_t cgMaxIterations;/* iterations per solve (default 20000)                         */

@@ -118,3 +118,29 @@ def test_cg_and_server_on_quad_storage(lib):
         for info, y in zip(infos, ys):
             assert info.status == 0 and info.cgIterations == sol[lib.STORE_F32][0]
             assert bits_equal(y, sol[lib.STORE_F32][1])
+
+
+def test_quad_iteration_storage_falls_back(lib):
+    """CG's default iteration storage is quad-interleaved FP32; a layout that
+    cannot take it (blockWidth 8) iterates on the per-block FP32 values,
+    which give the same iterates: same solution, bit for bit."""
+    import torch
+    g = 16
+    n = g ** 3
+    rows, cols, vals = lib.generate_stencil27_spd(g, g, g, 1e-3, 7)
+    b = lib.fill_uniform(n, -1.0, 1.0, 11)
+    m = lib.HBDIA(rows, cols, vals, n, n)
+    m.convertToHBDIAFormat(8, 2)
+    bt = torch.from_numpy(b).cuda()
+    out = []
+    for st in (lib.STORE_F32_QUAD, lib.STORE_F32):
+        xt = torch.zeros(n, dtype=torch.float64, device="cuda")
+        r = lib.cg_solve(m, bt.data_ptr(), xt.data_ptr(), tol=1e-10, iter_storage=st)
+        assert r.converged == 1
+        out.append((r.iterations, xt.cpu().numpy()))
+    assert out[0][0] == out[1][0] and bits_equal(out[0][1], out[1][1])
+    srv = lib.Server()  # default cgIterStorage: the quad-interleaved FP32 values
+    y = np.full(n, np.nan)
+    info = srv.wait(srv.submit(srv.add_matrix(m), lib.REQ_CG, b, y))
+    srv.close()
+    assert info.status == 0 and bits_equal(y, out[1][1])

@@ -352,6 +352,11 @@ def test_kernel_selection(lib):
     m.convertToHBDIAFormat(32, 2)
     xt = torch.zeros(n + 2, dtype=torch.float64, device="cuda")
     assert m.selectedKernel(xt.data_ptr()) == lib.KERNEL_PIPE          # AUTO: fastest measured
+    for st in (lib.STORE_F32, lib.STORE_BF16_SCALED, lib.STORE_F32_QUAD, lib.STORE_BF16_QUAD):
+        mq = lib.HBDIA(rows, cols, vals, n, n)
+        mq.convertToHBDIAFormat(32, 2, upload=False)
+        mq.prepareForGPU(st)
+        assert mq.selectedKernel(xt.data_ptr()) == lib.KERNEL_QUAD     # 4- and 2-byte values
     m.setKernel(lib.KERNEL_STAGED)
     assert m.selectedKernel(xt.data_ptr()) == lib.KERNEL_STAGED
     assert m.selectedKernel(xt.data_ptr() + 8) == lib.KERNEL_WARP      # x not 16-byte aligned
