@@ -49,8 +49,8 @@ namespace dev {
 constexpr int kQuadWarps = 8;  // warps per CTA
 
 // DIA sum of one 32-row block straight from its offset range [k0, k1): full
-// groups of 8 offsets with all loads in flight, then one at a time; ascending
-// order.
+// groups of 8 offsets with all loads in flight, then one group of 4 and one of
+// the remaining 1-3; ascending order.
 template <typename VT, typename XT, int U>
 __device__ __forceinline__ XT block_group(const XT *__restrict__ x, const VT *__restrict__ vp, int32_t myoff, int j,
                                           int32_t row, uint32_t n, float s, XT sum) {
@@ -84,7 +84,14 @@ __device__ __forceinline__ XT block_dia(const SpmvArgs<VT, XT> &a, const XT *__r
         const VT *vp = a.vals + static_cast<int64_t>(kb) * 32 + lane;
         int j = 0;
         for (; j + 8 <= cnt; j += 8) sum = block_group<VT, XT, 8>(x, vp, myoff, j, row, n, s, sum);
-        for (; j < cnt; ++j) sum = block_group<VT, XT, 1>(x, vp, myoff, j, row, n, s, sum);
+        if (j + 4 <= cnt) {
+            sum = block_group<VT, XT, 4>(x, vp, myoff, j, row, n, s, sum);
+            j += 4;
+        }
+        const int rest = cnt - j;  // 0-3, warp-uniform: one group
+        if (rest == 3) sum = block_group<VT, XT, 3>(x, vp, myoff, j, row, n, s, sum);
+        else if (rest == 2) sum = block_group<VT, XT, 2>(x, vp, myoff, j, row, n, s, sum);
+        else if (rest == 1) sum = block_group<VT, XT, 1>(x, vp, myoff, j, row, n, s, sum);
     }
     return sum;
 }
@@ -123,13 +130,22 @@ __device__ __forceinline__ void quad_group(const XT *__restrict__ x, Val val, in
 }
 
 // The K offsets of a uniform quad in ascending order: full groups of U, then
-// one at a time (no per-offset range test inside a group).
+// groups of 4 (when U > 4), then the remaining 1-3 offsets as one group -- no
+// per-offset range test inside a group, and every group one load round trip.
 template <typename VT, typename XT, int U, bool CHECK, typename Val>
 __device__ __forceinline__ void quad_offsets(const XT *__restrict__ x, Val val, int32_t K, int32_t myoff,
                                              int32_t row, uint32_t xn, const float (&sc)[4], XT (&sum)[4]) {
     int32_t g = 0;
     for (; g + U <= K; g += U) quad_group<VT, XT, U, CHECK>(x, val, g, myoff, row, xn, sc, sum);
-    for (; g < K; ++g) quad_group<VT, XT, 1, CHECK>(x, val, g, myoff, row, xn, sc, sum);
+    if constexpr (U > 4)
+        for (; g + 4 <= K; g += 4) quad_group<VT, XT, 4, CHECK>(x, val, g, myoff, row, xn, sc, sum);
+    const int32_t rest = K - g;  // < min(U, 4), warp-uniform
+    if constexpr (U > 3)
+        if (rest == 3) quad_group<VT, XT, 3, CHECK>(x, val, g, myoff, row, xn, sc, sum);
+    if constexpr (U > 2)
+        if (rest == 2) quad_group<VT, XT, 2, CHECK>(x, val, g, myoff, row, xn, sc, sum);
+    if constexpr (U > 1)
+        if (rest == 1) quad_group<VT, XT, 1, CHECK>(x, val, g, myoff, row, xn, sc, sum);
 }
 
 // Values of the four blocks in their own regions (vb[q] + k * 32 + lane).
