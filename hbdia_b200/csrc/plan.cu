@@ -385,10 +385,10 @@ void launch_quad(const DevicePlan &P, const dev::SpmvArgs<VT, XT> &a, const XT *
     const int device = plan_device(P);
     check_cuda(cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, device), "cudaDeviceGetAttribute(L2)");
     // default prefetch, measured on B200 (27-point 128^3 / 256^3): always for
-    // 2-byte values (+4-32 %), never for the quad-interleaved 4-byte ones
-    // (-4 %), else when x exceeds L2
+    // 2-byte values (+5-33 %), never for 4-byte ones (-2 to -9 %), for 8-byte
+    // ones when x exceeds L2
     const bool xBig = static_cast<int64_t>(std::max(P.n, P.numCols)) * static_cast<int64_t>(sizeof(XT)) > l2;
-    const bool pfAuto = sizeof(VT) == 2 || (!(sizeof(VT) == 4 && P.quadLayout) && xBig);
+    const bool pfAuto = sizeof(VT) == 2 || (sizeof(VT) == 8 && xBig);
     const bool pf = P.prefetchL2 > 0 || (P.prefetchL2 < 0 && pfAuto);
     // default: 4 offsets in flight, the fastest or within run-to-run noise of
     // it for every value storage on B200 (27-point 128^3 / 256^3, banded 8M)

@@ -427,7 +427,7 @@ int hbdia_matrix_selected_kernel(const hbdia_matrix *m, const void *x, int32_t *
  * tile's value rows while computing the current one (bulk L2 prefetch),
  * 0 = off, -1 (default) = on when the x vector is larger than the GPU's L2;
  * for the quad kernel (which prefetches the next quad's values) always with
- * BF16 values and never with the quad-interleaved FP32 ones.
+ * BF16 values and never with FP32 ones.
  * Measured on B200: with a 134 MB x, FP64 +1.5 % and FP32 storage +8 %; with
  * x in L2 (57 MB and below) -2 to -10 %, as the prefetched rows evict x.
  * HBDIA_TUNE_TAIL: the pipelined kernel takes a block's offsets in groups of
