@@ -105,7 +105,9 @@ __device__ __forceinline__ void spmm_group(const SpmvArgs<VT, XT> &a, const XS &
 
 // The offsets of one row block for one pass, in groups of U = 16 / KT (at
 // least 1), so about 16 x gathers per lane are in flight (32 measured slower
-// on B200 at every tile width).
+// on B200 at every tile width); the offsets after the last full group go in
+// groups of 4 and then one group of the remaining 1-3, so each group is one
+// load round trip.
 template <typename VT, typename XT, int KT, typename IT, bool FULL, typename XS>
 __device__ __forceinline__ void spmm_pass(const SpmvArgs<VT, XT> &a, const XS &xs, int32_t k0, int32_t k1,
                                           int64_t row, int lane, int kc, float s, XT (&acc)[KT]) {
@@ -117,8 +119,15 @@ __device__ __forceinline__ void spmm_pass(const SpmvArgs<VT, XT> &a, const XS &x
         int j = 0;
         for (; j + U <= cnt; j += U)
             spmm_group<VT, XT, KT, U, IT, FULL>(a, xs, vp, myoff, j, row, kc, s, acc);
-        for (; j < cnt; ++j)  // warp-uniform tail
-            spmm_group<VT, XT, KT, 1, IT, FULL>(a, xs, vp, myoff, j, row, kc, s, acc);
+        if constexpr (U > 4)
+            for (; j + 4 <= cnt; j += 4) spmm_group<VT, XT, KT, 4, IT, FULL>(a, xs, vp, myoff, j, row, kc, s, acc);
+        const int rest = cnt - j;  // < min(U, 4), warp-uniform
+        if constexpr (U > 3)
+            if (rest == 3) spmm_group<VT, XT, KT, 3, IT, FULL>(a, xs, vp, myoff, j, row, kc, s, acc);
+        if constexpr (U > 2)
+            if (rest == 2) spmm_group<VT, XT, KT, 2, IT, FULL>(a, xs, vp, myoff, j, row, kc, s, acc);
+        if constexpr (U > 1)
+            if (rest == 1) spmm_group<VT, XT, KT, 1, IT, FULL>(a, xs, vp, myoff, j, row, kc, s, acc);
     }
 }
 

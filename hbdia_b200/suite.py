@@ -642,7 +642,11 @@ def spmv(args):
     """The headline workload's shape at --grid (27-point stencil, centre 26,
     neighbours -1, 1 % extras U(0.1, 1) seed 1, blockWidth 32, threshold 2,
     x ~ U(-1, 1) seed 1) with --storage value storage and --kernel: --reps
-    SpMVs after 3 warm-up ones, each timed with CUDA events.  The profiles
+    SpMVs after 3 warm-up ones, each timed with CUDA events.  With --rhs K > 1
+    the same matrix's column-major SpMM of K right-hand sides (X[:, 0] = that
+    x, column j ~ U(-1, 1) seed 1 + j; --tile RHS per pass, 0 = default)
+    instead; its algorithmic bytes count the values, offsets and COO entries
+    once and x, y and the COO x gathers per right-hand side.  The profiles
     capture its launches."""
     import torch
     import hbdia_b200 as hb
@@ -658,6 +662,21 @@ def spmv(args):
     x = torch.from_numpy(hb.fill_uniform(n, -1.0, 1.0, 1)).cuda()
     y = torch.zeros(n, dtype=torch.float64, device="cuda")
     stream = torch.cuda.Stream()
+    if args.rhs > 1:
+        k = args.rhs
+        X = torch.stack([x] + [torch.from_numpy(hb.fill_uniform(n, -1.0, 1.0, 1 + j)).cuda()
+                               for j in range(1, k)])  # (k, n): column j contiguous
+        Y = torch.zeros((k, n), dtype=torch.float64, device="cuda")
+        m.setTuning(hb.TUNE_SPMM_TILE, args.tile)
+        ms = _time(lambda: hb.spmm_device_colmajor(m, X.data_ptr(), n, Y.data_ptr(), n, k, stream.cuda_stream),
+                   stream, reps=args.reps)
+        m.synchronize()
+        info = m.info()
+        b = m.bytesPerSpmv() + (k - 1) * (16 * n + 8 * info.numCoo)
+        print(json.dumps({"suite": "spmm", "workload": f"27-point stencil {g}^3 + 1% extras, column-major",
+                          "storage": args.storage, "k": k, "tile": args.tile, "ms": ms, "bytes": b,
+                          "gbs": b / (ms / 1e3) / 1e9, "frac_of_peak": b / (ms / 1e3) / 1e9 / _peak()}), flush=True)
+        return
     ms = _time(lambda: hb.spmv_device(m, x.data_ptr(), y.data_ptr(), stream.cuda_stream), stream, reps=args.reps)
     m.synchronize()
     b = m.bytesPerSpmv()
@@ -684,6 +703,8 @@ def main(argv=None):
     ap.add_argument("--device", action="store_true", help="serve: request vectors in device memory")
     ap.add_argument("--kernel", default="auto", choices=["auto", "pipe", "quad", "staged", "warp", "rowwise"])
     ap.add_argument("--reps", type=int, default=20)
+    ap.add_argument("--rhs", type=int, default=1, help="spmv: right-hand sides (> 1: column-major SpMM)")
+    ap.add_argument("--tile", type=int, default=0, help="spmv --rhs: right-hand sides per pass (0: default)")
     args = ap.parse_args(argv)
     import torch
     torch.cuda.set_device(0)
