@@ -80,7 +80,9 @@ struct XList {
 // values and all U x KT x gathers are issued before any product is formed, so
 // a group costs one memory round trip.  Column q's products are added in
 // ascending offset order.
-template <typename VT, typename XT, int KT, int U, typename IT, bool FULL, typename XS>
+// CHECK: some column of the group may fall outside [0, xn) (else every one
+// is inside: no range test, no index select).
+template <typename VT, typename XT, int KT, int U, typename IT, bool FULL, bool CHECK, typename XS>
 __device__ __forceinline__ void spmm_group(const SpmvArgs<VT, XT> &a, const XS &xs, const VT *vp, int32_t myoff, int j,
                                            int64_t row, int kc, float s, XT (&acc)[KT]) {
     VT v[U];
@@ -89,7 +91,7 @@ __device__ __forceinline__ void spmm_group(const SpmvArgs<VT, XT> &a, const XS &
 #pragma unroll
     for (int u = 0; u < U; ++u) {
         const int64_t col = row + __shfl_sync(kFull, myoff, j + u);
-        ok[u] = static_cast<uint64_t>(col) < static_cast<uint64_t>(a.xn);
+        ok[u] = !CHECK || static_cast<uint64_t>(col) < static_cast<uint64_t>(a.xn);
         v[u] = __ldg(vp + (j + u) * 32);
         xs.load(ok[u] ? static_cast<IT>(col) : IT(0), kc, xv[u]);
     }
@@ -108,26 +110,39 @@ __device__ __forceinline__ void spmm_group(const SpmvArgs<VT, XT> &a, const XS &
 // on B200 at every tile width); the offsets after the last full group go in
 // groups of 4 and then one group of the remaining 1-3, so each group is one
 // load round trip.
+template <typename VT, typename XT, int KT, typename IT, bool FULL, bool CHECK, typename XS>
+__device__ __forceinline__ void spmm_chunk(const SpmvArgs<VT, XT> &a, const XS &xs, const VT *vp, int32_t myoff,
+                                           int cnt, int64_t row, int kc, float s, XT (&acc)[KT]) {
+    constexpr int U = KT >= 16 ? 1 : 16 / KT;
+    int j = 0;
+    for (; j + U <= cnt; j += U)
+        spmm_group<VT, XT, KT, U, IT, FULL, CHECK>(a, xs, vp, myoff, j, row, kc, s, acc);
+    if constexpr (U > 4)
+        for (; j + 4 <= cnt; j += 4) spmm_group<VT, XT, KT, 4, IT, FULL, CHECK>(a, xs, vp, myoff, j, row, kc, s, acc);
+    const int rest = cnt - j;  // < min(U, 4), warp-uniform
+    if constexpr (U > 3)
+        if (rest == 3) spmm_group<VT, XT, KT, 3, IT, FULL, CHECK>(a, xs, vp, myoff, j, row, kc, s, acc);
+    if constexpr (U > 2)
+        if (rest == 2) spmm_group<VT, XT, KT, 2, IT, FULL, CHECK>(a, xs, vp, myoff, j, row, kc, s, acc);
+    if constexpr (U > 1)
+        if (rest == 1) spmm_group<VT, XT, KT, 1, IT, FULL, CHECK>(a, xs, vp, myoff, j, row, kc, s, acc);
+}
+
+// Chunks of up to 32 offsets (ascending) whose columns all lie in [0, xn) for
+// every row of the tile run without range tests.
 template <typename VT, typename XT, int KT, typename IT, bool FULL, typename XS>
 __device__ __forceinline__ void spmm_pass(const SpmvArgs<VT, XT> &a, const XS &xs, int32_t k0, int32_t k1,
                                           int64_t row, int lane, int kc, float s, XT (&acc)[KT]) {
-    constexpr int U = KT >= 16 ? 1 : 16 / KT;
+    const int64_t row0 = row - lane;
     for (int32_t kb = k0; kb < k1; kb += 32) {
         const int cnt = min(32, k1 - kb);
         const int32_t myoff = lane < cnt ? __ldg(a.offs + kb + lane) : 0;
         const VT *vp = a.vals + static_cast<int64_t>(kb) * 32 + lane;
-        int j = 0;
-        for (; j + U <= cnt; j += U)
-            spmm_group<VT, XT, KT, U, IT, FULL>(a, xs, vp, myoff, j, row, kc, s, acc);
-        if constexpr (U > 4)
-            for (; j + 4 <= cnt; j += 4) spmm_group<VT, XT, KT, 4, IT, FULL>(a, xs, vp, myoff, j, row, kc, s, acc);
-        const int rest = cnt - j;  // < min(U, 4), warp-uniform
-        if constexpr (U > 3)
-            if (rest == 3) spmm_group<VT, XT, KT, 3, IT, FULL>(a, xs, vp, myoff, j, row, kc, s, acc);
-        if constexpr (U > 2)
-            if (rest == 2) spmm_group<VT, XT, KT, 2, IT, FULL>(a, xs, vp, myoff, j, row, kc, s, acc);
-        if constexpr (U > 1)
-            if (rest == 1) spmm_group<VT, XT, KT, 1, IT, FULL>(a, xs, vp, myoff, j, row, kc, s, acc);
+        const int32_t offFirst = __shfl_sync(kFull, myoff, 0), offLast = __shfl_sync(kFull, myoff, cnt - 1);
+        if (row0 + offFirst >= 0 && row0 + 31 + offLast < a.xn)
+            spmm_chunk<VT, XT, KT, IT, FULL, false>(a, xs, vp, myoff, cnt, row, kc, s, acc);
+        else
+            spmm_chunk<VT, XT, KT, IT, FULL, true>(a, xs, vp, myoff, cnt, row, kc, s, acc);
     }
 }
 
