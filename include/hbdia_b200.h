@@ -486,8 +486,9 @@ int hbdia_matrix_test_skip_tile(hbdia_matrix *m, int32_t tile);
 /* Conjugate gradients for a symmetric positive definite double matrix.  No
  * counterpart in the reference (its SpMV has no solver); it runs on the same
  * SpMV kernels.  The iterations' SpMVs use the `iterStorage` copy of the
- * values (HBDIA_STORE_F32: mixed precision; HBDIA_STORE_NATIVE: plain FP64
- * CG); x, the residual r, the search direction, the dot products, norms and
+ * values (HBDIA_STORE_F32_QUAD, the fastest on B200, or HBDIA_STORE_F32: mixed
+ * precision, the same iterates; a quad storage the matrix's layout cannot take
+ * runs as its per-block form; HBDIA_STORE_NATIVE: plain FP64 CG); x, the residual r, the search direction, the dot products, norms and
  * the solution update are FP64.  Reliable updates: whenever the iterated
  * residual has fallen below updateFactor times the largest one since the last
  * update, and before convergence is declared, r is recomputed as b - A x with
