@@ -43,3 +43,17 @@ def test_status_strings_and_errors_without_gpu(lib):
     h = ctypes.c_void_p()
     rc = so.hbdia_matrix_create(0, None, None, None, 1, 4, 4, ctypes.byref(h))
     assert rc == -1 and b"null" in so.hbdia_last_error()
+
+
+def test_server_option_validation_without_gpu(lib):
+    """Server options are checked before any CUDA call: SpMV batches are SpMMs,
+    so the quad-interleaved storages (SpMV only) are refused for them; an
+    unknown CG iteration storage is refused too."""
+    import pytest
+    for bad in ({"spmvStorage": lib.STORE_F32_QUAD}, {"spmvStorage": lib.STORE_BF16_QUAD},
+                {"cgIterStorage": 5}, {"cgIterStorage": -1}, {"cgMaxGroup": 17}):
+        with pytest.raises(ValueError):
+            lib.Server(**bad)
+    o = lib._lib.ServerOptions()
+    lib._lib.load().hbdia_server_default_options(ctypes.byref(o))
+    assert o.spmvStorage == lib.STORE_F32 and o.cgIterStorage == lib.STORE_F32_QUAD and o.cgMaxGroup == 1

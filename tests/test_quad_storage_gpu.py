@@ -144,3 +144,17 @@ def test_quad_iteration_storage_falls_back(lib):
     info = srv.wait(srv.submit(srv.add_matrix(m), lib.REQ_CG, b, y))
     srv.close()
     assert info.status == 0 and bits_equal(y, out[1][1])
+
+
+def test_quad_storage_other_builders_refuse(lib):
+    """The GPU converter and plans over a caller's layout build per-block
+    layouts only: both refuse the quad-interleaved storage codes."""
+    n = 4096
+    rows, cols, vals = lib.generate_stencil27(16, 16, 16, 26.0, -1.0, 0.01, 0.1, 1.0, 1)
+    for st in (lib.STORE_F32_QUAD, lib.STORE_BF16_QUAD):
+        m = lib.HBDIA(rows, cols, vals, n, n)
+        with pytest.raises(ValueError):
+            m.convertOnDevice(32, 2, storage=st)
+        with pytest.raises(ValueError):  # refused on the host: no array is read
+            lib.LayoutPlan(storage=st, numRows=n, numCols=n, blockWidth=32, numBlocks=128, totalOffsets=1,
+                           numCoo=0, values=0, offsets=0, blockStart=0)
