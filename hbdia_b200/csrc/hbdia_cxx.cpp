@@ -122,6 +122,11 @@ void HBDIA<T>::prepareForGPU() {
 }
 
 template <typename T>
+void HBDIA<T>::prepareForGPU(hbdia_value_storage storage) {
+    raise(hbdia_matrix_prepare_gpu(h_, storage));
+}
+
+template <typename T>
 void HBDIA<T>::removeCOODuplicates() {
     raise(hbdia_matrix_remove_duplicates(h_));
     cooCached_ = false;

@@ -112,6 +112,11 @@ public:
 
     // device side
     void prepareForGPU();
+    // Addition to the reference's API: the device layout with another value
+    // storage (HBDIA_STORE_F32, _BF16_SCALED and the quad-interleaved
+    // _F32_QUAD / _BF16_QUAD keep the values narrow; x, y and the
+    // accumulation stay in the matrix's type).
+    void prepareForGPU(hbdia_value_storage storage);
     void initializeCuSparse() {}  // nothing to set up: the COO remainder is fused
     void *getBDIAStream() const;   // a cudaStream_t
     void synchronize() const;      // waits for the SpMVs on the matrix's stream

@@ -185,6 +185,26 @@ int main() {
         CHECK_CUDA(cudaMemcpy(z.data(), coo, 100 * sizeof(double), cudaMemcpyDeviceToHost));
         CHECK(z == std::vector<double>(100, 0.0), "COO result buffer starts zeroed");
     }
+    {  // narrow value storage through the C++ API: quad-interleaved FP32 == per-block FP32
+        HBDIA<double> m;
+        m.create3DStencil27Point(24, 24, 24, 0.01, 1);
+        m.convertToHBDIAFormat(32, 2);
+        std::vector<double> xv(m.getNumRows());
+        for (int i = 0; i < m.getNumRows(); i++) xv[i] = 1.0 + 0.25 * (i % 7);
+        auto run = [&](hbdia_value_storage st) {
+            m.prepareForGPU(st);
+            HBDIAVector<double> x(xv);
+            HBDIAVector<double> y(std::vector<double>(m.getNumRows(), 0.0));
+            hbdiaSpMV(m, x, y, true, false);
+            m.synchronize();
+            std::vector<double> got;
+            y.copyToHost(got);
+            return got;
+        };
+        const std::vector<double> f32 = run(HBDIA_STORE_F32), quad = run(HBDIA_STORE_F32_QUAD);
+        CHECK(!f32.empty() && f32 == quad, "prepareForGPU(HBDIA_STORE_F32_QUAD) gives the FP32 storage's y");
+        CHECK(run(HBDIA_STORE_NATIVE) == expected(m, xv), "prepareForGPU(HBDIA_STORE_NATIVE) gives the FP64 y");
+    }
     {  // CHECK_CUDA throws where the reference's exits
         bool threw = false;
         try {
