@@ -16,9 +16,17 @@
 // lane give the loads and FMAs room to overlap.  Quads whose blocks differ run
 // block by block with the single-block code.
 //
+// The offsets of a uniform quad go in full groups of U (all of a group's value
+// and x loads issued before its FMAs, no per-offset range test), then the 1-3
+// left over as one more group, so a 27-offset quad takes 7 load round trips;
+// quads whose columns all lie in [0, xn) skip the column checks.  Predicating
+// every load and FMA on the group's range instead doubled the instruction
+// count on B200.
+//
 // The COO remainder of the quad (row-sorted entries; its first 64 loaded one
-// quad ahead) goes 32 entries at a time; each entry's product is formed by its lane, and the first entry of
-// every row segment (its "head") sums the segment in list order with shuffles
+// quad ahead) goes 32 entries at a time; each entry's product is formed by its
+// lane, and the first entry of every row segment (its "head") sums the segment
+// in list order with shuffles
 // -- segments are short (1 % extra entries: mostly one entry per row).  A
 // segment cut by the 32-entry chunk boundary carries its partial sum into the
 // next chunk.  The quad's 128 DIA sums wait in a per-warp shared buffer, each
