@@ -98,10 +98,11 @@ __device__ __forceinline__ void spmm_group(const SpmvArgs<VT, XT> &a, const XS &
 #pragma unroll
     for (int u = 0; u < U; ++u) {
         const XT vv = widen<XT>(v[u], s);
-        const bool use = ok[u] && vv != XT(0);
+        if (ok[u] && vv != XT(0)) {
 #pragma unroll
-        for (int q = 0; q < KT; ++q)
-            if (FULL || q < kc) acc[q] = use ? fma_rn(vv, xv[u][q], acc[q]) : acc[q];
+            for (int q = 0; q < KT; ++q)
+                if (FULL || q < kc) acc[q] = fma_rn(vv, xv[u][q], acc[q]);
+        }
     }
 }
 
