@@ -61,7 +61,7 @@ def _stencil(lib, nx, ny, nz, noise, it):
     return m.getRowIndices(), m.getColIndices(), m.getValues(), nx * ny * nz
 
 
-def _emulated(lib, rows, cols, vals, n, P, bw, thr, x, kernel=None):
+def _emulated(lib, rows, cols, vals, n, P, bw, thr, x, kernel=None, storage=None):
     """P ranks on one GPU: returns the concatenated y and the per-rank oracle y."""
     import torch
     from hbdia_b200.distributed import _HaloPlan
@@ -69,7 +69,9 @@ def _emulated(lib, rows, cols, vals, n, P, bw, thr, x, kernel=None):
     ranks = []
     for p in range(P):
         m = g.partition(P, p)
-        m.convertToHBDIAFormat(bw, thr)
+        m.convertToHBDIAFormat(bw, thr, upload=storage is None)
+        if storage is not None and m.getHasHBDIA():
+            m.prepareForGPU(storage)
         if kernel is not None and m.getHasHBDIA():
             m.setKernel(kernel)
         w0, wl = m.window()
@@ -120,6 +122,20 @@ def test_emulated_ranks_equal_oracle(lib, orc, P, bw, thr, grid):
             assert bits_equal(y, whole)
         sc = orc.coo_spmv(rows, cols, np.abs(vals), np.abs(x), n)
         assert np.all(np.abs(y - whole) <= 1e-12 * sc)
+
+
+def test_emulated_ranks_quad_storage(lib):
+    """A rank's partial matrix (x read through its column window) with the
+    quad-interleaved FP32 / BF16 values gives the per-block storage's y, bit
+    for bit, on every rank."""
+    rows, cols, vals, n = _stencil(lib, 16, 32, 16, 0.01, 2)
+    x = np.random.default_rng(9).uniform(-1, 1, n)
+    for plain, quad in ((lib.STORE_F32, lib.STORE_F32_QUAD), (lib.STORE_BF16_SCALED, lib.STORE_BF16_QUAD)):
+        ya, ranks = _emulated(lib, rows, cols, vals, n, 4, 32, 2, x, storage=plain)
+        yb, ranks_q = _emulated(lib, rows, cols, vals, n, 4, 32, 2, x, storage=quad)
+        for a, b, (m, *_rest) in zip(ya, yb, ranks_q):
+            assert m.info().storage == quad
+            assert bits_equal(a, b)
 
 
 def test_emulated_ranks_random_extras_and_empty_rank(lib, orc):
